@@ -1,0 +1,144 @@
+/*
+ * litho_b200.h — C ABI of liblitho_b200.so, the sm_100a imaging engine.
+ *
+ * The library computes the partially coherent aerial image of a thin mask
+ * (the Abbe sum over source points, scalar or vector), its sum-of-coherent-
+ * systems (SOCS) form, and the inverse-lithography adjoint, on one CUDA
+ * device. It replaces the numpy hot path of Lithobat's imaging package
+ * (litho_sim.expose / litho_sim.opc.ilt); each entry point names the
+ * reference function it stands in for.
+ *
+ * Conventions
+ *   - Every pointer named *_dev is device memory; everything else is host.
+ *   - The caller owns every buffer, including the workspace. No entry point
+ *     allocates or frees device memory; size the workspace with the matching
+ *     *_workspace() call.
+ *   - Work is enqueued on the given stream and returns without a host
+ *     synchronisation. Entry points are re-entrant across streams as long as
+ *     each call has its own workspace.
+ *   - Return value: 0 on success, a negative LITHO_E* code for a rejected
+ *     argument (nothing was launched), or a positive CUDA error code if a
+ *     launch failed. litho_status_string() describes any of them.
+ *   - Frequencies follow numpy's FFT ordering: signed bin k in [-N/2, N/2)
+ *     is physical frequency k / (N * pixel_size).
+ */
+#ifndef LITHO_B200_H
+#define LITHO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define LITHO_OK 0
+#define LITHO_E_NULL -1          /* a required pointer is NULL               */
+#define LITHO_E_SIZE -2          /* a size or count is out of range          */
+#define LITHO_E_WORKSPACE -3     /* workspace smaller than *_workspace()     */
+#define LITHO_E_BAND -4          /* band / coarse-grid geometry inconsistent */
+#define LITHO_E_UNSUPPORTED -5   /* valid request this build does not serve  */
+#define LITHO_E_ALIGN -6         /* a pointer is not 16-byte aligned         */
+#define LITHO_E_DEVICE -7        /* device is not sm_100 or not reachable    */
+#define LITHO_E_TIMEOUT 1000001  /* a bounded device wait gave up           */
+
+/* ---- descriptors (plain data; layouts are fixed, see static sizes) ----- */
+
+/* One optical state: the pupil of one clip at one image plane.
+ * Replaces the arguments of expose/aerial_image.py:_pupil_phase (:142-166)
+ * and expose/pupil.py:vector_coefficients (:292-369). */
+typedef struct LithoPupil {
+    double wavelength;    /* m                                              */
+    double NA;
+    double defocus;       /* m, this plane's defocus                        */
+    double n_image;       /* image-space index of this plane                */
+    double zernike[21];   /* waves; zernike[j-1] multiplies Noll Z_j        */
+    int32_t exact_defocus;/* non-paraxial defocus OPD (pupil.py:214-221)    */
+    int32_t vector;       /* 1: three field components (Ex, Ey, Ez)         */
+    int32_t obliquity;    /* sqrt(cos theta) factor in the vector model     */
+    int32_t has_zernike;  /* any zernike[] non-zero                         */
+} LithoPupil;             /* 216 bytes */
+
+/* One coherent system of the Abbe sum: a source point, an image plane and
+ * (vector model) one incoherent polarisation state. Replaces one iteration of
+ * the source loop in expose/aerial_image.py:_abbe_sum (:421-486). */
+typedef struct LithoJob {
+    double fsx, fsy;      /* source-point frequency offset, 1/m             */
+    double jx, jy;        /* Jones vector of the state (vector model)       */
+    double weight;        /* source weight x state weight                   */
+    int32_t pupil;        /* index into the LithoPupil table                */
+    int32_t clip;         /* which mask                                     */
+    int32_t out;          /* which output image                             */
+    int32_t cx, cy;       /* integer bin nearest the source offset          */
+    int32_t ncomp;        /* 1 scalar, 3 vector                             */
+} LithoJob;               /* 64 bytes */
+
+/* A contiguous run of jobs, all for one output image, accumulated by one
+ * thread block. */
+typedef struct LithoItem {
+    int32_t out, job_begin, job_end, pad;
+} LithoItem;
+
+/* Per-output normalisation (expose/aerial_image.py:normalisation_scale,
+ * :217-241). mode 0: multiply by `scale` (clear, none, or 1 for raw output);
+ * mode 1: peak normalisation, scale = dose / peak computed on the device. */
+typedef struct LithoNorm {
+    int32_t mode;
+    float scale;          /* mode 0: the factor; mode 1: the dose           */
+} LithoNorm;
+
+/* Geometry and counts of one Abbe batch. All clips share the grid. The
+ * device "plan blob" holds the job/pupil/item/norm arrays at the byte
+ * offsets given here (each 16-byte aligned). */
+typedef struct LithoAbbePlan {
+    int32_t n;            /* grid side N                                    */
+    int32_t n_clips;      /* masks in the batch                             */
+    int32_t n_out;        /* output images (clips x planes)                 */
+    int32_t n_jobs;
+    int32_t n_items;
+    int32_t n_pupils;
+    int32_t h;            /* half-width of a source point's disc, bins      */
+    int32_t bm;           /* half-width of the mask band, bins              */
+    int32_t L;            /* coarse grid side (>= 4h+1, power of two)       */
+    int32_t mask_complex; /* 0: float32 masks, 1: complex64 masks           */
+    int32_t ncomp_max;    /* 1 or 3                                         */
+    int32_t flags;        /* reserved, 0                                    */
+    double pixel_size;    /* m                                              */
+    int64_t off_jobs, off_pupils, off_items, off_out_items, off_norm;
+} LithoAbbePlan;
+
+/* ---- library ----------------------------------------------------------- */
+
+/* Human-readable text for a status code returned by any entry point. */
+const char* litho_status_string(int status);
+
+/* ABI version (major * 10000 + minor * 100 + patch). */
+int litho_version(void);
+
+/* sizeof() of the public structs, in declaration order: LithoPupil,
+ * LithoJob, LithoItem, LithoNorm, LithoAbbePlan. Writes min(n, 5) values;
+ * returns how many structs the ABI has. For binding generators. */
+int litho_abi_sizes(int32_t* out, int n);
+
+/* ---- Abbe imaging ------------------------------------------------------ */
+
+/* Workspace bytes litho_abbe() needs for this plan. */
+int litho_abbe_workspace(const LithoAbbePlan* plan, size_t* bytes);
+
+/* The raw Abbe sum, normalised per output, for a batch of clips.
+ * Replaces expose/aerial_image.py:_abbe_sum (:351-494) together with
+ * compute_aerial_image (:502-548) and compute_aerial_planes (:551-587):
+ *   image_dev[o]  = raw_o * s_o   (s_o from LithoNorm, raw if scale 1)
+ *   peak_dev[o]   = max of raw_o (before scaling)
+ * mask_dev: [n_clips][N][N] float32 or complex64 (row = y, column = x). */
+int litho_abbe(const LithoAbbePlan* plan, const void* plan_blob_dev,
+               const void* mask_dev, float* image_dev, float* peak_dev,
+               void* workspace_dev, size_t workspace_bytes, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LITHO_B200_H */

@@ -1,0 +1,143 @@
+"""ctypes binding of liblitho_b200.so (the C ABI declared in include/litho_b200.h).
+
+The library is built in-tree by ``lithobat_b200/csrc/build.py`` and loaded from
+the package folder. There is no fallback: if the library or a CUDA device is
+missing, every entry point raises :class:`NativeUnavailable`.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "liblitho_b200.so"
+
+
+class NativeUnavailable(RuntimeError):
+    """The sm_100a engine cannot run here (library not built, or no GPU)."""
+
+
+class LithoError(RuntimeError):
+    """A C-ABI entry point returned a non-zero status."""
+
+    def __init__(self, fn: str, status: int, text: str):
+        super().__init__(f"{fn} failed with status {status}: {text}")
+        self.status = status
+
+
+# --- struct layouts (must match include/litho_b200.h) ------------------------
+
+PUPIL_DTYPE = np.dtype([
+    ("wavelength", "<f8"), ("NA", "<f8"), ("defocus", "<f8"), ("n_image", "<f8"),
+    ("zernike", "<f8", (21,)), ("exact_defocus", "<i4"), ("vector", "<i4"),
+    ("obliquity", "<i4"), ("has_zernike", "<i4"),
+], align=True)
+
+JOB_DTYPE = np.dtype([
+    ("fsx", "<f8"), ("fsy", "<f8"), ("jx", "<f8"), ("jy", "<f8"), ("weight", "<f8"),
+    ("pupil", "<i4"), ("clip", "<i4"), ("out", "<i4"), ("cx", "<i4"), ("cy", "<i4"),
+    ("ncomp", "<i4"),
+], align=True)
+
+ITEM_DTYPE = np.dtype([("out", "<i4"), ("job_begin", "<i4"), ("job_end", "<i4"), ("pad", "<i4")])
+NORM_DTYPE = np.dtype([("mode", "<i4"), ("scale", "<f4")])
+
+assert PUPIL_DTYPE.itemsize == 216 and JOB_DTYPE.itemsize == 64
+
+
+class AbbePlan(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32), ("n_clips", C.c_int32), ("n_out", C.c_int32), ("n_jobs", C.c_int32),
+        ("n_items", C.c_int32), ("n_pupils", C.c_int32), ("h", C.c_int32), ("bm", C.c_int32),
+        ("L", C.c_int32), ("mask_complex", C.c_int32), ("ncomp_max", C.c_int32), ("flags", C.c_int32),
+        ("pixel_size", C.c_double),
+        ("off_jobs", C.c_int64), ("off_pupils", C.c_int64), ("off_items", C.c_int64),
+        ("off_out_items", C.c_int64), ("off_norm", C.c_int64),
+    ]
+
+
+assert C.sizeof(AbbePlan) == 96
+
+_lib = None
+
+
+def lib():
+    """Load the engine once; raise NativeUnavailable if it cannot run."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise NativeUnavailable(
+            f"{LIB_PATH.name} is not built; run `python lithobat_b200/csrc/build.py` "
+            "(or __graft_entry__.build()) first")
+    L = C.CDLL(str(LIB_PATH))
+    L.litho_status_string.restype = C.c_char_p
+    L.litho_status_string.argtypes = [C.c_int]
+    L.litho_version.restype = C.c_int
+    L.litho_abbe_workspace.argtypes = [C.POINTER(AbbePlan), C.POINTER(C.c_size_t)]
+    L.litho_abbe.argtypes = [C.POINTER(AbbePlan), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                             C.c_void_p, C.c_size_t, C.c_void_p]
+    for fn in ("litho_abbe_workspace", "litho_abbe"):
+        getattr(L, fn).restype = C.c_int
+    _lib = L
+    return L
+
+
+def check(fn: str, status: int) -> None:
+    if status != 0:
+        raise LithoError(fn, status, lib().litho_status_string(status).decode())
+
+
+def exported_symbols() -> list[str]:
+    """Names the header declares; used by the ABI test."""
+    hdr = Path(__file__).resolve().parent.parent / "include" / "litho_b200.h"
+    import re
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\*?\s+\*?(litho_\w+)\s*\(", hdr.read_text(), re.M)))
+
+
+def require_cuda():
+    """torch with a visible CUDA device, or NativeUnavailable."""
+    import torch
+    if not torch.cuda.is_available():
+        raise NativeUnavailable("no CUDA device is visible; the sm_100a engine has no CPU path")
+    lib()
+    return torch
+
+
+def stream_ptr(torch, device=None) -> int:
+    return int(torch.cuda.current_stream(device).cuda_stream)
+
+
+class Workspace:
+    """A grow-only device scratch buffer per (device, purpose)."""
+
+    _bufs: dict = {}
+
+    @classmethod
+    def get(cls, torch, device, nbytes: int, tag: str = "main"):
+        key = (str(device), tag)
+        buf = cls._bufs.get(key)
+        if buf is None or buf.numel() < nbytes:
+            buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+            cls._bufs[key] = buf
+        return buf
+
+
+def blob(arrays: list[np.ndarray]) -> tuple[np.ndarray, list[int]]:
+    """Pack structured arrays into one 16-byte-aligned byte blob; return offsets."""
+    offs, size = [], 0
+    for a in arrays:
+        size = (size + 15) & ~15
+        offs.append(size)
+        size += a.nbytes
+    out = np.zeros(max(size, 16), dtype=np.uint8)
+    for a, o in zip(arrays, offs):
+        out[o:o + a.nbytes] = np.frombuffer(np.ascontiguousarray(a).tobytes(), dtype=np.uint8)
+    return out, offs
+
+
+def env_flag(name: str, default: str = "") -> str:
+    return os.environ.get(name, default)

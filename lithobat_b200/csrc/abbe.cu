@@ -1,0 +1,400 @@
+// Abbe imaging on the band-limited coarse grid.
+//
+// The reference sums, per source point s (expose/aerial_image.py:421-488),
+//     I(x) = sum_s w_s |ifft2_N(M(f) P(f - f_s))|^2
+// with one dense N x N inverse FFT per coherent system. Each coherent field
+// E_s has its spectrum on a disc of radius R = NA N px / lambda bins around
+// the source offset, so its intensity |E_s|^2 is band-limited to |g| <= 2R.
+// Shifting the disc by its integer centre c_s (which leaves |E_s|^2
+// unchanged) puts its spectrum in [-h, h]^2, and on any L x L grid with
+// L >= 4h + 1 the circular autocorrelation of that spectrum is exact. So:
+//
+//   1. pupil table : P_s(c_s + d) (x V_c for the vector model), FP64 math,
+//                    exact IEEE aperture test — k_pupil_table
+//   2. mask band   : M(k) / N^2 for |kx|, |ky| <= bm — band.cu, twice
+//   3. coarse      : e = IFFT_L(M P), J += w |e|^2, on chip — k_coarse32
+//   4. reduce      : J summed over thread blocks in a fixed order, then
+//                    B(g) = FFT_L(J)(g) / L^2 for |g| <= 2h — k_coarse_reduce
+//   5. synthesis   : I(x) = sum_g B(g) exp(2 pi i g.x / N), the only pass
+//                    over N^2 pixels — k_synth
+//   6. normalise   : peak / clear / none (aerial_image.py:217-241) — k_normalise
+//
+// Every step is deterministic (no floating-point atomics).
+#include <cstdio>
+#include <cstring>
+
+#include "common.cuh"
+#include "pupil.cuh"
+
+namespace litho {
+
+cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_per_clip, int n,
+                                int bm, float2* out, float scale, const float2* tw_inv,
+                                int num_sms, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// 1. pupil table: table[job][comp][(dy+h)(2h+1) + dx+h]
+// ---------------------------------------------------------------------------
+__global__ void k_pupil_table(const LithoJob* __restrict__ jobs, const LithoPupil* __restrict__ pupils,
+                              int n_jobs, int n, double pixel_size, int h, int ncomp_max,
+                              float2* __restrict__ table) {
+  const int j = blockIdx.x;
+  if (j >= n_jobs) return;
+  const LithoJob job = jobs[j];
+  const LithoPupil P = pupils[job.pupil];
+  const int side = 2 * h + 1, npts = side * side;
+  const double val = ddiv(1.0, dmul((double)n, pixel_size));
+  const double kmax = ddiv(P.NA, P.wavelength);
+  float2* out = table + (size_t)j * ncomp_max * npts;
+  for (int p = threadIdx.x; p < npts; p += blockDim.x) {
+    const int dy = p / side - h, dx = p % side - h;
+    const int kx = job.cx + dx, ky = job.cy + dy;
+    float2 v[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+    if (bin_valid(kx, n) && bin_valid(ky, n)) {
+      double fx, fy;
+      const double rho = aperture_rho(kx, ky, val, job.fsx, job.fsy, kmax, fx, fy);
+      if (rho <= 1.0) pupil_values(P, rho, fx, fy, job.jx, job.jy, v);
+    }
+    for (int c = 0; c < ncomp_max; ++c) out[(size_t)c * npts + p] = v[c];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 3. coarse accumulation, L = 32: one warp per coherent system at a time.
+//    Lane = spectral column dx in pass 1 (over ky), output row v in pass 2
+//    (over kx). Each lane keeps its row of J(u, v) in 32 registers.
+// ---------------------------------------------------------------------------
+constexpr int kCoarseWarps = 4;
+constexpr int kCoarseHMax32 = 7;  // 4h + 1 <= 32
+
+__global__ void __launch_bounds__(kCoarseWarps * 32)
+k_coarse32(const LithoItem* __restrict__ items, const LithoJob* __restrict__ jobs,
+           const float2* __restrict__ table, int h, int ncomp_max, const float2* __restrict__ Mb,
+           int bm, float* __restrict__ partial) {
+  extern __shared__ float2 smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* tb = smem + warp * (32 * 33);
+  const LithoItem it = items[blockIdx.x];
+  const int side = 2 * h + 1, npts = side * side, Bm = 2 * bm + 1;
+  const int dx = lane - h;
+  const bool col_live = lane < side;
+
+  float J[32];
+#pragma unroll
+  for (int u = 0; u < 32; ++u) J[u] = 0.f;
+
+  for (int j = it.job_begin + warp; j < it.job_end; j += kCoarseWarps) {
+    const LithoJob job = jobs[j];
+    const float w = (float)job.weight;
+    const float2* m = Mb + (size_t)job.clip * Bm * Bm;
+    const int mx = job.cx + dx + bm;
+    for (int c = 0; c < job.ncomp; ++c) {
+      const float2* tp = table + ((size_t)j * ncomp_max + c) * npts;
+      float2 v[32];
+#pragma unroll
+      for (int i = 0; i < 32; ++i) v[i] = make_float2(0.f, 0.f);
+      if (col_live && mx >= 0 && mx < Bm) {
+#pragma unroll
+        for (int d = -kCoarseHMax32; d <= kCoarseHMax32; ++d) {
+          const int my = job.cy + d + bm;
+          if (d >= -h && d <= h && my >= 0 && my < Bm)
+            v[(d + 32) & 31] = cmul(__ldg(tp + (d + h) * side + (dx + h)), __ldg(m + (size_t)my * Bm + mx));
+        }
+      }
+      fft_reg<32, +1>(v);  // over ky: T(kx = dx, v)
+      __syncwarp();
+#pragma unroll
+      for (int i = 0; i < 32; ++i) tb[lane * 33 + i] = v[i];
+      __syncwarp();
+      // Pass-2 input: row `lane` of T, non-zero only at kx = d in [-h, h],
+      // i.e. register positions 0..7 and 25..31; 8..24 are cleared.
+#pragma unroll
+      for (int i = kCoarseHMax32 + 1; i < 32 - kCoarseHMax32; ++i) v[i] = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int d = -kCoarseHMax32; d <= kCoarseHMax32; ++d)
+        v[(d + 32) & 31] = (d >= -h && d <= h) ? tb[(d + h) * 33 + lane] : make_float2(0.f, 0.f);
+      fft_reg<32, +1>(v);  // over kx: e(u, v = lane)
+#pragma unroll
+      for (int u = 0; u < 32; ++u) J[u] = fmaf(w, cabs2(v[u]), J[u]);
+    }
+  }
+
+  // Fixed-order reduction of the warps' J into this block's partial.
+  __syncthreads();
+  float* js = reinterpret_cast<float*>(smem);  // [warp][v][u], kCoarseWarps x 1024 floats
+#pragma unroll
+  for (int u = 0; u < 32; ++u) js[warp * 1024 + lane * 32 + u] = J[u];
+  __syncthreads();
+  float* dst = partial + (size_t)blockIdx.x * 1024;
+  for (int idx = threadIdx.x; idx < 1024; idx += blockDim.x) {
+    float s = 0.f;
+#pragma unroll
+    for (int wp = 0; wp < kCoarseWarps; ++wp) s += js[wp * 1024 + idx];
+    dst[idx] = s;  // idx = v * 32 + u  (row = y, column = x)
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 4. per output: J = sum of its items' partials (in item order), then
+//    B(gx, gy) = (1/L^2) sum_{u,v} J(v, u) exp(-2 pi i (gx u + gy v) / L).
+// ---------------------------------------------------------------------------
+__global__ void k_coarse_reduce(const int32_t* __restrict__ out_items, const float* __restrict__ partial,
+                                int L, int h, float2* __restrict__ Bout) {
+  extern __shared__ float sm_f[];
+  const int o = blockIdx.x;
+  const int LL = L * L, G = 4 * h + 1, g0 = 2 * h;
+  float* J = sm_f;                                         // [v][u]
+  float2* R = reinterpret_cast<float2*>(sm_f + LL);        // [u][gy]
+  float2* tw = R + (size_t)L * G;                          // exp(-2 pi i t / L)
+  for (int t = threadIdx.x; t < L; t += blockDim.x) {
+    double s, c;
+    sincospi(2.0 * t / (double)L, &s, &c);
+    tw[t] = make_float2((float)c, (float)-s);
+  }
+  const int i0 = out_items[o], i1 = out_items[o + 1];
+  for (int idx = threadIdx.x; idx < LL; idx += blockDim.x) {
+    float s = 0.f;
+    for (int i = i0; i < i1; ++i) s += partial[(size_t)i * LL + idx];
+    J[idx] = s;
+  }
+  __syncthreads();
+  for (int id = threadIdx.x; id < L * G; id += blockDim.x) {
+    const int u = id / G, gy = id % G - g0;
+    float2 s = make_float2(0.f, 0.f);
+    for (int v = 0; v < L; ++v) {
+      const int t = ((gy * v) % L + L) % L;
+      s = cadd(s, cscale(tw[t], J[v * L + u]));
+    }
+    R[u * G + (gy + g0)] = s;
+  }
+  __syncthreads();
+  const float inv = 1.0f / (float)LL;
+  float2* B = Bout + (size_t)o * G * G;
+  for (int id = threadIdx.x; id < G * G; id += blockDim.x) {
+    const int gyi = id / G, gx = id % G - g0;
+    float2 s = make_float2(0.f, 0.f);
+    for (int u = 0; u < L; ++u) {
+      const int t = ((gx * u) % L + L) % L;
+      s = cadd(s, cmul(R[u * G + gyi], tw[t]));
+    }
+    B[gyi * G + (gx + g0)] = cscale(s, inv);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 5. synthesis: I(x, y) = Re C(y, 0) + 2 sum_{gx >= 1} Re[C(y, gx) w^(gx x)],
+//    C(y, gx) = sum_gy B(gx, gy) w^(gy y), w = exp(2 pi i / N).
+// ---------------------------------------------------------------------------
+constexpr int kSynthRows = 4;
+
+__global__ void __launch_bounds__(256)
+k_synth(const float2* __restrict__ Bbox, int G, int n, const float2* __restrict__ tw_inv,
+        const LithoNorm* __restrict__ norm, float* __restrict__ image, float* __restrict__ blockmax) {
+  extern __shared__ float2 sm2[];
+  float2* tw = sm2;                       // n entries
+  float2* C = sm2 + n;                    // [kSynthRows][gh + 1]
+  __shared__ float red[256 / 32];
+  const int o = blockIdx.y, y0 = blockIdx.x * kSynthRows;
+  const int gh = G / 2;
+  const bool pow2 = (n & (n - 1)) == 0;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) tw[j] = tw_inv[j];
+  __syncthreads();
+  const float2* B = Bbox + (size_t)o * G * G;
+  for (int id = threadIdx.x; id < kSynthRows * (gh + 1); id += blockDim.x) {
+    const int r = id / (gh + 1), gx = id % (gh + 1), y = y0 + r;
+    float2 s = make_float2(0.f, 0.f);
+    if (y < n) {
+      for (int gy = -gh; gy <= gh; ++gy) {
+        long long e = (long long)gy * y;
+        int t = (int)(pow2 ? (e & (n - 1)) : (((e % n) + n) % n));
+        s = cadd(s, cmul(B[(gy + gh) * G + (gx + gh)], tw[t]));
+      }
+    }
+    C[r * (gh + 1) + gx] = s;
+  }
+  __syncthreads();
+  const LithoNorm nm = norm[o];
+  const float sc = nm.mode == 0 ? nm.scale : 1.0f;
+  float mx = 0.f;
+  for (int r = 0; r < kSynthRows; ++r) {
+    const int y = y0 + r;
+    if (y >= n) break;
+    const float2* Cr = C + r * (gh + 1);
+    float* dst = image + ((size_t)o * n + y) * n;
+    for (int x = threadIdx.x; x < n; x += blockDim.x) {
+      float acc = 0.f;
+      for (int gx = 1; gx <= gh; ++gx) {
+        long long e = (long long)gx * x;
+        int t = (int)(pow2 ? (e & (n - 1)) : (e % n));
+        const float2 c = Cr[gx], wv = tw[t];
+        acc = fmaf(c.x, wv.x, fmaf(-c.y, wv.y, acc));
+      }
+      const float val = fmaf(2.f, acc, Cr[0].x);
+      mx = fmaxf(mx, val);
+      dst[x] = val * sc;
+    }
+  }
+  // block max of the raw intensity
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = red[0];
+    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) m = fmaxf(m, red[i]);
+    blockmax[(size_t)o * gridDim.x + blockIdx.x] = m;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 6. peak and peak normalisation
+// ---------------------------------------------------------------------------
+__global__ void k_normalise(const float* __restrict__ blockmax, int nblk, const LithoNorm* __restrict__ norm,
+                            int n, float* __restrict__ image, float* __restrict__ peak) {
+  __shared__ float s_peak;
+  const int o = blockIdx.y;
+  if (threadIdx.x == 0) {
+    float m = blockmax[(size_t)o * nblk];
+    for (int i = 1; i < nblk; ++i) m = fmaxf(m, blockmax[(size_t)o * nblk + i]);
+    s_peak = m;
+    if (blockIdx.x == 0) peak[o] = m;
+  }
+  __syncthreads();
+  const LithoNorm nm = norm[o];
+  if (nm.mode != 1) return;
+  const float pk = s_peak;
+  const float sc = pk > 0.f ? nm.scale / pk : nm.scale;
+  const size_t NN = (size_t)n * n;
+  float* img = image + (size_t)o * NN;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < NN; i += (size_t)gridDim.x * blockDim.x)
+    img[i] *= sc;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct AbbeLayout {
+  int64_t tw, u1, mb, table, partial, bbox, blockmax, total;
+};
+
+static int synth_blocks(int n) { return (n + kSynthRows - 1) / kSynthRows; }
+
+static AbbeLayout abbe_layout(const LithoAbbePlan& p) {
+  AbbeLayout l{};
+  const int64_t Bm = 2 * p.bm + 1, side = 2 * p.h + 1, G = 4 * p.h + 1;
+  int64_t off = 0;
+  l.tw = off;       off = align16(off + (int64_t)p.n * 8);
+  l.u1 = off;       off = align16(off + (int64_t)p.n_clips * Bm * p.n * 8);
+  l.mb = off;       off = align16(off + (int64_t)p.n_clips * Bm * Bm * 8);
+  l.table = off;    off = align16(off + (int64_t)p.n_jobs * p.ncomp_max * side * side * 8);
+  l.partial = off;  off = align16(off + (int64_t)p.n_items * p.L * p.L * 4);
+  l.bbox = off;     off = align16(off + (int64_t)p.n_out * G * G * 8);
+  l.blockmax = off; off = align16(off + (int64_t)p.n_out * synth_blocks(p.n) * 4);
+  l.total = off;
+  return l;
+}
+
+static int check_plan(const LithoAbbePlan* p) {
+  if (!p) return LITHO_E_NULL;
+  if (p->n < 2 || p->n > 8192 || p->n_clips < 1 || p->n_out < 1 || p->n_jobs < 0 || p->n_items < 0 ||
+      p->n_pupils < 1 || p->h < 0 || p->bm < 0)
+    return LITHO_E_SIZE;
+  if (p->ncomp_max != 1 && p->ncomp_max != 3) return LITHO_E_SIZE;
+  if (p->L != 32) return LITHO_E_UNSUPPORTED;
+  if (4 * p->h + 1 > p->L || p->h > kCoarseHMax32) return LITHO_E_BAND;
+  if (p->bm < p->h) return LITHO_E_BAND;
+  if (!(p->pixel_size > 0.0)) return LITHO_E_SIZE;
+  const int64_t offs[5] = {p->off_jobs, p->off_pupils, p->off_items, p->off_out_items, p->off_norm};
+  for (int i = 0; i < 5; ++i)
+    if (offs[i] < 0 || (offs[i] & 15)) return LITHO_E_ALIGN;
+  return LITHO_OK;
+}
+
+static int num_sms_cached() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+}  // namespace litho
+
+using namespace litho;
+
+extern "C" int litho_abbe_workspace(const LithoAbbePlan* plan, size_t* bytes) {
+  const int st = check_plan(plan);
+  if (st) return st;
+  if (!bytes) return LITHO_E_NULL;
+  *bytes = (size_t)abbe_layout(*plan).total;
+  return LITHO_OK;
+}
+
+extern "C" int litho_abbe(const LithoAbbePlan* plan, const void* blob, const void* mask, float* image,
+                          float* peak, void* ws, size_t ws_bytes, cudaStream_t s) {
+  int st = check_plan(plan);
+  if (st) return st;
+  if (!blob || !mask || !image || !peak || !ws) return LITHO_E_NULL;
+  if (((uintptr_t)ws & 15) || ((uintptr_t)blob & 15) || ((uintptr_t)mask & 7)) return LITHO_E_ALIGN;
+  const LithoAbbePlan& p = *plan;
+  const AbbeLayout l = abbe_layout(p);
+  if ((int64_t)ws_bytes < l.total) return LITHO_E_WORKSPACE;
+  if (p.n_items == 0 || p.n_jobs == 0) return LITHO_E_SIZE;
+
+  const char* b = static_cast<const char*>(blob);
+  const LithoJob* jobs = reinterpret_cast<const LithoJob*>(b + p.off_jobs);
+  const LithoPupil* pupils = reinterpret_cast<const LithoPupil*>(b + p.off_pupils);
+  const LithoItem* items = reinterpret_cast<const LithoItem*>(b + p.off_items);
+  const int32_t* out_items = reinterpret_cast<const int32_t*>(b + p.off_out_items);
+  const LithoNorm* norm = reinterpret_cast<const LithoNorm*>(b + p.off_norm);
+
+  char* w = static_cast<char*>(ws);
+  float2* tw = reinterpret_cast<float2*>(w + l.tw);
+  float2* u1 = reinterpret_cast<float2*>(w + l.u1);
+  float2* mb = reinterpret_cast<float2*>(w + l.mb);
+  float2* table = reinterpret_cast<float2*>(w + l.table);
+  float* partial = reinterpret_cast<float*>(w + l.partial);
+  float2* bbox = reinterpret_cast<float2*>(w + l.bbox);
+  float* blockmax = reinterpret_cast<float*>(w + l.blockmax);
+
+  const int sms = num_sms_cached();
+  const int Bm = 2 * p.bm + 1, G = 4 * p.h + 1;
+  cudaError_t e;
+
+  k_twiddle_table<<<(p.n + 255) / 256, 256, 0, s>>>(tw, p.n, +1);
+  k_pupil_table<<<p.n_jobs, 128, 0, s>>>(jobs, pupils, p.n_jobs, p.n, p.pixel_size, p.h, p.ncomp_max, table);
+  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+
+  // mask band spectrum: rows then columns, 1/N^2 folded into the second pass
+  e = launch_row_band_dft(mask, p.mask_complex != 0, p.n_clips * p.n, p.n, p.n, p.bm, u1, 1.0f, tw, sms, s);
+  if (e != cudaSuccess) return (int)e;
+  e = launch_row_band_dft(u1, true, p.n_clips * Bm, Bm, p.n, p.bm, mb, 1.0f / ((float)p.n * (float)p.n), tw,
+                          sms, s);
+  if (e != cudaSuccess) return (int)e;
+
+  const size_t sm_coarse = (size_t)kCoarseWarps * 32 * 33 * sizeof(float2);
+  cudaFuncSetAttribute(k_coarse32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_coarse);
+  k_coarse32<<<p.n_items, kCoarseWarps * 32, sm_coarse, s>>>(items, jobs, table, p.h, p.ncomp_max, mb, p.bm,
+                                                              partial);
+  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+
+  const size_t sm_red = (size_t)p.L * p.L * 4 + (size_t)p.L * G * 8 + (size_t)p.L * 8;
+  cudaFuncSetAttribute(k_coarse_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_red);
+  k_coarse_reduce<<<p.n_out, 256, sm_red, s>>>(out_items, partial, p.L, p.h, bbox);
+  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+
+  const int gh = G / 2;
+  const size_t sm_syn = (size_t)p.n * 8 + (size_t)kSynthRows * (gh + 1) * 8;
+  cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_syn);
+  dim3 gs(synth_blocks(p.n), p.n_out);
+  k_synth<<<gs, 256, sm_syn, s>>>(bbox, G, p.n, tw, norm, image, blockmax);
+  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+
+  dim3 gn((unsigned)((((size_t)p.n * p.n + 255) / 256) < 512 ? (((size_t)p.n * p.n + 255) / 256) : 512), p.n_out);
+  k_normalise<<<gn, 256, 0, s>>>(blockmax, synth_blocks(p.n), norm, p.n, image, peak);
+  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  return LITHO_OK;
+}

@@ -1,0 +1,109 @@
+// Shared device helpers for liblitho_b200: complex arithmetic, register-
+// resident radix-2 FFTs, twiddle tables and launch checks.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/litho_b200.h"
+#include "twiddles.cuh"
+
+namespace litho {
+
+// ---------------------------------------------------------------------------
+// complex float2
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
+  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y; }
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+
+// ---------------------------------------------------------------------------
+// Register FFT: natural-order in and out, radix-2 decimation in time,
+// SIGN = +1 computes sum_k v_k exp(+2 pi i k j / N) (unnormalised inverse),
+// SIGN = -1 the forward transform. N <= 64, fully unrolled so every index and
+// twiddle is a compile-time constant and the array stays in registers.
+// ---------------------------------------------------------------------------
+template <int N>
+struct Log2 { static constexpr int value = 1 + Log2<N / 2>::value; };
+template <>
+struct Log2<1> { static constexpr int value = 0; };
+
+__host__ __device__ constexpr int bitrev(int i, int bits) {
+  int r = 0;
+  for (int b = 0; b < bits; ++b) r |= ((i >> b) & 1) << (bits - 1 - b);
+  return r;
+}
+
+// b * exp(SIGN * 2 pi i t / 64), with the four trivial angles special-cased so
+// no multiply by an exact 0 or 1 is emitted.
+template <int SIGN>
+__device__ __forceinline__ float2 twiddle64(float2 b, int t) {
+  t &= 63;
+  if (t == 0) return b;
+  if (t == 32) return make_float2(-b.x, -b.y);
+  if (t == 16) return SIGN > 0 ? make_float2(-b.y, b.x) : make_float2(b.y, -b.x);
+  if (t == 48) return SIGN > 0 ? make_float2(b.y, -b.x) : make_float2(-b.y, b.x);
+  const float c = tw64_re(t);
+  const float s = SIGN > 0 ? tw64_im(t) : -tw64_im(t);
+  return make_float2(b.x * c - b.y * s, b.x * s + b.y * c);
+}
+
+template <int N, int SIGN>
+__device__ __forceinline__ void fft_reg(float2 (&v)[N]) {
+  static_assert(N >= 2 && N <= 64 && (N & (N - 1)) == 0, "fft_reg: N in {2..64}");
+  constexpr int LOG = Log2<N>::value;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const int j = bitrev(i, LOG);
+    if (j > i) {
+      const float2 t = v[i];
+      v[i] = v[j];
+      v[j] = t;
+    }
+  }
+#pragma unroll
+  for (int half = 1; half < N; half <<= 1) {
+#pragma unroll
+    for (int base = 0; base < N; base += 2 * half) {
+#pragma unroll
+      for (int k = 0; k < half; ++k) {
+        const float2 a = v[base + k];
+        const float2 bw = twiddle64<SIGN>(v[base + k + half], k * (64 / (2 * half)));
+        v[base + k] = cadd(a, bw);
+        v[base + k + half] = csub(a, bw);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 with every rounding explicit (no FMA contraction), so that decisions
+// like "rho <= 1" reproduce numpy's IEEE double arithmetic bit for bit.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double dsqrt(double a) { return __dsqrt_rn(a); }
+
+// Signed FFT bin k of an N-point grid -> physical frequency, exactly as
+// numpy.fft.fftfreq(N, d)[k mod N] = float(k) * (1.0 / (N * d)).
+__device__ __forceinline__ double bin_freq(int k, double val) { return dmul((double)k, val); }
+
+// Does signed bin k exist on an N-point FFT grid?
+__device__ __forceinline__ bool bin_valid(int k, int n) { return k >= -(n / 2) && k <= (n - 1) / 2; }
+
+__host__ __device__ __forceinline__ int64_t align16(int64_t x) { return (x + 15) & ~int64_t(15); }
+
+// Device twiddle table w[j] = exp(sign * 2 pi i j / n), FP64 evaluated, FP32 stored.
+__global__ void k_twiddle_table(float2* w, int n, int sign);
+
+}  // namespace litho

@@ -1,0 +1,146 @@
+"""Abbe imaging on the GPU against the reference (golden fixtures) and the oracle.
+
+Tolerance: max |I_gpu - I_ref| / max I_ref <= 1e-5 (FP32 engine vs FP64
+reference), the bar the accelerated path is held to.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import load_golden, ns_grid, ns_optics
+from oracle import litho_oracle as O
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def lb():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import lithobat_b200
+    return lithobat_b200
+
+
+def _optics(lb, od):
+    od = dict(od)
+    od["zernike_coeffs"] = {int(k): v for k, v in (od.get("zernike_coeffs") or {}).items()}
+    keep = {k: od[k] for k in lb.OpticsConfig.__dataclass_fields__ if k in od}
+    return lb.OpticsConfig(**keep)
+
+
+def rel_err(a, b):
+    return float(np.abs(np.asarray(a, np.float64) - b).max() / np.abs(b).max())
+
+
+ABBE = ["abbe_conventional", "abbe_annular_aberrated", "abbe_dipole_exact_clear",
+        "abbe_vector_te", "abbe_vector_tm", "abbe_vector_x", "abbe_vector_y",
+        "abbe_vector_unpolarised", "c3_vector_128"]
+
+
+@pytest.mark.parametrize("name", ABBE)
+def test_raw_sum_matches_reference(lb, name):
+    a, od, gd = load_golden(name)
+    o, g = _optics(lb, od), lb.GridConfig(**gd)
+    raw, peak, clear = lb.compute_aerial_image(a["mask"], o, g, return_raw=True)
+    assert raw.shape == a["raw"].shape and raw.dtype == np.float64
+    assert rel_err(raw, a["raw"]) <= TOL
+    assert peak == pytest.approx(float(a["peak"]), rel=TOL)
+    assert clear == pytest.approx(float(a["clear"]), rel=1e-12)
+
+
+@pytest.mark.parametrize("name", ["abbe_conventional", "abbe_annular_aberrated", "abbe_dipole_exact_clear"])
+def test_normalised_dosed_image(lb, name):
+    a, od, gd = load_golden(name)
+    img = lb.compute_aerial_image(a["mask"], _optics(lb, od), lb.GridConfig(**gd), dose=1.3)
+    assert rel_err(img, a["image_dose13"]) <= TOL
+
+
+def test_first_workload_full_size(lb):
+    """Scalar Abbe, ArF dry annular (264 source points), 256^2 at 4 nm, L/S 200/100 nm."""
+    a, od, gd = load_golden("c1_scalar_256")
+    mask = lb.patterns.lines_and_spaces(256, 4e-9, 200e-9, 100e-9)
+    o, g = _optics(lb, od), lb.GridConfig(**gd)
+    raw, peak, clear = lb.compute_aerial_image(mask, o, g, return_raw=True)
+    assert rel_err(raw, a["raw"]) <= TOL
+    assert rel_err(lb.compute_aerial_image(mask, o, g), a["image"]) <= TOL
+
+
+def test_batched_clip_with_aberrations(lb):
+    a, od, gd = load_golden("c2_clip_128")
+    o, g = _optics(lb, od), lb.GridConfig(**gd)
+    raw, peak, clear = lb.compute_aerial_image(a["mask"].astype(np.complex64), o, g, return_raw=True)
+    assert rel_err(raw, a["raw"]) <= TOL
+
+
+@pytest.mark.parametrize("name", ["planes_scalar", "planes_vector"])
+def test_planes(lb, name):
+    a, od, gd = load_golden(name)
+    dose = 1.3 if name == "planes_scalar" else 1.0
+    st = lb.compute_aerial_planes(a["mask"], _optics(lb, od), lb.GridConfig(**gd),
+                                  [tuple(p) for p in a["planes"]], dose=dose)
+    assert st.shape == a["stack"].shape
+    for p in range(st.shape[0]):
+        assert rel_err(st[p], a["stack"][p]) <= TOL
+
+
+def test_batch_equals_one_clip_at_a_time(lb):
+    """Per-clip optics in one batched call == each clip imaged on its own."""
+    import torch
+    rng = np.random.default_rng(4)
+    g = lb.GridConfig(n_pixels=128, pixel_size=2e-9)
+    masks = np.stack([lb.patterns.manhattan_clip(rng, 128, 2e-9, (6, 12)) for _ in range(5)])
+    optics = [lb.OpticsConfig(NA=1.35, n_immersion=1.44, defocus=float(rng.uniform(-60e-9, 60e-9)),
+                              zernike_coeffs={j: float(rng.uniform(-0.02, 0.02)) for j in range(4, 22)},
+                              source_spec=lb.Source.quadrupole(0.9, 0.7, 30, 0).to_dict())
+              for _ in range(5)]
+    img, peak, clear = lb.compute_aerial_batch(masks, optics, g, return_raw=True)
+    for c in range(5):
+        one = lb.compute_aerial_image(masks[c], optics[c], g, return_raw=True)
+        np.testing.assert_allclose(img[c, 0].cpu().numpy(), one[0], rtol=0, atol=1e-6 * one[1])
+        ref = O.compute_aerial_image(masks[c], optics[c], g, return_raw=True)
+        assert rel_err(img[c, 0].cpu().numpy(), ref[0]) <= TOL
+
+
+def test_large_grid_against_oracle(lb):
+    """1024^2 at 1 nm, immersion vector TE, att-PSM contacts, a small source."""
+    g = lb.GridConfig(n_pixels=1024, pixel_size=1e-9)
+    c = lb.patterns.contact_array(1024, 1e-9, 110e-9, 110e-9, 55e-9)
+    mask = lb.patterns.to_attenuated_psm(1.0 - c, 0.06, 180.0)
+    o = lb.OpticsConfig(NA=1.35, n_immersion=1.44, imaging_model="vector", polarisation="te",
+                        source_type="annular", sigma_inner=0.5, sigma_outer=0.9, source_grid=5)
+    raw, peak, clear = lb.compute_aerial_image(mask, o, g, return_raw=True)
+    ref = O.compute_aerial_image(mask, o, g, return_raw=True)
+    assert rel_err(raw, ref[0]) <= TOL
+    assert clear == pytest.approx(ref[2], rel=1e-12)
+
+
+def test_open_frame_prints_exactly_one_under_clear_normalisation(lb):
+    """A clear mask images to its own open-frame throughput everywhere."""
+    g = lb.GridConfig(n_pixels=256, pixel_size=2e-9)
+    for kw in (dict(), dict(imaging_model="vector", polarisation="te"),
+               dict(imaging_model="vector", polarisation="unpolarised")):
+        o = lb.OpticsConfig(NA=1.35, n_immersion=1.44, source_type="annular", sigma_inner=0.5,
+                            sigma_outer=0.9, source_grid=11, normalisation="clear", **kw)
+        img = lb.compute_aerial_image(np.ones((256, 256)), o, g)
+        assert np.abs(img - 1.0).max() < 1e-5
+
+
+def test_torch_in_torch_out(lb):
+    import torch
+    g = lb.GridConfig(n_pixels=64, pixel_size=4e-9)
+    m = torch.tensor(lb.patterns.lines_and_spaces(64, 4e-9, 128e-9, 64e-9), device="cuda")
+    out = lb.compute_aerial_image(m, lb.OpticsConfig(), g)
+    assert isinstance(out, torch.Tensor) and out.is_cuda and out.dtype == torch.float32
+    assert abs(float(out.max()) - 1.0) < 1e-6
+
+
+def test_dose_is_a_pure_multiplier_and_raw_reconstructs(lb):
+    a, od, gd = load_golden("abbe_annular_aberrated")
+    o, g = _optics(lb, od), lb.GridConfig(**gd)
+    raw, peak, clear = lb.compute_aerial_image(a["mask"], o, g, return_raw=True)
+    img = lb.compute_aerial_image(a["mask"], o, g, dose=0.7)
+    np.testing.assert_allclose(img, raw * lb.normalisation_scale("peak", peak, clear, 0.7), atol=1e-6)

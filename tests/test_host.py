@@ -1,0 +1,105 @@
+"""Host-side logic of the product package, checked without a GPU."""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from lithobat_b200 import GridConfig, OpticsConfig, normalisation_scale, source_points
+from lithobat_b200.aerial import disc_halfwidth, plan_abbe
+from lithobat_b200.config import optics_view
+from lithobat_b200.pupil import clear_throughput
+from lithobat_b200.source import Source
+
+SOURCE_CASES = ["annular31", "annular31_imm", "conventional21", "dipole_legacy",
+                "quadrupole_legacy", "cquad_spec", "euv_dipole43", "quasar_blur", "monopole"]
+
+
+def _optics(od):
+    od = dict(od)
+    od["zernike_coeffs"] = {int(k): v for k, v in (od.get("zernike_coeffs") or {}).items()}
+    keep = {k: od[k] for k in OpticsConfig.__dataclass_fields__ if k in od}
+    return OpticsConfig(**keep)
+
+
+@pytest.mark.parametrize("name", SOURCE_CASES)
+def test_source_points_are_bit_identical_to_the_reference(name):
+    a, od, _ = load_golden(f"source_{name}")
+    sp = source_points(_optics(od))
+    for k in ("weight", "fx", "fy", "phi"):
+        np.testing.assert_array_equal(getattr(sp, k), a[k])
+
+
+ABBE = ["abbe_conventional", "abbe_annular_aberrated", "abbe_dipole_exact_clear",
+        "abbe_vector_te", "abbe_vector_tm", "abbe_vector_x", "abbe_vector_y",
+        "abbe_vector_unpolarised", "c2_clip_128", "c3_vector_128", "c1_scalar_256"]
+
+
+@pytest.mark.parametrize("name", ABBE)
+def test_clear_throughput_matches_the_reference(name):
+    a, od, gd = load_golden(name)
+    o = _optics(od)
+    v = optics_view(o)
+    got = clear_throughput(source_points(o), v, v.image_index, v.imaging_model == "vector")
+    assert got == pytest.approx(float(a["clear"]), rel=1e-12, abs=1e-300)
+
+
+def test_normalisation_scale_modes():
+    assert normalisation_scale("peak", 2.0, 5.0, 1.5) == 0.75
+    assert normalisation_scale("clear", 2.0, 5.0, 1.5) == 0.3
+    assert normalisation_scale("none", 2.0, 5.0, 1.5) == 1.5
+    assert normalisation_scale("PEAK", 0.0, 5.0, 1.5) == 1.5
+    with pytest.raises(ValueError, match="normalisation must be"):
+        normalisation_scale("max", 1, 1)
+
+
+@pytest.mark.parametrize("NA,lam,n,px", [(0.93, 193e-9, 256, 4e-9), (1.35, 193e-9, 1024, 1e-9),
+                                         (1.35, 193e-9, 512, 2e-9), (0.33, 13.5e-9, 256, 2e-9),
+                                         (1.35, 193e-9, 64, 4e-9)])
+def test_every_in_aperture_bin_lies_in_the_coarse_box(NA, lam, n, px):
+    """The box [c - h, c + h]^2 around a source point's nearest bin must hold
+    every bin the reference's exact aperture test admits."""
+    R, h = disc_halfwidth(NA, lam, n, px)
+    val = 1.0 / (n * px)
+    k_max = NA / lam
+    rng = np.random.default_rng(0)
+    fs = rng.uniform(-1, 1, size=(400, 2)) * k_max
+    k = np.arange(-(n // 2), (n - 1) // 2 + 1)
+    for fsx, fsy in fs:
+        cx, cy = int(np.rint(fsx / val)), int(np.rint(fsy / val))
+        sel = np.abs(k * val - fsx) <= 1.01 * k_max
+        kx = k[sel]
+        sel = np.abs(k * val - fsy) <= 1.01 * k_max
+        ky = k[sel]
+        KX, KY = np.meshgrid(kx, ky)
+        rho = np.sqrt((KX * val - fsx) ** 2 + (KY * val - fsy) ** 2) / k_max
+        inside = rho <= 1.0
+        assert np.all(np.abs(KX[inside] - cx) <= h) and np.all(np.abs(KY[inside] - cy) <= h)
+
+
+def test_plan_groups_jobs_by_output_and_counts_transforms():
+    o = OpticsConfig(NA=1.35, n_immersion=1.44, imaging_model="vector", polarisation="unpolarised",
+                     source_type="annular", sigma_outer=0.9, sigma_inner=0.5, source_grid=9)
+    v = optics_view(o)
+    pd = plan_abbe([v, v], 64, 4e-9, [[(0.0, 1.44), (50e-9, 1.7)]] * 2, 1.0, False, False)
+    S = len(source_points(o))
+    assert pd.n_out == 4 and pd.jobs == 4 * S * 2 and pd.transforms == 3 * pd.jobs
+    assert pd.plan.ncomp_max == 3 and 4 * pd.plan.h + 1 <= pd.plan.L
+    assert pd.plan.bm >= pd.plan.h
+
+
+def test_thick_masks_and_bad_models_are_refused():
+    with pytest.raises(ValueError, match="thin"):
+        plan_abbe([optics_view(OpticsConfig(mask_model="fdtd"))], 64, 4e-9, [[(0.0, 1.0)]], 1.0, False, False)
+    with pytest.raises(ValueError, match="imaging_model"):
+        OpticsConfig(imaging_model="quantum")
+
+
+def test_source_presets_round_trip_through_dicts():
+    s = Source.quadrupole(0.9, 0.7, opening_deg=30, rotation_deg=0)
+    d = s.to_dict()
+    assert Source.from_dict(d).render(21).tolist() == s.render(21).tolist()
+    assert s.n_points(21) == 34
