@@ -1,0 +1,367 @@
+"""Benchmark of the imaging hot path on B200s (one process per GPU).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python -m torch.distributed.run --nproc-per-node N bench.py --gpus N ...
+
+Workload (one step, per GPU): a batch of 512 seeded 1024 x 1024 clips at 1 nm —
+6 %-transmission attenuated phase-shift masks (phase pi) of contact-hole
+arrays, pitch 80-140 nm, hole 40-70 nm — imaged with the vector (Ex, Ey, Ez)
+Abbe model, NA 1.35 water immersion, azimuthal (TE) polarisation, annular
+source sigma 0.5-0.9 sampled on a 31 x 31 grid (400 source points, 1200
+coherent transforms per image), peak normalisation. Each rank images its own
+clips (weak scaling, no collective on the data path).
+
+Prints one JSON line (rank 0). ``value`` is whole-job images/s with inputs
+resident in HBM; ``e2e`` is the same metric through the public API
+(``compute_aerial_batch``) from pinned host buffers, copies included.
+``--impl reference`` times the reference's algorithm on the host CPU (the
+FP64 numpy restatement in ``oracle/``, the same numpy/scipy calls), on a
+bounded sample of source points, and prints the same line for it.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Abbe images/s & ILT grad-steps/s @1024² fused vs plain, 1 B200, err≤1e-5"
+N, PX = 1024, 1e-9
+IMAGES_PER_STEP = 512    # one batched call per step
+ROTATE = 2               # distinct input batches of 4 GiB each (> 126 MiB L2)
+E2E_IMAGES = 64          # images per public-API call in the end-to-end measurement
+PLAIN_IMAGES = 8         # images per call of the plain (full-grid) comparison engine
+WORKLOAD = ("vector Abbe 1024^2 @1 nm, NA 1.35/1.44 TE, annular 0.5-0.9 (source_grid 31, 400 pts), "
+            "6% att-PSM contact holes")
+
+
+def optics_c3():
+    import lithobat_b200 as lb
+    return lb.OpticsConfig(NA=1.35, n_immersion=1.44, imaging_model="vector", polarisation="te",
+                           source_type="annular", sigma_inner=0.5, sigma_outer=0.9, source_grid=31)
+
+
+def masks_c3(seed: int, count: int) -> np.ndarray:
+    from lithobat_b200 import patterns
+    rng = np.random.default_rng(seed)
+    out = np.empty((count, N, N), dtype=np.complex64)
+    for i in range(count):
+        p = rng.uniform(80e-9, 140e-9)
+        hole = rng.uniform(40e-9, 70e-9)
+        c = patterns.contact_array(N, PX, p, p, hole)
+        out[i] = patterns.to_attenuated_psm(1.0 - c, 0.06, 180.0)
+    return out
+
+
+def masks_c3_device(torch, seed: int, count: int, dev):
+    """The same seeded clip family, generated on the device (complex64)."""
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    pitch = 80e-9 + 60e-9 * torch.rand(count, generator=g, dtype=torch.float64)
+    hole = 40e-9 + 30e-9 * torch.rand(count, generator=g, dtype=torch.float64)
+    coords = ((torch.arange(N, dtype=torch.float64) - N // 2) * PX).to(dev)
+    p, h = pitch.to(dev)[:, None], hole.to(dev)[:, None]
+    opened = (torch.remainder(coords[None, :] + p / 2, p) < h).to(torch.float32)   # (count, N)
+    chrome = 1.0 - opened[:, :, None] * opened[:, None, :]
+    absorber = torch.tensor(complex(np.sqrt(0.06) * np.exp(1j * np.pi)), dtype=torch.complex64, device=dev)
+    one = torch.ones((), dtype=torch.complex64, device=dev)
+    return torch.where(chrome > 0.5, absorber, one).contiguous()
+
+
+def measured_peaks() -> dict:
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        return json.loads(f.read_text())
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0, "_fallback": True}
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "20"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self) -> dict:
+        self.f.flush()
+        rows = []
+        for line in Path(self.f.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU (reference algorithm) timing
+# ---------------------------------------------------------------------------
+def cpu_sample_seconds(n_src: int = 12, repeats: int = 2) -> tuple[float, int, int]:
+    """Median seconds of the FP64 numpy Abbe sum over the first n_src source
+    points of the workload (one image); returns (t, n_src, S_total)."""
+    from oracle import litho_oracle as O
+    o = optics_c3()
+    S = len(O.source_points(o))
+    mask = masks_c3(1, 1)[0].astype(np.complex128)
+
+    class G:
+        n_pixels, pixel_size = N, PX
+    planes = [(o.defocus, o.image_index)]
+    O.abbe_sum(mask, o, G, planes, source_subset=range(2))  # warm the FFT plans
+    ts = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        O.abbe_sum(mask, o, G, planes, source_subset=range(n_src))
+        ts.append(time.perf_counter() - t0)
+    return statistics.median(ts), n_src, S
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    vals = []
+    for i in range(args.warmup + args.steps):
+        t, k, S = cpu_sample_seconds(repeats=1)
+        if i >= args.warmup:
+            vals.append(1.0 / (t * S / k))
+    v = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "images/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128/f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "images_per_step": 1},
+        "cpu_baseline": {"value": v, "unit": "images/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"{k} of {S} source points of one image per step, scaled by {S}/{k}"},
+        "e2e": {"value": v, "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU
+# ---------------------------------------------------------------------------
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    import lithobat_b200 as lb
+    from lithobat_b200 import aerial
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier(device_ids=[local])
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    o = optics_c3()
+    g = lb.GridConfig(n_pixels=N, pixel_size=PX)
+    B = args.images
+    dmasks = [masks_c3_device(torch, 1000 * rank + r, B, dev) for r in range(ROTATE)]
+    view = lb.config.optics_view(o)
+    pd = aerial.plan_abbe([view] * B, N, PX, [[(view.defocus, view.image_index)]] * B, 1.0, False, True)
+    out = torch.empty((B, N, N), dtype=torch.float32, device=dev)
+    peak = torch.empty((B,), dtype=torch.float32, device=dev)
+    launches_per_step = 7   # twiddles, band rows, band columns, coarse, reduce, synthesis, normalise
+
+    def step(i):
+        aerial.run_abbe(pd, dmasks[i % ROTATE], out, peak)
+
+    # ---- device-resident throughput (fused engine) ----
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0.record()
+        for i in range(args.steps):
+            step(i)
+        e1.record()
+        torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    clocks = clk.summary()
+    value = world * B * args.steps / (ms / 1000.0)
+    line = {
+        "metric": METRIC, "value": value, "unit": "images/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64/f32", "data": "synthetic (seeded att-PSM contact-hole clips)",
+        "clocks": clocks, "gpu_launches": launches_per_step * args.steps,
+    }
+    if "profile" in args.skip:
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    # ---- per-stage device times (CUDA events between the stages) ----
+    stages = aerial.profile_abbe(pd, dmasks[0], reps=max(3, args.steps))
+    step_ms = sum(stages.values())
+    dom = max(stages, key=stages.get)
+    pd_small = aerial.plan_abbe([view] * PLAIN_IMAGES, N, PX, [[(view.defocus, view.image_index)]] * PLAIN_IMAGES,
+                                1.0, False, True)
+    table_ms = aerial.profile_abbe(pd_small, dmasks[0][:PLAIN_IMAGES].contiguous(), reps=3,
+                                   rebuild_table=True)["pupil_table"]
+
+    # ---- fused vs plain on the same clips, and their agreement ----
+    sub = dmasks[0][:PLAIN_IMAGES].contiguous()
+    fused_img, _ = aerial.run_abbe(pd_small, sub)
+    fused_img = fused_img.clone()
+    plain_img, _ = aerial.run_abbe(pd_small, sub, engine="plain")  # warm
+    torch.cuda.synchronize()
+    p_steps = 2
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record()
+    for i in range(p_steps):
+        plain_img, _ = aerial.run_abbe(pd_small, sub, engine="plain")
+    e3.record()
+    torch.cuda.synchronize()
+    plain_ms = max_over_ranks(e2.elapsed_time(e3) / p_steps)
+    plain_value = world * PLAIN_IMAGES / (plain_ms / 1000.0)
+    agree = float(((fused_img.double() - plain_img.double()).abs().amax(dim=(1, 2))
+                   / plain_img.double().abs().amax(dim=(1, 2))).max())
+    del plain_img
+
+    # ---- end to end through the public API from pinned host memory ----
+    pinned = [dmasks[r][:E2E_IMAGES].cpu().pin_memory() for r in range(ROTATE)]
+    res = torch.empty((E2E_IMAGES, N, N), dtype=torch.float32).pin_memory()
+    for i in range(max(1, args.warmup)):
+        img, _pk, _cl = lb.compute_aerial_batch(pinned[i % ROTATE], o, g)
+        res.copy_(img[:, 0])
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e4.record()
+    for i in range(args.steps):
+        img, _pk, _cl = lb.compute_aerial_batch(pinned[i % ROTATE], o, g)
+        res.copy_(img[:, 0])
+    e5.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(max(e4.elapsed_time(e5), (time.perf_counter() - t0) * 1000.0))
+    e2e_value = world * E2E_IMAGES * args.steps / (e2e_ms / 1000.0)
+
+    # ---- roofline of the dominant stage ----
+    peaks = measured_peaks()
+    hbm = float(peaks["hbm_gbs"])
+    Bm = 2 * pd.plan.bm + 1
+    NN = N * N
+    stage_bytes = {   # algorithmic bytes of each stage per launch (the whole batch)
+        "pupil_table": pd.plan.n_tab * 3 * (2 * pd.plan.h + 1) ** 2 * 8,
+        "band_rows": B * (NN * 8 + N * Bm * 8),
+        "band_cols": B * (N * Bm * 8 + Bm * Bm * 8),
+        "coarse": pd.plan.n_tab * 3 * (2 * pd.plan.h + 1) ** 2 * 8 + pd.plan.n_items * 32 * 32 * 4,
+        "coarse_reduce": pd.plan.n_items * 32 * 32 * 4,
+        "synthesis": B * NN * 4,
+        "normalise": B * NN * 8,
+    }
+    achieved = stage_bytes[dom] / (stages[dom] / 1000.0) / 1e9
+    transforms = pd.transforms // B
+    formula_bytes = NN * (16 * transforms + 24)  # dense two-pass FFT equivalent, per image
+    line.update({
+        "config": {"workload": WORKLOAD, "images_per_step": B, "grid": N, "pixel_nm": 1.0,
+                   "source_points": pd.jobs // B, "transforms_per_image": transforms,
+                   "coarse_grid": int(pd.plan.L), "parallelism": f"replicas x{world}",
+                   "l2": f"{ROTATE} rotating input batches of {B * NN * 8 >> 20} MiB",
+                   "pupil_table": f"built once per optics ({table_ms:.3f} ms), reused across steps"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None,
+                     "peak_source": "measured" if not peaks.get("_fallback") else "fallback"},
+        "stages_ms": stages,
+        "dense_fft_equivalent": {"bytes_per_image": formula_bytes,
+                                 "GBps": formula_bytes * B / (step_ms / 1000.0) / 1e9},
+        "plain": {"value": plain_value, "unit": "images/s", "fused_over_plain": value / plain_value,
+                  "images_per_call": PLAIN_IMAGES, "max_rel_diff_fused_vs_plain": agree},
+        "e2e": {"value": e2e_value, "unit": "images/s", "h2d_bytes_per_step": E2E_IMAGES * NN * 8,
+                "d2h_bytes_per_step": E2E_IMAGES * NN * 4, "images_per_step": E2E_IMAGES},
+    })
+    if rank == 0 and world == 1 and not args.no_cpu:
+        t, k, S = cpu_sample_seconds()
+        cv = 1.0 / (t * S / k)
+        line["cpu_baseline"] = {"value": cv, "unit": "images/s", "cores": os.cpu_count(), "kind": "port",
+                                "sample": f"{k} of {S} source points of one image, scaled by {S}/{k}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--images", type=int, default=IMAGES_PER_STEP,
+                    help="images per step (a small value makes a profiling case)")
+    ap.add_argument("--skip", default="", help="comma list of phases to skip: plain,e2e,profile,cpu")
+    args = ap.parse_args()
+    args.skip = set(x for x in args.skip.split(",") if x)
+    if "cpu" in args.skip:
+        args.no_cpu = True
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

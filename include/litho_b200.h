@@ -73,7 +73,9 @@ typedef struct LithoJob {
     int32_t out;          /* which output image                             */
     int32_t cx, cy;       /* integer bin nearest the source offset          */
     int32_t ncomp;        /* 1 scalar, 3 vector                             */
-} LithoJob;               /* 64 bytes */
+    int32_t tab;          /* pupil-table slot; jobs of clips that share an  */
+                          /* optical state and source point share a slot    */
+} LithoJob;               /* 72 bytes */
 
 /* A contiguous run of jobs, all for one output image, accumulated by one
  * thread block. */
@@ -104,9 +106,10 @@ typedef struct LithoAbbePlan {
     int32_t L;            /* coarse grid side (>= 4h+1, power of two)       */
     int32_t mask_complex; /* 0: float32 masks, 1: complex64 masks           */
     int32_t ncomp_max;    /* 1 or 3                                         */
-    int32_t flags;        /* reserved, 0                                    */
+    int32_t n_tab;        /* pupil-table slots (max LithoJob.tab + 1)       */
     double pixel_size;    /* m                                              */
     int64_t off_jobs, off_pupils, off_items, off_out_items, off_norm;
+    int64_t off_slots;    /* int32[n_tab]: a job that owns each table slot  */
 } LithoAbbePlan;
 
 /* ---- library ----------------------------------------------------------- */
@@ -127,6 +130,29 @@ int litho_abi_sizes(int32_t* out, int n);
 /* Workspace bytes litho_abbe() needs for this plan. */
 int litho_abbe_workspace(const LithoAbbePlan* plan, size_t* bytes);
 
+/* Synchronise `stream` and return the device status word of the last
+ * litho_abbe*() call that used this workspace: 0, or LITHO_E_TIMEOUT if a
+ * bounded wait inside a kernel gave up (its outputs are then invalid). */
+int litho_abbe_status(const LithoAbbePlan* plan, const void* workspace_dev, cudaStream_t stream);
+
+/* Bytes of the pupil table of a plan: n_tab x ncomp_max x (2h+1)^2 complex
+ * float. The table depends on the optics and source only, not on the masks,
+ * so a caller imaging many batches with the same plan builds it once. */
+int litho_abbe_table_bytes(const LithoAbbePlan* plan, size_t* bytes);
+
+/* Fill table_dev with every slot's pupil P (x V_c) on its (2h+1)^2 box:
+ * expose/aerial_image.py:_pupil_geometry/_pupil_phase (:86-166) and
+ * expose/pupil.py:vector_coefficients (:292-369), evaluated in FP64 with the
+ * reference's exact aperture test rho <= 1, stored as complex float. */
+int litho_abbe_pupil_table(const LithoAbbePlan* plan, const void* plan_blob_dev,
+                           void* table_dev, cudaStream_t stream);
+
+/* litho_abbe() with a table built by litho_abbe_pupil_table() for this plan. */
+int litho_abbe_tabled(const LithoAbbePlan* plan, const void* plan_blob_dev,
+                      const void* table_dev, const void* mask_dev, float* image_dev,
+                      float* peak_dev, void* workspace_dev, size_t workspace_bytes,
+                      cudaStream_t stream);
+
 /* The raw Abbe sum, normalised per output, for a batch of clips.
  * Replaces expose/aerial_image.py:_abbe_sum (:351-494) together with
  * compute_aerial_image (:502-548) and compute_aerial_planes (:551-587):
@@ -136,6 +162,29 @@ int litho_abbe_workspace(const LithoAbbePlan* plan, size_t* bytes);
 int litho_abbe(const LithoAbbePlan* plan, const void* plan_blob_dev,
                const void* mask_dev, float* image_dev, float* peak_dev,
                void* workspace_dev, size_t workspace_bytes, cudaStream_t stream);
+
+/* litho_abbe() run `reps` times with CUDA events between its stages, for
+ * measurement. stage_ms[0..6] receives the mean milliseconds of: pupil
+ * table, mask band rows, mask band columns, coarse accumulation, coarse
+ * reduction, synthesis, normalisation. Synchronises the stream. */
+int litho_abbe_profile(const LithoAbbePlan* plan, const void* plan_blob_dev,
+                       const void* table_dev /* NULL: built each run */, const void* mask_dev, float* image_dev, float* peak_dev,
+                       void* workspace_dev, size_t workspace_bytes, cudaStream_t stream,
+                       int reps, float* stage_ms);
+
+/* Workspace bytes litho_abbe_plain() needs when it transforms `batch`
+ * coherent systems (times their field components) at a time. */
+int litho_abbe_plain_workspace(const LithoAbbePlan* plan, int batch, size_t* bytes);
+
+/* The same images as litho_abbe(), by the plain per-source-point method:
+ * every coherent system gets a full N x N spectrum in HBM, a row and a
+ * column inverse FFT and a separate |E|^2 accumulate — the reference's
+ * _abbe_sum loop and batched flush (expose/aerial_image.py:421-488, :336-348)
+ * moved to the GPU unchanged. Power-of-two N in [16, 4096]. The comparison
+ * baseline for the band-limited engine. */
+int litho_abbe_plain(const LithoAbbePlan* plan, int batch, const void* plan_blob_dev,
+                     const void* mask_dev, float* image_dev, float* peak_dev,
+                     void* workspace_dev, size_t workspace_bytes, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

@@ -39,27 +39,27 @@ PUPIL_DTYPE = np.dtype([
 JOB_DTYPE = np.dtype([
     ("fsx", "<f8"), ("fsy", "<f8"), ("jx", "<f8"), ("jy", "<f8"), ("weight", "<f8"),
     ("pupil", "<i4"), ("clip", "<i4"), ("out", "<i4"), ("cx", "<i4"), ("cy", "<i4"),
-    ("ncomp", "<i4"),
+    ("ncomp", "<i4"), ("tab", "<i4"),
 ], align=True)
 
 ITEM_DTYPE = np.dtype([("out", "<i4"), ("job_begin", "<i4"), ("job_end", "<i4"), ("pad", "<i4")])
 NORM_DTYPE = np.dtype([("mode", "<i4"), ("scale", "<f4")])
 
-assert PUPIL_DTYPE.itemsize == 216 and JOB_DTYPE.itemsize == 64
+assert PUPIL_DTYPE.itemsize == 216 and JOB_DTYPE.itemsize == 72
 
 
 class AbbePlan(C.Structure):
     _fields_ = [
         ("n", C.c_int32), ("n_clips", C.c_int32), ("n_out", C.c_int32), ("n_jobs", C.c_int32),
         ("n_items", C.c_int32), ("n_pupils", C.c_int32), ("h", C.c_int32), ("bm", C.c_int32),
-        ("L", C.c_int32), ("mask_complex", C.c_int32), ("ncomp_max", C.c_int32), ("flags", C.c_int32),
+        ("L", C.c_int32), ("mask_complex", C.c_int32), ("ncomp_max", C.c_int32), ("n_tab", C.c_int32),
         ("pixel_size", C.c_double),
         ("off_jobs", C.c_int64), ("off_pupils", C.c_int64), ("off_items", C.c_int64),
-        ("off_out_items", C.c_int64), ("off_norm", C.c_int64),
+        ("off_out_items", C.c_int64), ("off_norm", C.c_int64), ("off_slots", C.c_int64),
     ]
 
 
-assert C.sizeof(AbbePlan) == 96
+assert C.sizeof(AbbePlan) == 104
 
 _lib = None
 
@@ -80,7 +80,20 @@ def lib():
     L.litho_abbe_workspace.argtypes = [C.POINTER(AbbePlan), C.POINTER(C.c_size_t)]
     L.litho_abbe.argtypes = [C.POINTER(AbbePlan), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                              C.c_void_p, C.c_size_t, C.c_void_p]
-    for fn in ("litho_abbe_workspace", "litho_abbe"):
+    L.litho_abbe_plain_workspace.argtypes = [C.POINTER(AbbePlan), C.c_int, C.POINTER(C.c_size_t)]
+    L.litho_abbe_plain.argtypes = [C.POINTER(AbbePlan), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
+    L.litho_abbe_profile.argtypes = [C.POINTER(AbbePlan), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_int,
+                                     C.POINTER(C.c_float)]
+    L.litho_abbe_table_bytes.argtypes = [C.POINTER(AbbePlan), C.POINTER(C.c_size_t)]
+    L.litho_abbe_pupil_table.argtypes = [C.POINTER(AbbePlan), C.c_void_p, C.c_void_p, C.c_void_p]
+    L.litho_abbe_tabled.argtypes = [C.POINTER(AbbePlan), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
+    L.litho_abbe_status.argtypes = [C.POINTER(AbbePlan), C.c_void_p, C.c_void_p]
+    for fn in ("litho_abbe_workspace", "litho_abbe", "litho_abbe_plain_workspace", "litho_abbe_plain",
+               "litho_abbe_profile", "litho_abbe_table_bytes", "litho_abbe_pupil_table",
+               "litho_abbe_tabled", "litho_abbe_status"):
         getattr(L, fn).restype = C.c_int
     _lib = L
     return L

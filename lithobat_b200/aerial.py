@@ -74,37 +74,62 @@ def _validate_view(v) -> None:
             "thick-mask spectra are outside the accelerated path")
 
 
+_PLANS: dict = {}
+
+
 def plan_abbe(views: Sequence, n: int, pixel_size: float, planes: Sequence[Sequence[tuple]],
               dose: float, return_raw: bool, mask_complex: bool, items_per_job_group: int = 4) -> AbbePlanData:
-    """Build the device descriptors of one batched Abbe sum.
+    """Build (or fetch from a small cache) the device descriptors of one
+    batched Abbe sum. views[c] is the optics of clip c, planes[c] its list of
+    (defocus, n_image); every clip has the same number of planes."""
+    key = (tuple(repr(v) for v in views), n, pixel_size, tuple(tuple(map(tuple, p)) for p in planes),
+           float(dose), bool(return_raw), bool(mask_complex), items_per_job_group)
+    hit = _PLANS.get(key)
+    if hit is not None:
+        return hit
+    pd = _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, items_per_job_group)
+    if len(_PLANS) > 32:
+        _PLANS.clear()
+    _PLANS[key] = pd
+    return pd
 
-    views[c] is the optics of clip c, planes[c] its list of (defocus, n_image).
-    Every clip must have the same number of planes.
-    """
+
+def _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, items_per_job_group):
     C = len(views)
     P = len(planes[0])
     if any(len(p) != P for p in planes):
         raise ValueError("every clip needs the same number of planes")
     val = 1.0 / (n * pixel_size)
     pupils = np.zeros(C * P, dtype=nat.PUPIL_DTYPE)
-    job_rows = []
     clears = np.zeros(C * P, dtype=np.float64)
     h = 0
     vec_any = False
+    cols = {k: [] for k in nat.JOB_DTYPE.names}
+    slot_of_state: dict = {}     # (optics, plane) -> first slot of its (source, state) run
+    slot_reps: list[np.ndarray] = []
+    n_tab = 0
+    n_jobs = 0
     for c, v in enumerate(views):
         _validate_view(v)
         vector = v.imaging_model.lower() == "vector"
         vec_any |= vector
         exact = v.exact_defocus or vector
         src = source_points(v)
+        S = len(src)
+        if S == 0:
+            raise ValueError("the source has no points")
         _, hc = disc_halfwidth(v.NA, v.wavelength, n, pixel_size)
         h = max(h, hc)
         zern = np.zeros(21)
         for j, coef in v.zernike:
             if 1 <= j <= 21:
                 zern[j - 1] = coef
-        cxs = np.rint(src.fx / val).astype(np.int64)
-        cys = np.rint(src.fy / val).astype(np.int64)
+        # incoherent states of every source point (one for scalar / polarised)
+        st = [jones_states(v.polarisation, float(ph)) for ph in src.phi] if vector else [[(0.0, 0.0, 1.0)]] * S
+        nst = len(st[0])
+        jxy = np.array(st, dtype=np.float64).reshape(S * nst, 3)
+        s_idx = np.repeat(np.arange(S), nst)
+        vkey = repr(v)
         for p, (dz, n_img) in enumerate(planes[c]):
             k = c * P + p
             pupils[k]["wavelength"] = v.wavelength
@@ -117,28 +142,39 @@ def plan_abbe(views: Sequence, n: int, pixel_size: float, planes: Sequence[Seque
             pupils[k]["obliquity"] = int(v.obliquity)
             pupils[k]["has_zernike"] = int(bool(np.any(zern != 0.0)))
             clears[k] = clear_throughput(src, v, float(n_img), vector)
-            for s in range(len(src)):
-                states = jones_states(v.polarisation, float(src.phi[s])) if vector else [(0.0, 0.0, 1.0)]
-                for jx, jy, wp in states:
-                    job_rows.append((src.fx[s], src.fy[s], jx, jy, src.weight[s] * wp, k, c, k,
-                                     cxs[s], cys[s], 3 if vector else 1))
-    if not job_rows:
-        raise ValueError("the source has no points")
-    jobs = np.zeros(len(job_rows), dtype=nat.JOB_DTYPE)
-    arr = np.array(job_rows, dtype=object)
-    for i, name in enumerate(nat.JOB_DTYPE.names):
-        jobs[name] = arr[:, i].astype(nat.JOB_DTYPE[name])
-    # jobs are already grouped by output (k); chunk each output's run
+            m = S * nst
+            skey = (vkey, float(dz), float(n_img))
+            base = slot_of_state.get(skey)
+            if base is None:
+                base = n_tab
+                slot_of_state[skey] = base
+                slot_reps.append(n_jobs + np.arange(m, dtype=np.int32))
+                n_tab += m
+            cols["fsx"].append(src.fx[s_idx]); cols["fsy"].append(src.fy[s_idx])
+            cols["jx"].append(jxy[:, 0]); cols["jy"].append(jxy[:, 1])
+            cols["weight"].append(src.weight[s_idx] * jxy[:, 2])
+            cols["pupil"].append(np.full(m, k)); cols["clip"].append(np.full(m, c))
+            cols["out"].append(np.full(m, k))
+            cols["cx"].append(np.rint(src.fx / val).astype(np.int64)[s_idx])
+            cols["cy"].append(np.rint(src.fy / val).astype(np.int64)[s_idx])
+            cols["ncomp"].append(np.full(m, 3 if vector else 1))
+            cols["tab"].append(base + np.arange(m))
+            n_jobs += m
+    jobs = np.zeros(n_jobs, dtype=nat.JOB_DTYPE)
+    for name in nat.JOB_DTYPE.names:
+        jobs[name] = np.concatenate(cols[name]).astype(nat.JOB_DTYPE[name])
+    slots = np.concatenate(slot_reps).astype(np.int32)
+    # jobs are grouped by output (k); chunk each output's run into work items
     n_out = C * P
-    items, out_items = [], [0]
     per = max(1, int(items_per_job_group))
     starts = np.searchsorted(jobs["out"], np.arange(n_out + 1), side="left")
+    item_rows, out_items = [], [0]
     for o in range(n_out):
-        b, e = int(starts[o]), int(starts[o + 1])
-        for j in range(b, e, per):
-            items.append((o, j, min(j + per, e), 0))
-        out_items.append(len(items))
-    items = np.array(items, dtype=np.int32).view(nat.ITEM_DTYPE).reshape(-1)
+        b0, e0 = int(starts[o]), int(starts[o + 1])
+        for j in range(b0, e0, per):
+            item_rows.append((o, j, min(j + per, e0), 0))
+        out_items.append(len(item_rows))
+    items = np.array(item_rows, dtype=np.int32).view(nat.ITEM_DTYPE).reshape(-1)
     out_items = np.array(out_items, dtype=np.int32)
     norm = np.zeros(n_out, dtype=nat.NORM_DTYPE)
     for c, v in enumerate(views):
@@ -146,24 +182,22 @@ def plan_abbe(views: Sequence, n: int, pixel_size: float, planes: Sequence[Seque
             k = c * P + p
             if return_raw:
                 norm[k] = (0, 1.0)
+            elif v.normalisation.lower() == "peak":
+                norm[k] = (1, dose)
             else:
-                m = v.normalisation.lower()
-                if m == "peak":
-                    norm[k] = (1, dose)
-                else:
-                    norm[k] = (0, normalisation_scale(m, 1.0, clears[k], dose))
+                norm[k] = (0, normalisation_scale(v.normalisation, 1.0, clears[k], dose))
     bm = int(max(np.abs(jobs["cx"]).max(), np.abs(jobs["cy"]).max())) + h
-    blob, offs = nat.blob([jobs, pupils, items, out_items, norm])
+    blob, offs = nat.blob([jobs, pupils, items, out_items, norm, slots])
+    L = 32
+    while L < 4 * h + 1:
+        L *= 2
     plan = nat.AbbePlan(
-        n=n, n_clips=C, n_out=n_out, n_jobs=len(jobs), n_items=len(items), n_pupils=len(pupils),
-        h=h, bm=bm, L=32, mask_complex=int(mask_complex), ncomp_max=3 if vec_any else 1, flags=0,
+        n=n, n_clips=C, n_out=n_out, n_jobs=n_jobs, n_items=len(items), n_pupils=len(pupils),
+        h=h, bm=bm, L=L, mask_complex=int(mask_complex), ncomp_max=3 if vec_any else 1, n_tab=n_tab,
         pixel_size=pixel_size, off_jobs=offs[0], off_pupils=offs[1], off_items=offs[2],
-        off_out_items=offs[3], off_norm=offs[4])
-    if 4 * h + 1 > 32:
-        raise NotImplementedError(
-            f"pupil radius {h} bins needs a coarse grid above 32; this build serves 4h+1 <= 32")
+        off_out_items=offs[3], off_norm=offs[4], off_slots=offs[5])
     transforms = int(np.sum(jobs["ncomp"]))
-    return AbbePlanData(plan, blob, clears, n_out, len(jobs), transforms)
+    return AbbePlanData(plan, blob, clears, n_out, n_jobs, transforms)
 
 
 # ---------------------------------------------------------------------------
@@ -201,36 +235,106 @@ def _as_device_masks(torch, masks, n: int):
     return t.contiguous()
 
 
-def run_abbe(pd: AbbePlanData, masks_dev, out=None, peak=None, stream=None):
-    """Launch one planned Abbe batch; returns (images (n_out, N, N), peaks (n_out,))."""
+ENGINES = ("fused", "plain")
+
+
+def pupil_table(pd: AbbePlanData, dev, stream: int):
+    """The plan's pupil table on `dev`, built once (it depends on the optics
+    and source only) and kept with the plan."""
+    torch = nat.require_cuda()
+    t = getattr(pd, "_table_dev", None)
+    if t is not None and t.device == dev:
+        return t
+    import ctypes as C
+    L = nat.lib()
+    nb = C.c_size_t(0)
+    nat.check("litho_abbe_table_bytes", L.litho_abbe_table_bytes(C.byref(pd.plan), C.byref(nb)))
+    t = torch.empty(max(nb.value, 16), dtype=torch.uint8, device=dev)
+    blob = getattr(pd, "_blob_dev", None)
+    if blob is None or blob.device != dev:
+        blob = torch.from_numpy(pd.blob).to(dev)
+        pd._blob_dev = blob
+    nat.check("litho_abbe_pupil_table", L.litho_abbe_pupil_table(C.byref(pd.plan), blob.data_ptr(),
+                                                                  t.data_ptr(), stream))
+    pd._table_dev = t
+    return t
+
+
+def plain_batch_size(pd: AbbePlanData, budget_bytes: int = 2 << 30) -> int:
+    """Coherent systems the plain engine transforms per batch (HBM budget)."""
+    per = pd.plan.ncomp_max * pd.plan.n * pd.plan.n * 8
+    return int(max(1, min(pd.jobs, budget_bytes // per)))
+
+
+def run_abbe(pd: AbbePlanData, masks_dev, out=None, peak=None, stream=None, engine: str = "fused"):
+    """Launch one planned Abbe batch; returns (images (n_out, N, N), peaks (n_out,)).
+
+    engine "fused" is the band-limited on-chip engine; "plain" transforms every
+    coherent system on the full N x N grid (the comparison baseline)."""
     torch = nat.require_cuda()
     L = nat.lib()
     dev = masks_dev.device
     n = pd.plan.n
+    if engine not in ENGINES:
+        raise ValueError(f"engine must be one of {ENGINES}, got {engine!r}")
     if out is None:
         out = torch.empty((pd.n_out, n, n), dtype=torch.float32, device=dev)
     if peak is None:
         peak = torch.empty((pd.n_out,), dtype=torch.float32, device=dev)
     import ctypes as C
     ws_bytes = C.c_size_t(0)
-    nat.check("litho_abbe_workspace", L.litho_abbe_workspace(C.byref(pd.plan), C.byref(ws_bytes)))
-    ws = nat.Workspace.get(torch, dev, ws_bytes.value)
+    if engine == "fused":
+        nat.check("litho_abbe_workspace", L.litho_abbe_workspace(C.byref(pd.plan), C.byref(ws_bytes)))
+    else:
+        batch = plain_batch_size(pd)
+        nat.check("litho_abbe_plain_workspace",
+                  L.litho_abbe_plain_workspace(C.byref(pd.plan), batch, C.byref(ws_bytes)))
+    ws = nat.Workspace.get(torch, dev, ws_bytes.value, tag=engine)
     blob = getattr(pd, "_blob_dev", None)
     if blob is None or blob.device != dev:
         blob = torch.from_numpy(pd.blob).to(dev)
         pd._blob_dev = blob
     s = stream if stream is not None else nat.stream_ptr(torch, dev)
-    nat.check("litho_abbe", L.litho_abbe(C.byref(pd.plan), blob.data_ptr(), masks_dev.data_ptr(),
-                                          out.data_ptr(), peak.data_ptr(), ws.data_ptr(),
-                                          ws.numel(), s))
+    if engine == "fused":
+        table = pupil_table(pd, dev, s)
+        nat.check("litho_abbe_tabled", L.litho_abbe_tabled(C.byref(pd.plan), blob.data_ptr(), table.data_ptr(),
+                                                            masks_dev.data_ptr(), out.data_ptr(), peak.data_ptr(),
+                                                            ws.data_ptr(), ws.numel(), s))
+    else:
+        nat.check("litho_abbe_plain", L.litho_abbe_plain(C.byref(pd.plan), batch, blob.data_ptr(),
+                                                          masks_dev.data_ptr(), out.data_ptr(),
+                                                          peak.data_ptr(), ws.data_ptr(), ws.numel(), s))
     return out, peak
+
+
+STAGES = ("pupil_table", "band_rows", "band_cols", "coarse", "coarse_reduce", "synthesis", "normalise")
+
+
+def profile_abbe(pd: AbbePlanData, masks_dev, reps: int = 10, rebuild_table: bool = False) -> dict:
+    """Mean device milliseconds of each pipeline stage over `reps` runs
+    (stage "pupil_table" is ~0 unless rebuild_table)."""
+    torch = nat.require_cuda()
+    import ctypes as C
+    L = nat.lib()
+    dev = masks_dev.device
+    out = torch.empty((pd.n_out, pd.plan.n, pd.plan.n), dtype=torch.float32, device=dev)
+    peak = torch.empty((pd.n_out,), dtype=torch.float32, device=dev)
+    run_abbe(pd, masks_dev, out, peak)
+    ws = nat.Workspace.get(torch, dev, 0, tag="fused")
+    ms = (C.c_float * 8)()
+    table = None if rebuild_table else pupil_table(pd, dev, nat.stream_ptr(torch, dev)).data_ptr()
+    nat.check("litho_abbe_profile", L.litho_abbe_profile(
+        C.byref(pd.plan), pd._blob_dev.data_ptr(), table, masks_dev.data_ptr(), out.data_ptr(),
+        peak.data_ptr(), ws.data_ptr(), ws.numel(), nat.stream_ptr(torch, dev), int(reps), ms))
+    return {name: float(ms[i]) for i, name in enumerate(STAGES)}
 
 
 def _grid(grid):
     return int(grid.n_pixels), float(grid.pixel_size)
 
 
-def compute_aerial_batch(masks, optics, grid, planes=None, dose: float = 1.0, return_raw: bool = False):
+def compute_aerial_batch(masks, optics, grid, planes=None, dose: float = 1.0, return_raw: bool = False,
+                         engine: str = "fused"):
     """Abbe images of a batch of clips on the GPU.
 
     masks: (C, N, N) numpy array or torch tensor (real or complex).
@@ -256,7 +360,7 @@ def compute_aerial_batch(masks, optics, grid, planes=None, dose: float = 1.0, re
     else:
         pl = [list(planes)] * Cn
     pd = plan_abbe(views, n, px, pl, dose, return_raw, md.is_complex())
-    img, pk = run_abbe(pd, md)
+    img, pk = run_abbe(pd, md, engine=engine)
     P = len(pl[0])
     return img.view(Cn, P, n, n), pk.view(Cn, P), pd.clears.reshape(Cn, P)
 

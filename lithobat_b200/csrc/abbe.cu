@@ -30,22 +30,23 @@ namespace litho {
 
 cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_per_clip, int n,
                                 int bm, float2* out, float scale, const float2* tw_inv,
-                                int num_sms, cudaStream_t st);
+                                int num_sms, cudaStream_t st, int* status);
 
 // ---------------------------------------------------------------------------
-// 1. pupil table: table[job][comp][(dy+h)(2h+1) + dx+h]
+// 1. pupil table: table[slot][comp][(dy+h)(2h+1) + dx+h], one block per slot,
+//    evaluated for the slot's representative job.
 // ---------------------------------------------------------------------------
-__global__ void k_pupil_table(const LithoJob* __restrict__ jobs, const LithoPupil* __restrict__ pupils,
-                              int n_jobs, int n, double pixel_size, int h, int ncomp_max,
-                              float2* __restrict__ table) {
-  const int j = blockIdx.x;
-  if (j >= n_jobs) return;
-  const LithoJob job = jobs[j];
+__global__ void k_pupil_table(const LithoJob* __restrict__ jobs, const int32_t* __restrict__ slots,
+                              const LithoPupil* __restrict__ pupils, int n_tab, int n, double pixel_size, int h,
+                              int ncomp_max, float2* __restrict__ table) {
+  const int t = blockIdx.x;
+  if (t >= n_tab) return;
+  const LithoJob job = jobs[slots[t]];
   const LithoPupil P = pupils[job.pupil];
   const int side = 2 * h + 1, npts = side * side;
   const double val = ddiv(1.0, dmul((double)n, pixel_size));
   const double kmax = ddiv(P.NA, P.wavelength);
-  float2* out = table + (size_t)j * ncomp_max * npts;
+  float2* out = table + (size_t)t * ncomp_max * npts;
   for (int p = threadIdx.x; p < npts; p += blockDim.x) {
     const int dy = p / side - h, dx = p % side - h;
     const int kx = job.cx + dx, ky = job.cy + dy;
@@ -89,7 +90,7 @@ k_coarse32(const LithoItem* __restrict__ items, const LithoJob* __restrict__ job
     const float2* m = Mb + (size_t)job.clip * Bm * Bm;
     const int mx = job.cx + dx + bm;
     for (int c = 0; c < job.ncomp; ++c) {
-      const float2* tp = table + ((size_t)j * ncomp_max + c) * npts;
+      const float2* tp = table + ((size_t)job.tab * ncomp_max + c) * npts;
       float2 v[32];
 #pragma unroll
       for (int i = 0; i < 32; ++i) v[i] = make_float2(0.f, 0.f);
@@ -137,101 +138,129 @@ k_coarse32(const LithoItem* __restrict__ items, const LithoJob* __restrict__ job
 // ---------------------------------------------------------------------------
 // 4. per output: J = sum of its items' partials (in item order), then
 //    B(gx, gy) = (1/L^2) sum_{u,v} J(v, u) exp(-2 pi i (gx u + gy v) / L).
+//    One block of 1024 threads per output; L is a power of two.
 // ---------------------------------------------------------------------------
-__global__ void k_coarse_reduce(const int32_t* __restrict__ out_items, const float* __restrict__ partial,
-                                int L, int h, float2* __restrict__ Bout) {
+__global__ void __launch_bounds__(1024)
+k_coarse_reduce(const int32_t* __restrict__ out_items, const float* __restrict__ partial, int L, int h,
+                float2* __restrict__ Bout) {
   extern __shared__ float sm_f[];
   const int o = blockIdx.x;
-  const int LL = L * L, G = 4 * h + 1, g0 = 2 * h;
+  const int LL = L * L, G = 4 * h + 1, g0 = 2 * h, msk = L - 1;
   float* J = sm_f;                                         // [v][u]
   float2* R = reinterpret_cast<float2*>(sm_f + LL);        // [u][gy]
   float2* tw = R + (size_t)L * G;                          // exp(-2 pi i t / L)
   for (int t = threadIdx.x; t < L; t += blockDim.x) {
-    double s, c;
-    sincospi(2.0 * t / (double)L, &s, &c);
-    tw[t] = make_float2((float)c, (float)-s);
+    double sn, cs;
+    sincospi(2.0 * t / (double)L, &sn, &cs);
+    tw[t] = make_float2((float)cs, (float)-sn);
   }
   const int i0 = out_items[o], i1 = out_items[o + 1];
   for (int idx = threadIdx.x; idx < LL; idx += blockDim.x) {
-    float s = 0.f;
-    for (int i = i0; i < i1; ++i) s += partial[(size_t)i * LL + idx];
-    J[idx] = s;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+    int i = i0;
+    for (; i + 3 < i1; i += 4) {
+      s0 += partial[(size_t)i * LL + idx];
+      s1 += partial[(size_t)(i + 1) * LL + idx];
+      s2 += partial[(size_t)(i + 2) * LL + idx];
+      s3 += partial[(size_t)(i + 3) * LL + idx];
+    }
+    for (; i < i1; ++i) s0 += partial[(size_t)i * LL + idx];
+    J[idx] = (s0 + s1) + (s2 + s3);
   }
   __syncthreads();
   for (int id = threadIdx.x; id < L * G; id += blockDim.x) {
     const int u = id / G, gy = id % G - g0;
-    float2 s = make_float2(0.f, 0.f);
-    for (int v = 0; v < L; ++v) {
-      const int t = ((gy * v) % L + L) % L;
-      s = cadd(s, cscale(tw[t], J[v * L + u]));
-    }
-    R[u * G + (gy + g0)] = s;
+    float2 acc = make_float2(0.f, 0.f);
+    for (int v = 0; v < L; ++v) acc = cadd(acc, cscale(tw[(gy * v) & msk], J[v * L + u]));
+    R[u * G + (gy + g0)] = acc;
   }
   __syncthreads();
   const float inv = 1.0f / (float)LL;
   float2* B = Bout + (size_t)o * G * G;
   for (int id = threadIdx.x; id < G * G; id += blockDim.x) {
     const int gyi = id / G, gx = id % G - g0;
-    float2 s = make_float2(0.f, 0.f);
-    for (int u = 0; u < L; ++u) {
-      const int t = ((gx * u) % L + L) % L;
-      s = cadd(s, cmul(R[u * G + gyi], tw[t]));
-    }
-    B[gyi * G + (gx + g0)] = cscale(s, inv);
+    float2 acc = make_float2(0.f, 0.f);
+    for (int u = 0; u < L; ++u) acc = cadd(acc, cmul(R[u * G + gyi], tw[(gx * u) & msk]));
+    B[gyi * G + (gx + g0)] = cscale(acc, inv);
   }
 }
 
 // ---------------------------------------------------------------------------
 // 5. synthesis: I(x, y) = Re C(y, 0) + 2 sum_{gx >= 1} Re[C(y, gx) w^(gx x)],
 //    C(y, gx) = sum_gy B(gx, gy) w^(gy y), w = exp(2 pi i / N).
+//    A block writes kSynthRows full rows; a thread owns kSynthCols columns
+//    and reuses each twiddle for all the block's rows.
 // ---------------------------------------------------------------------------
-constexpr int kSynthRows = 4;
+constexpr int kSynthRows = 8;
+constexpr int kSynthCols = 4;
+constexpr int kSynthThreads = 256;
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kSynthThreads, 3)
 k_synth(const float2* __restrict__ Bbox, int G, int n, const float2* __restrict__ tw_inv,
         const LithoNorm* __restrict__ norm, float* __restrict__ image, float* __restrict__ blockmax) {
   extern __shared__ float2 sm2[];
+  const int gh = G / 2, gp = gh + 1;
   float2* tw = sm2;                       // n entries
-  float2* C = sm2 + n;                    // [kSynthRows][gh + 1]
-  __shared__ float red[256 / 32];
+  float2* C = sm2 + n;                    // [kSynthRows][gp]
+  float2* B = C + kSynthRows * gp;        // [G][G]
+  __shared__ float red[kSynthThreads / 32];
   const int o = blockIdx.y, y0 = blockIdx.x * kSynthRows;
-  const int gh = G / 2;
   const bool pow2 = (n & (n - 1)) == 0;
   for (int j = threadIdx.x; j < n; j += blockDim.x) tw[j] = tw_inv[j];
+  for (int j = threadIdx.x; j < G * G; j += blockDim.x) B[j] = Bbox[(size_t)o * G * G + j];
   __syncthreads();
-  const float2* B = Bbox + (size_t)o * G * G;
-  for (int id = threadIdx.x; id < kSynthRows * (gh + 1); id += blockDim.x) {
-    const int r = id / (gh + 1), gx = id % (gh + 1), y = y0 + r;
-    float2 s = make_float2(0.f, 0.f);
+  for (int id = threadIdx.x; id < kSynthRows * gp; id += blockDim.x) {
+    const int r = id / gp, gx = id % gp, y = y0 + r;
+    float2 acc = make_float2(0.f, 0.f);
     if (y < n) {
       for (int gy = -gh; gy <= gh; ++gy) {
-        long long e = (long long)gy * y;
-        int t = (int)(pow2 ? (e & (n - 1)) : (((e % n) + n) % n));
-        s = cadd(s, cmul(B[(gy + gh) * G + (gx + gh)], tw[t]));
+        const int e = gy * y;
+        const int t = pow2 ? (e & (n - 1)) : ((e % n) + n) % n;
+        acc = cadd(acc, cmul(B[(gy + gh) * G + (gx + gh)], tw[t]));
       }
     }
-    C[r * (gh + 1) + gx] = s;
+    C[r * gp + gx] = acc;
   }
   __syncthreads();
   const LithoNorm nm = norm[o];
   const float sc = nm.mode == 0 ? nm.scale : 1.0f;
+  const int rows = (n - y0) < kSynthRows ? (n - y0) : kSynthRows;
   float mx = 0.f;
-  for (int r = 0; r < kSynthRows; ++r) {
-    const int y = y0 + r;
-    if (y >= n) break;
-    const float2* Cr = C + r * (gh + 1);
-    float* dst = image + ((size_t)o * n + y) * n;
-    for (int x = threadIdx.x; x < n; x += blockDim.x) {
-      float acc = 0.f;
-      for (int gx = 1; gx <= gh; ++gx) {
-        long long e = (long long)gx * x;
-        int t = (int)(pow2 ? (e & (n - 1)) : (e % n));
-        const float2 c = Cr[gx], wv = tw[t];
-        acc = fmaf(c.x, wv.x, fmaf(-c.y, wv.y, acc));
+  for (int xb = threadIdx.x; xb < n; xb += kSynthThreads * kSynthCols) {
+    float acc[kSynthRows][kSynthCols];
+#pragma unroll
+    for (int r = 0; r < kSynthRows; ++r)
+#pragma unroll
+      for (int j = 0; j < kSynthCols; ++j) acc[r][j] = 0.f;
+    for (int gx = 1; gx <= gh; ++gx) {
+      float2 w[kSynthCols];
+#pragma unroll
+      for (int j = 0; j < kSynthCols; ++j) {
+        const int x = xb + j * kSynthThreads;
+        const int e = gx * x;
+        w[j] = x < n ? tw[pow2 ? (e & (n - 1)) : (e % n)] : make_float2(0.f, 0.f);
       }
-      const float val = fmaf(2.f, acc, Cr[0].x);
-      mx = fmaxf(mx, val);
-      dst[x] = val * sc;
+#pragma unroll
+      for (int r = 0; r < kSynthRows; ++r) {
+        const float2 c = C[r * gp + gx];
+#pragma unroll
+        for (int j = 0; j < kSynthCols; ++j) acc[r][j] = fmaf(c.x, w[j].x, fmaf(-c.y, w[j].y, acc[r][j]));
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < kSynthRows; ++r) {
+      if (r >= rows) break;
+      const float c0 = C[r * gp].x;
+      float* dst = image + ((size_t)o * n + y0 + r) * n;
+#pragma unroll
+      for (int j = 0; j < kSynthCols; ++j) {
+        const int x = xb + j * kSynthThreads;
+        if (x < n) {
+          const float val = fmaf(2.f, acc[r][j], c0);
+          mx = fmaxf(mx, val);
+          dst[x] = val * sc;
+        }
+      }
     }
   }
   // block max of the raw intensity
@@ -241,7 +270,7 @@ k_synth(const float2* __restrict__ Bbox, int G, int n, const float2* __restrict_
   __syncthreads();
   if (threadIdx.x == 0) {
     float m = red[0];
-    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) m = fmaxf(m, red[i]);
+    for (int i = 1; i < kSynthThreads / 32; ++i) m = fmaxf(m, red[i]);
     blockmax[(size_t)o * gridDim.x + blockIdx.x] = m;
   }
 }
@@ -250,43 +279,72 @@ k_synth(const float2* __restrict__ Bbox, int G, int n, const float2* __restrict_
 // 6. peak and peak normalisation
 // ---------------------------------------------------------------------------
 __global__ void k_normalise(const float* __restrict__ blockmax, int nblk, const LithoNorm* __restrict__ norm,
-                            int n, float* __restrict__ image, float* __restrict__ peak) {
+                            int n, float* __restrict__ image, float* __restrict__ peak, int apply_mode0) {
   __shared__ float s_peak;
   const int o = blockIdx.y;
-  if (threadIdx.x == 0) {
-    float m = blockmax[(size_t)o * nblk];
-    for (int i = 1; i < nblk; ++i) m = fmaxf(m, blockmax[(size_t)o * nblk + i]);
-    s_peak = m;
-    if (blockIdx.x == 0) peak[o] = m;
+  if (threadIdx.x < 32) {
+    float m = 0.f;
+    for (int i = threadIdx.x; i < nblk; i += 32) m = fmaxf(m, blockmax[(size_t)o * nblk + i]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if (threadIdx.x == 0) {
+      s_peak = m;
+      if (blockIdx.x == 0) peak[o] = m;
+    }
   }
   __syncthreads();
   const LithoNorm nm = norm[o];
-  if (nm.mode != 1) return;
-  const float pk = s_peak;
-  const float sc = pk > 0.f ? nm.scale / pk : nm.scale;
+  float sc;
+  if (nm.mode == 1) {
+    const float pk = s_peak;
+    sc = pk > 0.f ? nm.scale / pk : nm.scale;
+  } else {
+    if (!apply_mode0 || nm.scale == 1.0f) return;  // already applied by the producer
+    sc = nm.scale;
+  }
   const size_t NN = (size_t)n * n;
   float* img = image + (size_t)o * NN;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < NN; i += (size_t)gridDim.x * blockDim.x)
-    img[i] *= sc;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  if ((NN & 3) == 0 && (((uintptr_t)img) & 15) == 0) {
+    float4* v4 = reinterpret_cast<float4*>(img);
+    const size_t n4 = NN >> 2;
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + stride < n4; i += 2 * stride) {
+      float4 a = v4[i], b = v4[i + stride];
+      a.x *= sc; a.y *= sc; a.z *= sc; a.w *= sc;
+      b.x *= sc; b.y *= sc; b.z *= sc; b.w *= sc;
+      v4[i] = a;
+      v4[i + stride] = b;
+    }
+    for (; i < n4; i += stride) {
+      float4 a = v4[i];
+      a.x *= sc; a.y *= sc; a.z *= sc; a.w *= sc;
+      v4[i] = a;
+    }
+  } else {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < NN; i += stride) img[i] *= sc;
+  }
 }
 
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+static int synth_blocks(int n) { return (n + kSynthRows - 1) / kSynthRows; }
+
 struct AbbeLayout {
-  int64_t tw, u1, mb, table, partial, bbox, blockmax, total;
+  int64_t status, tw, u1, mb, table, partial, bbox, blockmax, total;
 };
 
-static int synth_blocks(int n) { return (n + kSynthRows - 1) / kSynthRows; }
 
 static AbbeLayout abbe_layout(const LithoAbbePlan& p) {
   AbbeLayout l{};
   const int64_t Bm = 2 * p.bm + 1, side = 2 * p.h + 1, G = 4 * p.h + 1;
   int64_t off = 0;
+  l.status = off;   off = align16(off + 16);
   l.tw = off;       off = align16(off + (int64_t)p.n * 8);
   l.u1 = off;       off = align16(off + (int64_t)p.n_clips * Bm * p.n * 8);
   l.mb = off;       off = align16(off + (int64_t)p.n_clips * Bm * Bm * 8);
-  l.table = off;    off = align16(off + (int64_t)p.n_jobs * p.ncomp_max * side * side * 8);
+  l.table = off;    off = align16(off + (int64_t)p.n_tab * p.ncomp_max * side * side * 8);
   l.partial = off;  off = align16(off + (int64_t)p.n_items * p.L * p.L * 4);
   l.bbox = off;     off = align16(off + (int64_t)p.n_out * G * G * 8);
   l.blockmax = off; off = align16(off + (int64_t)p.n_out * synth_blocks(p.n) * 4);
@@ -297,15 +355,16 @@ static AbbeLayout abbe_layout(const LithoAbbePlan& p) {
 static int check_plan(const LithoAbbePlan* p) {
   if (!p) return LITHO_E_NULL;
   if (p->n < 2 || p->n > 8192 || p->n_clips < 1 || p->n_out < 1 || p->n_jobs < 0 || p->n_items < 0 ||
-      p->n_pupils < 1 || p->h < 0 || p->bm < 0)
+      p->n_pupils < 1 || p->h < 0 || p->bm < 0 || p->n_tab < 1 || p->n_tab > p->n_jobs)
     return LITHO_E_SIZE;
   if (p->ncomp_max != 1 && p->ncomp_max != 3) return LITHO_E_SIZE;
   if (p->L != 32) return LITHO_E_UNSUPPORTED;
   if (4 * p->h + 1 > p->L || p->h > kCoarseHMax32) return LITHO_E_BAND;
   if (p->bm < p->h) return LITHO_E_BAND;
   if (!(p->pixel_size > 0.0)) return LITHO_E_SIZE;
-  const int64_t offs[5] = {p->off_jobs, p->off_pupils, p->off_items, p->off_out_items, p->off_norm};
-  for (int i = 0; i < 5; ++i)
+  const int64_t offs[6] = {p->off_jobs, p->off_pupils, p->off_items, p->off_out_items, p->off_norm,
+                           p->off_slots};
+  for (int i = 0; i < 6; ++i)
     if (offs[i] < 0 || (offs[i] & 15)) return LITHO_E_ALIGN;
   return LITHO_OK;
 }
@@ -333,12 +392,17 @@ extern "C" int litho_abbe_workspace(const LithoAbbePlan* plan, size_t* bytes) {
   return LITHO_OK;
 }
 
-extern "C" int litho_abbe(const LithoAbbePlan* plan, const void* blob, const void* mask, float* image,
-                          float* peak, void* ws, size_t ws_bytes, cudaStream_t s) {
+namespace litho {
+
+// The pipeline, optionally bracketing each stage with events ev[0..7].
+// table == nullptr: the pupil table is built into the workspace first.
+static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* table_in, const void* mask,
+                    float* image, float* peak, void* ws, size_t ws_bytes, cudaStream_t s, cudaEvent_t* ev) {
   int st = check_plan(plan);
   if (st) return st;
   if (!blob || !mask || !image || !peak || !ws) return LITHO_E_NULL;
-  if (((uintptr_t)ws & 15) || ((uintptr_t)blob & 15) || ((uintptr_t)mask & 7)) return LITHO_E_ALIGN;
+  if (((uintptr_t)ws & 15) || ((uintptr_t)blob & 15) || ((uintptr_t)mask & 7) || ((uintptr_t)table_in & 7))
+    return LITHO_E_ALIGN;
   const LithoAbbePlan& p = *plan;
   const AbbeLayout l = abbe_layout(p);
   if ((int64_t)ws_bytes < l.total) return LITHO_E_WORKSPACE;
@@ -350,12 +414,14 @@ extern "C" int litho_abbe(const LithoAbbePlan* plan, const void* blob, const voi
   const LithoItem* items = reinterpret_cast<const LithoItem*>(b + p.off_items);
   const int32_t* out_items = reinterpret_cast<const int32_t*>(b + p.off_out_items);
   const LithoNorm* norm = reinterpret_cast<const LithoNorm*>(b + p.off_norm);
+  const int32_t* slots = reinterpret_cast<const int32_t*>(b + p.off_slots);
 
   char* w = static_cast<char*>(ws);
+  int* status = reinterpret_cast<int*>(w + l.status);
   float2* tw = reinterpret_cast<float2*>(w + l.tw);
   float2* u1 = reinterpret_cast<float2*>(w + l.u1);
   float2* mb = reinterpret_cast<float2*>(w + l.mb);
-  float2* table = reinterpret_cast<float2*>(w + l.table);
+  float2* table = table_in ? (float2*)table_in : reinterpret_cast<float2*>(w + l.table);
   float* partial = reinterpret_cast<float*>(w + l.partial);
   float2* bbox = reinterpret_cast<float2*>(w + l.bbox);
   float* blockmax = reinterpret_cast<float*>(w + l.blockmax);
@@ -363,38 +429,122 @@ extern "C" int litho_abbe(const LithoAbbePlan* plan, const void* blob, const voi
   const int sms = num_sms_cached();
   const int Bm = 2 * p.bm + 1, G = 4 * p.h + 1;
   cudaError_t e;
+  auto mark = [&](int i) { if (ev) cudaEventRecord(ev[i], s); };
 
+  mark(0);
+  if ((e = cudaMemsetAsync(status, 0, sizeof(int), s)) != cudaSuccess) return (int)e;
   k_twiddle_table<<<(p.n + 255) / 256, 256, 0, s>>>(tw, p.n, +1);
-  k_pupil_table<<<p.n_jobs, 128, 0, s>>>(jobs, pupils, p.n_jobs, p.n, p.pixel_size, p.h, p.ncomp_max, table);
+  if (!table_in)
+    k_pupil_table<<<p.n_tab, 128, 0, s>>>(jobs, slots, pupils, p.n_tab, p.n, p.pixel_size, p.h, p.ncomp_max,
+                                           table);
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
-
+  mark(1);
   // mask band spectrum: rows then columns, 1/N^2 folded into the second pass
-  e = launch_row_band_dft(mask, p.mask_complex != 0, p.n_clips * p.n, p.n, p.n, p.bm, u1, 1.0f, tw, sms, s);
+  e = launch_row_band_dft(mask, p.mask_complex != 0, p.n_clips * p.n, p.n, p.n, p.bm, u1, 1.0f, tw, sms, s,
+                          status);
   if (e != cudaSuccess) return (int)e;
+  mark(2);
   e = launch_row_band_dft(u1, true, p.n_clips * Bm, Bm, p.n, p.bm, mb, 1.0f / ((float)p.n * (float)p.n), tw,
-                          sms, s);
+                          sms, s, status);
   if (e != cudaSuccess) return (int)e;
-
+  mark(3);
   const size_t sm_coarse = (size_t)kCoarseWarps * 32 * 33 * sizeof(float2);
   cudaFuncSetAttribute(k_coarse32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_coarse);
   k_coarse32<<<p.n_items, kCoarseWarps * 32, sm_coarse, s>>>(items, jobs, table, p.h, p.ncomp_max, mb, p.bm,
                                                               partial);
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
-
+  mark(4);
   const size_t sm_red = (size_t)p.L * p.L * 4 + (size_t)p.L * G * 8 + (size_t)p.L * 8;
   cudaFuncSetAttribute(k_coarse_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_red);
-  k_coarse_reduce<<<p.n_out, 256, sm_red, s>>>(out_items, partial, p.L, p.h, bbox);
+  k_coarse_reduce<<<p.n_out, 1024, sm_red, s>>>(out_items, partial, p.L, p.h, bbox);
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
-
+  mark(5);
   const int gh = G / 2;
-  const size_t sm_syn = (size_t)p.n * 8 + (size_t)kSynthRows * (gh + 1) * 8;
+  const size_t sm_syn = (size_t)p.n * 8 + (size_t)kSynthRows * (gh + 1) * 8 + (size_t)G * G * 8;
   cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_syn);
   dim3 gs(synth_blocks(p.n), p.n_out);
-  k_synth<<<gs, 256, sm_syn, s>>>(bbox, G, p.n, tw, norm, image, blockmax);
+  k_synth<<<gs, kSynthThreads, sm_syn, s>>>(bbox, G, p.n, tw, norm, image, blockmax);
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
-
+  mark(6);
   dim3 gn((unsigned)((((size_t)p.n * p.n + 255) / 256) < 512 ? (((size_t)p.n * p.n + 255) / 256) : 512), p.n_out);
-  k_normalise<<<gn, 256, 0, s>>>(blockmax, synth_blocks(p.n), norm, p.n, image, peak);
+  k_normalise<<<gn, 256, 0, s>>>(blockmax, synth_blocks(p.n), norm, p.n, image, peak, 0);
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  mark(7);
   return LITHO_OK;
+}
+
+}  // namespace litho
+
+extern "C" int litho_abbe(const LithoAbbePlan* plan, const void* blob, const void* mask, float* image,
+                          float* peak, void* ws, size_t ws_bytes, cudaStream_t s) {
+  return abbe_run(plan, blob, nullptr, mask, image, peak, ws, ws_bytes, s, nullptr);
+}
+
+extern "C" int litho_abbe_tabled(const LithoAbbePlan* plan, const void* blob, const void* table, const void* mask,
+                                 float* image, float* peak, void* ws, size_t ws_bytes, cudaStream_t s) {
+  if (!table) return LITHO_E_NULL;
+  return abbe_run(plan, blob, table, mask, image, peak, ws, ws_bytes, s, nullptr);
+}
+
+extern "C" int litho_abbe_status(const LithoAbbePlan* plan, const void* ws, cudaStream_t s) {
+  const int st = check_plan(plan);
+  if (st) return st;
+  if (!ws) return LITHO_E_NULL;
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, static_cast<const char*>(ws) + abbe_layout(*plan).status, sizeof(int),
+                                  cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return (int)e;
+  return h;
+}
+
+extern "C" int litho_abbe_table_bytes(const LithoAbbePlan* plan, size_t* bytes) {
+  const int st = check_plan(plan);
+  if (st) return st;
+  if (!bytes) return LITHO_E_NULL;
+  const int64_t side = 2 * plan->h + 1;
+  *bytes = (size_t)plan->n_tab * plan->ncomp_max * side * side * 8;
+  return LITHO_OK;
+}
+
+extern "C" int litho_abbe_pupil_table(const LithoAbbePlan* plan, const void* blob, void* table, cudaStream_t s) {
+  const int st = check_plan(plan);
+  if (st) return st;
+  if (!blob || !table) return LITHO_E_NULL;
+  if (((uintptr_t)blob & 15) || ((uintptr_t)table & 7)) return LITHO_E_ALIGN;
+  const LithoAbbePlan& p = *plan;
+  const char* b = static_cast<const char*>(blob);
+  k_pupil_table<<<p.n_tab, 128, 0, s>>>(reinterpret_cast<const LithoJob*>(b + p.off_jobs),
+                                         reinterpret_cast<const int32_t*>(b + p.off_slots),
+                                         reinterpret_cast<const LithoPupil*>(b + p.off_pupils), p.n_tab, p.n,
+                                         p.pixel_size, p.h, p.ncomp_max, static_cast<float2*>(table));
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+extern "C" int litho_abbe_profile(const LithoAbbePlan* plan, const void* blob, const void* table,
+                                  const void* mask, float* image,
+                                  float* peak, void* ws, size_t ws_bytes, cudaStream_t s, int reps,
+                                  float* stage_ms) {
+  if (!stage_ms || reps < 1) return LITHO_E_SIZE;
+  const int K = 8;
+  cudaEvent_t ev[K];
+  for (int i = 0; i < K; ++i)
+    if (cudaEventCreate(&ev[i]) != cudaSuccess) return (int)cudaErrorUnknown;
+  double acc[K - 1] = {0};
+  int st = LITHO_OK;
+  for (int r = 0; r < reps && st == LITHO_OK; ++r) {
+    st = abbe_run(plan, blob, table, mask, image, peak, ws, ws_bytes, s, ev);
+    if (st) break;
+    cudaError_t e = cudaEventSynchronize(ev[K - 1]);
+    if (e != cudaSuccess) { st = (int)e; break; }
+    for (int i = 0; i < K - 1; ++i) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+      acc[i] += ms;
+    }
+  }
+  for (int i = 0; i < K; ++i) cudaEventDestroy(ev[i]);
+  for (int i = 0; i < K - 1; ++i) stage_ms[i] = (float)(acc[i] / reps);
+  return st;
 }

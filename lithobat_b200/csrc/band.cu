@@ -19,81 +19,149 @@ namespace litho {
 
 constexpr int kBandWarps = 4;
 
+
+// Pass p handles, for each residue k' = k mod 32, the p-th frequency of
+// [-bm, bm] congruent to k' (in increasing order from -bm).
+__device__ __forceinline__ int band_k(int kp, int p, int bm) {
+  return -bm + ((kp + bm) & 31) + 32 * p;
+}
+
+// Shared-memory plan of one block of k_row_band_tma.
+struct BandSmem {
+  int warps, G, ld, tile_rows;
+  size_t tile_bytes, off_stage1, off_tw, off_y, total;
+};
+
+__host__ __device__ inline BandSmem band_smem(int n, int esz, int warps) {
+  BandSmem b{};
+  const int M = n >> 5, Mp = M < 32 ? M : 32, per = M / Mp;
+  b.warps = warps;
+  b.G = 32 / Mp;
+  b.ld = Mp * per + 1;
+  b.tile_rows = warps * b.G;
+  b.tile_bytes = (size_t)b.tile_rows * n * esz;
+  b.off_stage1 = 16 + b.tile_bytes;
+  b.off_tw = 16 + 2 * b.tile_bytes;
+  b.off_y = b.off_tw + (size_t)n * sizeof(float2);
+  b.total = b.off_y + (size_t)warps * b.G * 32 * b.ld * sizeof(float2);
+  return b;
+}
+
+// Rows arrive in tiles of `tile_rows` contiguous rows through a two-stage
+// TMA pipeline (one elected thread issues cp.async.bulk; consumers wait on
+// the stage's mbarrier); every warp owns G rows of a tile.
 template <bool CPLX>
-__global__ void __launch_bounds__(kBandWarps * 32)
-k_row_band_dft(const void* __restrict__ in, int n_rows, int rows_per_clip, int n, int bm,
-               float2* __restrict__ out, float scale, const float2* __restrict__ tw_inv) {
-  extern __shared__ float2 smem[];
-  float2* tw = smem;                                   // exp(+2 pi i j / n), j < n
+__global__ void __launch_bounds__(128)
+k_row_band_tma(const void* __restrict__ in, int n_rows, int rows_per_clip, int n, int bm,
+               float2* __restrict__ out, float scale, const float2* __restrict__ tw_inv,
+               int* __restrict__ status) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  const int esz = CPLX ? 8 : 4;
+  const BandSmem L = band_smem(n, esz, blockDim.x >> 5);
+  const int M = n >> 5;
+  const int Mp = M < 32 ? M : 32;
+  const int per_lane = M / Mp;
+  const int G = L.G, ld = L.ld;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float2* tb = smem + n + warp * (32 * 33);            // per-warp 32 x 33 transpose buffer
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smraw);
+  unsigned char* stage[2] = {smraw + 16, smraw + L.off_stage1};
+  float2* tw = reinterpret_cast<float2*>(smraw + L.off_tw);
+  float2* Y = reinterpret_cast<float2*>(smraw + L.off_y) + warp * (G * 32 * ld);
+  __shared__ int s_fail;
+
+  const int n_tiles = (n_rows + L.tile_rows - 1) / L.tile_rows;
+  auto issue = [&](int t, int st) {
+    const int r0 = t * L.tile_rows;
+    const int rows = (n_rows - r0) < L.tile_rows ? (n_rows - r0) : L.tile_rows;
+    const uint32_t bytes = (uint32_t)((size_t)rows * n * esz);
+    mbar_expect_tx(&mbar[st], bytes);
+    bulk_g2s(stage[st], static_cast<const unsigned char*>(in) + (size_t)r0 * n * esz, bytes, &mbar[st]);
+  };
+  if (threadIdx.x == 0) {
+    s_fail = 0;
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    fence_mbar_init();
+  }
   for (int j = threadIdx.x; j < n; j += blockDim.x) tw[j] = tw_inv[j];
   __syncthreads();
+  if (threadIdx.x == 0) {
+    if ((int)blockIdx.x < n_tiles) issue(blockIdx.x, 0);
+    if ((int)(blockIdx.x + gridDim.x) < n_tiles) issue(blockIdx.x + gridDim.x, 1);
+  }
 
-  const int M = n >> 5;
-  const int Mp = M < 32 ? M : 32;          // lanes per row
-  const int G = 32 / Mp;                   // rows per warp pass
-  const int per_lane = M / Mp;             // residues b per lane
   const int Bm = 2 * bm + 1;
+  const int npass = (Bm + 31) >> 5;
   const int r_loc = lane / Mp, bl = lane % Mp;
-  const int wmin = -((bm + 31) >> 5), wmax = (bm + 31) >> 5;
-  const int total_warps = gridDim.x * kBandWarps;
-
-  for (int rg = blockIdx.x * kBandWarps + warp; rg * G < n_rows; rg += total_warps) {
-    const int row = rg * G + r_loc;
+  const bool pow2 = (n & (n - 1)) == 0;
+  int it = 0;
+  for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
+    const int st = it & 1;
+    if (!mbar_wait(&mbar[st], (it >> 1) & 1)) atomicExch(&s_fail, 1);
+    __syncthreads();
+    if (s_fail) break;  // uniform: every thread saw the same flag
+    const unsigned char* tile = stage[st];
+    const int row_in_tile = warp * G + r_loc;
+    const int row = t * L.tile_rows + row_in_tile;
     const bool active = row < n_rows;
-    float2 v[32];
-    int have = -1;  // residue index q whose transform v holds
-    // Accumulate sum_b X_b(k') * exp(-2 pi i (k' + 32 w) b / n) per wrap w.
-    for (int w = wmin; w <= wmax; ++w) {
-      // does any k = k' + 32 w fall in [-bm, bm]?
-      if (32 * w + 31 < -bm || 32 * w > bm) continue;
-#pragma unroll 1
-      for (int c = 0; c < 32; ++c) tb[c * 33 + lane] = make_float2(0.f, 0.f);
-      __syncwarp();
+    for (int p = 0; p < npass; ++p) {
       for (int q = 0; q < per_lane; ++q) {
         const int b = bl + q * Mp;
-        if (have != q) {
-        have = q;
+        float2 v[32];
         if (active) {
           if (CPLX) {
-            const float2* src = reinterpret_cast<const float2*>(in) + (size_t)row * n + b;
+            const float2* src = reinterpret_cast<const float2*>(tile) + (size_t)row_in_tile * n + b;
 #pragma unroll
-            for (int a = 0; a < 32; ++a) v[a] = __ldg(src + (size_t)a * M);
+            for (int a = 0; a < 32; ++a) v[a] = src[a * M];
           } else {
-            const float* src = reinterpret_cast<const float*>(in) + (size_t)row * n + b;
+            const float* src = reinterpret_cast<const float*>(tile) + (size_t)row_in_tile * n + b;
 #pragma unroll
-            for (int a = 0; a < 32; ++a) v[a] = make_float2(__ldg(src + (size_t)a * M), 0.f);
+            for (int a = 0; a < 32; ++a) v[a] = make_float2(src[a * M], 0.f);
           }
         } else {
 #pragma unroll
           for (int a = 0; a < 32; ++a) v[a] = make_float2(0.f, 0.f);
         }
         fft_reg<32, -1>(v);
-        }
+        float2* yr = Y + (r_loc * 32) * ld + b;
 #pragma unroll
         for (int kp = 0; kp < 32; ++kp) {
-          const int k = kp + 32 * w;
-          int t = (int)(((long long)k * b) % n);
-          t = t < 0 ? -t : (t == 0 ? 0 : n - t);       // exponent -k b mod n
-          const float2 y = cmul(v[kp], tw[t]);
-          float2 acc = tb[kp * 33 + lane];
-          tb[kp * 33 + lane] = cadd(acc, y);
+          const int k = band_k(kp, p, bm);
+          const int e = -k * b;  // |e| < 2^24
+          const int tt = pow2 ? (e & (n - 1)) : ((e % n) + n) % n;
+          yr[kp * ld] = k <= bm ? cmul(v[kp], tw[tt]) : make_float2(0.f, 0.f);
         }
       }
       __syncwarp();
-      // lane kp sums over the residues of each of the G rows
+      const int k = band_k(lane, p, bm);
       for (int r = 0; r < G; ++r) {
-        float2 s = make_float2(0.f, 0.f);
-        for (int j = 0; j < Mp; ++j) s = cadd(s, tb[lane * 33 + r * Mp + j]);
-        const int orow = rg * G + r;
-        const int k = lane + 32 * w;
-        if (orow < n_rows && k >= -bm && k <= bm) {
+        const float2* yr = Y + (r * 32 + lane) * ld;
+        float2 s0 = make_float2(0.f, 0.f), s1 = make_float2(0.f, 0.f);
+        int j = 0;
+        for (; j + 1 < M; j += 2) {
+          s0 = cadd(s0, yr[j]);
+          s1 = cadd(s1, yr[j + 1]);
+        }
+        if (j < M) s0 = cadd(s0, yr[j]);
+        const int orow = t * L.tile_rows + warp * G + r;
+        if (orow < n_rows && k <= bm) {
           const int clip = orow / rows_per_clip, i = orow % rows_per_clip;
-          out[((size_t)clip * Bm + (k + bm)) * rows_per_clip + i] = cscale(s, scale);
+          out[((size_t)clip * Bm + (k + bm)) * rows_per_clip + i] = cscale(cadd(s0, s1), scale);
         }
       }
       __syncwarp();
+    }
+    __syncthreads();  // stage st fully consumed
+    if (threadIdx.x == 0 && t + 2 * (int)gridDim.x < n_tiles) {
+      fence_proxy_async();
+      issue(t + 2 * gridDim.x, st);
+    }
+  }
+  if (s_fail) {
+    // drain: give any copy still in flight a bounded chance to land, then report
+    if (threadIdx.x == 0) {
+      mbar_wait(&mbar[0], (it >> 1) & 1);
+      atomicExch(status, LITHO_E_TIMEOUT);
     }
   }
 }
@@ -110,8 +178,7 @@ __global__ void k_row_band_direct(const void* __restrict__ in, int n_rows, int r
     const int row = (int)(id / Bm), k = (int)(id % Bm) - bm;
     float2 s = make_float2(0.f, 0.f);
     for (int x = 0; x < n; ++x) {
-      int t = (int)(((long long)k * x) % n);
-      t = t < 0 ? -t : (t == 0 ? 0 : n - t);
+      const int t = ((-k * x) % n + n) % n;
       float2 v = CPLX ? reinterpret_cast<const float2*>(in)[(size_t)row * n + x]
                       : make_float2(reinterpret_cast<const float*>(in)[(size_t)row * n + x], 0.f);
       s = cadd(s, cmul(v, tw_inv[t]));
@@ -129,27 +196,28 @@ __global__ void k_twiddle_table(float2* w, int n, int sign) {
   }
 }
 
-size_t band_dft_smem(int n) { return (size_t)(n + kBandWarps * 32 * 33) * sizeof(float2); }
-
 // Launch the row-band DFT for n_rows rows (grouped rows_per_clip per clip).
 cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_per_clip, int n,
                                 int bm, float2* out, float scale, const float2* tw_inv,
-                                int num_sms, cudaStream_t st) {
-  if (n % 32 == 0) {
-    const int M = n / 32, Mp = M < 32 ? M : 32, G = 32 / Mp;
-    const int warps = (n_rows + G - 1) / G;
-    int blocks = (warps + kBandWarps - 1) / kBandWarps;
-    const int cap = num_sms * 16;
-    if (blocks > cap) blocks = cap;
-    const size_t sm = band_dft_smem(n);
+                                int num_sms, cudaStream_t st, int* status) {
+  const int esz = cplx ? 8 : 4;
+  if (n % 32 == 0 && ((uintptr_t)in & 15) == 0) {
+    int warps = 4;
+    while (warps > 1 && band_smem(n, esz, warps).total > 200 * 1024) warps >>= 1;
+    const BandSmem L = band_smem(n, esz, warps);
+    if (L.total > 227 * 1024) return cudaErrorInvalidValue;
+    const int tiles = (n_rows + L.tile_rows - 1) / L.tile_rows;
+    const int per_sm = (int)((227 * 1024) / L.total) > 0 ? (int)((227 * 1024) / L.total) : 1;
+    int blocks = num_sms * per_sm;
+    if (blocks > tiles) blocks = tiles;
     if (cplx) {
-      cudaFuncSetAttribute(k_row_band_dft<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      k_row_band_dft<true><<<blocks, kBandWarps * 32, sm, st>>>(in, n_rows, rows_per_clip, n, bm,
-                                                                out, scale, tw_inv);
+      cudaFuncSetAttribute(k_row_band_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+      k_row_band_tma<true><<<blocks, warps * 32, L.total, st>>>(in, n_rows, rows_per_clip, n, bm, out, scale,
+                                                                 tw_inv, status);
     } else {
-      cudaFuncSetAttribute(k_row_band_dft<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      k_row_band_dft<false><<<blocks, kBandWarps * 32, sm, st>>>(in, n_rows, rows_per_clip, n, bm,
-                                                                 out, scale, tw_inv);
+      cudaFuncSetAttribute(k_row_band_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+      k_row_band_tma<false><<<blocks, warps * 32, L.total, st>>>(in, n_rows, rows_per_clip, n, bm, out, scale,
+                                                                  tw_inv, status);
     }
   } else {
     const long long total = (long long)n_rows * (2 * bm + 1);

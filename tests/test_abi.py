@@ -43,7 +43,7 @@ def test_bad_plans_are_rejected_before_any_launch():
     """Argument checks run on the host and need no device."""
     L = nat.lib()
     p = nat.AbbePlan(n=64, n_clips=1, n_out=1, n_jobs=1, n_items=1, n_pupils=1, h=3, bm=3, L=32,
-                     mask_complex=0, ncomp_max=1, flags=0, pixel_size=4e-9)
+                     mask_complex=0, ncomp_max=1, n_tab=1, pixel_size=4e-9)
     sz = C.c_size_t(0)
     assert L.litho_abbe_workspace(C.byref(p), C.byref(sz)) == 0 and sz.value > 0
     bad = nat.AbbePlan.from_buffer_copy(p); bad.h = 8          # 4h+1 > 32
@@ -53,6 +53,8 @@ def test_bad_plans_are_rejected_before_any_launch():
     bad = nat.AbbePlan.from_buffer_copy(p); bad.off_pupils = 8
     assert L.litho_abbe_workspace(C.byref(bad), C.byref(sz)) == -6
     bad = nat.AbbePlan.from_buffer_copy(p); bad.n = 0
+    assert L.litho_abbe_workspace(C.byref(bad), C.byref(sz)) == -2
+    bad = nat.AbbePlan.from_buffer_copy(p); bad.n_tab = 2       # more slots than jobs
     assert L.litho_abbe_workspace(C.byref(bad), C.byref(sz)) == -2
     # workspace too small / null pointers: rejected without touching the device
     assert L.litho_abbe(C.byref(p), None, None, None, None, None, 0, None) == -1

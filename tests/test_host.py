@@ -89,6 +89,8 @@ def test_plan_groups_jobs_by_output_and_counts_transforms():
     assert pd.n_out == 4 and pd.jobs == 4 * S * 2 and pd.transforms == 3 * pd.jobs
     assert pd.plan.ncomp_max == 3 and 4 * pd.plan.h + 1 <= pd.plan.L
     assert pd.plan.bm >= pd.plan.h
+    # two clips with the same optics share the pupil-table slots of each plane
+    assert pd.plan.n_tab == 2 * S * 2
 
 
 def test_thick_masks_and_bad_models_are_refused():
