@@ -17,8 +17,6 @@
 
 namespace litho {
 
-constexpr int kBandWarps = 4;
-
 
 // Pass p handles, for each residue k' = k mod 32, the p-th frequency of
 // [-bm, bm] congruent to k' (in increasing order from -bm).
