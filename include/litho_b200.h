@@ -42,7 +42,11 @@ extern "C" {
 #define LITHO_E_UNSUPPORTED -5   /* valid request this build does not serve  */
 #define LITHO_E_ALIGN -6         /* a pointer is not 16-byte aligned         */
 #define LITHO_E_DEVICE -7        /* device is not sm_100 or not reachable    */
+#define LITHO_E_SCRATCH -8       /* needs more than the fixed no-allocation scratch */
 #define LITHO_E_TIMEOUT 1000001  /* a bounded device wait gave up           */
+
+/* Size of the fixed device scratch litho_abbe_noalloc() runs in. */
+#define LITHO_NOALLOC_SCRATCH_BYTES (32u << 20)
 
 /* ---- descriptors (plain data; layouts are fixed, see static sizes) ----- */
 
@@ -129,6 +133,22 @@ int litho_abi_sizes(int32_t* out, int n);
 
 /* Workspace bytes litho_abbe() needs for this plan. */
 int litho_abbe_workspace(const LithoAbbePlan* plan, size_t* bytes);
+
+/* litho_abbe() for callers that cannot allocate device memory for a
+ * workspace (every device byte owned by another allocator, or a loop that
+ * must not pay cudaMalloc's implicit synchronisation). It has no counterpart
+ * in the reference, which allocates freely on the host. The kernels run in a
+ * fixed LITHO_NOALLOC_SCRATCH_BYTES (32 MiB) buffer compiled into the
+ * library, held on every GPU that loads it until exit; plans whose
+ * litho_abbe_workspace() exceeds that are rejected with LITHO_E_SCRATCH
+ * before anything is launched. The entry point allocates nothing. Its first
+ * call on each device looks up that device's copy of the buffer
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the one buffer: calls that may overlap on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller. */
+int litho_abbe_noalloc(const LithoAbbePlan* plan, const void* plan_blob_dev,
+                       const void* mask_dev, float* image_dev, float* peak_dev,
+                       cudaStream_t stream);
 
 /* Synchronise `stream` and return the device status word of the last
  * litho_abbe*() call that used this workspace: 0, or LITHO_E_TIMEOUT if a

@@ -16,6 +16,9 @@ import numpy as np
 LIB_PATH = Path(__file__).resolve().parent / "liblitho_b200.so"
 
 
+NOALLOC_SCRATCH_BYTES = 32 << 20   # LITHO_NOALLOC_SCRATCH_BYTES
+
+
 class NativeUnavailable(RuntimeError):
     """The sm_100a engine cannot run here (library not built, or no GPU)."""
 
@@ -91,9 +94,11 @@ def lib():
     L.litho_abbe_tabled.argtypes = [C.POINTER(AbbePlan), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
     L.litho_abbe_status.argtypes = [C.POINTER(AbbePlan), C.c_void_p, C.c_void_p]
+    L.litho_abbe_noalloc.argtypes = [C.POINTER(AbbePlan), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]
     for fn in ("litho_abbe_workspace", "litho_abbe", "litho_abbe_plain_workspace", "litho_abbe_plain",
                "litho_abbe_profile", "litho_abbe_table_bytes", "litho_abbe_pupil_table",
-               "litho_abbe_tabled", "litho_abbe_status"):
+               "litho_abbe_tabled", "litho_abbe_status", "litho_abbe_noalloc"):
         getattr(L, fn).restype = C.c_int
     _lib = L
     return L

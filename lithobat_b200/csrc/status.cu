@@ -13,6 +13,9 @@ extern "C" const char* litho_status_string(int status) {
     case LITHO_E_UNSUPPORTED: return "request is valid but not served by this build";
     case LITHO_E_ALIGN: return "a pointer or offset is not aligned";
     case LITHO_E_DEVICE: return "no usable sm_100 device";
+    case LITHO_E_SCRATCH:
+      return "plan needs more scratch than the fixed no-allocation buffer holds; use litho_abbe() with a "
+             "caller workspace or a smaller batch";
     case LITHO_E_TIMEOUT: return "a bounded device-side wait gave up";
   }
   if (status > 0) return cudaGetErrorString(static_cast<cudaError_t>(status));
