@@ -206,6 +206,44 @@ int litho_abbe_plain(const LithoAbbePlan* plan, int batch, const void* plan_blob
                      const void* mask_dev, float* image_dev, float* peak_dev,
                      void* workspace_dev, size_t workspace_bytes, cudaStream_t stream);
 
+/* ---- SOCS (Hopkins) decomposition ---------------------------------------- */
+
+/* Workspace bytes of litho_socs_build() for n_source points and n_band band
+ * frequencies. */
+int litho_socs_workspace(int n_source, int n_band, size_t* bytes);
+
+/* Eigen-decomposition of one optical state's transmission cross-coefficient.
+ * Replaces expose/hopkins.py:SOCSKernels.build (:103-198) up to the
+ * selection of kernels, via the dual form: with A[s][b] = sqrt(w_s)
+ * exp(i W) on the band (zero where inside_dev[s*n_band+b] == 0, the
+ * reference's hypot aperture test made by the caller), G = conj(A) A^T
+ * (S x S) is assembled on the tensor cores (gram_mode 0: tcgen05 TF32 with
+ * hi/lo operand splitting, FP32 accumulate, FP64 reduction) or in FP64 on
+ * CUDA cores (gram_mode 1, a check), diagonalised by FP64 Jacobi, and
+ *   phi_out[j][b] = (A^T u_j)[b]       (complex128, unnormalised)
+ *   lambda_out[j] = |A^T u_j|^2        (the eigenvalue, FP64 Rayleigh quotient)
+ * for every j < n_source, unsorted. phi_j / sqrt(lambda_j) are the TCC's
+ * unit eigenvectors (the reference's kernels on the band). gram_out (may be
+ * NULL) receives G, row-major with an even leading dimension >= n_source. */
+int litho_socs_build(const LithoPupil* pupil_dev, const double* fsx_dev, const double* fsy_dev,
+                     const double* w_dev, int n_source, const int32_t* band_kx_dev,
+                     const int32_t* band_ky_dev, int n_band, const uint8_t* inside_dev, int n,
+                     double pixel_size, int gram_mode, double2* phi_out_dev,
+                     double* lambda_out_dev, double2* gram_out_dev, void* workspace_dev,
+                     size_t workspace_bytes, cudaStream_t stream);
+
+/* Copy, after litho_socs_build(), the diagonalised Gram matrix, its
+ * eigenvector matrix (columns) and the Jacobi eigenvalues out of the
+ * workspace (each n x n / n with n = n_source rounded up to even; any output
+ * may be NULL). For checking the eigensolver. */
+int litho_socs_debug(int n_source, int n_band, const void* workspace_dev, double2* H_out,
+                     double2* V_out, double* evals_out, cudaStream_t stream);
+
+/* Synchronise and report litho_socs_build()'s device status (0 or
+ * LITHO_E_TIMEOUT) and the Jacobi sweeps it took. */
+int litho_socs_status(int n_source, int n_band, const void* workspace_dev, int* sweeps,
+                      cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

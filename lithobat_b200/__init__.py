@@ -8,11 +8,12 @@ Drop-in replacements for ``litho_sim.expose.compute_aerial_image`` and
 from .aerial import (SOURCE_TILT_SIGN, compute_aerial_batch, compute_aerial_image,
                      compute_aerial_planes, normalisation_scale)
 from .config import GridConfig, OpticsConfig
+from .hopkins import SOCSKernels
 from .source import Pole, Source, SourcePoints, build_source, source_points
 from . import patterns
 
 __all__ = [
-    "GridConfig", "OpticsConfig", "Pole", "Source", "SourcePoints", "SOURCE_TILT_SIGN",
+    "GridConfig", "OpticsConfig", "Pole", "SOCSKernels", "Source", "SourcePoints", "SOURCE_TILT_SIGN",
     "build_source", "compute_aerial_batch", "compute_aerial_image", "compute_aerial_planes",
     "normalisation_scale", "source_points",
 ]

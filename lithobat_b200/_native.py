@@ -96,6 +96,14 @@ def lib():
     L.litho_abbe_status.argtypes = [C.POINTER(AbbePlan), C.c_void_p, C.c_void_p]
     L.litho_abbe_noalloc.argtypes = [C.POINTER(AbbePlan), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p]
+    L.litho_socs_workspace.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_size_t)]
+    L.litho_socs_build.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                   C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
+    L.litho_socs_status.argtypes = [C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_int), C.c_void_p]
+    L.litho_socs_debug.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    for fn in ("litho_socs_workspace", "litho_socs_build", "litho_socs_status", "litho_socs_debug"):
+        getattr(L, fn).restype = C.c_int
     for fn in ("litho_abbe_workspace", "litho_abbe", "litho_abbe_plain_workspace", "litho_abbe_plain",
                "litho_abbe_profile", "litho_abbe_table_bytes", "litho_abbe_pupil_table",
                "litho_abbe_tabled", "litho_abbe_status", "litho_abbe_noalloc"):

@@ -84,6 +84,11 @@ def plan_abbe(views: Sequence, n: int, pixel_size: float, planes: Sequence[Seque
     (defocus, n_image); every clip has the same number of planes."""
     key = (tuple(repr(v) for v in views), n, pixel_size, tuple(tuple(map(tuple, p)) for p in planes),
            float(dose), bool(return_raw), bool(mask_complex), items_per_job_group)
+    h = max(disc_halfwidth(v.NA, v.wavelength, n, pixel_size)[1] for v in views)
+    if 4 * h + 1 > 64:
+        raise NotImplementedError(
+            f"pupil half-width {h} bins needs a coarse grid above 64 (4h+1 = {4 * h + 1}); "
+            "use engine='plain' for this grid")
     hit = _PLANS.get(key)
     if hit is not None:
         return hit
@@ -198,6 +203,47 @@ def _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, ite
         off_out_items=offs[3], off_norm=offs[4], off_slots=offs[5])
     transforms = int(np.sum(jobs["ncomp"]))
     return AbbePlanData(plan, blob, clears, n_out, n_jobs, transforms)
+
+
+def plan_from_table(n: int, pixel_size: float, n_clips: int, weights, h: int, mask_complex: bool,
+                    norm_mode=(0, 1.0), items_per_job_group: int = 4) -> AbbePlanData:
+    """Plan that images every clip with K unshifted coherent systems whose
+    spectra are given by a caller-built table (the SOCS forward,
+    hopkins.py:215-217): job (clip c, kernel k) has weight weights[k] and
+    table slot k; there is no pupil to evaluate."""
+    K = len(weights)
+    if K == 0:
+        raise ValueError("no kernels to image with")
+    L = 32
+    while L < 4 * h + 1:
+        L *= 2
+    if L > 64:
+        raise NotImplementedError(f"kernel band half-width {h} bins needs a coarse grid above 64")
+    jobs = np.zeros(n_clips * K, dtype=nat.JOB_DTYPE)
+    jobs["weight"] = np.tile(np.asarray(weights, dtype=np.float64), n_clips)
+    jobs["clip"] = np.repeat(np.arange(n_clips), K)
+    jobs["out"] = jobs["clip"]
+    jobs["ncomp"] = 1
+    jobs["tab"] = np.tile(np.arange(K), n_clips)
+    pupils = np.zeros(1, dtype=nat.PUPIL_DTYPE)
+    pupils["wavelength"], pupils["NA"], pupils["n_image"] = 1.0, 1.0, 1.0
+    slots = np.arange(K, dtype=np.int32)
+    per = max(1, int(items_per_job_group))
+    item_rows, out_items = [], [0]
+    for c in range(n_clips):
+        for j in range(c * K, (c + 1) * K, per):
+            item_rows.append((c, j, min(j + per, (c + 1) * K), 0))
+        out_items.append(len(item_rows))
+    items = np.array(item_rows, dtype=np.int32).view(nat.ITEM_DTYPE).reshape(-1)
+    out_items = np.array(out_items, dtype=np.int32)
+    norm = np.zeros(n_clips, dtype=nat.NORM_DTYPE)
+    norm["mode"], norm["scale"] = norm_mode
+    blob, offs = nat.blob([jobs, pupils, items, out_items, norm, slots])
+    plan = nat.AbbePlan(
+        n=n, n_clips=n_clips, n_out=n_clips, n_jobs=len(jobs), n_items=len(items), n_pupils=1, h=h, bm=h, L=L,
+        mask_complex=int(mask_complex), ncomp_max=1, n_tab=K, pixel_size=pixel_size, off_jobs=offs[0],
+        off_pupils=offs[1], off_items=offs[2], off_out_items=offs[3], off_norm=offs[4], off_slots=offs[5])
+    return AbbePlanData(plan, blob, np.zeros(n_clips), n_clips, len(jobs), len(jobs))
 
 
 # ---------------------------------------------------------------------------

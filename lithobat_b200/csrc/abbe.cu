@@ -136,6 +136,113 @@ k_coarse32(const LithoItem* __restrict__ items, const LithoJob* __restrict__ job
 }
 
 // ---------------------------------------------------------------------------
+// 3b. coarse accumulation, L = 64 (h <= 15): one warp per coherent system.
+//    A 64-point transform of a sequence supported on [-15, 15] is two 32-point
+//    FFTs: X(2v') = FFT32[g](v'), X(2v'+1) = FFT32[g(d) w64^d](v'), with
+//    w64 = exp(2 pi i / 64). Pass 1 (over ky): lane = column kx, results to a
+//    per-warp T[kx][v]; pass 2 (over kx): lane owns rows v and v + 32, and
+//    J(v, u) += w |e|^2 lives in a per-warp shared-memory tile.
+// ---------------------------------------------------------------------------
+constexpr int kCoarse64Warps = 2;
+constexpr int kCoarseHMax64 = 15;  // 4h + 1 <= 64
+constexpr int kT64Ld = 65;         // T row pitch (complex), J row pitch (float)
+
+__device__ __forceinline__ void fft64_of_box(float2 (&a)[32], float2 (&b)[32]) {
+  // a holds g(d) at position d & 31 for d in [-15, 15]; on return a = X(2v'),
+  // b = X(2v'+1), v' = 0..31.
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    const int d = i < 16 ? i : i - 32;  // signed position
+    b[i] = twiddle64<+1>(a[i], d & 63);
+  }
+  fft_reg<32, +1>(a);
+  fft_reg<32, +1>(b);
+}
+
+__global__ void __launch_bounds__(kCoarse64Warps * 32)
+k_coarse64(const LithoItem* __restrict__ items, const LithoJob* __restrict__ jobs,
+           const float2* __restrict__ table, int h, int ncomp_max, const float2* __restrict__ Mb,
+           int bm, float* __restrict__ partial) {
+  extern __shared__ float2 smem64[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // per warp: T [31][kT64Ld] complex, then J [64][kT64Ld] float
+  const int per_warp = 31 * kT64Ld + (64 * kT64Ld + 1) / 2;
+  float2* T = smem64 + warp * per_warp;
+  float* Jw = reinterpret_cast<float*>(T + 31 * kT64Ld);
+  const LithoItem it = items[blockIdx.x];
+  const int side = 2 * h + 1, npts = side * side, Bm = 2 * bm + 1;
+  const int dx = lane - h;
+  const bool col_live = lane < side;
+  for (int i = lane; i < 64 * kT64Ld; i += 32) Jw[i] = 0.f;
+  __syncwarp();
+
+  for (int j = it.job_begin + warp; j < it.job_end; j += kCoarse64Warps) {
+    const LithoJob job = jobs[j];
+    const float w = (float)job.weight;
+    const float2* m = Mb + (size_t)job.clip * Bm * Bm;
+    const int mx = job.cx + dx + bm;
+    for (int c = 0; c < job.ncomp; ++c) {
+      const float2* tp = table + ((size_t)job.tab * ncomp_max + c) * npts;
+      float2 a[32], b[32];
+#pragma unroll
+      for (int i = 0; i < 32; ++i) a[i] = make_float2(0.f, 0.f);
+      if (col_live && mx >= 0 && mx < Bm) {
+#pragma unroll
+        for (int d = -kCoarseHMax64; d <= kCoarseHMax64; ++d) {
+          const int my = job.cy + d + bm;
+          if (d >= -h && d <= h && my >= 0 && my < Bm)
+            a[d & 31] = cmul(__ldg(tp + (d + h) * side + (dx + h)), __ldg(m + (size_t)my * Bm + mx));
+        }
+      }
+      fft64_of_box(a, b);  // column kx = dx: T(kx, 2v') = a[v'], T(kx, 2v'+1) = b[v']
+      __syncwarp();
+      if (col_live) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          T[lane * kT64Ld + 2 * i] = a[i];
+          T[lane * kT64Ld + 2 * i + 1] = b[i];
+        }
+      }
+      __syncwarp();
+#pragma unroll 1
+      for (int half = 0; half < 2; ++half) {
+        const int v = lane + 32 * half;
+#pragma unroll
+        for (int i = 0; i < 32; ++i) a[i] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int d = -kCoarseHMax64; d <= kCoarseHMax64; ++d)
+          if (d >= -h && d <= h) a[d & 31] = T[(d + h) * kT64Ld + v];
+        fft64_of_box(a, b);  // e(2u', v) = a[u'], e(2u'+1, v) = b[u']
+        float* jr = Jw + v * kT64Ld;
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          jr[2 * i] = fmaf(w, cabs2(a[i]), jr[2 * i]);
+          jr[2 * i + 1] = fmaf(w, cabs2(b[i]), jr[2 * i + 1]);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // fixed-order reduction over the block's warps: partial[item][v * 64 + u]
+  float* dst = partial + (size_t)blockIdx.x * 4096;
+  for (int idx = threadIdx.x; idx < 4096; idx += blockDim.x) {
+    const int v = idx >> 6, u = idx & 63;
+    float s = 0.f;
+#pragma unroll
+    for (int wp = 0; wp < kCoarse64Warps; ++wp) {
+      const float* jw = reinterpret_cast<const float*>(smem64 + wp * per_warp + 31 * kT64Ld);
+      s += jw[v * kT64Ld + u];
+    }
+    dst[idx] = s;
+  }
+}
+
+static size_t coarse64_smem() {
+  const int per_warp = 31 * kT64Ld + (64 * kT64Ld + 1) / 2;
+  return (size_t)kCoarse64Warps * per_warp * sizeof(float2);
+}
+
+// ---------------------------------------------------------------------------
 // 4. per output: J = sum of its items' partials (in item order), then
 //    B(gx, gy) = (1/L^2) sum_{u,v} J(v, u) exp(-2 pi i (gx u + gy v) / L).
 //    One block of 1024 threads per output; L is a power of two.
@@ -358,8 +465,8 @@ static int check_plan(const LithoAbbePlan* p) {
       p->n_pupils < 1 || p->h < 0 || p->bm < 0 || p->n_tab < 1 || p->n_tab > p->n_jobs)
     return LITHO_E_SIZE;
   if (p->ncomp_max != 1 && p->ncomp_max != 3) return LITHO_E_SIZE;
-  if (p->L != 32) return LITHO_E_UNSUPPORTED;
-  if (4 * p->h + 1 > p->L || p->h > kCoarseHMax32) return LITHO_E_BAND;
+  if (p->L != 32 && p->L != 64) return LITHO_E_UNSUPPORTED;
+  if (4 * p->h + 1 > p->L || p->h > (p->L == 32 ? kCoarseHMax32 : kCoarseHMax64)) return LITHO_E_BAND;
   if (p->bm < p->h) return LITHO_E_BAND;
   if (!(p->pixel_size > 0.0)) return LITHO_E_SIZE;
   const int64_t offs[6] = {p->off_jobs, p->off_pupils, p->off_items, p->off_out_items, p->off_norm,
@@ -448,10 +555,17 @@ static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* tab
                           sms, s, status);
   if (e != cudaSuccess) return (int)e;
   mark(3);
-  const size_t sm_coarse = (size_t)kCoarseWarps * 32 * 33 * sizeof(float2);
-  cudaFuncSetAttribute(k_coarse32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_coarse);
-  k_coarse32<<<p.n_items, kCoarseWarps * 32, sm_coarse, s>>>(items, jobs, table, p.h, p.ncomp_max, mb, p.bm,
-                                                              partial);
+  if (p.L == 32) {
+    const size_t sm_coarse = (size_t)kCoarseWarps * 32 * 33 * sizeof(float2);
+    cudaFuncSetAttribute(k_coarse32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_coarse);
+    k_coarse32<<<p.n_items, kCoarseWarps * 32, sm_coarse, s>>>(items, jobs, table, p.h, p.ncomp_max, mb, p.bm,
+                                                                partial);
+  } else {
+    const size_t sm_coarse = coarse64_smem();
+    cudaFuncSetAttribute(k_coarse64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_coarse);
+    k_coarse64<<<p.n_items, kCoarse64Warps * 32, sm_coarse, s>>>(items, jobs, table, p.h, p.ncomp_max, mb, p.bm,
+                                                                  partial);
+  }
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
   mark(4);
   const size_t sm_red = (size_t)p.L * p.L * 4 + (size_t)p.L * G * 8 + (size_t)p.L * 8;
