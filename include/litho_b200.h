@@ -244,6 +244,88 @@ int litho_socs_debug(int n_source, int n_band, const void* workspace_dev, double
 int litho_socs_status(int n_source, int n_band, const void* workspace_dev, int* sweeps,
                       cudaStream_t stream);
 
+/* ---- band-limited transforms and the ILT adjoint --------------------------- */
+
+/* Coarse-grid image band of a plan whose mask band box mb_dev (per clip,
+ * (2 bm + 1)^2, from litho_band_spectrum with scale 1/N^2) is already known:
+ * the accumulation and reduction stages of litho_abbe() alone. bbox_out:
+ * per output (4h+1)^2 complex, ready for litho_band_synthesis(h' = 2h). */
+int litho_coarse_image(const LithoAbbePlan* plan, const void* plan_blob_dev, const void* table_dev,
+                       const void* mb_dev, void* bbox_out_dev, void* workspace_dev,
+                       size_t workspace_bytes, cudaStream_t stream);
+
+/* Workspace bytes of litho_band_spectrum(). */
+int litho_band_spectrum_workspace(int n_fields, int n, int bm, size_t* bytes);
+
+/* box_out[f][ky + bm][kx + bm] = scale * sum_{x,y} in[f][y][x] exp(-2 pi i (kx x + ky y) / N)
+ * for |kx|, |ky| <= bm: the part of numpy.fft.fft2 a band-limited consumer
+ * needs (the reference calls fft2 at opc/ilt.py:227, :263 and
+ * expose/hopkins.py:215). in: float32 (is_complex 0) or complex64. */
+int litho_band_spectrum(const void* in_dev, int is_complex, int n_fields, int n, int bm, float scale,
+                        void* box_out_dev, void* workspace_dev, size_t workspace_bytes,
+                        cudaStream_t stream);
+
+/* Workspace bytes of litho_band_synthesis(). */
+int litho_band_synthesis_workspace(int n_fields, int n, size_t* bytes);
+
+/* out[f][y][x] = sum_{|kx|,|ky| <= h} box[f][ky + h][kx + h] exp(2 pi i (kx x + ky y) / N):
+ * float32 output for Hermitian boxes (complex_out 0), complex64 otherwise —
+ * numpy.fft.ifft2 (times N^2) of a band-limited spectrum (opc/ilt.py:228). */
+int litho_band_synthesis(const void* box_dev, int n_fields, int n, int h, int complex_out,
+                         void* out_dev, void* workspace_dev, size_t workspace_bytes,
+                         cudaStream_t stream);
+
+/* Workspace bytes of litho_socs_adjoint(). */
+int litho_socs_adjoint_workspace(int n_clips, int n_items, int h, size_t* bytes);
+
+/* The band of the SOCS adjoint (opc/ilt.py:socs_gradient, :235-266):
+ *   grad_box[c] = H, H(f) = A(f) + conj(A(-f)),
+ *   A(f) = sum_k lambda_k conj(phi_k(f)) [ (phi_k M_c) (*) G_c ](f),  |f| <= h,
+ * with M_c = mask_box[c] ((2h+1)^2, F(m)/N^2), G_c = sens_box[c]
+ * ((4h+1)^2, F(dJ/dI)/N^2), phi_k = table slot k, lambda_k = job weight, the
+ * jobs/items of a litho_abbe plan with one job per (clip, kernel) and
+ * bm == h <= 15. When field_box_dev is given (per job, (2h+1)^2: the band
+ * spectrum of each coherent field, F(E_k)/N^2) it replaces phi_k M_c and
+ * mask_box_dev may be NULL. litho_band_synthesis(grad_box, h, real) gives d/dm. */
+int litho_socs_adjoint(const LithoAbbePlan* plan, const void* plan_blob_dev, const void* table_dev,
+                       const void* mask_box_dev, const void* field_box_dev, const void* sens_box_dev,
+                       void* grad_box_out_dev, void* workspace_dev, size_t workspace_bytes,
+                       cudaStream_t stream);
+
+/* Relaxed resist objective (opc/ilt.py:_Objective, :313-336) on an image that
+ * is already blurred: signed = sign (scale img - level); z = sigmoid(a
+ * signed) (argument clipped to +-60); dfield = sign (2/npix) (z - t) a z (1-z).
+ * Writes dfield (dJ/d field), optionally signed, and per-block partial sums
+ * of (z - t)^2 (cost_part) and of pattern errors (perr_part): n_part blocks
+ * per field, partial arrays [n_fields][n_part]. */
+int litho_ilt_objective(const float* img_dev, const float* target_dev, int n_fields, int n, float scale,
+                        float level, float sign, float steepness_a, float* dfield_dev,
+                        float* signed_out_dev, double* cost_part_dev, unsigned int* perr_part_dev,
+                        int n_part, cudaStream_t stream);
+
+/* TV (periodic neighbours) and discreteness penalties (opc/ilt.py:339-357):
+ * adds their gradients to grad_dev and their costs to cost_part_dev. */
+int litho_ilt_penalties(const float* mask_dev, int n_fields, int n, float w_tv, float w_disc,
+                        float* grad_dev, double* cost_part_dev, int n_part, cudaStream_t stream);
+
+/* mask = sigmoid(clip(beta field, +-60)) (opc/ilt.py:_mask_of, :368-378). */
+int litho_ilt_mask(const float* field_dev, long long count, float beta, float* mask_dev,
+                   cudaStream_t stream);
+
+/* q = grad_m beta m (1 - m), the sigmoid's slope of opc/ilt.py:_grad_theta (:381-389). */
+int litho_ilt_theta_grad(const float* grad_m_dev, const float* mask_dev, long long count, float beta,
+                         float* q_dev, cudaStream_t stream);
+
+/* One Adam step at iteration it >= 1 (opc/ilt.py:582-591), in place. */
+int litho_ilt_adam(const float* g_dev, long long count, float step, float b1, float b2, float eps,
+                   int it, float* theta_dev, float* m1_dev, float* m2_dev, cudaStream_t stream);
+
+/* scipy.ndimage.gaussian_filter (mode 'reflect') of n_fields N x N images:
+ * the 1-D weights[2 radius + 1] along rows, then along columns
+ * (opc/ilt.py:_blur, :274-289). tmp_dev: scratch of the input's size. */
+int litho_gaussian_blur(const float* in_dev, float* out_dev, float* tmp_dev, int n_fields, int n,
+                        const float* weights_dev, int radius, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

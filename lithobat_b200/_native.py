@@ -104,6 +104,25 @@ def lib():
     L.litho_socs_debug.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     for fn in ("litho_socs_workspace", "litho_socs_build", "litho_socs_status", "litho_socs_debug"):
         getattr(L, fn).restype = C.c_int
+    vp, i32, f32, sz = C.c_void_p, C.c_int, C.c_float, C.c_size_t
+    sigs = {
+        "litho_coarse_image": [C.POINTER(AbbePlan), vp, vp, vp, vp, vp, sz, vp],
+        "litho_band_spectrum_workspace": [i32, i32, i32, C.POINTER(sz)],
+        "litho_band_spectrum": [vp, i32, i32, i32, i32, f32, vp, vp, sz, vp],
+        "litho_band_synthesis_workspace": [i32, i32, C.POINTER(sz)],
+        "litho_band_synthesis": [vp, i32, i32, i32, i32, vp, vp, sz, vp],
+        "litho_socs_adjoint_workspace": [i32, i32, i32, C.POINTER(sz)],
+        "litho_socs_adjoint": [C.POINTER(AbbePlan), vp, vp, vp, vp, vp, vp, vp, sz, vp],
+        "litho_ilt_objective": [vp, vp, i32, i32, f32, f32, f32, f32, vp, vp, vp, vp, i32, vp],
+        "litho_ilt_penalties": [vp, i32, i32, f32, f32, vp, vp, i32, vp],
+        "litho_ilt_mask": [vp, C.c_longlong, f32, vp, vp],
+        "litho_ilt_theta_grad": [vp, vp, C.c_longlong, f32, vp, vp],
+        "litho_ilt_adam": [vp, C.c_longlong, f32, f32, f32, f32, i32, vp, vp, vp, vp],
+        "litho_gaussian_blur": [vp, vp, vp, i32, i32, vp, i32, vp],
+    }
+    for fn, at in sigs.items():
+        getattr(L, fn).argtypes = at
+        getattr(L, fn).restype = C.c_int
     for fn in ("litho_abbe_workspace", "litho_abbe", "litho_abbe_plain_workspace", "litho_abbe_plain",
                "litho_abbe_profile", "litho_abbe_table_bytes", "litho_abbe_pupil_table",
                "litho_abbe_tabled", "litho_abbe_status", "litho_abbe_noalloc"):

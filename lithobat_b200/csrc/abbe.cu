@@ -329,7 +329,7 @@ k_synth(const float2* __restrict__ Bbox, int G, int n, const float2* __restrict_
     C[r * gp + gx] = acc;
   }
   __syncthreads();
-  const LithoNorm nm = norm[o];
+  const LithoNorm nm = norm ? norm[o] : LithoNorm{0, 1.0f};
   const float sc = nm.mode == 0 ? nm.scale : 1.0f;
   const int rows = (n - y0) < kSynthRows ? (n - y0) : kSynthRows;
   float mx = 0.f;
@@ -380,6 +380,19 @@ k_synth(const float2* __restrict__ Bbox, int G, int n, const float2* __restrict_
     for (int i = 1; i < kSynthThreads / 32; ++i) m = fmaxf(m, red[i]);
     blockmax[(size_t)o * gridDim.x + blockIdx.x] = m;
   }
+}
+
+int synth_blocks_for(int n) { return (n + kSynthRows - 1) / kSynthRows; }
+
+// Real synthesis of n_fields Hermitian boxes of side G into n x n images.
+cudaError_t launch_synth_real(const float2* box, int G, int n, int n_fields, const float2* tw, const LithoNorm* norm,
+                              float* out, float* blockmax, cudaStream_t s) {
+  const int gh = G / 2;
+  const size_t sm = (size_t)n * 8 + (size_t)kSynthRows * (gh + 1) * 8 + (size_t)G * G * 8;
+  cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  dim3 gs((n + kSynthRows - 1) / kSynthRows, n_fields);
+  k_synth<<<gs, kSynthThreads, sm, s>>>(box, G, n, tw, norm, out, blockmax);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
@@ -598,6 +611,40 @@ extern "C" int litho_abbe_tabled(const LithoAbbePlan* plan, const void* blob, co
                                  float* image, float* peak, void* ws, size_t ws_bytes, cudaStream_t s) {
   if (!table) return LITHO_E_NULL;
   return abbe_run(plan, blob, table, mask, image, peak, ws, ws_bytes, s, nullptr);
+}
+
+extern "C" int litho_coarse_image(const LithoAbbePlan* plan, const void* blob, const void* table, const void* mb,
+                                  void* bbox_out, void* ws, size_t ws_bytes, cudaStream_t s) {
+  const int st = check_plan(plan);
+  if (st) return st;
+  if (!blob || !table || !mb || !bbox_out || !ws) return LITHO_E_NULL;
+  const LithoAbbePlan& p = *plan;
+  const AbbeLayout l = abbe_layout(p);
+  if ((int64_t)ws_bytes < l.total) return LITHO_E_WORKSPACE;
+  const char* b = static_cast<const char*>(blob);
+  const LithoJob* jobs = reinterpret_cast<const LithoJob*>(b + p.off_jobs);
+  const LithoItem* items = reinterpret_cast<const LithoItem*>(b + p.off_items);
+  const int32_t* out_items = reinterpret_cast<const int32_t*>(b + p.off_out_items);
+  float* partial = reinterpret_cast<float*>(static_cast<char*>(ws) + l.partial);
+  const int G = 4 * p.h + 1;
+  if (p.L == 32) {
+    const size_t sm = (size_t)kCoarseWarps * 32 * 33 * sizeof(float2);
+    cudaFuncSetAttribute(k_coarse32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_coarse32<<<p.n_items, kCoarseWarps * 32, sm, s>>>(items, jobs, static_cast<const float2*>(table), p.h,
+                                                        p.ncomp_max, static_cast<const float2*>(mb), p.bm, partial);
+  } else {
+    const size_t sm = coarse64_smem();
+    cudaFuncSetAttribute(k_coarse64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_coarse64<<<p.n_items, kCoarse64Warps * 32, sm, s>>>(items, jobs, static_cast<const float2*>(table), p.h,
+                                                          p.ncomp_max, static_cast<const float2*>(mb), p.bm, partial);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return (int)e;
+  const size_t sm_red = (size_t)p.L * p.L * 4 + (size_t)p.L * G * 8 + (size_t)p.L * 8;
+  cudaFuncSetAttribute(k_coarse_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_red);
+  k_coarse_reduce<<<p.n_out, 1024, sm_red, s>>>(out_items, partial, p.L, p.h, static_cast<float2*>(bbox_out));
+  e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
 }
 
 extern "C" int litho_abbe_status(const LithoAbbePlan* plan, const void* ws, cudaStream_t s) {

@@ -1,0 +1,614 @@
+// Inverse lithography on the GPU: the SOCS adjoint and the relaxed-resist
+// objective, as composable device stages.
+//
+// Reference: opc/ilt.py — socs_fields (:208-232), socs_gradient (:235-266),
+// _blur (:274-289), _Objective.__call__ (:311-360), _mask_of (:368-378),
+// _grad_theta (:381-389) and the Adam update of run_ilt (:582-591).
+//
+// The adjoint, with E_k = F^-1(phi_k F(m)) and sensitivity G = dJ/dI,
+//     grad(x) = 2 Re sum_k lambda_k F^-1( conj(phi_k) F(G E_k) )(x),
+// needs F(G E_k) only on the kernel band |f| <= h, where it is the circular
+// convolution of E_k's band spectrum (|h'| <= h) with G's spectrum on
+// |g| <= 2h. On a 64 x 64 grid that convolution is exact, so per kernel:
+//     e_k = IFFT64(phi_k M),  g = IFFT64(G band),  Y_k = FFT64(e_k g) / 64^2,
+//     A(f) += lambda_k conj(phi_k(f)) Y_k(f)     for |f| <= h,
+// and grad(x) = sum_f H(f) exp(2 pi i f.x / N) with H(f) = A(f) + conj(A(-f)),
+// one band-limited synthesis (csrc/abbe.cu k_synth). Scale: M = F(m) / N^2,
+// G band = F(G) / N^2, as the band-spectrum stage produces them.
+#include "common.cuh"
+
+namespace litho {
+
+cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_per_clip, int n, int bm,
+                                float2* out, float scale, const float2* tw_inv, int num_sms, cudaStream_t st,
+                                int* status);
+cudaError_t launch_synth_real(const float2* box, int G, int n, int n_fields, const float2* tw, const LithoNorm* norm,
+                              float* out, float* blockmax, cudaStream_t s);
+int synth_blocks_for(int n);
+
+// ---------------------------------------------------------------------------
+// g_L(u, v) = sum_{|g| <= 2h} Gb(g) w64^(g.(u, v)), one block per clip.
+// Gb: (4h+1)^2 box [gy][gx]. Output [clip][v][u] complex.
+// ---------------------------------------------------------------------------
+__global__ void k_gl64(const float2* __restrict__ Gb, int h, float2* __restrict__ gl) {
+  __shared__ float2 T[64 * 61];   // [v][gx], gx index < 4h+1 <= 61
+  __shared__ float2 tw[64];
+  const int c = blockIdx.x, G = 4 * h + 1, g0 = 2 * h;
+  for (int t = threadIdx.x; t < 64; t += blockDim.x) {
+    double s, co;
+    sincospi(2.0 * t / 64.0, &s, &co);
+    tw[t] = make_float2((float)co, (float)s);
+  }
+  __syncthreads();
+  const float2* B = Gb + (size_t)c * G * G;
+  for (int id = threadIdx.x; id < 64 * G; id += blockDim.x) {
+    const int v = id / G, gx = id % G;
+    float2 acc = make_float2(0.f, 0.f);
+    for (int gy = 0; gy < G; ++gy) acc = cadd(acc, cmul(B[gy * G + gx], tw[((gy - g0) * v) & 63]));
+    T[v * 61 + gx] = acc;
+  }
+  __syncthreads();
+  float2* out = gl + (size_t)c * 4096;
+  for (int id = threadIdx.x; id < 4096; id += blockDim.x) {
+    const int v = id >> 6, u = id & 63;
+    float2 acc = make_float2(0.f, 0.f);
+    for (int gx = 0; gx < G; ++gx) acc = cadd(acc, cmul(T[v * 61 + gx], tw[((gx - g0) * u) & 63]));
+    out[id] = acc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Coarse adjoint, one warp per (clip, kernel) job; h <= 15.
+// ---------------------------------------------------------------------------
+constexpr int kAdjWarps = 2;
+constexpr int kAdjHMax = 15;
+constexpr int kAdjLd = 65;
+
+// 64-point forward DFT outputs X(k), k in [-h, h], of a full sequence held as
+// even (ev[i] = x(2i)) and odd (od[i] = x(2i+1)) halves:
+//   X(k) = FFT32(ev)(k mod 32) + w64^(-k) FFT32(od)(k mod 32).
+__device__ __forceinline__ float2 combine64(const float2 (&ev)[32], const float2 (&od)[32], int kk) {
+  // kk compile-time in [-15, 15]
+  return cadd(ev[kk & 31], twiddle64<-1>(od[kk & 31], kk & 63));
+}
+
+__global__ void __launch_bounds__(kAdjWarps * 32)
+k_coarse64_adjoint(const LithoItem* __restrict__ items, const LithoJob* __restrict__ jobs,
+                   const float2* __restrict__ table, int h, const float2* __restrict__ Mb,
+                   const float2* __restrict__ etab, const float2* __restrict__ gl, float2* __restrict__ partial) {
+  extern __shared__ float2 adj_sm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int side = 2 * h + 1, npts = side * side;
+  const int per_warp = 31 * kAdjLd + 31 * 32;
+  float2* T = adj_sm + warp * per_warp;          // [kx or fx][v], 31 x 65
+  float2* Aw = T + 31 * kAdjLd;                   // [fx][fy] accumulator, 31 x 32
+  const LithoItem it = items[blockIdx.x];
+  const int dx = lane - h;
+  const bool col_live = lane < side;
+  for (int i = lane; i < 31 * 32; i += 32) Aw[i] = make_float2(0.f, 0.f);
+  __syncwarp();
+  const float inv = 1.0f / 4096.0f;
+  for (int j = it.job_begin + warp; j < it.job_end; j += kAdjWarps) {
+    const LithoJob job = jobs[j];
+    const float lam = (float)job.weight;
+    const float2* tp = table + (size_t)job.tab * npts;
+    const float2* m = Mb + (size_t)job.clip * npts;
+    const float2* g = gl + (size_t)job.clip * 4096;
+    float2 a[32], b[32];
+    // pass 1: columns kx = dx of E = phi M, inverse over ky
+#pragma unroll
+    for (int i = 0; i < 32; ++i) a[i] = make_float2(0.f, 0.f);
+    if (col_live) {
+#pragma unroll
+      for (int d = -kAdjHMax; d <= kAdjHMax; ++d)
+        if (d >= -h && d <= h) {
+          const int p = (d + h) * side + (dx + h);
+          a[d & 31] = etab ? __ldg(etab + (size_t)j * npts + p) : cmul(__ldg(tp + p), __ldg(m + p));
+        }
+    }
+    {
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        const int d = i < 16 ? i : i - 32;
+        b[i] = twiddle64<+1>(a[i], d & 63);
+      }
+      fft_reg<32, +1>(a);
+      fft_reg<32, +1>(b);
+    }
+    __syncwarp();
+    if (col_live) {
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        T[lane * kAdjLd + 2 * i] = a[i];
+        T[lane * kAdjLd + 2 * i + 1] = b[i];
+      }
+    }
+    __syncwarp();
+    // pass 2: rows v = lane, lane + 32: e(u, v) over kx, times g(u, v), then
+    // the forward DFT over u restricted to fx in [-h, h]; in place in T[., v].
+#pragma unroll 1
+    for (int half = 0; half < 2; ++half) {
+      const int v = lane + 32 * half;
+#pragma unroll
+      for (int i = 0; i < 32; ++i) a[i] = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int d = -kAdjHMax; d <= kAdjHMax; ++d)
+        if (d >= -h && d <= h) a[d & 31] = T[(d + h) * kAdjLd + v];
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        const int d = i < 16 ? i : i - 32;
+        b[i] = twiddle64<+1>(a[i], d & 63);
+      }
+      fft_reg<32, +1>(a);   // e(2u', v)
+      fft_reg<32, +1>(b);   // e(2u'+1, v)
+      const float2* gr = g + (size_t)v * 64;
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        a[i] = cmul(a[i], __ldg(gr + 2 * i));
+        b[i] = cmul(b[i], __ldg(gr + 2 * i + 1));
+      }
+      fft_reg<32, -1>(a);
+      fft_reg<32, -1>(b);
+#pragma unroll
+      for (int f = -kAdjHMax; f <= kAdjHMax; ++f)
+        if (f >= -h && f <= h) T[(f + h) * kAdjLd + v] = combine64(a, b, f);
+    }
+    __syncwarp();
+    // pass 3: lane = fx, forward over v restricted to fy in [-h, h]
+    if (col_live) {
+      const float2* tr = T + lane * kAdjLd;
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        a[i] = tr[2 * i];
+        b[i] = tr[2 * i + 1];
+      }
+      fft_reg<32, -1>(a);
+      fft_reg<32, -1>(b);
+      float2* arow = Aw + lane * 32;
+#pragma unroll
+      for (int f = -kAdjHMax; f <= kAdjHMax; ++f)
+        if (f >= -h && f <= h) {
+          const float2 y = cscale(combine64(a, b, f), inv);
+          const float2 ph = __ldg(tp + (f + h) * side + lane);   // phi(fx = dx, fy = f)
+          const float2 acc = arow[f + h];
+          arow[f + h] = cadd(acc, cscale(cmulc(y, ph), lam));    // lambda conj(phi) Y
+        }
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  // fixed-order sum over the block's warps -> partial[item][(fy+h) side + fx+h]
+  float2* dst = partial + (size_t)blockIdx.x * npts;
+  for (int id = threadIdx.x; id < npts; id += blockDim.x) {
+    const int fy = id / side, fx = id % side;
+    float2 s = make_float2(0.f, 0.f);
+    for (int wp = 0; wp < kAdjWarps; ++wp) s = cadd(s, adj_sm[wp * per_warp + 31 * kAdjLd + fx * 32 + fy]);
+    dst[id] = s;
+  }
+}
+
+// Per clip: A = sum of its items' partials (item order); H(f) = A(f) + conj(A(-f)).
+__global__ void k_adjoint_reduce(const int32_t* __restrict__ out_items, const float2* __restrict__ partial, int h,
+                                 float2* __restrict__ Hbox) {
+  const int c = blockIdx.x, side = 2 * h + 1, npts = side * side;
+  const int i0 = out_items[c], i1 = out_items[c + 1];
+  for (int id = threadIdx.x; id < npts; id += blockDim.x) {
+    const int fy = id / side, fx = id % side;
+    const int mid = (2 * h - fy) * side + (2 * h - fx);  // -f
+    float2 s = make_float2(0.f, 0.f), t = make_float2(0.f, 0.f);
+    for (int i = i0; i < i1; ++i) {
+      s = cadd(s, partial[(size_t)i * npts + id]);
+      t = cadd(t, partial[(size_t)i * npts + mid]);
+    }
+    Hbox[(size_t)c * npts + id] = cadd(s, cconj(t));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Complex band-limited synthesis: out(x, y) = sum_{|g| <= h} box(g) w^(g.(x, y)).
+// ---------------------------------------------------------------------------
+constexpr int kCsRows = 8, kCsCols = 2;
+
+__global__ void __launch_bounds__(256)
+k_synth_complex(const float2* __restrict__ box, int h, int n, const float2* __restrict__ tw_inv,
+                float2* __restrict__ out) {
+  extern __shared__ float2 cs_sm[];
+  const int side = 2 * h + 1;
+  float2* tw = cs_sm;
+  float2* C = cs_sm + n;          // [kCsRows][side]
+  const int f = blockIdx.y, y0 = blockIdx.x * kCsRows;
+  const bool pow2 = (n & (n - 1)) == 0;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) tw[j] = tw_inv[j];
+  __syncthreads();
+  const float2* B = box + (size_t)f * side * side;
+  for (int id = threadIdx.x; id < kCsRows * side; id += blockDim.x) {
+    const int r = id / side, gx = id % side, y = y0 + r;
+    float2 acc = make_float2(0.f, 0.f);
+    if (y < n)
+      for (int gy = -h; gy <= h; ++gy) {
+        const int e = gy * y;
+        acc = cadd(acc, cmul(B[(gy + h) * side + gx], tw[pow2 ? (e & (n - 1)) : ((e % n) + n) % n]));
+      }
+    C[id] = acc;
+  }
+  __syncthreads();
+  for (int xb = threadIdx.x; xb < n; xb += blockDim.x * kCsCols) {
+    float2 acc[kCsRows][kCsCols];
+#pragma unroll
+    for (int r = 0; r < kCsRows; ++r)
+#pragma unroll
+      for (int j = 0; j < kCsCols; ++j) acc[r][j] = make_float2(0.f, 0.f);
+    for (int gx = -h; gx <= h; ++gx) {
+      float2 w[kCsCols];
+#pragma unroll
+      for (int j = 0; j < kCsCols; ++j) {
+        const int x = xb + j * blockDim.x, e = gx * x;
+        w[j] = x < n ? tw[pow2 ? (e & (n - 1)) : ((e % n) + n) % n] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int r = 0; r < kCsRows; ++r) {
+        const float2 c = C[r * side + gx + h];
+#pragma unroll
+        for (int j = 0; j < kCsCols; ++j) acc[r][j] = cadd(acc[r][j], cmul(c, w[j]));
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < kCsRows; ++r) {
+      const int y = y0 + r;
+      if (y >= n) break;
+#pragma unroll
+      for (int j = 0; j < kCsCols; ++j) {
+        const int x = xb + j * blockDim.x;
+        if (x < n) out[((size_t)f * n + y) * n + x] = acc[r][j];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise stages (n_fields x N x N, row-major).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float sigmoid_clipped(float s) {
+  s = fminf(fmaxf(s, -60.f), 60.f);
+  return 1.0f / (1.0f + expf(-s));
+}
+
+// Relaxed resist objective (opc/ilt.py:313-336), after the optional blur of
+// the image: fld = scale * img; signed = sign (fld - level);
+// z = sigmoid(a signed); resid = z - target; dfield = sign (2/npix) resid a z (1 - z).
+__global__ void k_ilt_objective(const float* __restrict__ img, const float* __restrict__ target, long long npix,
+                                float scale, float level, float sign, float a, float inv_npix2,
+                                float* __restrict__ dfield, float* __restrict__ signed_out,
+                                double* __restrict__ cost_part, unsigned int* __restrict__ perr_part) {
+  __shared__ double sc[32];
+  __shared__ unsigned int sp[32];
+  double cost = 0.0;
+  unsigned int perr = 0;
+  const long long base = (long long)blockIdx.y * npix;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < npix;
+       k += (long long)gridDim.x * blockDim.x) {
+    const long long i = base + k;
+    const float fld = img[i] * scale;
+    const float s = sign * (fld - level);
+    const float z = sigmoid_clipped(a * s);
+    const float t = target[i];
+    const float r = z - t;
+    cost += (double)r * (double)r;
+    dfield[i] = sign * (inv_npix2 * r * (a * z * (1.0f - z)));
+    if (signed_out) signed_out[i] = s;
+    perr += ((s > 0.f) != (t > 0.5f)) ? 1u : 0u;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    cost += __shfl_xor_sync(0xffffffffu, cost, o);
+    perr += __shfl_xor_sync(0xffffffffu, perr, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sc[threadIdx.x >> 5] = cost;
+    sp[threadIdx.x >> 5] = perr;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double c = 0.0;
+    unsigned int p = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      c += sc[w];
+      p += sp[w];
+    }
+    cost_part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = c;
+    perr_part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = p;
+  }
+}
+
+// TV and discreteness penalties (opc/ilt.py:339-357) on the mask, periodic
+// neighbours, added to grad; their costs to cost_part (per block).
+__global__ void k_ilt_penalties(const float* __restrict__ mask, int n_fields, int n, float w_tv, float w_disc,
+                                float inv_npix, float* __restrict__ grad, double* __restrict__ cost_part) {
+  __shared__ double sc[32];
+  double cost = 0.0;
+  const long long npix = (long long)n * n;
+  const long long f = blockIdx.y;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < npix;
+       k += (long long)gridDim.x * blockDim.x) {
+    const long long i = f * npix + k;
+    const int rem = (int)k, y = rem / n, x = rem % n;
+    const float* m = mask + f * npix;
+    const float c = m[rem];
+    float g = 0.f;
+    if (w_tv > 0.f) {
+      const float up = m[((y + n - 1) % n) * n + x], dn = m[((y + 1) % n) * n + x];
+      const float lf = m[y * n + (x + n - 1) % n], rt = m[y * n + (x + 1) % n];
+      const float lap = up + dn + lf + rt - 4.f * c;
+      const float gx = c - lf, gy = c - up;
+      cost += (double)w_tv * ((double)gx * gx + (double)gy * gy) * inv_npix;
+      g += w_tv * (-2.f * inv_npix) * lap;
+    }
+    if (w_disc > 0.f) {
+      cost += (double)w_disc * (double)c * (1.0 - (double)c) * inv_npix;
+      g += w_disc * (1.f - 2.f * c) * inv_npix;
+    }
+    grad[i] += g;
+  }
+  for (int o = 16; o > 0; o >>= 1) cost += __shfl_xor_sync(0xffffffffu, cost, o);
+  if ((threadIdx.x & 31) == 0) sc[threadIdx.x >> 5] = cost;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double c = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) c += sc[w];
+    cost_part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = c;
+  }
+}
+
+// m = sigmoid(clip(beta * field, +-60))  (opc/ilt.py:368-378)
+__global__ void k_ilt_mask(const float* __restrict__ field, long long total, float beta, float* __restrict__ mask) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x)
+    mask[i] = sigmoid_clipped(beta * field[i]);
+}
+
+// q = grad_m * beta * m (1 - m)  (opc/ilt.py:381-389, before its blur)
+__global__ void k_ilt_theta_grad(const float* __restrict__ grad_m, const float* __restrict__ mask, long long total,
+                                 float beta, float* __restrict__ q) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float m = mask[i];
+    q[i] = grad_m[i] * (beta * m * (1.f - m));
+  }
+}
+
+// Adam (opc/ilt.py:582-591) with bias corrections c1 = 1 - b1^t, c2 = 1 - b2^t.
+__global__ void k_ilt_adam(const float* __restrict__ g, long long total, float step, float b1, float b2, float eps,
+                           float c1, float c2, float* __restrict__ theta, float* __restrict__ m1,
+                           float* __restrict__ m2) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float a = b1 * m1[i] + (1.f - b1) * gi;
+    const float v = b2 * m2[i] + (1.f - b2) * gi * gi;
+    m1[i] = a;
+    m2[i] = v;
+    theta[i] -= step * (a / c1) / (sqrtf(v / c2) + eps);
+  }
+}
+
+// One axis of scipy.ndimage.gaussian_filter (mode 'reflect', i.e. the edge
+// sample repeated: ... b a | a b ... ), weights w[0..2r] (host-built, FP64
+// normalised). axis 0: along y (rows), axis 1: along x.
+__device__ __forceinline__ int reflect_idx(int j, int n) {
+  const int p = 2 * n;
+  j %= p;
+  if (j < 0) j += p;
+  return j < n ? j : p - 1 - j;
+}
+
+__global__ void k_blur_axis(const float* __restrict__ in, float* __restrict__ out, int n_fields, int n,
+                            const float* __restrict__ w, int r, int axis) {
+  const long long total = (long long)n_fields * n * n;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long f = i / ((long long)n * n);
+    const int rem = (int)(i - f * n * n), y = rem / n, x = rem % n;
+    const float* src = in + f * (long long)n * n;
+    float acc = 0.f;
+    if (axis == 0) {
+      for (int k = -r; k <= r; ++k) acc = fmaf(w[k + r], src[reflect_idx(y + k, n) * n + x], acc);
+    } else {
+      for (int k = -r; k <= r; ++k) acc = fmaf(w[k + r], src[y * n + reflect_idx(x + k, n)], acc);
+    }
+    out[i] = acc;
+  }
+}
+
+static int grid_for(long long total, int threads, int cap) {
+  long long b = (total + threads - 1) / threads;
+  if (b > cap) b = cap;
+  return (int)(b < 1 ? 1 : b);
+}
+
+static int sms_here() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+}  // namespace litho
+
+using namespace litho;
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+static int64_t band_ws(int n_fields, int n, int bm) {
+  return align16(16) + align16((int64_t)n * 8) + align16((int64_t)n_fields * (2 * bm + 1) * n * 8);
+}
+
+extern "C" int litho_band_spectrum_workspace(int n_fields, int n, int bm, size_t* bytes) {
+  if (!bytes) return LITHO_E_NULL;
+  if (n_fields < 1 || n < 2 || bm < 0) return LITHO_E_SIZE;
+  *bytes = (size_t)band_ws(n_fields, n, bm);
+  return LITHO_OK;
+}
+
+extern "C" int litho_band_spectrum(const void* in, int is_complex, int n_fields, int n, int bm, float scale,
+                                   void* box_out, void* ws, size_t ws_bytes, cudaStream_t s) {
+  if (!in || !box_out || !ws) return LITHO_E_NULL;
+  if (n_fields < 1 || n < 2 || bm < 0) return LITHO_E_SIZE;
+  if ((int64_t)ws_bytes < band_ws(n_fields, n, bm)) return LITHO_E_WORKSPACE;
+  if (((uintptr_t)ws & 15) || ((uintptr_t)in & 7)) return LITHO_E_ALIGN;
+  char* w = static_cast<char*>(ws);
+  int* status = reinterpret_cast<int*>(w);
+  float2* tw = reinterpret_cast<float2*>(w + align16(16));
+  float2* u1 = reinterpret_cast<float2*>(w + align16(16) + align16((int64_t)n * 8));
+  const int Bm = 2 * bm + 1;
+  cudaError_t e = cudaMemsetAsync(status, 0, sizeof(int), s);
+  if (e != cudaSuccess) return (int)e;
+  k_twiddle_table<<<(n + 255) / 256, 256, 0, s>>>(tw, n, +1);
+  e = launch_row_band_dft(in, is_complex != 0, n_fields * n, n, n, bm, u1, 1.0f, tw, sms_here(), s, status);
+  if (e != cudaSuccess) return (int)e;
+  e = launch_row_band_dft(u1, true, n_fields * Bm, Bm, n, bm, static_cast<float2*>(box_out), scale, tw, sms_here(), s,
+                          status);
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+extern "C" int litho_band_synthesis_workspace(int n_fields, int n, size_t* bytes) {
+  if (!bytes) return LITHO_E_NULL;
+  if (n_fields < 1 || n < 2) return LITHO_E_SIZE;
+  *bytes = (size_t)(align16((int64_t)n * 8) + align16((int64_t)n_fields * synth_blocks_for(n) * 4));
+  return LITHO_OK;
+}
+
+extern "C" int litho_band_synthesis(const void* box, int n_fields, int n, int h, int complex_out, void* out,
+                                   void* ws, size_t ws_bytes, cudaStream_t s) {
+  if (!box || !out || !ws) return LITHO_E_NULL;
+  if (n_fields < 1 || n < 2 || h < 0) return LITHO_E_SIZE;
+  size_t need = 0;
+  litho_band_synthesis_workspace(n_fields, n, &need);
+  if (ws_bytes < need) return LITHO_E_WORKSPACE;
+  float2* tw = static_cast<float2*>(ws);
+  float* blockmax = reinterpret_cast<float*>(static_cast<char*>(ws) + align16((int64_t)n * 8));
+  k_twiddle_table<<<(n + 255) / 256, 256, 0, s>>>(tw, n, +1);
+  cudaError_t e;
+  if (complex_out) {
+    const int side = 2 * h + 1;
+    const size_t sm = (size_t)n * 8 + (size_t)kCsRows * side * 8;
+    cudaFuncSetAttribute(k_synth_complex, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    dim3 g((n + kCsRows - 1) / kCsRows, n_fields);
+    k_synth_complex<<<g, 256, sm, s>>>(static_cast<const float2*>(box), h, n, tw, static_cast<float2*>(out));
+    e = cudaGetLastError();
+  } else {
+    e = launch_synth_real(static_cast<const float2*>(box), 2 * h + 1, n, n_fields, tw, nullptr,
+                          static_cast<float*>(out), blockmax, s);
+  }
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+static int64_t adj_ws(int n_clips, int n_items, int h) {
+  const int npts = (2 * h + 1) * (2 * h + 1);
+  return align16((int64_t)n_clips * 4096 * 8) + align16((int64_t)n_items * npts * 8);
+}
+
+extern "C" int litho_socs_adjoint_workspace(int n_clips, int n_items, int h, size_t* bytes) {
+  if (!bytes) return LITHO_E_NULL;
+  if (n_clips < 1 || n_items < 1 || h < 0 || h > kAdjHMax) return LITHO_E_SIZE;
+  *bytes = (size_t)adj_ws(n_clips, n_items, h);
+  return LITHO_OK;
+}
+
+// Band of the SOCS adjoint: see the file comment. The job list is the SOCS
+// forward's (one job per clip x kernel: weight lambda_k, table slot k, clip c),
+// grouped per clip by items/out_items as in LithoAbbePlan.
+extern "C" int litho_socs_adjoint(const LithoAbbePlan* plan, const void* blob, const void* table, const void* mask_box,
+                                  const void* field_box, const void* sens_box, void* grad_box_out, void* ws,
+                                  size_t ws_bytes, cudaStream_t s) {
+  if (!plan || !blob || !table || !sens_box || !grad_box_out || !ws) return LITHO_E_NULL;
+  if (!mask_box && !field_box) return LITHO_E_NULL;
+  const LithoAbbePlan& p = *plan;
+  if (p.h < 0 || p.h > kAdjHMax || p.n_clips < 1 || p.n_items < 1 || p.bm != p.h) return LITHO_E_SIZE;
+  if ((int64_t)ws_bytes < adj_ws(p.n_clips, p.n_items, p.h)) return LITHO_E_WORKSPACE;
+  const char* b = static_cast<const char*>(blob);
+  const LithoJob* jobs = reinterpret_cast<const LithoJob*>(b + p.off_jobs);
+  const LithoItem* items = reinterpret_cast<const LithoItem*>(b + p.off_items);
+  const int32_t* out_items = reinterpret_cast<const int32_t*>(b + p.off_out_items);
+  float2* gl = static_cast<float2*>(ws);
+  float2* part = reinterpret_cast<float2*>(static_cast<char*>(ws) + align16((int64_t)p.n_clips * 4096 * 8));
+  k_gl64<<<p.n_clips, 256, 0, s>>>(static_cast<const float2*>(sens_box), p.h, gl);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return (int)e;
+  const size_t sm = (size_t)kAdjWarps * (31 * kAdjLd + 31 * 32) * sizeof(float2);
+  cudaFuncSetAttribute(k_coarse64_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_coarse64_adjoint<<<p.n_items, kAdjWarps * 32, sm, s>>>(items, jobs, static_cast<const float2*>(table), p.h,
+                                                            static_cast<const float2*>(mask_box),
+                                                            static_cast<const float2*>(field_box), gl, part);
+  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  k_adjoint_reduce<<<p.n_clips, 256, 0, s>>>(out_items, part, p.h, static_cast<float2*>(grad_box_out));
+  e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+extern "C" int litho_ilt_objective(const float* img, const float* target, int n_fields, int n, float scale,
+                                   float level, float sign, float steepness_a, float* dfield, float* signed_out,
+                                   double* cost_part, unsigned int* perr_part, int n_part, cudaStream_t s) {
+  if (!img || !target || !dfield || !cost_part || !perr_part) return LITHO_E_NULL;
+  if (n_fields < 1 || n < 1 || n_part < 1) return LITHO_E_SIZE;
+  const double npix = (double)n * n;
+  dim3 g(n_part, n_fields);
+  k_ilt_objective<<<g, 256, 0, s>>>(img, target, (long long)n * n, scale, level, sign, steepness_a,
+                                    (float)(2.0 / npix), dfield, signed_out, cost_part, perr_part);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+extern "C" int litho_ilt_penalties(const float* mask, int n_fields, int n, float w_tv, float w_disc, float* grad,
+                                   double* cost_part, int n_part, cudaStream_t s) {
+  if (!mask || !grad || !cost_part) return LITHO_E_NULL;
+  if (n_fields < 1 || n < 1 || n_part < 1) return LITHO_E_SIZE;
+  dim3 g(n_part, n_fields);
+  k_ilt_penalties<<<g, 256, 0, s>>>(mask, n_fields, n, w_tv, w_disc, (float)(1.0 / ((double)n * n)), grad,
+                                    cost_part);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+extern "C" int litho_ilt_mask(const float* field, long long count, float beta, float* mask, cudaStream_t s) {
+  if (!field || !mask) return LITHO_E_NULL;
+  if (count < 0) return LITHO_E_SIZE;
+  k_ilt_mask<<<grid_for(count, 256, sms_here() * 16), 256, 0, s>>>(field, count, beta, mask);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+extern "C" int litho_ilt_theta_grad(const float* grad_m, const float* mask, long long count, float beta, float* q,
+                                    cudaStream_t s) {
+  if (!grad_m || !mask || !q) return LITHO_E_NULL;
+  if (count < 0) return LITHO_E_SIZE;
+  k_ilt_theta_grad<<<grid_for(count, 256, sms_here() * 16), 256, 0, s>>>(grad_m, mask, count, beta, q);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+extern "C" int litho_ilt_adam(const float* g, long long count, float step, float b1, float b2, float eps, int it,
+                              float* theta, float* m1, float* m2, cudaStream_t s) {
+  if (!g || !theta || !m1 || !m2) return LITHO_E_NULL;
+  if (count < 0 || it < 1) return LITHO_E_SIZE;
+  const float c1 = (float)(1.0 - pow((double)b1, it)), c2 = (float)(1.0 - pow((double)b2, it));
+  k_ilt_adam<<<grid_for(count, 256, sms_here() * 16), 256, 0, s>>>(g, count, step, b1, b2, eps, c1, c2, theta, m1,
+                                                                   m2);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+extern "C" int litho_gaussian_blur(const float* in, float* out, float* tmp, int n_fields, int n,
+                                   const float* weights_dev, int radius, cudaStream_t s) {
+  if (!in || !out || !tmp || !weights_dev) return LITHO_E_NULL;
+  if (n_fields < 1 || n < 1 || radius < 0) return LITHO_E_SIZE;
+  const long long total = (long long)n_fields * n * n;
+  const int g = grid_for(total, 256, sms_here() * 16);
+  k_blur_axis<<<g, 256, 0, s>>>(in, tmp, n_fields, n, weights_dev, radius, 0);
+  k_blur_axis<<<g, 256, 0, s>>>(tmp, out, n_fields, n, weights_dev, radius, 1);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}

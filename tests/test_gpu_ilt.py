@@ -1,0 +1,161 @@
+"""ILT forward, adjoint and objective on the GPU against the reference."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import load_golden, ns_grid, ns_optics
+from oracle import litho_oracle as O
+
+pytestmark = pytest.mark.gpu
+TOL_I = 1e-5      # intensities
+TOL_G = 1e-4      # gradients: FP32 engine vs FP64 reference, relative to max |grad|
+
+
+@pytest.fixture(scope="module")
+def lb():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import lithobat_b200
+    return lithobat_b200
+
+
+def _optics(lb, od):
+    od = dict(od)
+    od["zernike_coeffs"] = {int(k): v for k, v in (od.get("zernike_coeffs") or {}).items()}
+    keep = {k: od[k] for k in lb.OpticsConfig.__dataclass_fields__ if k in od}
+    return lb.OpticsConfig(**keep)
+
+
+def rel(a, b):
+    return float(np.abs(np.asarray(a, np.float64) - b).max() / np.abs(b).max())
+
+
+@pytest.fixture(scope="module")
+def small(lb):
+    a, od, gd = load_golden("ilt_small")
+    k = lb.SOCSKernels.build(_optics(lb, od), lb.GridConfig(**gd), tol=1e-6)
+    np.testing.assert_allclose(k.weights, a["weights"], rtol=1e-8)
+    return a, k
+
+
+def test_socs_fields_intensity(lb, small):
+    from lithobat_b200 import ilt
+    a, k = small
+    fields, inten = ilt.socs_fields(k, a["mask"])
+    assert fields.shape == (len(k), 32, 32)
+    assert rel(inten, a["intensity"]) <= TOL_I
+    # the fields' intensities sum to the image
+    summed = np.tensordot(k.weights, np.abs(np.asarray(fields)) ** 2, axes=1)
+    assert rel(summed, a["intensity"]) <= TOL_I
+
+
+def test_socs_adjoint_matches_reference(lb, small):
+    from lithobat_b200 import ilt
+    a, k = small
+    fields, _ = ilt.socs_fields(k, a["mask"])
+    g = ilt.socs_gradient(k, fields, a["sens"])
+    assert rel(g, a["grad"]) <= TOL_G
+    # a plain array of fields takes the general route
+    g2 = ilt.socs_gradient(k, np.asarray(fields).copy(), a["sens"])
+    assert rel(g2, a["grad"]) <= TOL_G
+
+
+def test_full_objective_with_blur_and_penalties(lb, small):
+    from lithobat_b200 import ilt
+    a, k = small
+    obj = ilt.Objective(k, a["target3"], 1.7, 0.3, 1.5, 1.0, 12.0, 1e-3, 1e-3)
+    cost, grad, signed, perr = obj(a["mask3"])
+    assert cost == pytest.approx(float(a["cost"]), rel=1e-5)
+    assert rel(signed, a["signed"]) <= TOL_I
+    assert abs(perr - int(a["perr"])) <= 2
+    assert rel(grad, a["grad_obj"]) <= TOL_G
+
+
+def test_dark_tone_objective(lb, small):
+    from lithobat_b200 import ilt
+    a, k = small
+    obj = ilt.Objective(k, a["target3"], 2.0, 0.3, 0.0, -1.0, 20.0)
+    cost, grad, signed, perr = obj(a["mask3"])
+    assert cost == pytest.approx(float(a["cost0"]), rel=1e-5)
+    assert rel(grad, a["grad_obj0"]) <= TOL_G
+    assert abs(perr - int(a["perr0"])) <= 2
+
+
+def test_parameterisation(lb, small):
+    from lithobat_b200 import ilt
+    a, _ = small
+    m = ilt.mask_of(a["theta"], 6.0, 2.0)
+    np.testing.assert_allclose(m, a["mask_of"], atol=2e-6)
+    gt = ilt.grad_theta(a["grad_obj"], a["mask_of"], 6.0, 2.0)
+    assert rel(gt, a["grad_theta"]) <= 1e-5
+
+
+def test_mid_size_k24_objective(lb):
+    """The fourth workload's optics and objective at 128^2, K = 24, a = 50."""
+    from lithobat_b200 import ilt
+    a, od, gd = load_golden("ilt_imm_128_k24")
+    k = lb.SOCSKernels.build(_optics(lb, od), lb.GridConfig(**gd), tol=0.0, max_kernels=24)
+    m = O.mask_of(a["theta"], float(a["beta"]), 0.0)
+    obj = ilt.Objective(k, a["target"].astype(np.float64), 1.0 / k.clear, 0.3, 0.0, 1.0, 15.0)
+    cost, grad, signed, perr = obj(m)
+    assert cost == pytest.approx(float(a["cost"]), rel=1e-5)
+    assert rel(grad, a["grad"]) <= TOL_G
+    assert abs(perr - int(a["perr"])) <= 4
+
+
+def test_adjoint_against_finite_differences_of_the_reference(lb, small):
+    """The GPU gradient against central differences of the FP64 objective."""
+    from lithobat_b200 import ilt
+    a, k = small
+    ref = O.socs_build(ns_optics(load_golden("ilt_small")[1]), ns_grid(load_golden("ilt_small")[2]), tol=1e-6)
+    obj = ilt.Objective(k, a["target3"], 1.7, 0.3, 1.5, 1.0, 12.0, 1e-3, 1e-3)
+    _, grad, _, _ = obj(a["mask3"])
+    rng = np.random.default_rng(8)
+    h = 1e-6
+    for i, j in rng.integers(0, 32, size=(8, 2)):
+        up, dn = a["mask3"].copy(), a["mask3"].copy()
+        up[i, j] += h
+        dn[i, j] -= h
+        f = lambda m: O.objective(ref, a["target3"], m, 1.7, 0.3, 1.5, 1.0, 12.0, 1e-3, 1e-3)[0]  # noqa: E731
+        fd = (f(up) - f(dn)) / (2 * h)
+        assert grad[i, j] == pytest.approx(fd, rel=1e-3, abs=1e-4 * np.abs(grad).max())
+
+
+def test_autograd_function(lb, small):
+    import torch
+    from lithobat_b200 import ilt
+    a, k = small
+    m = torch.tensor(np.stack([a["mask"], a["mask3"]]), dtype=torch.float32, device="cuda", requires_grad=True)
+    sens = torch.tensor(np.stack([a["sens"], a["sens"] * 0.5]), dtype=torch.float32, device="cuda")
+    img = ilt.socs_image(m, k)
+    assert rel(img[0].detach().cpu().numpy(), a["intensity"]) <= TOL_I
+    (img * sens).sum().backward()
+    assert rel(m.grad[0].cpu().numpy(), a["grad"]) <= TOL_G
+
+
+def test_fused_steps_follow_the_reference_loop(lb):
+    """Three fused iterations against the oracle's Adam loop (opc/ilt.py:576-596)."""
+    from lithobat_b200 import ilt
+    a, od, gd = load_golden("ilt_imm_128_k24")
+    o, g = _optics(lb, od), lb.GridConfig(**gd)
+    k = lb.SOCSKernels.build(o, g, tol=0.0, max_kernels=24)
+    ref = O.socs_build(ns_optics(od), ns_grid(gd), tol=0.0, max_kernels=24)
+    tgt = a["target"].astype(np.float64)
+    theta = a["theta"] * 0.2
+    p = ilt.IltParams(scale=1.0 / k.clear, level=0.3, steepness=15.0, step=0.05, beta=4.0, growth=1.02)
+    b = ilt.IltBatch(k, tgt[None], theta[None], p)
+    th, m1, m2, beta = theta.copy(), np.zeros_like(theta), np.zeros_like(theta), 4.0
+    mk = O.mask_of(th, beta, 0.0)
+    _, gm, _, _ = O.objective(ref, tgt, mk, 1.0 / ref.clear, 0.3, 0.0, 1.0, 15.0)
+    for it in range(1, 4):
+        gt = O.grad_theta(gm, mk, beta, 0.0)
+        th, m1, m2 = O.adam_step(th, m1, m2, gt, it, 0.05)
+        beta *= 1.02
+        mk = O.mask_of(th, beta, 0.0)
+        cost, gm, _, _ = O.objective(ref, tgt, mk, 1.0 / ref.clear, 0.3, 0.0, 1.0, 15.0)
+        b.step()
+        assert float(b.cost[0]) == pytest.approx(cost, rel=1e-4)
+    assert np.abs(b.theta[0].cpu().numpy() - th).max() <= 1e-3 * np.abs(th).max()
