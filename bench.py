@@ -78,6 +78,145 @@ def masks_c3_device(torch, seed: int, count: int, dev):
     return torch.where(chrome > 0.5, absorber, one).contiguous()
 
 
+ILT_CLIPS = 16
+ILT_WORKLOAD = ("ILT 1024^2 @1 nm x16 clips, ArF-imm annular 0.5-0.8 (124 pts), SOCS K=24 (TCC Gram on "
+                "tensor cores, FP64 eig), resist level 0.3 a=50, clear normalisation, Adam")
+
+
+def ilt_optics():
+    import lithobat_b200 as lb
+    return lb.OpticsConfig(wavelength=193e-9, NA=1.35, n_immersion=1.44, source_type="annular",
+                           sigma_inner=0.5, sigma_outer=0.8, normalisation="clear")
+
+
+def ilt_inputs(seed: int, count: int):
+    from lithobat_b200 import patterns
+    rng = np.random.default_rng(seed)
+    targets = np.stack([patterns.manhattan_clip(rng, N, PX) for _ in range(count)]).astype(np.float32)
+    theta = (0.5 * rng.standard_normal((count, N, N))).astype(np.float32)
+    return targets, theta
+
+
+def bench_ilt(args, torch, dev, world, max_over_ranks, barrier) -> dict:
+    """ILT gradient steps/s: the fused band-limited iteration and the plain one."""
+    import lithobat_b200 as lb
+    from lithobat_b200 import ilt
+    rank = int(os.environ.get("RANK", "0"))
+    g = lb.GridConfig(n_pixels=N, pixel_size=PX)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lb.SOCSKernels.build(ilt_optics(), g, tol=0.0, max_kernels=24)  # warm
+    torch.cuda.synchronize()
+    e0.record()
+    k = lb.SOCSKernels.build(ilt_optics(), g, tol=0.0, max_kernels=24)
+    e1.record()
+    torch.cuda.synchronize()
+    build_ms = e0.elapsed_time(e1)
+    targets, theta = ilt_inputs(500 + rank, ILT_CLIPS)
+    params = ilt.IltParams(scale=1.0 / k.clear, level=0.3, steepness=15.0, step=0.4, beta=4.0, growth=1.0)
+    b = ilt.IltBatch(k, torch.from_numpy(targets).to(dev), torch.from_numpy(theta).to(dev), params)
+    for _ in range(args.warmup):
+        b.step(want_signed=False)
+    torch.cuda.synchronize()
+    barrier()
+    e0.record()
+    for _ in range(args.steps):
+        b.step(want_signed=False)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = world * ILT_CLIPS * args.steps / (ms / 1000.0)
+    # stage times of one step (events on the launching stream)
+    st = b.st
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(9)]
+    ev[0].record()
+    gt = st.grad_theta(b.grad_m, b.mask, b.beta, 0.0)
+    ev[1].record()
+    th = b.theta.clone(); m1 = b.m1.clone(); m2 = b.m2.clone()
+    nat_ = __import__("lithobat_b200._native", fromlist=["x"])
+    nat_.check("adam", st.L.litho_ilt_adam(gt.data_ptr(), gt.numel(), 0.4, 0.9, 0.999, 1e-8, 5, th.data_ptr(),
+                                           m1.data_ptr(), m2.data_ptr(), st.stream()))
+    mk = st.mask_of(th, b.beta, 0.0)
+    ev[2].record()
+    mbox = st.mask_box(mk)
+    ev[3].record()
+    raw = st.image(mbox)
+    ev[4].record()
+    dfield = torch.empty_like(raw)
+    cpart = torch.empty((ILT_CLIPS, 64), dtype=torch.float64, device=dev)
+    ppart = torch.empty((ILT_CLIPS, 64), dtype=torch.int32, device=dev)
+    nat_.check("obj", st.L.litho_ilt_objective(raw.data_ptr(), b.target.data_ptr(), ILT_CLIPS, N,
+                                               float(params.scale), 0.3, 1.0, 50.0, dfield.data_ptr(), None,
+                                               cpart.data_ptr(), ppart.data_ptr(), 64, st.stream()))
+    ev[5].record()
+    gbox = st.band(dfield, 2 * st.h, float(params.scale) / (N * N))
+    ev[6].record()
+    grad = st.adjoint(dfield, scale=float(params.scale), mbox=mbox)
+    ev[7].record()
+    torch.cuda.synchronize()
+    names = ["grad_theta", "adam_and_mask", "mask_band_spectrum", "coarse_image_and_synthesis", "objective",
+             "sensitivity_band_spectrum", "adjoint_band_spectrum+coarse+synthesis"]
+    stages = {nm: ev[i].elapsed_time(ev[i + 1]) for i, nm in enumerate(names)}
+    # plain engine, same inputs
+    pb = ilt.IltBatch(k, torch.from_numpy(targets).to(dev), torch.from_numpy(theta).to(dev), params,
+                      engine="plain")
+    fb = ilt.IltBatch(k, torch.from_numpy(targets).to(dev), torch.from_numpy(theta).to(dev), params)
+    agree = float(((fb.grad_m.double() - pb.grad_m.double()).abs().amax(dim=(1, 2))
+                   / pb.grad_m.double().abs().amax(dim=(1, 2))).max())
+    pb.step(want_signed=False)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(2):
+        pb.step(want_signed=False)
+    e1.record()
+    torch.cuda.synchronize()
+    plain_ms = max_over_ranks(e0.elapsed_time(e1) / 2)
+    plain_value = world * ILT_CLIPS / (plain_ms / 1000.0)
+    del pb, fb
+    # end to end from pinned host memory: upload theta/targets, K steps reading
+    # the cost back every step, download theta
+    tp = torch.from_numpy(targets).pin_memory()
+    hp = torch.from_numpy(theta).pin_memory()
+    out = torch.empty_like(hp).pin_memory()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record()
+    eb = ilt.IltBatch(k, tp.to(dev, non_blocking=True), hp.to(dev, non_blocking=True), params)
+    for _ in range(args.steps):
+        eb.step(want_signed=False)
+        float(eb.cost.sum())
+    out.copy_(eb.theta)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1000.0))
+    NN = N * N
+    return {
+        "metric": "ILT gradient steps/s @1024^2 (clip-steps)", "value": value, "unit": "clip-steps/s",
+        "ms_per_step": ms / args.steps, "clips_per_step": ILT_CLIPS, "workload": ILT_WORKLOAD,
+        "kernels": len(k), "socs_build_ms": build_ms, "stages_ms": stages,
+        "plain": {"value": plain_value, "unit": "clip-steps/s", "fused_over_plain": value / plain_value,
+                  "max_rel_diff_grad_fused_vs_plain": agree},
+        "e2e": {"value": world * ILT_CLIPS * args.steps / (e2e_ms / 1000.0), "unit": "clip-steps/s",
+                "h2d_bytes_per_step": 2 * ILT_CLIPS * NN * 4 // args.steps, "d2h_bytes_per_step":
+                ILT_CLIPS * 8 + ILT_CLIPS * NN * 4 // args.steps},
+        "dense_fft_equivalent_bytes_per_clip_step": NN * (16 * (2 * len(k) + 2) + 40),
+    }
+
+
+def cpu_ilt_seconds() -> tuple[float, int]:
+    """FP64 numpy objective (forward + adjoint) of one clip of the ILT workload, K = 24."""
+    from oracle import litho_oracle as O
+    o = ilt_optics()
+
+    class G:
+        n_pixels, pixel_size = N, PX
+    k = O.socs_build(o, G, tol=0.0, max_kernels=24)
+    targets, theta = ilt_inputs(500, 1)
+    m = O.mask_of(theta[0].astype(np.float64), 4.0, 0.0)
+    t0 = time.perf_counter()
+    O.objective(k, targets[0].astype(np.float64), m, 1.0 / k.clear, 0.3, 0.0, 1.0, 15.0)
+    return time.perf_counter() - t0, 1
+
+
 def measured_peaks() -> dict:
     f = ROOT / "MEASURED_PEAKS.json"
     if f.exists():
@@ -332,11 +471,17 @@ def run_ours(args) -> None:
         "e2e": {"value": e2e_value, "unit": "images/s", "h2d_bytes_per_step": E2E_IMAGES * NN * 8,
                 "d2h_bytes_per_step": E2E_IMAGES * NN * 4, "images_per_step": E2E_IMAGES},
     })
+    if "ilt" not in args.skip:
+        line["ilt"] = bench_ilt(args, torch, dev, world, max_over_ranks, barrier)
     if rank == 0 and world == 1 and not args.no_cpu:
         t, k, S = cpu_sample_seconds()
         cv = 1.0 / (t * S / k)
         line["cpu_baseline"] = {"value": cv, "unit": "images/s", "cores": os.cpu_count(), "kind": "port",
                                 "sample": f"{k} of {S} source points of one image, scaled by {S}/{k}"}
+        if "ilt" in line:
+            ti, _ = cpu_ilt_seconds()
+            line["ilt"]["cpu_baseline"] = {"value": 1.0 / ti, "unit": "clip-steps/s", "cores": os.cpu_count(),
+                                           "kind": "port", "sample": "one 1024^2 clip objective + adjoint (K=24)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -352,7 +497,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--images", type=int, default=IMAGES_PER_STEP,
                     help="images per step (a small value makes a profiling case)")
-    ap.add_argument("--skip", default="", help="comma list of phases to skip: plain,e2e,profile,cpu")
+    ap.add_argument("--skip", default="", help="comma list of phases to skip: plain,e2e,profile,cpu,ilt")
     args = ap.parse_args()
     args.skip = set(x for x in args.skip.split(",") if x)
     if "cpu" in args.skip:

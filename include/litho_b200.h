@@ -206,6 +206,26 @@ int litho_abbe_plain(const LithoAbbePlan* plan, int batch, const void* plan_blob
                      const void* mask_dev, float* image_dev, float* peak_dev,
                      void* workspace_dev, size_t workspace_bytes, cudaStream_t stream);
 
+/* Workspace bytes of litho_plain_socs_forward() / litho_plain_socs_adjoint(). */
+int litho_plain_socs_workspace(int n_clips, int n, size_t* bytes);
+
+/* The plain SOCS forward of opc/ilt.py:socs_fields (:227-231) on full grids:
+ * fields_out[k][c] = ifft2(phi_k fft2(mask_c)) (complex64, K x C x N x N),
+ * I_out[c] = sum_k lambda_k |fields|^2; phi: K x nb band values at signed
+ * bins (bkx, bky); lam_host: K host floats. Power-of-two N. The comparison
+ * baseline for the band-limited ILT stages. */
+int litho_plain_socs_forward(const float* masks_dev, int n_clips, int n, int K, const float2* phi_dev,
+                             const float* lam_host, const int32_t* bkx_dev, const int32_t* bky_dev,
+                             int nb, float2* fields_out_dev, float* I_out_dev, void* workspace_dev,
+                             size_t workspace_bytes, cudaStream_t stream);
+
+/* The plain adjoint of opc/ilt.py:socs_gradient (:262-266) on full grids:
+ * grad_out[c] = 2 Re sum_k lambda_k ifft2(conj(phi_k) fft2(sens_c fields[k][c])). */
+int litho_plain_socs_adjoint(const float2* fields_dev, const float* sens_dev, int n_clips, int n, int K,
+                             const float2* phi_dev, const float* lam_host, const int32_t* bkx_dev,
+                             const int32_t* bky_dev, int nb, float* grad_out_dev, void* workspace_dev,
+                             size_t workspace_bytes, cudaStream_t stream);
+
 /* ---- SOCS (Hopkins) decomposition ---------------------------------------- */
 
 /* Workspace bytes of litho_socs_build() for n_source points and n_band band

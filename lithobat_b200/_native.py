@@ -119,6 +119,9 @@ def lib():
         "litho_ilt_theta_grad": [vp, vp, C.c_longlong, f32, vp, vp],
         "litho_ilt_adam": [vp, C.c_longlong, f32, f32, f32, f32, i32, vp, vp, vp, vp],
         "litho_gaussian_blur": [vp, vp, vp, i32, i32, vp, i32, vp],
+        "litho_plain_socs_workspace": [i32, i32, C.POINTER(sz)],
+        "litho_plain_socs_forward": [vp, i32, i32, i32, vp, vp, vp, vp, i32, vp, vp, vp, sz, vp],
+        "litho_plain_socs_adjoint": [vp, vp, i32, i32, i32, vp, vp, vp, vp, i32, vp, vp, sz, vp],
     }
     for fn, at in sigs.items():
         getattr(L, fn).argtypes = at

@@ -295,3 +295,130 @@ extern "C" int litho_abbe_plain(const LithoAbbePlan* plan, int batch, const void
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
   return LITHO_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Plain SOCS forward and adjoint on full N x N grids (the reference's
+// opc/ilt.py:socs_fields :227-231 and socs_gradient :262-266 moved to the GPU
+// unchanged): one full 2-D FFT per kernel and direction, kernels scattered
+// from their band values. The comparison baseline for csrc/ilt.cu.
+// ---------------------------------------------------------------------------
+namespace litho {
+
+// out[c] = 0 off the band, phi(b) * M[c](b) (conj(phi) if CONJ) on it.
+template <bool CONJ>
+__global__ void k_plain_band_mul(const float2* __restrict__ M, const float2* __restrict__ phi,
+                                 const int32_t* __restrict__ bkx, const int32_t* __restrict__ bky, int nb, int n,
+                                 int n_clips, float2* __restrict__ out) {
+  const long long total = (long long)n_clips * nb;
+  for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < total;
+       id += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(id / nb), b = (int)(id % nb);
+    const int ix = (bkx[b] + n) % n, iy = (bky[b] + n) % n;
+    const size_t at = ((size_t)c * n + iy) * n + ix;
+    const float2 f = phi[b];
+    out[at] = CONJ ? cmulc(M[at], f) : cmul(f, M[at]);
+  }
+}
+
+__global__ void k_plain_intensity(const float2* __restrict__ E, long long total, float lam, int first,
+                                  float* __restrict__ I) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float v = lam * cabs2(E[i]);
+    I[i] = first ? v : I[i] + v;
+  }
+}
+
+__global__ void k_plain_mul_real(const float* __restrict__ g, const float2* __restrict__ E, long long total,
+                                 float2* __restrict__ out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = cscale(E[i], g[i]);
+}
+
+__global__ void k_plain_grad(const float2* __restrict__ adj, long long total, float two_lam, int first,
+                             float* __restrict__ grad) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float v = two_lam * adj[i].x;
+    grad[i] = first ? v : grad[i] + v;
+  }
+}
+
+static unsigned grid_elems(long long total) {
+  long long b = (total + 255) / 256;
+  return (unsigned)(b > 8192 ? 8192 : (b < 1 ? 1 : b));
+}
+
+}  // namespace litho
+
+static int64_t plain_socs_ws(int n_clips, int n) {
+  return align16((int64_t)n * 8) + 2 * align16((int64_t)n_clips * n * n * 8);
+}
+
+extern "C" int litho_plain_socs_workspace(int n_clips, int n, size_t* bytes) {
+  if (!bytes) return LITHO_E_NULL;
+  if (n_clips < 1 || n < 16 || n > 4096 || (n & (n - 1))) return LITHO_E_UNSUPPORTED;
+  *bytes = (size_t)plain_socs_ws(n_clips, n);
+  return LITHO_OK;
+}
+
+// fields_out[k][c] = ifft2(phi_k * fft2(mask_c)), I_out[c] = sum_k lambda_k |fields|^2.
+extern "C" int litho_plain_socs_forward(const float* masks, int n_clips, int n, int K, const float2* phi,
+                                        const float* lam_host, const int32_t* bkx, const int32_t* bky, int nb,
+                                        float2* fields_out, float* I_out, void* ws, size_t ws_bytes,
+                                        cudaStream_t s) {
+  if (!masks || !phi || !lam_host || !bkx || !bky || !fields_out || !I_out || !ws) return LITHO_E_NULL;
+  if (n_clips < 1 || n < 16 || n > 4096 || (n & (n - 1)) || K < 1 || nb < 1) return LITHO_E_UNSUPPORTED;
+  if ((int64_t)ws_bytes < plain_socs_ws(n_clips, n)) return LITHO_E_WORKSPACE;
+  char* w = static_cast<char*>(ws);
+  float2* tw = reinterpret_cast<float2*>(w);
+  float2* M = reinterpret_cast<float2*>(w + align16((int64_t)n * 8));
+  const long long NN = (long long)n * n, tot = NN * n_clips;
+  const float inv = 1.0f / ((float)n * (float)n);
+  k_twiddle_table<<<(n + 255) / 256, 256, 0, s>>>(tw, n, +1);
+  cudaError_t e = plain_fft2(masks, true, M, n_clips, n, -1, 1.0f, 1.0f, tw, s);
+  if (e != cudaSuccess) return (int)e;
+  for (int k = 0; k < K; ++k) {
+    float2* E = fields_out + (size_t)k * tot;
+    if ((e = cudaMemsetAsync(E, 0, (size_t)tot * sizeof(float2), s)) != cudaSuccess) return (int)e;
+    k_plain_band_mul<false><<<grid_elems((long long)n_clips * nb), 256, 0, s>>>(M, phi + (size_t)k * nb, bkx, bky,
+                                                                                nb, n, n_clips, E);
+    e = plain_fft2(nullptr, false, E, n_clips, n, +1, 1.0f, inv, tw, s);
+    if (e != cudaSuccess) return (int)e;
+    k_plain_intensity<<<grid_elems(tot), 256, 0, s>>>(E, tot, lam_host[k], k == 0, I_out);
+  }
+  e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+// grad_out[c] = 2 Re sum_k lambda_k ifft2(conj(phi_k) fft2(sens_c fields[k][c])).
+extern "C" int litho_plain_socs_adjoint(const float2* fields, const float* sens, int n_clips, int n, int K,
+                                        const float2* phi, const float* lam_host, const int32_t* bkx,
+                                        const int32_t* bky, int nb, float* grad_out, void* ws, size_t ws_bytes,
+                                        cudaStream_t s) {
+  if (!fields || !sens || !phi || !lam_host || !bkx || !bky || !grad_out || !ws) return LITHO_E_NULL;
+  if (n_clips < 1 || n < 16 || n > 4096 || (n & (n - 1)) || K < 1 || nb < 1) return LITHO_E_UNSUPPORTED;
+  if ((int64_t)ws_bytes < plain_socs_ws(n_clips, n)) return LITHO_E_WORKSPACE;
+  char* w = static_cast<char*>(ws);
+  float2* tw = reinterpret_cast<float2*>(w);
+  float2* Bk = reinterpret_cast<float2*>(w + align16((int64_t)n * 8));
+  float2* Sk = reinterpret_cast<float2*>(w + align16((int64_t)n * 8) + align16((int64_t)n_clips * n * n * 8));
+  const long long NN = (long long)n * n, tot = NN * n_clips;
+  const float inv = 1.0f / ((float)n * (float)n);
+  k_twiddle_table<<<(n + 255) / 256, 256, 0, s>>>(tw, n, +1);
+  cudaError_t e;
+  for (int k = 0; k < K; ++k) {
+    k_plain_mul_real<<<grid_elems(tot), 256, 0, s>>>(sens, fields + (size_t)k * tot, tot, Bk);
+    e = plain_fft2(nullptr, false, Bk, n_clips, n, -1, 1.0f, 1.0f, tw, s);
+    if (e != cudaSuccess) return (int)e;
+    if ((e = cudaMemsetAsync(Sk, 0, (size_t)tot * sizeof(float2), s)) != cudaSuccess) return (int)e;
+    k_plain_band_mul<true><<<grid_elems((long long)n_clips * nb), 256, 0, s>>>(Bk, phi + (size_t)k * nb, bkx, bky,
+                                                                               nb, n, n_clips, Sk);
+    e = plain_fft2(nullptr, false, Sk, n_clips, n, +1, 1.0f, inv, tw, s);
+    if (e != cudaSuccess) return (int)e;
+    k_plain_grad<<<grid_elems(tot), 256, 0, s>>>(Sk, tot, 2.0f * lam_host[k], k == 0, grad_out);
+  }
+  e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}

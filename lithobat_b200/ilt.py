@@ -193,16 +193,72 @@ class _Stages:
         return cost, grad, signed, ppart.sum(dim=1)
 
 
+class _PlainStages(_Stages):
+    """The same objective through the plain full-grid SOCS forward and
+    adjoint (one 2-D FFT per kernel and direction), for comparison."""
+
+    def __init__(self, kernels: SOCSKernels, n_clips: int):
+        super().__init__(kernels, n_clips)
+        torch = self.torch
+        self.phi = kernels._phi.to(torch.complex64).contiguous()
+        self.lam = (C.c_float * len(kernels))(*[float(x) for x in kernels.weights])
+        self.bkx = torch.from_numpy(kernels.band_kx).to(self.dev)
+        self.bky = torch.from_numpy(kernels.band_ky).to(self.dev)
+        self._fields = None
+
+    def _pws(self):
+        nb = C.c_size_t(0)
+        nat.check("litho_plain_socs_workspace", self.L.litho_plain_socs_workspace(self.C, self.n, C.byref(nb)))
+        return self.ws("plain", nb.value)
+
+    def objective(self, mask, target, scale, level, sigma_px, sign, steepness, weight_tv, weight_discrete,
+                  want_signed=True):
+        torch, L = self.torch, self.L
+        K = len(self.k)
+        if self._fields is None:
+            self._fields = torch.empty((K, self.C, self.n, self.n), dtype=torch.complex64, device=self.dev)
+        raw = torch.empty((self.C, self.n, self.n), dtype=torch.float32, device=self.dev)
+        ws = self._pws()
+        nat.check("litho_plain_socs_forward", L.litho_plain_socs_forward(
+            mask.data_ptr(), self.C, self.n, K, self.phi.data_ptr(), self.lam, self.bkx.data_ptr(),
+            self.bky.data_ptr(), self.phi.shape[1], self._fields.data_ptr(), raw.data_ptr(), ws.data_ptr(),
+            ws.numel(), self.stream()))
+        fld = self.blur(raw, sigma_px)
+        a = steepness / max(abs(level), 1e-12)
+        dfield = torch.empty_like(raw)
+        signed = torch.empty_like(raw) if want_signed else None
+        cpart = torch.empty((self.C, N_PART), dtype=torch.float64, device=self.dev)
+        ppart = torch.empty((self.C, N_PART), dtype=torch.int32, device=self.dev)
+        nat.check("litho_ilt_objective", L.litho_ilt_objective(
+            fld.data_ptr(), target.data_ptr(), self.C, self.n, float(scale), float(level), float(sign), float(a),
+            dfield.data_ptr(), None if signed is None else signed.data_ptr(), cpart.data_ptr(), ppart.data_ptr(),
+            N_PART, self.stream()))
+        sens = self.blur(dfield, sigma_px) * float(scale)
+        grad = torch.empty_like(raw)
+        nat.check("litho_plain_socs_adjoint", L.litho_plain_socs_adjoint(
+            self._fields.data_ptr(), sens.data_ptr(), self.C, self.n, K, self.phi.data_ptr(), self.lam,
+            self.bkx.data_ptr(), self.bky.data_ptr(), self.phi.shape[1], grad.data_ptr(), ws.data_ptr(),
+            ws.numel(), self.stream()))
+        cost = cpart.sum(dim=1) / float(self.n * self.n)
+        if weight_tv > 0.0 or weight_discrete > 0.0:
+            pc = torch.empty((self.C, N_PART), dtype=torch.float64, device=self.dev)
+            nat.check("litho_ilt_penalties", L.litho_ilt_penalties(
+                mask.data_ptr(), self.C, self.n, float(weight_tv), float(weight_discrete), grad.data_ptr(),
+                pc.data_ptr(), N_PART, self.stream()))
+            cost = cost + pc.sum(dim=1)
+        return cost, grad, signed, ppart.sum(dim=1)
+
+
 _STAGES: dict = {}
 
 
-def stages(kernels: SOCSKernels, n_clips: int) -> _Stages:
-    key = (id(kernels), int(n_clips))
+def stages(kernels: SOCSKernels, n_clips: int, engine: str = "fused") -> _Stages:
+    key = (id(kernels), int(n_clips), engine)
     st = _STAGES.get(key)
     if st is None or st.k is not kernels:
         if len(_STAGES) > 16:
             _STAGES.clear()
-        st = _Stages(kernels, n_clips)
+        st = (_Stages if engine == "fused" else _PlainStages)(kernels, n_clips)
         _STAGES[key] = st
     return st
 
@@ -403,8 +459,8 @@ class IltBatch:
     ``step()`` is one iteration of opc/ilt.py:576-596: grad_theta, Adam, the
     beta anneal, mask_of and the objective (SOCS forward + adjoint)."""
 
-    def __init__(self, kernels: SOCSKernels, targets, theta0, params: IltParams):
-        self.st = stages(kernels, int(theta0.shape[0]))
+    def __init__(self, kernels: SOCSKernels, targets, theta0, params: IltParams, engine: str = "fused"):
+        self.st = stages(kernels, int(theta0.shape[0]), engine)
         torch = self.st.torch
         n = self.st.n
         self.p = params

@@ -159,3 +159,16 @@ def test_fused_steps_follow_the_reference_loop(lb):
         b.step()
         assert float(b.cost[0]) == pytest.approx(cost, rel=1e-4)
     assert np.abs(b.theta[0].cpu().numpy() - th).max() <= 1e-3 * np.abs(th).max()
+
+
+def test_plain_engine_gives_the_same_objective(lb):
+    from lithobat_b200 import ilt
+    a, od, gd = load_golden("ilt_imm_128_k24")
+    k = lb.SOCSKernels.build(_optics(lb, od), lb.GridConfig(**gd), tol=0.0, max_kernels=24)
+    tgt = a["target"].astype(np.float64)
+    p = ilt.IltParams(scale=1.0 / k.clear, level=0.3, steepness=15.0)
+    fused = ilt.IltBatch(k, tgt[None], a["theta"][None], p)
+    plain = ilt.IltBatch(k, tgt[None], a["theta"][None], p, engine="plain")
+    assert float(plain.cost[0]) == pytest.approx(float(a["cost"]), rel=1e-5)
+    assert rel(plain.grad_m[0].cpu().numpy(), a["grad"]) <= TOL_G
+    assert rel(fused.grad_m[0].cpu().numpy(), plain.grad_m[0].cpu().numpy().astype(np.float64)) <= TOL_G
