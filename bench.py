@@ -111,7 +111,8 @@ def bench_ilt(args, torch, dev, world, max_over_ranks, barrier) -> dict:
     e1.record()
     torch.cuda.synchronize()
     build_ms = e0.elapsed_time(e1)
-    targets, theta = ilt_inputs(500 + rank, ILT_CLIPS)
+    nclip = args.ilt_clips
+    targets, theta = ilt_inputs(500 + rank, nclip)
     params = ilt.IltParams(scale=1.0 / k.clear, level=0.3, steepness=15.0, step=0.4, beta=4.0, growth=1.0)
     b = ilt.IltBatch(k, torch.from_numpy(targets).to(dev), torch.from_numpy(theta).to(dev), params)
     for _ in range(args.warmup):
@@ -124,7 +125,7 @@ def bench_ilt(args, torch, dev, world, max_over_ranks, barrier) -> dict:
     e1.record()
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1))
-    value = world * ILT_CLIPS * args.steps / (ms / 1000.0)
+    value = world * nclip * args.steps / (ms / 1000.0)
     # stage times of one step (events on the launching stream)
     st = b.st
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(9)]
@@ -142,9 +143,9 @@ def bench_ilt(args, torch, dev, world, max_over_ranks, barrier) -> dict:
     raw = st.image(mbox)
     ev[4].record()
     dfield = torch.empty_like(raw)
-    cpart = torch.empty((ILT_CLIPS, 64), dtype=torch.float64, device=dev)
-    ppart = torch.empty((ILT_CLIPS, 64), dtype=torch.int32, device=dev)
-    nat_.check("obj", st.L.litho_ilt_objective(raw.data_ptr(), b.target.data_ptr(), ILT_CLIPS, N,
+    cpart = torch.empty((nclip, 64), dtype=torch.float64, device=dev)
+    ppart = torch.empty((nclip, 64), dtype=torch.int32, device=dev)
+    nat_.check("obj", st.L.litho_ilt_objective(raw.data_ptr(), b.target.data_ptr(), nclip, N,
                                                float(params.scale), 0.3, 1.0, 50.0, dfield.data_ptr(), None,
                                                cpart.data_ptr(), ppart.data_ptr(), 64, st.stream()))
     ev[5].record()
@@ -156,22 +157,26 @@ def bench_ilt(args, torch, dev, world, max_over_ranks, barrier) -> dict:
     names = ["grad_theta", "adam_and_mask", "mask_band_spectrum", "coarse_image_and_synthesis", "objective",
              "sensitivity_band_spectrum", "adjoint_band_spectrum+coarse+synthesis"]
     stages = {nm: ev[i].elapsed_time(ev[i + 1]) for i, nm in enumerate(names)}
-    # plain engine, same inputs
-    pb = ilt.IltBatch(k, torch.from_numpy(targets).to(dev), torch.from_numpy(theta).to(dev), params,
-                      engine="plain")
-    fb = ilt.IltBatch(k, torch.from_numpy(targets).to(dev), torch.from_numpy(theta).to(dev), params)
-    agree = float(((fb.grad_m.double() - pb.grad_m.double()).abs().amax(dim=(1, 2))
-                   / pb.grad_m.double().abs().amax(dim=(1, 2))).max())
-    pb.step(want_signed=False)
-    torch.cuda.synchronize()
-    e0.record()
-    for _ in range(2):
+    plain = None
+    if "iltplain" not in args.skip:
+        # plain engine, same inputs
+        pb = ilt.IltBatch(k, torch.from_numpy(targets).to(dev), torch.from_numpy(theta).to(dev), params,
+                          engine="plain")
+        fb = ilt.IltBatch(k, torch.from_numpy(targets).to(dev), torch.from_numpy(theta).to(dev), params)
+        agree = float(((fb.grad_m.double() - pb.grad_m.double()).abs().amax(dim=(1, 2))
+                       / pb.grad_m.double().abs().amax(dim=(1, 2))).max())
         pb.step(want_signed=False)
-    e1.record()
-    torch.cuda.synchronize()
-    plain_ms = max_over_ranks(e0.elapsed_time(e1) / 2)
-    plain_value = world * ILT_CLIPS / (plain_ms / 1000.0)
-    del pb, fb
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(2):
+            pb.step(want_signed=False)
+        e1.record()
+        torch.cuda.synchronize()
+        plain_ms = max_over_ranks(e0.elapsed_time(e1) / 2)
+        plain_value = world * nclip / (plain_ms / 1000.0)
+        plain = {"value": plain_value, "unit": "clip-steps/s", "fused_over_plain": value / plain_value,
+                 "max_rel_diff_grad_fused_vs_plain": agree}
+        del pb, fb
     # end to end from pinned host memory: upload theta/targets, K steps reading
     # the cost back every step, download theta
     tp = torch.from_numpy(targets).pin_memory()
@@ -191,13 +196,11 @@ def bench_ilt(args, torch, dev, world, max_over_ranks, barrier) -> dict:
     NN = N * N
     return {
         "metric": "ILT gradient steps/s @1024^2 (clip-steps)", "value": value, "unit": "clip-steps/s",
-        "ms_per_step": ms / args.steps, "clips_per_step": ILT_CLIPS, "workload": ILT_WORKLOAD,
-        "kernels": len(k), "socs_build_ms": build_ms, "stages_ms": stages,
-        "plain": {"value": plain_value, "unit": "clip-steps/s", "fused_over_plain": value / plain_value,
-                  "max_rel_diff_grad_fused_vs_plain": agree},
-        "e2e": {"value": world * ILT_CLIPS * args.steps / (e2e_ms / 1000.0), "unit": "clip-steps/s",
-                "h2d_bytes_per_step": 2 * ILT_CLIPS * NN * 4 // args.steps, "d2h_bytes_per_step":
-                ILT_CLIPS * 8 + ILT_CLIPS * NN * 4 // args.steps},
+        "ms_per_step": ms / args.steps, "clips_per_step": nclip, "workload": ILT_WORKLOAD,
+        "kernels": len(k), "socs_build_ms": build_ms, "stages_ms": stages, "plain": plain,
+        "e2e": {"value": world * nclip * args.steps / (e2e_ms / 1000.0), "unit": "clip-steps/s",
+                "h2d_bytes_per_step": 2 * nclip * NN * 4 // args.steps, "d2h_bytes_per_step":
+                nclip * 8 + nclip * NN * 4 // args.steps},
         "dense_fft_equivalent_bytes_per_clip_step": NN * (16 * (2 * len(k) + 2) + 40),
     }
 
@@ -383,94 +386,87 @@ def run_ours(args) -> None:
         "vs_baseline": None, "dtype": "c64/f32", "data": "synthetic (seeded att-PSM contact-hole clips)",
         "clocks": clocks, "gpu_launches": launches_per_step * args.steps,
     }
-    if "profile" in args.skip:
-        if rank == 0:
-            print(json.dumps(line), flush=True)
-        if world > 1:
-            dist.destroy_process_group()
-        return
-
-    # ---- per-stage device times (CUDA events between the stages) ----
-    stages = aerial.profile_abbe(pd, dmasks[0], reps=max(3, args.steps))
-    step_ms = sum(stages.values())
-    dom = max(stages, key=stages.get)
+    NN = N * N
+    transforms = pd.transforms // B
+    line["config"] = {"workload": WORKLOAD, "images_per_step": B, "grid": N, "pixel_nm": 1.0,
+                      "source_points": pd.jobs // B, "transforms_per_image": transforms,
+                      "coarse_grid": int(pd.plan.L), "parallelism": f"replicas x{world}",
+                      "l2": f"{ROTATE} rotating input batches of {B * NN * 8 >> 20} MiB"}
     pd_small = aerial.plan_abbe([view] * PLAIN_IMAGES, N, PX, [[(view.defocus, view.image_index)]] * PLAIN_IMAGES,
                                 1.0, False, True)
-    table_ms = aerial.profile_abbe(pd_small, dmasks[0][:PLAIN_IMAGES].contiguous(), reps=3,
-                                   rebuild_table=True)["pupil_table"]
+
+    # ---- per-stage device times (CUDA events between the stages) ----
+    if "profile" not in args.skip:
+        stages = aerial.profile_abbe(pd, dmasks[0], reps=max(3, args.steps))
+        step_ms = sum(stages.values())
+        dom = max(stages, key=stages.get)
+        table_ms = aerial.profile_abbe(pd_small, dmasks[0][:PLAIN_IMAGES].contiguous(), reps=3,
+                                       rebuild_table=True)["pupil_table"]
+        peaks = measured_peaks()
+        hbm = float(peaks["hbm_gbs"])
+        Bm = 2 * pd.plan.bm + 1
+        stage_bytes = {   # algorithmic bytes of each stage per launch (the whole batch)
+            "pupil_table": pd.plan.n_tab * 3 * (2 * pd.plan.h + 1) ** 2 * 8,
+            "band_rows": B * (NN * 8 + N * Bm * 8),
+            "band_cols": B * (N * Bm * 8 + Bm * Bm * 8),
+            "coarse": pd.plan.n_tab * 3 * (2 * pd.plan.h + 1) ** 2 * 8 + pd.plan.n_items * 32 * 32 * 4,
+            "coarse_reduce": pd.plan.n_items * 32 * 32 * 4,
+            "synthesis": B * NN * 4,
+            "normalise": B * NN * 8,
+        }
+        achieved = stage_bytes[dom] / (stages[dom] / 1000.0) / 1e9
+        formula_bytes = NN * (16 * transforms + 24)  # dense two-pass FFT equivalent, per image
+        line["config"]["pupil_table"] = f"built once per optics ({table_ms:.3f} ms), reused across steps"
+        line["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                            "frac": achieved / hbm, "traffic": None,
+                            "peak_source": "measured" if not peaks.get("_fallback") else "fallback"}
+        line["stages_ms"] = stages
+        line["dense_fft_equivalent"] = {"bytes_per_image": formula_bytes,
+                                        "GBps": formula_bytes * B / (step_ms / 1000.0) / 1e9}
 
     # ---- fused vs plain on the same clips, and their agreement ----
-    sub = dmasks[0][:PLAIN_IMAGES].contiguous()
-    fused_img, _ = aerial.run_abbe(pd_small, sub)
-    fused_img = fused_img.clone()
-    plain_img, _ = aerial.run_abbe(pd_small, sub, engine="plain")  # warm
-    torch.cuda.synchronize()
-    p_steps = 2
-    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2.record()
-    for i in range(p_steps):
-        plain_img, _ = aerial.run_abbe(pd_small, sub, engine="plain")
-    e3.record()
-    torch.cuda.synchronize()
-    plain_ms = max_over_ranks(e2.elapsed_time(e3) / p_steps)
-    plain_value = world * PLAIN_IMAGES / (plain_ms / 1000.0)
-    agree = float(((fused_img.double() - plain_img.double()).abs().amax(dim=(1, 2))
-                   / plain_img.double().abs().amax(dim=(1, 2))).max())
-    del plain_img
+    if "plain" not in args.skip:
+        sub = dmasks[0][:PLAIN_IMAGES].contiguous()
+        fused_img, _ = aerial.run_abbe(pd_small, sub)
+        fused_img = fused_img.clone()
+        plain_img, _ = aerial.run_abbe(pd_small, sub, engine="plain")  # warm
+        torch.cuda.synchronize()
+        p_steps = 2
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record()
+        for i in range(p_steps):
+            plain_img, _ = aerial.run_abbe(pd_small, sub, engine="plain")
+        e3.record()
+        torch.cuda.synchronize()
+        plain_ms = max_over_ranks(e2.elapsed_time(e3) / p_steps)
+        plain_value = world * PLAIN_IMAGES / (plain_ms / 1000.0)
+        agree = float(((fused_img.double() - plain_img.double()).abs().amax(dim=(1, 2))
+                       / plain_img.double().abs().amax(dim=(1, 2))).max())
+        del plain_img
+        line["plain"] = {"value": plain_value, "unit": "images/s", "fused_over_plain": value / plain_value,
+                         "images_per_call": PLAIN_IMAGES, "max_rel_diff_fused_vs_plain": agree}
 
     # ---- end to end through the public API from pinned host memory ----
-    pinned = [dmasks[r][:E2E_IMAGES].cpu().pin_memory() for r in range(ROTATE)]
-    res = torch.empty((E2E_IMAGES, N, N), dtype=torch.float32).pin_memory()
-    for i in range(max(1, args.warmup)):
-        img, _pk, _cl = lb.compute_aerial_batch(pinned[i % ROTATE], o, g)
-        res.copy_(img[:, 0])
-    torch.cuda.synchronize()
-    barrier()
-    t0 = time.perf_counter()
-    e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e4.record()
-    for i in range(args.steps):
-        img, _pk, _cl = lb.compute_aerial_batch(pinned[i % ROTATE], o, g)
-        res.copy_(img[:, 0])
-    e5.record()
-    torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(max(e4.elapsed_time(e5), (time.perf_counter() - t0) * 1000.0))
-    e2e_value = world * E2E_IMAGES * args.steps / (e2e_ms / 1000.0)
-
-    # ---- roofline of the dominant stage ----
-    peaks = measured_peaks()
-    hbm = float(peaks["hbm_gbs"])
-    Bm = 2 * pd.plan.bm + 1
-    NN = N * N
-    stage_bytes = {   # algorithmic bytes of each stage per launch (the whole batch)
-        "pupil_table": pd.plan.n_tab * 3 * (2 * pd.plan.h + 1) ** 2 * 8,
-        "band_rows": B * (NN * 8 + N * Bm * 8),
-        "band_cols": B * (N * Bm * 8 + Bm * Bm * 8),
-        "coarse": pd.plan.n_tab * 3 * (2 * pd.plan.h + 1) ** 2 * 8 + pd.plan.n_items * 32 * 32 * 4,
-        "coarse_reduce": pd.plan.n_items * 32 * 32 * 4,
-        "synthesis": B * NN * 4,
-        "normalise": B * NN * 8,
-    }
-    achieved = stage_bytes[dom] / (stages[dom] / 1000.0) / 1e9
-    transforms = pd.transforms // B
-    formula_bytes = NN * (16 * transforms + 24)  # dense two-pass FFT equivalent, per image
-    line.update({
-        "config": {"workload": WORKLOAD, "images_per_step": B, "grid": N, "pixel_nm": 1.0,
-                   "source_points": pd.jobs // B, "transforms_per_image": transforms,
-                   "coarse_grid": int(pd.plan.L), "parallelism": f"replicas x{world}",
-                   "l2": f"{ROTATE} rotating input batches of {B * NN * 8 >> 20} MiB",
-                   "pupil_table": f"built once per optics ({table_ms:.3f} ms), reused across steps"},
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
-                     "peak_source": "measured" if not peaks.get("_fallback") else "fallback"},
-        "stages_ms": stages,
-        "dense_fft_equivalent": {"bytes_per_image": formula_bytes,
-                                 "GBps": formula_bytes * B / (step_ms / 1000.0) / 1e9},
-        "plain": {"value": plain_value, "unit": "images/s", "fused_over_plain": value / plain_value,
-                  "images_per_call": PLAIN_IMAGES, "max_rel_diff_fused_vs_plain": agree},
-        "e2e": {"value": e2e_value, "unit": "images/s", "h2d_bytes_per_step": E2E_IMAGES * NN * 8,
-                "d2h_bytes_per_step": E2E_IMAGES * NN * 4, "images_per_step": E2E_IMAGES},
-    })
+    if "e2e" not in args.skip:
+        pinned = [dmasks[r][:E2E_IMAGES].cpu().pin_memory() for r in range(ROTATE)]
+        res = torch.empty((E2E_IMAGES, N, N), dtype=torch.float32).pin_memory()
+        for i in range(max(1, args.warmup)):
+            img, _pk, _cl = lb.compute_aerial_batch(pinned[i % ROTATE], o, g)
+            res.copy_(img[:, 0])
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e4.record()
+        for i in range(args.steps):
+            img, _pk, _cl = lb.compute_aerial_batch(pinned[i % ROTATE], o, g)
+            res.copy_(img[:, 0])
+        e5.record()
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(max(e4.elapsed_time(e5), (time.perf_counter() - t0) * 1000.0))
+        line["e2e"] = {"value": world * E2E_IMAGES * args.steps / (e2e_ms / 1000.0), "unit": "images/s",
+                       "h2d_bytes_per_step": E2E_IMAGES * NN * 8, "d2h_bytes_per_step": E2E_IMAGES * NN * 4,
+                       "images_per_step": E2E_IMAGES}
     if "ilt" not in args.skip:
         line["ilt"] = bench_ilt(args, torch, dev, world, max_over_ranks, barrier)
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -497,7 +493,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--images", type=int, default=IMAGES_PER_STEP,
                     help="images per step (a small value makes a profiling case)")
-    ap.add_argument("--skip", default="", help="comma list of phases to skip: plain,e2e,profile,cpu,ilt")
+    ap.add_argument("--skip", default="", help="comma list of phases to skip: plain,e2e,profile,cpu,ilt,iltplain")
+    ap.add_argument("--ilt-clips", type=int, default=ILT_CLIPS, help="clips per ILT step")
     args = ap.parse_args()
     args.skip = set(x for x in args.skip.split(",") if x)
     if "cpu" in args.skip:
