@@ -353,7 +353,10 @@ def run_abbe(pd: AbbePlanData, masks_dev, out=None, peak=None, stream=None, engi
     return out, peak
 
 
-STAGES = ("pupil_table", "band_rows", "band_cols", "coarse", "coarse_reduce", "synthesis", "normalise")
+# Stage names of litho_abbe_profile. "peak_pass" is the compute-only synthesis
+# pass of peak-normalised outputs (on grids without the pair-FFT synthesis it
+# is the direct synthesis and "synthesis" the separate normalising pass).
+STAGES = ("pupil_table", "band_rows", "band_cols", "coarse", "coarse_reduce", "peak_pass", "synthesis")
 
 
 def profile_abbe(pd: AbbePlanData, masks_dev, reps: int = 10, rebuild_table: bool = False) -> dict:

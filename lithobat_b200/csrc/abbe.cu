@@ -25,6 +25,7 @@
 
 #include "common.cuh"
 #include "pupil.cuh"
+#include "rows.cuh"
 
 namespace litho {
 
@@ -388,6 +389,8 @@ int synth_blocks_for(int n) { return (n + kSynthRows - 1) / kSynthRows; }
 cudaError_t launch_synth_real(const float2* box, int G, int n, int n_fields, const float2* tw, const LithoNorm* norm,
                               float* out, float* blockmax, cudaStream_t s) {
   const int gh = G / 2;
+  if (!norm && synth_pairs_ok(n, gh))
+    return launch_synth_pairs(box, gh, n, n_fields, tw, nullptr, out, nullptr, blockmax, s, nullptr);
   const size_t sm = (size_t)n * 8 + (size_t)kSynthRows * (gh + 1) * 8 + (size_t)G * G * 8;
   cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   dim3 gs((n + kSynthRows - 1) / kSynthRows, n_fields);
@@ -586,16 +589,23 @@ static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* tab
   k_coarse_reduce<<<p.n_out, 1024, sm_red, s>>>(out_items, partial, p.L, p.h, bbox);
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
   mark(5);
-  const int gh = G / 2;
-  const size_t sm_syn = (size_t)p.n * 8 + (size_t)kSynthRows * (gh + 1) * 8 + (size_t)G * G * 8;
-  cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_syn);
-  dim3 gs(synth_blocks(p.n), p.n_out);
-  k_synth<<<gs, kSynthThreads, sm_syn, s>>>(bbox, G, p.n, tw, norm, image, blockmax);
-  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
-  mark(6);
-  dim3 gn((unsigned)((((size_t)p.n * p.n + 255) / 256) < 512 ? (((size_t)p.n * p.n + 255) / 256) : 512), p.n_out);
-  k_normalise<<<gn, 256, 0, s>>>(blockmax, synth_blocks(p.n), norm, p.n, image, peak, 0);
-  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  if (synth_pairs_ok(p.n, 2 * p.h)) {
+    // peak pass (peak-normalised outputs), then the writing pass
+    e = launch_synth_pairs(bbox, 2 * p.h, p.n, p.n_out, tw, norm, image, peak, blockmax, s, ev ? ev[6] : nullptr);
+    if (e != cudaSuccess) return (int)e;
+  } else {
+    const int gh = G / 2;
+    const size_t sm_syn = (size_t)p.n * 8 + (size_t)kSynthRows * (gh + 1) * 8 + (size_t)G * G * 8;
+    cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_syn);
+    dim3 gs(synth_blocks(p.n), p.n_out);
+    k_synth<<<gs, kSynthThreads, sm_syn, s>>>(bbox, G, p.n, tw, norm, image, blockmax);
+    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+    mark(6);
+    dim3 gn((unsigned)((((size_t)p.n * p.n + 255) / 256) < 512 ? (((size_t)p.n * p.n + 255) / 256) : 512),
+            p.n_out);
+    k_normalise<<<gn, 256, 0, s>>>(blockmax, synth_blocks(p.n), norm, p.n, image, peak, 0);
+    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  }
   mark(7);
   return LITHO_OK;
 }

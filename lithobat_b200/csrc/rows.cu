@@ -1,0 +1,195 @@
+// Row engines: band-limited synthesis of real images by 32-point FFTs over
+// pairs of rows, and the per-output peak.
+//
+// Synthesis (the last stage of the Abbe sum, expose/aerial_image.py:488-494,
+// and of the SOCS image and gradient, opc/ilt.py:227-232, 263-266):
+//     I(x, y) = sum_{|gx|,|gy| <= g0} B(gx, gy) w^(gx x + gy y),  w = exp(2 pi i / N),
+// with B Hermitian (B(-g) = conj B(g)), so I is real.
+//   column stage: C(gx, y) = sum_gy B(gx, gy) w^(gy y), for gx >= 0 (C(-gx) = conj C(gx));
+//   row stage   : two real rows at once, Z(x) = sum_g (C(g, y1) + i C(g, y2)) w^(g x)
+//                 = I(x, y1) + i I(x, y2). With N = 32 M and x = b + M a,
+//                 Z(b + M a) = sum_r w32^(r a) Q_b(r),  Q_b(r) = sum_{g = r mod 32} D(g) w^(g b),
+//                 a 32-point inverse FFT per residue b held in one lane's registers.
+// About 10 FP32 operations per pixel instead of the ~60 of a direct sum, so
+// the pass is bound by its HBM writes.
+//
+// Peak normalisation needs the peak before the scaled image is written, so
+// peak-normalised outputs run the synthesis twice: pass 0 computes only the
+// block maxima (no HBM traffic), pass 1 recomputes and writes
+// raw * scale / peak. Every reduction is in a fixed order.
+#include "common.cuh"
+#include "rows.cuh"
+
+namespace litho {
+
+constexpr int kSyWarps = 8;
+constexpr int kSyRows = 64;      // rows per block
+constexpr int kSyG0Max = 31;     // box half-width limit: G = 2 g0 + 1 <= 63
+
+// Shared-memory plan of one synthesis block.
+struct SynthSmem {
+  int M, Lp, P, q, G, gp;
+  size_t off_tw, off_tb, off_c, off_b, total;
+};
+
+__host__ __device__ inline SynthSmem synth_smem(int n, int g0) {
+  SynthSmem s{};
+  s.M = n >> 5;
+  s.Lp = s.M < 32 ? s.M : 32;
+  s.P = 32 / s.Lp;
+  s.q = s.M / s.Lp;
+  s.G = 2 * g0 + 1;
+  s.gp = g0 + 1;
+  s.off_tw = 0;
+  s.off_tb = s.off_tw + (size_t)n * 8;
+  s.off_c = s.off_tb + (size_t)s.gp * s.M * 8;
+  s.off_b = s.off_c + (size_t)kSyRows * s.gp * 8;
+  s.total = s.off_b + (size_t)s.G * s.G * 8;
+  return s;
+}
+
+// Is the pair-FFT synthesis available for this grid and box?
+bool synth_pairs_ok(int n, int g0) {
+  return n >= 256 && n <= 2048 && (n & (n - 1)) == 0 && g0 >= 0 && g0 <= kSyG0Max &&
+         synth_smem(n, g0).total <= 200 * 1024;
+}
+
+// PASS 0: block maxima only, for peak-normalised outputs (others return).
+// PASS 1: write raw * scale (scale / peak for peak-normalised outputs) and
+//         the block maxima of the raw image.
+template <int PASS>
+__global__ void __launch_bounds__(kSyWarps * 32, 2)
+k_synth_pairs(const float2* __restrict__ Bbox, int g0, int n, const float2* __restrict__ tw_inv,
+              const LithoNorm* __restrict__ norm, const float* __restrict__ peak, float* __restrict__ image,
+              float* __restrict__ blockmax) {
+  extern __shared__ __align__(16) unsigned char sy_raw[];
+  const SynthSmem L = synth_smem(n, g0);
+  const int o = blockIdx.y, y0 = blockIdx.x * kSyRows;
+  const LithoNorm nm = norm ? norm[o] : LithoNorm{0, 1.0f};
+  if (PASS == 0 && nm.mode != 1) return;
+  float2* tw = reinterpret_cast<float2*>(sy_raw + L.off_tw);
+  float2* TB = reinterpret_cast<float2*>(sy_raw + L.off_tb);   // [g][b] = w^(g b), g = 0..g0
+  float2* C = reinterpret_cast<float2*>(sy_raw + L.off_c);     // [row][gx], gx = 0..g0
+  float2* B = reinterpret_cast<float2*>(sy_raw + L.off_b);     // [gy + g0][gx + g0]
+  __shared__ float red[kSyWarps];
+  const int M = L.M, G = L.G, gp = L.gp, nmask = n - 1;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) tw[j] = tw_inv[j];
+  const float2* Bo = Bbox + (size_t)o * G * G;
+  for (int j = threadIdx.x; j < G * G; j += blockDim.x) B[j] = Bo[j];
+  __syncthreads();
+  for (int j = threadIdx.x; j < gp * M; j += blockDim.x) {
+    const int g = j / M, b = j % M;
+    TB[j] = tw[(g * b) & nmask];
+  }
+  // column stage for the block's rows
+  for (int id = threadIdx.x; id < kSyRows * gp; id += blockDim.x) {
+    const int r = id / gp, gx = id % gp, y = y0 + r;
+    float2 acc = make_float2(0.f, 0.f);
+    const float2* bc = B + gx + g0;
+    for (int gy = -g0; gy <= g0; ++gy) acc = cadd(acc, cmul(bc[(gy + g0) * G], tw[(gy * y) & nmask]));
+    C[id] = acc;
+  }
+  __syncthreads();
+
+  float sc = nm.scale;
+  if (PASS == 1 && nm.mode == 1) {
+    const float pk = peak[o];
+    sc = pk > 0.f ? nm.scale / pk : nm.scale;
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pg = lane / L.Lp, bl = lane % L.Lp;
+  const int iters = kSyRows / (2 * kSyWarps * L.P);
+  float mx = 0.f;
+  for (int it = 0; it < iters; ++it) {
+    const int pair = (it * kSyWarps + warp) * L.P + pg;
+    const float2* c1 = C + (2 * pair) * gp;
+    const float2* c2 = c1 + gp;
+    float* row1 = image + ((size_t)o * n + y0 + 2 * pair) * n;
+    float* row2 = row1 + n;
+    for (int qq = 0; qq < L.q; ++qq) {
+      const int b = bl + qq * L.Lp;
+      float2 Q[32];
+#pragma unroll
+      for (int i = 0; i < 32; ++i) Q[i] = make_float2(0.f, 0.f);
+      {  // g = 0, then +g and -g together: D(-g) = conj C(g, y1) + i conj C(g, y2), w^(-g b) = conj w^(g b)
+        const float2 a1 = c1[0], a2 = c2[0];
+        Q[0] = make_float2(a1.x - a2.y, a1.y + a2.x);
+      }
+#pragma unroll
+      for (int g = 1; g <= kSyG0Max; ++g) {
+        if (g <= g0) {
+          const float2 a1 = c1[g], a2 = c2[g];
+          const float2 t = TB[g * M + b];
+          const float2 dp = make_float2(a1.x - a2.y, a1.y + a2.x);
+          const float2 dm = make_float2(a1.x + a2.y, a2.x - a1.y);
+          Q[g & 31] = cadd(Q[g & 31], cmul(dp, t));
+          Q[(-g) & 31] = cadd(Q[(-g) & 31], cmulc(dm, t));
+        }
+      }
+      fft_reg<32, +1>(Q);
+#pragma unroll
+      for (int a = 0; a < 32; ++a) mx = fmaxf(mx, fmaxf(Q[a].x, Q[a].y));
+      if (PASS == 1) {
+#pragma unroll
+        for (int a = 0; a < 32; ++a) {
+          __stcs(row1 + b + M * a, Q[a].x * sc);
+          __stcs(row2 + b + M * a, Q[a].y * sc);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  if (lane == 0) red[warp] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = red[0];
+    for (int i = 1; i < kSyWarps; ++i) m = fmaxf(m, red[i]);
+    blockmax[(size_t)o * gridDim.x + blockIdx.x] = m;
+  }
+}
+
+// peak[o] = max of its block maxima, for outputs whose mode matches `which`
+// (1: peak-normalised only, 0: all others, -1: every output). One warp each.
+__global__ void k_peak(const float* __restrict__ blockmax, int nblk, const LithoNorm* __restrict__ norm, int n_out,
+                       int which, float* __restrict__ peak) {
+  const int o = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (o >= n_out) return;
+  if (which >= 0) {
+    const int mode = norm ? norm[o].mode : 0;
+    if ((which == 1) != (mode == 1)) return;
+  }
+  float m = 0.f;
+  for (int i = lane; i < nblk; i += 32) m = fmaxf(m, blockmax[(size_t)o * nblk + i]);
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if (lane == 0) peak[o] = m;
+}
+
+int synth_pairs_blocks(int n) { return n / kSyRows; }
+
+// Synthesis of n_out Hermitian boxes of side 2 g0 + 1 into n x n images with
+// the normalisation of `norm` (nullptr: scale 1), the raw peaks into `peak`
+// (may be nullptr when norm is) and `mid` (optional) recorded between the
+// peak pass and the writing pass. Requires synth_pairs_ok(n, g0).
+cudaError_t launch_synth_pairs(const float2* box, int g0, int n, int n_out, const float2* tw, const LithoNorm* norm,
+                               float* image, float* peak, float* blockmax, cudaStream_t s, cudaEvent_t mid) {
+  const SynthSmem L = synth_smem(n, g0);
+  const dim3 grid(n / kSyRows, n_out);
+  const int pk_blocks = (n_out + 7) / 8;
+  cudaError_t e;
+  if (norm) {
+    if (!peak) return cudaErrorInvalidValue;
+    cudaFuncSetAttribute(k_synth_pairs<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+    k_synth_pairs<0><<<grid, kSyWarps * 32, L.total, s>>>(box, g0, n, tw, norm, peak, image, blockmax);
+    k_peak<<<pk_blocks, 256, 0, s>>>(blockmax, grid.x, norm, n_out, 1, peak);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  if (mid) cudaEventRecord(mid, s);
+  cudaFuncSetAttribute(k_synth_pairs<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
+  k_synth_pairs<1><<<grid, kSyWarps * 32, L.total, s>>>(box, g0, n, tw, norm, peak, image, blockmax);
+  if (peak) k_peak<<<pk_blocks, 256, 0, s>>>(blockmax, grid.x, norm, n_out, norm ? 0 : -1, peak);
+  return cudaGetLastError();
+}
+
+}  // namespace litho

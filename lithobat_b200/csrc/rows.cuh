@@ -1,0 +1,17 @@
+// Row engines shared by the Abbe, SOCS and ILT pipelines (rows.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/litho_b200.h"
+
+namespace litho {
+
+// Pair-FFT synthesis of real images from Hermitian band boxes of half-width
+// g0: available for power-of-two n in [256, 2048] and g0 <= 31.
+bool synth_pairs_ok(int n, int g0);
+int synth_pairs_blocks(int n);
+cudaError_t launch_synth_pairs(const float2* box, int g0, int n, int n_out, const float2* tw, const LithoNorm* norm,
+                               float* image, float* peak, float* blockmax, cudaStream_t s, cudaEvent_t mid);
+
+}  // namespace litho
