@@ -78,7 +78,7 @@ _PLANS: dict = {}
 
 
 def plan_abbe(views: Sequence, n: int, pixel_size: float, planes: Sequence[Sequence[tuple]],
-              dose: float, return_raw: bool, mask_complex: bool, items_per_job_group: int = 4) -> AbbePlanData:
+              dose: float, return_raw: bool, mask_complex: bool, items_per_job_group: int = 0) -> AbbePlanData:
     """Build (or fetch from a small cache) the device descriptors of one
     batched Abbe sum. views[c] is the optics of clip c, planes[c] its list of
     (defocus, n_image); every clip has the same number of planes."""
@@ -170,8 +170,9 @@ def _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, ite
         jobs[name] = np.concatenate(cols[name]).astype(nat.JOB_DTYPE[name])
     slots = np.concatenate(slot_reps).astype(np.int32)
     # jobs are grouped by output (k); chunk each output's run into work items
+    # (0: as many jobs per item as keeps about two waves of blocks, at most 32)
     n_out = C * P
-    per = max(1, int(items_per_job_group))
+    per = int(items_per_job_group) or min(32, max(1, n_jobs // (2 * 4 * 148)))
     starts = np.searchsorted(jobs["out"], np.arange(n_out + 1), side="left")
     item_rows, out_items = [], [0]
     for o in range(n_out):

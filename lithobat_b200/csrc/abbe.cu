@@ -62,68 +62,130 @@ __global__ void k_pupil_table(const LithoJob* __restrict__ jobs, const int32_t* 
 }
 
 // ---------------------------------------------------------------------------
-// 3. coarse accumulation, L = 32: one warp per coherent system at a time.
-//    Lane = spectral column dx in pass 1 (over ky), output row v in pass 2
-//    (over kx). Each lane keeps its row of J(u, v) in 32 registers.
+// 3. coarse accumulation, L = 32 (h <= 7). A block takes one work item (a run
+//    of one output's jobs, all on the same clip); the clip's mask band box is
+//    staged once in shared memory. A warp takes the item's coherent transforms
+//    two at a time: in pass 1 (inverse over ky) lanes 0-15 are the spectral
+//    columns of the first transform and lanes 16-31 those of the second, so
+//    no lane idles on an empty column; in pass 2 (inverse over kx) lane = row
+//    v, once per transform, and J(u, v) += w |e|^2 stays in the lane's 32
+//    registers. Both transforms are pruned FFTs (only d in [-h, h] non-zero).
+//    The next pair's pupil-table blocks are fetched with cp.async while the
+//    current pair's pass 2 runs.
 // ---------------------------------------------------------------------------
 constexpr int kCoarseWarps = 4;
 constexpr int kCoarseHMax32 = 7;  // 4h + 1 <= 32
+constexpr int kC32TLd = 33;
 
-__global__ void __launch_bounds__(kCoarseWarps * 32)
+struct C32Smem {
+  int side, npts, npad, Bm;
+  size_t off_warp, per_warp, total;
+};
+
+__host__ __device__ inline C32Smem c32_smem(int h, int bm) {
+  C32Smem g{};
+  g.side = 2 * h + 1;
+  g.npts = g.side * g.side;
+  g.npad = (g.npts + 1) & ~1;
+  g.Bm = 2 * bm + 1;
+  g.off_warp = (((size_t)g.Bm * g.Bm * 8) + 15) & ~(size_t)15;
+  g.per_warp = (size_t)2 * g.npad * 8 + (size_t)2 * g.side * kC32TLd * 8;
+  g.total = g.off_warp + kCoarseWarps * g.per_warp;
+  const size_t red = (size_t)kCoarseWarps * 1024 * 4;  // the final reduction reuses the buffer
+  if (g.total < red) g.total = red;
+  return g;
+}
+
+__global__ void __launch_bounds__(kCoarseWarps * 32, 4)
 k_coarse32(const LithoItem* __restrict__ items, const LithoJob* __restrict__ jobs,
            const float2* __restrict__ table, int h, int ncomp_max, const float2* __restrict__ Mb,
            int bm, float* __restrict__ partial) {
-  extern __shared__ float2 smem[];
+  extern __shared__ __align__(16) unsigned char c32_raw[];
+  const C32Smem g = c32_smem(h, bm);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float2* tb = smem + warp * (32 * 33);
+  const int side = g.side, npts = g.npts, npad = g.npad, Bm = g.Bm;
+  float2* msk = reinterpret_cast<float2*>(c32_raw);
+  float2* TAB = reinterpret_cast<float2*>(c32_raw + g.off_warp + warp * g.per_warp);   // [2][npad]
+  float2* T = TAB + 2 * npad;                                                          // [2][side][kC32TLd]
   const LithoItem it = items[blockIdx.x];
-  const int side = 2 * h + 1, npts = side * side, Bm = 2 * bm + 1;
-  const int dx = lane - h;
-  const bool col_live = lane < side;
+  const int clip = jobs[it.job_begin].clip, ncomp = jobs[it.job_begin].ncomp;
+  {
+    const float2* src = Mb + (size_t)clip * Bm * Bm;
+    for (int i = threadIdx.x; i < Bm * Bm; i += blockDim.x) msk[i] = src[i];
+  }
+  const int n_t = (it.job_end - it.job_begin) * ncomp;
+  const int n_pairs = (n_t + 1) >> 1;
+  auto fetch = [&](int pp) {
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const int t = 2 * pp + half;
+      if (t < n_t) {
+        const int j = it.job_begin + t / ncomp, c = t % ncomp;
+        const float2* src = table + ((size_t)__ldg(&jobs[j].tab) * ncomp_max + c) * npts;
+        for (int e = lane; e < npts; e += 32) cp_async8(TAB + half * npad + e, src + e);
+      }
+    }
+    cp_async_commit();
+  };
+  if (warp < n_pairs) fetch(warp);
+  __syncthreads();  // mask box staged
 
   float J[32];
 #pragma unroll
   for (int u = 0; u < 32; ++u) J[u] = 0.f;
-
-  for (int j = it.job_begin + warp; j < it.job_end; j += kCoarseWarps) {
-    const LithoJob job = jobs[j];
-    const float w = (float)job.weight;
-    const float2* m = Mb + (size_t)job.clip * Bm * Bm;
-    const int mx = job.cx + dx + bm;
-    for (int c = 0; c < job.ncomp; ++c) {
-      const float2* tp = table + ((size_t)job.tab * ncomp_max + c) * npts;
+  const int half = lane >> 4, col = lane & 15;
+  constexpr uint64_t kNZ = band_mask32(kCoarseHMax32);
+  for (int pp = warp; pp < n_pairs; pp += kCoarseWarps) {
+    cp_async_wait_all();
+    __syncwarp();
+    {
+      const int t = 2 * pp + half;
       float2 v[32];
 #pragma unroll
       for (int i = 0; i < 32; ++i) v[i] = make_float2(0.f, 0.f);
-      if (col_live && mx >= 0 && mx < Bm) {
+      if (t < n_t && col < side) {
+        const LithoJob* jb = jobs + it.job_begin + t / ncomp;
+        const int mx = __ldg(&jb->cx) + (col - h) + bm, cy = __ldg(&jb->cy);
+        if (mx >= 0 && mx < Bm) {
+          const float2* tp = TAB + half * npad + col;
 #pragma unroll
-        for (int d = -kCoarseHMax32; d <= kCoarseHMax32; ++d) {
-          const int my = job.cy + d + bm;
-          if (d >= -h && d <= h && my >= 0 && my < Bm)
-            v[(d + 32) & 31] = cmul(__ldg(tp + (d + h) * side + (dx + h)), __ldg(m + (size_t)my * Bm + mx));
+          for (int d = -kCoarseHMax32; d <= kCoarseHMax32; ++d) {
+            const int my = cy + d + bm;
+            if (d >= -h && d <= h && my >= 0 && my < Bm) v[d & 31] = cmul(tp[(d + h) * side], msk[my * Bm + mx]);
+          }
         }
       }
-      fft_reg<32, +1>(v);  // over ky: T(kx = dx, v)
-      __syncwarp();
+      fft_reg_sparse<32, +1, kNZ>(v);  // over ky: T(kx = col - h, v)
+      if (col < side) {
+        float2* tr = T + (half * side + col) * kC32TLd;
 #pragma unroll
-      for (int i = 0; i < 32; ++i) tb[lane * 33 + i] = v[i];
-      __syncwarp();
-      // Pass-2 input: row `lane` of T, non-zero only at kx = d in [-h, h],
-      // i.e. register positions 0..7 and 25..31; 8..24 are cleared.
+        for (int i = 0; i < 32; ++i) tr[i] = v[i];
+      }
+    }
+    __syncwarp();
+    if (pp + kCoarseWarps < n_pairs) fetch(pp + kCoarseWarps);  // TAB is free again
 #pragma unroll
-      for (int i = kCoarseHMax32 + 1; i < 32 - kCoarseHMax32; ++i) v[i] = make_float2(0.f, 0.f);
+    for (int hh = 0; hh < 2; ++hh) {
+      const int t = 2 * pp + hh;
+      if (t >= n_t) break;
+      const float w = (float)__ldg(&jobs[it.job_begin + t / ncomp].weight);
+      float2 r[32];
+#pragma unroll
+      for (int i = 0; i < 32; ++i) r[i] = make_float2(0.f, 0.f);
+      const float2* tc = T + (hh * side) * kC32TLd + lane;
 #pragma unroll
       for (int d = -kCoarseHMax32; d <= kCoarseHMax32; ++d)
-        v[(d + 32) & 31] = (d >= -h && d <= h) ? tb[(d + h) * 33 + lane] : make_float2(0.f, 0.f);
-      fft_reg<32, +1>(v);  // over kx: e(u, v = lane)
+        if (d >= -h && d <= h) r[d & 31] = tc[(d + h) * kC32TLd];
+      fft_reg_sparse<32, +1, kNZ>(r);  // over kx: e(u, v = lane)
 #pragma unroll
-      for (int u = 0; u < 32; ++u) J[u] = fmaf(w, cabs2(v[u]), J[u]);
+      for (int u = 0; u < 32; ++u) J[u] = fmaf(w, cabs2(r[u]), J[u]);
     }
+    __syncwarp();
   }
 
   // Fixed-order reduction of the warps' J into this block's partial.
   __syncthreads();
-  float* js = reinterpret_cast<float*>(smem);  // [warp][v][u], kCoarseWarps x 1024 floats
+  float* js = reinterpret_cast<float*>(c32_raw);  // [warp][v][u]
 #pragma unroll
   for (int u = 0; u < 32; ++u) js[warp * 1024 + lane * 32 + u] = J[u];
   __syncthreads();
@@ -572,7 +634,7 @@ static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* tab
   if (e != cudaSuccess) return (int)e;
   mark(3);
   if (p.L == 32) {
-    const size_t sm_coarse = (size_t)kCoarseWarps * 32 * 33 * sizeof(float2);
+    const size_t sm_coarse = c32_smem(p.h, p.bm).total;
     cudaFuncSetAttribute(k_coarse32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_coarse);
     k_coarse32<<<p.n_items, kCoarseWarps * 32, sm_coarse, s>>>(items, jobs, table, p.h, p.ncomp_max, mb, p.bm,
                                                                 partial);
@@ -638,7 +700,7 @@ extern "C" int litho_coarse_image(const LithoAbbePlan* plan, const void* blob, c
   float* partial = reinterpret_cast<float*>(static_cast<char*>(ws) + l.partial);
   const int G = 4 * p.h + 1;
   if (p.L == 32) {
-    const size_t sm = (size_t)kCoarseWarps * 32 * 33 * sizeof(float2);
+    const size_t sm = c32_smem(p.h, p.bm).total;
     cudaFuncSetAttribute(k_coarse32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_coarse32<<<p.n_items, kCoarseWarps * 32, sm, s>>>(items, jobs, static_cast<const float2*>(table), p.h,
                                                         p.ncomp_max, static_cast<const float2*>(mb), p.bm, partial);

@@ -164,6 +164,137 @@ k_row_band_tma(const void* __restrict__ in, int n_rows, int rows_per_clip, int n
   }
 }
 
+// ---------------------------------------------------------------------------
+// Register-direct variant for power-of-two N in [32, 2048] (the common case).
+// Each lane loads the 32 samples of its residue b with coalesced loads
+// straight into registers (a warp reads 32 consecutive elements per load), so
+// no staging buffer limits the number of resident warps; the 32-point FFT
+// result stays in registers across the passes over the band. Real rows go two
+// at a time as one complex row z = r1 + i r2 and are separated on the band:
+// R1(k) = (Z(k) + conj Z(-k)) / 2, R2(k) = (Z(k) - conj Z(-k)) / 2i.
+// ---------------------------------------------------------------------------
+struct BandGeo {
+  int M, Lp, P, q, ld, Bm, npass, warps;
+  size_t y_per_warp, z_per_warp, off_y, off_z, total;
+};
+
+__host__ __device__ inline BandGeo band_geo(int n, int bm, int warps) {
+  BandGeo g{};
+  g.M = n >> 5;
+  g.Lp = g.M < 32 ? g.M : 32;
+  g.P = 32 / g.Lp;
+  g.q = g.M / g.Lp;
+  g.ld = g.M + 1;
+  g.Bm = 2 * bm + 1;
+  g.npass = (g.Bm + 31) >> 5;
+  g.warps = warps;
+  g.y_per_warp = (size_t)g.P * 32 * g.ld;          // float2
+  g.z_per_warp = (size_t)g.P * g.npass * 32;       // float2
+  g.off_y = (size_t)g.Bm * g.M * 8;                // after the twiddle table
+  g.off_z = g.off_y + (size_t)warps * g.y_per_warp * 8;
+  g.total = g.off_z + (size_t)warps * g.z_per_warp * 8;
+  return g;
+}
+
+template <bool CPLX>
+__global__ void __launch_bounds__(256, 2)
+k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int n, int bm,
+            float2* __restrict__ out, float scale, const float2* __restrict__ tw_inv) {
+  extern __shared__ __align__(16) float2 bsm[];
+  const BandGeo g = band_geo(n, bm, blockDim.x >> 5);
+  const int M = g.M, Bm = g.Bm, nmask = n - 1;
+  float2* TB = bsm;                                        // [k + bm][b] = w^(-k b)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* Y = bsm + g.off_y / 8 + warp * g.y_per_warp;   // [group][kp][b]
+  float2* Z = bsm + g.off_z / 8 + warp * g.z_per_warp;   // [group][k + bm] (real pairs)
+  for (int j = threadIdx.x; j < Bm * M; j += blockDim.x) {
+    const int k = j / M - bm, b = j % M;
+    TB[j] = tw_inv[(-k * b) & nmask];
+  }
+  __syncthreads();
+  const int pg = lane / g.Lp, bl = lane % g.Lp;
+  const int rows_per_iter = CPLX ? g.P : 2 * g.P;
+  const int n_iter = (n_rows + rows_per_iter - 1) / rows_per_iter;
+  for (int wi = blockIdx.x * g.warps + warp; wi < n_iter; wi += gridDim.x * g.warps) {
+    const int row0 = wi * rows_per_iter;
+    const int r1 = CPLX ? row0 + pg : row0 + 2 * pg;
+    const bool live = r1 < n_rows;
+    float2 v[32];
+    for (int p = 0; p < g.npass; ++p) {
+      for (int qq = 0; qq < g.q; ++qq) {
+        const int b = bl + qq * g.Lp;
+        if (p == 0 || g.q > 1) {
+          if (live) {
+            if (CPLX) {
+              const float2* src = static_cast<const float2*>(in) + (size_t)r1 * n + b;
+#pragma unroll
+              for (int a = 0; a < 32; ++a) v[a] = __ldcs(src + M * a);
+            } else {
+              const float* s1 = static_cast<const float*>(in) + (size_t)r1 * n + b;
+              const float* s2 = s1 + n;
+#pragma unroll
+              for (int a = 0; a < 32; ++a) v[a] = make_float2(__ldcs(s1 + M * a), __ldcs(s2 + M * a));
+            }
+          } else {
+#pragma unroll
+            for (int a = 0; a < 32; ++a) v[a] = make_float2(0.f, 0.f);
+          }
+          fft_reg<32, -1>(v);
+        }
+        float2* yr = Y + (pg * 32) * g.ld + b;
+#pragma unroll
+        for (int kp = 0; kp < 32; ++kp) {
+          const int k = band_k(kp, p, bm);
+          yr[kp * g.ld] = k <= bm ? cmul(v[kp], TB[(k + bm) * M + b]) : make_float2(0.f, 0.f);
+        }
+      }
+      __syncwarp();
+      const int k = band_k(lane, p, bm);
+      for (int r = 0; r < g.P; ++r) {
+        const float2* yr = Y + (r * 32 + lane) * g.ld;
+        float2 s0 = make_float2(0.f, 0.f), s1 = make_float2(0.f, 0.f);
+        int j = 0;
+        for (; j + 1 < M; j += 2) {
+          s0 = cadd(s0, yr[j]);
+          s1 = cadd(s1, yr[j + 1]);
+        }
+        if (j < M) s0 = cadd(s0, yr[j]);
+        const float2 sum = cadd(s0, s1);
+        if (k <= bm) {
+          if (CPLX) {
+            const int row = row0 + r;
+            if (row < n_rows) {
+              const int clip = row / rows_per_clip, i = row % rows_per_clip;
+              out[((size_t)clip * Bm + (k + bm)) * rows_per_clip + i] = cscale(sum, scale);
+            }
+          } else {
+            Z[r * g.npass * 32 + (k + bm)] = sum;
+          }
+        }
+      }
+      __syncwarp();
+    }
+    if (!CPLX) {
+      const float hs = 0.5f * scale;
+      for (int r = 0; r < g.P; ++r) {
+        const int ra = row0 + 2 * r;
+        if (ra >= n_rows) break;
+        const int clip = ra / rows_per_clip, i = ra % rows_per_clip;
+        const float2* zr = Z + r * g.npass * 32;
+        for (int kk = lane; kk < Bm; kk += 32) {
+          const float2 z = zr[kk], zm = zr[Bm - 1 - kk];       // Z(k), Z(-k)
+          const float2 o1 = make_float2((z.x + zm.x) * hs, (z.y - zm.y) * hs);
+          const float2 o2 = make_float2((z.y + zm.y) * hs, (zm.x - z.x) * hs);
+          float2* dst = out + ((size_t)clip * Bm + kk) * rows_per_clip + i;
+          dst[0] = o1;
+          dst[1] = o2;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
 // Fallback for N not a multiple of 32: one thread per (row, k), direct sum.
 template <bool CPLX>
 __global__ void k_row_band_direct(const void* __restrict__ in, int n_rows, int rows_per_clip, int n,
@@ -199,7 +330,27 @@ cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_
                                 int bm, float2* out, float scale, const float2* tw_inv,
                                 int num_sms, cudaStream_t st, int* status) {
   const int esz = cplx ? 8 : 4;
-  if (n % 32 == 0 && ((uintptr_t)in & 15) == 0) {
+  const int M = n >> 5;
+  if (n >= 32 && n <= 2048 && (n & (n - 1)) == 0 && (cplx || (rows_per_clip % 2 == 0 && n_rows % 2 == 0))) {
+    const int warps = n <= 1024 ? 8 : 4;
+    const BandGeo g = band_geo(n, bm, warps);
+    if (g.total > 200 * 1024) return cudaErrorInvalidValue;
+    const int rows_per_iter = cplx ? g.P : 2 * g.P;
+    const long long n_iter = ((long long)n_rows + rows_per_iter - 1) / rows_per_iter;
+    const int per_sm = (int)((227 * 1024) / g.total) >= 2 ? 2 : 1;
+    long long blocks = (n_iter + warps - 1) / warps;
+    if (blocks > (long long)num_sms * per_sm) blocks = (long long)num_sms * per_sm;
+    if (cplx) {
+      cudaFuncSetAttribute(k_band_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.total);
+      k_band_rows<true><<<(int)blocks, warps * 32, g.total, st>>>(in, n_rows, rows_per_clip, n, bm, out, scale,
+                                                                  tw_inv);
+    } else {
+      cudaFuncSetAttribute(k_band_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.total);
+      k_band_rows<false><<<(int)blocks, warps * 32, g.total, st>>>(in, n_rows, rows_per_clip, n, bm, out, scale,
+                                                                   tw_inv);
+    }
+  } else if (n % 32 == 0 && (32 % M == 0 || M % 32 == 0) && ((uintptr_t)in & 15) == 0) {
+    // TMA-staged variant: the residue layout needs M to divide 32 or 32 to divide M
     int warps = 4;
     while (warps > 1 && band_smem(n, esz, warps).total > 200 * 1024) warps >>= 1;
     const BandSmem L = band_smem(n, esz, warps);

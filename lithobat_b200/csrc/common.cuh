@@ -84,6 +84,82 @@ __device__ __forceinline__ void fft_reg(float2 (&v)[N]) {
   }
 }
 
+// The same transform for inputs known to be zero outside the bit mask NZ
+// (bit i set: v[i] may be non-zero). Butterflies with a known-zero operand
+// become copies or a single twiddle, so a pruned transform (a band of 2h+1
+// of 32 inputs) costs only the work its non-zeros need. The masks are
+// compile-time constants after unrolling, so every test below folds away.
+__host__ __device__ constexpr uint64_t nz_bitrev(uint64_t m, int log) {
+  uint64_t r = 0;
+  for (int i = 0; i < (1 << log); ++i)
+    if ((m >> i) & 1ull) r |= 1ull << bitrev(i, log);
+  return r;
+}
+__host__ __device__ constexpr uint64_t nz_after(uint64_t m, int n, int half) {
+  // non-zero mask after the butterfly stage of span `half`
+  uint64_t r = 0;
+  for (int base = 0; base < n; base += 2 * half)
+    for (int k = 0; k < half; ++k) {
+      const bool any = ((m >> (base + k)) & 1ull) || ((m >> (base + k + half)) & 1ull);
+      if (any) r |= (1ull << (base + k)) | (1ull << (base + k + half));
+    }
+  return r;
+}
+template <int N, int SIGN, uint64_t M, int HALF>
+struct SparseStage {
+  // one radix-2 stage of span HALF with non-zero mask M, then the next stage
+  static __device__ __forceinline__ void run(float2 (&v)[N]) {
+    if constexpr (HALF < N) {
+#pragma unroll
+      for (int base = 0; base < N; base += 2 * HALF) {
+#pragma unroll
+        for (int k = 0; k < HALF; ++k) {
+          const bool za = !((M >> (base + k)) & 1ull), zb = !((M >> (base + k + HALF)) & 1ull);
+          if (za && zb) {
+            // both zero: stays zero
+          } else if (zb) {
+            v[base + k + HALF] = v[base + k];
+          } else {
+            const float2 bw = twiddle64<SIGN>(v[base + k + HALF], k * (64 / (2 * HALF)));
+            if (za) {
+              v[base + k] = bw;
+              v[base + k + HALF] = make_float2(-bw.x, -bw.y);
+            } else {
+              const float2 a = v[base + k];
+              v[base + k] = cadd(a, bw);
+              v[base + k + HALF] = csub(a, bw);
+            }
+          }
+        }
+      }
+      SparseStage<N, SIGN, nz_after(M, N, HALF), 2 * HALF>::run(v);
+    }
+  }
+};
+
+template <int N, int SIGN, uint64_t NZ>
+__device__ __forceinline__ void fft_reg_sparse(float2 (&v)[N]) {
+  static_assert(N >= 2 && N <= 64 && (N & (N - 1)) == 0, "fft_reg_sparse: N in {2..64}");
+  constexpr int LOG = Log2<N>::value;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const int j = bitrev(i, LOG);
+    if (j > i) {
+      const float2 t = v[i];
+      v[i] = v[j];
+      v[j] = t;
+    }
+  }
+  SparseStage<N, SIGN, nz_bitrev(NZ, LOG), 1>::run(v);
+}
+
+// Non-zero mask of a 32-point sequence supported on d in [-H, H] (d mod 32).
+__host__ __device__ constexpr uint64_t band_mask32(int H) {
+  uint64_t m = 0;
+  for (int d = -H; d <= H; ++d) m |= 1ull << (d & 31);
+  return m;
+}
+
 // ---------------------------------------------------------------------------
 // FP64 with every rounding explicit (no FMA contraction), so that decisions
 // like "rho <= 1" reproduce numpy's IEEE double arithmetic bit for bit.
@@ -153,6 +229,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
+
+// Ampere-style asynchronous 8-byte global -> shared copies (LDGSTS), grouped
+// and waited on per thread.
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Device twiddle table w[j] = exp(sign * 2 pi i j / n), FP64 evaluated, FP32 stored.
 __global__ void k_twiddle_table(float2* w, int n, int sign);

@@ -81,20 +81,20 @@ def test_noalloc_matches_workspace_entry_point_on_two_calls_in_a_row(env):
 def test_noalloc_rejects_plans_beyond_its_scratch(env):
     torch, lb, nat, plan_abbe = env
     L = nat.lib()
-    # 1024^2 vector clips: ~36 clips need more than 32 MiB of scratch
+    # 1024^2 vector clips: ~100 clips need more than 32 MiB of scratch
     o = lb.OpticsConfig(NA=1.35, n_immersion=1.44, imaging_model="vector", polarisation="te",
                         source_type="annular", sigma_inner=0.5, sigma_outer=0.9, source_grid=31)
     v = lb.config.optics_view(o)
-    pd = plan_abbe([v] * 64, 1024, 1e-9, [[(v.defocus, v.image_index)]] * 64, 1.0, False, True)
+    pd = plan_abbe([v] * 128, 1024, 1e-9, [[(v.defocus, v.image_index)]] * 128, 1.0, False, True)
     ws_bytes = C.c_size_t(0)
     nat.check("litho_abbe_workspace", L.litho_abbe_workspace(C.byref(pd.plan), C.byref(ws_bytes)))
     assert ws_bytes.value > nat.NOALLOC_SCRATCH_BYTES
     # rejected on the host before anything is launched; the outputs stay untouched
     dev = torch.device("cuda", torch.cuda.current_device())
     blob = torch.from_numpy(pd.blob).to(dev)
-    m = torch.zeros((64, 1024, 1024), dtype=torch.complex64, device=dev)
-    img = torch.full((64, 1024, 1024), 7.0, dtype=torch.float32, device=dev)
-    pk = torch.full((64,), 7.0, dtype=torch.float32, device=dev)
+    m = torch.zeros((128, 1024, 1024), dtype=torch.complex64, device=dev)
+    img = torch.full((128, 1024, 1024), 7.0, dtype=torch.float32, device=dev)
+    pk = torch.full((128,), 7.0, dtype=torch.float32, device=dev)
     st = L.litho_abbe_noalloc(C.byref(pd.plan), blob.data_ptr(), m.data_ptr(), img.data_ptr(), pk.data_ptr(),
                               torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
