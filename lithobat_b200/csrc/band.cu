@@ -190,40 +190,46 @@ __host__ __device__ inline BandGeo band_geo(int n, int bm, int warps) {
   g.warps = warps;
   g.y_per_warp = (size_t)g.P * 32 * g.ld;          // float2
   g.z_per_warp = (size_t)g.P * g.npass * 32;       // float2
-  g.off_y = (size_t)g.Bm * g.M * 8;                // after the twiddle table
+  g.off_y = (size_t)g.npass * 32 * g.M * 8;        // after the twiddle table
   g.off_z = g.off_y + (size_t)warps * g.y_per_warp * 8;
   g.total = g.off_z + (size_t)warps * g.z_per_warp * 8;
   return g;
 }
 
-template <bool CPLX>
+// M = N / 32 is a template constant, so every shared-memory offset below is
+// an immediate; the twiddle table is laid out per (pass, register kp, residue
+// b) with zeros where band_k(kp, pass) falls outside the band.
+template <bool CPLX, int M>
 __global__ void __launch_bounds__(256, 2)
-k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int n, int bm,
-            float2* __restrict__ out, float scale, const float2* __restrict__ tw_inv) {
+k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int bm, float2* __restrict__ out,
+            float scale, const float2* __restrict__ tw_inv) {
+  constexpr int n = 32 * M, Lp = M < 32 ? M : 32, P = 32 / Lp, Q = M / Lp, LD = M + 1;
   extern __shared__ __align__(16) float2 bsm[];
   const BandGeo g = band_geo(n, bm, blockDim.x >> 5);
-  const int M = g.M, Bm = g.Bm, nmask = n - 1;
-  float2* TB = bsm;                                        // [k + bm][b] = w^(-k b)
+  const int Bm = g.Bm, npass = g.npass;
+  float2* TB = bsm;                                        // [pass][kp][b] = w^(-k b) or 0
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float2* Y = bsm + g.off_y / 8 + warp * g.y_per_warp;   // [group][kp][b]
   float2* Z = bsm + g.off_z / 8 + warp * g.z_per_warp;   // [group][k + bm] (real pairs)
-  for (int j = threadIdx.x; j < Bm * M; j += blockDim.x) {
-    const int k = j / M - bm, b = j % M;
-    TB[j] = tw_inv[(-k * b) & nmask];
+  for (int j = threadIdx.x; j < npass * 32 * M; j += blockDim.x) {
+    const int p = j / (32 * M), kp = (j / M) & 31, b = j % M;
+    const int k = band_k(kp, p, bm);
+    TB[j] = k <= bm ? tw_inv[(-k * b) & (n - 1)] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  const int pg = lane / g.Lp, bl = lane % g.Lp;
-  const int rows_per_iter = CPLX ? g.P : 2 * g.P;
+  const int pg = lane / Lp, bl = lane % Lp;
+  constexpr int rows_per_iter = CPLX ? P : 2 * P;
   const int n_iter = (n_rows + rows_per_iter - 1) / rows_per_iter;
   for (int wi = blockIdx.x * g.warps + warp; wi < n_iter; wi += gridDim.x * g.warps) {
     const int row0 = wi * rows_per_iter;
     const int r1 = CPLX ? row0 + pg : row0 + 2 * pg;
     const bool live = r1 < n_rows;
     float2 v[32];
-    for (int p = 0; p < g.npass; ++p) {
-      for (int qq = 0; qq < g.q; ++qq) {
-        const int b = bl + qq * g.Lp;
-        if (p == 0 || g.q > 1) {
+    for (int p = 0; p < npass; ++p) {
+#pragma unroll
+      for (int qq = 0; qq < Q; ++qq) {
+        const int b = bl + qq * Lp;
+        if (p == 0 || Q > 1) {
           if (live) {
             if (CPLX) {
               const float2* src = static_cast<const float2*>(in) + (size_t)r1 * n + b;
@@ -231,9 +237,8 @@ k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int n, i
               for (int a = 0; a < 32; ++a) v[a] = __ldcs(src + M * a);
             } else {
               const float* s1 = static_cast<const float*>(in) + (size_t)r1 * n + b;
-              const float* s2 = s1 + n;
 #pragma unroll
-              for (int a = 0; a < 32; ++a) v[a] = make_float2(__ldcs(s1 + M * a), __ldcs(s2 + M * a));
+              for (int a = 0; a < 32; ++a) v[a] = make_float2(__ldcs(s1 + M * a), __ldcs(s1 + n + M * a));
             }
           } else {
 #pragma unroll
@@ -241,24 +246,23 @@ k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int n, i
           }
           fft_reg<32, -1>(v);
         }
-        float2* yr = Y + (pg * 32) * g.ld + b;
+        const float2* tb = TB + p * 32 * M + b;
+        float2* yr = Y + pg * 32 * LD + b;
 #pragma unroll
-        for (int kp = 0; kp < 32; ++kp) {
-          const int k = band_k(kp, p, bm);
-          yr[kp * g.ld] = k <= bm ? cmul(v[kp], TB[(k + bm) * M + b]) : make_float2(0.f, 0.f);
-        }
+        for (int kp = 0; kp < 32; ++kp) yr[kp * LD] = cmul(v[kp], tb[kp * M]);
       }
       __syncwarp();
       const int k = band_k(lane, p, bm);
-      for (int r = 0; r < g.P; ++r) {
-        const float2* yr = Y + (r * 32 + lane) * g.ld;
+#pragma unroll
+      for (int r = 0; r < P; ++r) {
+        const float2* yr = Y + (r * 32 + lane) * LD;
         float2 s0 = make_float2(0.f, 0.f), s1 = make_float2(0.f, 0.f);
-        int j = 0;
-        for (; j + 1 < M; j += 2) {
+#pragma unroll
+        for (int j = 0; j + 1 < M; j += 2) {
           s0 = cadd(s0, yr[j]);
           s1 = cadd(s1, yr[j + 1]);
         }
-        if (j < M) s0 = cadd(s0, yr[j]);
+        if (M & 1) s0 = cadd(s0, yr[M - 1]);
         const float2 sum = cadd(s0, s1);
         if (k <= bm) {
           if (CPLX) {
@@ -268,7 +272,7 @@ k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int n, i
               out[((size_t)clip * Bm + (k + bm)) * rows_per_clip + i] = cscale(sum, scale);
             }
           } else {
-            Z[r * g.npass * 32 + (k + bm)] = sum;
+            Z[r * npass * 32 + (k + bm)] = sum;
           }
         }
       }
@@ -276,22 +280,56 @@ k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int n, i
     }
     if (!CPLX) {
       const float hs = 0.5f * scale;
-      for (int r = 0; r < g.P; ++r) {
+#pragma unroll
+      for (int r = 0; r < P; ++r) {
         const int ra = row0 + 2 * r;
-        if (ra >= n_rows) break;
-        const int clip = ra / rows_per_clip, i = ra % rows_per_clip;
-        const float2* zr = Z + r * g.npass * 32;
-        for (int kk = lane; kk < Bm; kk += 32) {
-          const float2 z = zr[kk], zm = zr[Bm - 1 - kk];       // Z(k), Z(-k)
-          const float2 o1 = make_float2((z.x + zm.x) * hs, (z.y - zm.y) * hs);
-          const float2 o2 = make_float2((z.y + zm.y) * hs, (zm.x - z.x) * hs);
-          float2* dst = out + ((size_t)clip * Bm + kk) * rows_per_clip + i;
-          dst[0] = o1;
-          dst[1] = o2;
+        if (ra < n_rows) {
+          const int clip = ra / rows_per_clip, i = ra % rows_per_clip;
+          const float2* zr = Z + r * npass * 32;
+          for (int kk = lane; kk < Bm; kk += 32) {
+            const float2 z = zr[kk], zm = zr[Bm - 1 - kk];       // Z(k), Z(-k)
+            const float2 o1 = make_float2((z.x + zm.x) * hs, (z.y - zm.y) * hs);
+            const float2 o2 = make_float2((z.y + zm.y) * hs, (zm.x - z.x) * hs);
+            float2* dst = out + ((size_t)clip * Bm + kk) * rows_per_clip + i;
+            dst[0] = o1;
+            dst[1] = o2;
+          }
         }
       }
       __syncwarp();
     }
+  }
+}
+
+template <bool CPLX, int M>
+static cudaError_t launch_band_rows_m(const void* in, int n_rows, int rows_per_clip, int bm, float2* out,
+                                      float scale, const float2* tw_inv, int num_sms, cudaStream_t st) {
+  const int n = 32 * M;
+  const int warps = n <= 1024 ? 8 : 4;
+  const BandGeo g = band_geo(n, bm, warps);
+  if (g.total > 200 * 1024) return cudaErrorInvalidValue;
+  const int rows_per_iter = CPLX ? g.P : 2 * g.P;
+  const long long n_iter = ((long long)n_rows + rows_per_iter - 1) / rows_per_iter;
+  const int per_sm = (int)((227 * 1024) / g.total) >= 2 ? 2 : 1;
+  long long blocks = (n_iter + warps - 1) / warps;
+  if (blocks > (long long)num_sms * per_sm) blocks = (long long)num_sms * per_sm;
+  cudaFuncSetAttribute(k_band_rows<CPLX, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.total);
+  k_band_rows<CPLX, M><<<(int)blocks, warps * 32, g.total, st>>>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv);
+  return cudaGetLastError();
+}
+
+template <bool CPLX>
+static cudaError_t launch_band_rows(const void* in, int n_rows, int rows_per_clip, int n, int bm, float2* out,
+                                    float scale, const float2* tw_inv, int num_sms, cudaStream_t st) {
+  switch (n) {
+    case 32: return launch_band_rows_m<CPLX, 1>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms, st);
+    case 64: return launch_band_rows_m<CPLX, 2>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms, st);
+    case 128: return launch_band_rows_m<CPLX, 4>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms, st);
+    case 256: return launch_band_rows_m<CPLX, 8>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms, st);
+    case 512: return launch_band_rows_m<CPLX, 16>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms, st);
+    case 1024: return launch_band_rows_m<CPLX, 32>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms, st);
+    case 2048: return launch_band_rows_m<CPLX, 64>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms, st);
+    default: return cudaErrorInvalidValue;
   }
 }
 
@@ -332,23 +370,10 @@ cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_
   const int esz = cplx ? 8 : 4;
   const int M = n >> 5;
   if (n >= 32 && n <= 2048 && (n & (n - 1)) == 0 && (cplx || (rows_per_clip % 2 == 0 && n_rows % 2 == 0))) {
-    const int warps = n <= 1024 ? 8 : 4;
-    const BandGeo g = band_geo(n, bm, warps);
-    if (g.total > 200 * 1024) return cudaErrorInvalidValue;
-    const int rows_per_iter = cplx ? g.P : 2 * g.P;
-    const long long n_iter = ((long long)n_rows + rows_per_iter - 1) / rows_per_iter;
-    const int per_sm = (int)((227 * 1024) / g.total) >= 2 ? 2 : 1;
-    long long blocks = (n_iter + warps - 1) / warps;
-    if (blocks > (long long)num_sms * per_sm) blocks = (long long)num_sms * per_sm;
-    if (cplx) {
-      cudaFuncSetAttribute(k_band_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.total);
-      k_band_rows<true><<<(int)blocks, warps * 32, g.total, st>>>(in, n_rows, rows_per_clip, n, bm, out, scale,
-                                                                  tw_inv);
-    } else {
-      cudaFuncSetAttribute(k_band_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.total);
-      k_band_rows<false><<<(int)blocks, warps * 32, g.total, st>>>(in, n_rows, rows_per_clip, n, bm, out, scale,
-                                                                   tw_inv);
-    }
+    const cudaError_t e = cplx ? launch_band_rows<true>(in, n_rows, rows_per_clip, n, bm, out, scale, tw_inv, num_sms, st)
+                               : launch_band_rows<false>(in, n_rows, rows_per_clip, n, bm, out, scale, tw_inv, num_sms,
+                                                         st);
+    if (e != cudaSuccess) return e;
   } else if (n % 32 == 0 && (32 % M == 0 || M % 32 == 0) && ((uintptr_t)in & 15) == 0) {
     // TMA-staged variant: the residue layout needs M to divide 32 or 32 to divide M
     int warps = 4;
