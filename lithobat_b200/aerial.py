@@ -207,7 +207,7 @@ def _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, ite
 
 
 def plan_from_table(n: int, pixel_size: float, n_clips: int, weights, h: int, mask_complex: bool,
-                    norm_mode=(0, 1.0), items_per_job_group: int = 4) -> AbbePlanData:
+                    norm_mode=(0, 1.0), items_per_job_group: int = 0) -> AbbePlanData:
     """Plan that images every clip with K unshifted coherent systems whose
     spectra are given by a caller-built table (the SOCS forward,
     hopkins.py:215-217): job (clip c, kernel k) has weight weights[k] and
@@ -229,7 +229,9 @@ def plan_from_table(n: int, pixel_size: float, n_clips: int, weights, h: int, ma
     pupils = np.zeros(1, dtype=nat.PUPIL_DTYPE)
     pupils["wavelength"], pupils["NA"], pupils["n_image"] = 1.0, 1.0, 1.0
     slots = np.arange(K, dtype=np.int32)
-    per = max(1, int(items_per_job_group))
+    # 0: two jobs per item (one per warp of the L = 64 kernels) until there are
+    # enough items to fill the GPU, then up to 8
+    per = int(items_per_job_group) or min(8, max(2, (n_clips * K) // (4 * 148)))
     item_rows, out_items = [], [0]
     for c in range(n_clips):
         for j in range(c * K, (c + 1) * K, per):

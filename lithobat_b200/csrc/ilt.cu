@@ -27,13 +27,16 @@ cudaError_t launch_synth_real(const float2* box, int G, int n, int n_fields, con
 int synth_blocks_for(int n);
 
 // ---------------------------------------------------------------------------
-// g_L(u, v) = sum_{|g| <= 2h} Gb(g) w64^(g.(u, v)), one block per clip.
-// Gb: (4h+1)^2 box [gy][gx]. Output [clip][v][u] complex.
+// g_L(u, v) = sum_{|g| <= 2h} Gb(g) w64^(g.(u, v)). Grid (clip, 64 / kGlRows):
+// a block forms kGlRows rows v of one clip. Gb: (4h+1)^2 box [gy][gx].
+// Output [clip][v][u] complex.
 // ---------------------------------------------------------------------------
+constexpr int kGlRows = 4;
+
 __global__ void k_gl64(const float2* __restrict__ Gb, int h, float2* __restrict__ gl) {
-  __shared__ float2 T[64 * 61];   // [v][gx], gx index < 4h+1 <= 61
+  __shared__ float2 T[kGlRows * 61];   // [v][gx], gx index < 4h+1 <= 61
   __shared__ float2 tw[64];
-  const int c = blockIdx.x, G = 4 * h + 1, g0 = 2 * h;
+  const int c = blockIdx.x, v0 = blockIdx.y * kGlRows, G = 4 * h + 1, g0 = 2 * h;
   for (int t = threadIdx.x; t < 64; t += blockDim.x) {
     double s, co;
     sincospi(2.0 * t / 64.0, &s, &co);
@@ -41,18 +44,18 @@ __global__ void k_gl64(const float2* __restrict__ Gb, int h, float2* __restrict_
   }
   __syncthreads();
   const float2* B = Gb + (size_t)c * G * G;
-  for (int id = threadIdx.x; id < 64 * G; id += blockDim.x) {
-    const int v = id / G, gx = id % G;
+  for (int id = threadIdx.x; id < kGlRows * G; id += blockDim.x) {
+    const int r = id / G, gx = id % G, v = v0 + r;
     float2 acc = make_float2(0.f, 0.f);
-    for (int gy = 0; gy < G; ++gy) acc = cadd(acc, cmul(B[gy * G + gx], tw[((gy - g0) * v) & 63]));
-    T[v * 61 + gx] = acc;
+    for (int gy = 0; gy < G; ++gy) acc = cadd(acc, cmul(__ldg(B + gy * G + gx), tw[((gy - g0) * v) & 63]));
+    T[r * 61 + gx] = acc;
   }
   __syncthreads();
-  float2* out = gl + (size_t)c * 4096;
-  for (int id = threadIdx.x; id < 4096; id += blockDim.x) {
-    const int v = id >> 6, u = id & 63;
+  float2* out = gl + (size_t)c * 4096 + (size_t)v0 * 64;
+  for (int id = threadIdx.x; id < kGlRows * 64; id += blockDim.x) {
+    const int r = id >> 6, u = id & 63;
     float2 acc = make_float2(0.f, 0.f);
-    for (int gx = 0; gx < G; ++gx) acc = cadd(acc, cmul(T[v * 61 + gx], tw[((gx - g0) * u) & 63]));
+    for (int gx = 0; gx < G; ++gx) acc = cadd(acc, cmul(T[r * 61 + gx], tw[((gx - g0) * u) & 63]));
     out[id] = acc;
   }
 }
@@ -535,7 +538,7 @@ extern "C" int litho_socs_adjoint(const LithoAbbePlan* plan, const void* blob, c
   const int32_t* out_items = reinterpret_cast<const int32_t*>(b + p.off_out_items);
   float2* gl = static_cast<float2*>(ws);
   float2* part = reinterpret_cast<float2*>(static_cast<char*>(ws) + align16((int64_t)p.n_clips * 4096 * 8));
-  k_gl64<<<p.n_clips, 256, 0, s>>>(static_cast<const float2*>(sens_box), p.h, gl);
+  k_gl64<<<dim3(p.n_clips, 64 / kGlRows), 256, 0, s>>>(static_cast<const float2*>(sens_box), p.h, gl);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
   const size_t sm = (size_t)kAdjWarps * (31 * kAdjLd + 31 * 32) * sizeof(float2);
