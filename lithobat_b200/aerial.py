@@ -53,6 +53,23 @@ def disc_halfwidth(NA: float, wavelength: float, n: int, pixel_size: float) -> t
     return R, int(math.floor(R + 0.5 + 1e-9 * (1.0 + R)))
 
 
+def coarse_grid(h: int) -> int:
+    """The coarse grid side: the smallest power of two L >= 32 with L >= 4h + 1,
+    on which |E|^2 of a (2h+1)^2 spectrum is exact."""
+    L = 32
+    while L < 4 * h + 1:
+        L *= 2
+    return L
+
+
+def fused_supported(n: int, L: int) -> bool:
+    """Can the band-limited engine run this grid? (L <= 64 on chip; 128..1024
+    through the wide engine, which also needs a power-of-two N >= L.)"""
+    if L <= 64:
+        return True
+    return L <= 1024 and L <= n <= 4096 and (n & (n - 1)) == 0
+
+
 @dataclass
 class AbbePlanData:
     plan: nat.AbbePlan
@@ -84,11 +101,6 @@ def plan_abbe(views: Sequence, n: int, pixel_size: float, planes: Sequence[Seque
     (defocus, n_image); every clip has the same number of planes."""
     key = (tuple(repr(v) for v in views), n, pixel_size, tuple(tuple(map(tuple, p)) for p in planes),
            float(dose), bool(return_raw), bool(mask_complex), items_per_job_group)
-    h = max(disc_halfwidth(v.NA, v.wavelength, n, pixel_size)[1] for v in views)
-    if 4 * h + 1 > 64:
-        raise NotImplementedError(
-            f"pupil half-width {h} bins needs a coarse grid above 64 (4h+1 = {4 * h + 1}); "
-            "use engine='plain' for this grid")
     hit = _PLANS.get(key)
     if hit is not None:
         return hit
@@ -172,7 +184,13 @@ def _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, ite
     # jobs are grouped by output (k); chunk each output's run into work items
     # (0: as many jobs per item as keeps about two waves of blocks, at most 32)
     n_out = C * P
-    per = int(items_per_job_group) or min(32, max(1, n_jobs // (2 * 4 * 148)))
+    L = coarse_grid(h)
+    if items_per_job_group:
+        per = int(items_per_job_group)
+    elif L > 64:
+        per = 8   # wide engine: one partial L x L image per item
+    else:
+        per = min(32, max(1, n_jobs // (2 * 4 * 148)))
     starts = np.searchsorted(jobs["out"], np.arange(n_out + 1), side="left")
     item_rows, out_items = [], [0]
     for o in range(n_out):
@@ -194,9 +212,6 @@ def _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, ite
                 norm[k] = (0, normalisation_scale(v.normalisation, 1.0, clears[k], dose))
     bm = int(max(np.abs(jobs["cx"]).max(), np.abs(jobs["cy"]).max())) + h
     blob, offs = nat.blob([jobs, pupils, items, out_items, norm, slots])
-    L = 32
-    while L < 4 * h + 1:
-        L *= 2
     plan = nat.AbbePlan(
         n=n, n_clips=C, n_out=n_out, n_jobs=n_jobs, n_items=len(items), n_pupils=len(pupils),
         h=h, bm=bm, L=L, mask_complex=int(mask_complex), ncomp_max=3 if vec_any else 1, n_tab=n_tab,
@@ -215,11 +230,7 @@ def plan_from_table(n: int, pixel_size: float, n_clips: int, weights, h: int, ma
     K = len(weights)
     if K == 0:
         raise ValueError("no kernels to image with")
-    L = 32
-    while L < 4 * h + 1:
-        L *= 2
-    if L > 64:
-        raise NotImplementedError(f"kernel band half-width {h} bins needs a coarse grid above 64")
+    L = coarse_grid(h)
     jobs = np.zeros(n_clips * K, dtype=nat.JOB_DTYPE)
     jobs["weight"] = np.tile(np.asarray(weights, dtype=np.float64), n_clips)
     jobs["clip"] = np.repeat(np.arange(n_clips), K)
@@ -231,7 +242,7 @@ def plan_from_table(n: int, pixel_size: float, n_clips: int, weights, h: int, ma
     slots = np.arange(K, dtype=np.int32)
     # 0: two jobs per item (one per warp of the L = 64 kernels) until there are
     # enough items to fill the GPU, then up to 8
-    per = int(items_per_job_group) or min(8, max(2, (n_clips * K) // (4 * 148)))
+    per = int(items_per_job_group) or (8 if L > 64 else min(8, max(2, (n_clips * K) // (4 * 148))))
     item_rows, out_items = [], [0]
     for c in range(n_clips):
         for j in range(c * K, (c + 1) * K, per):
@@ -326,6 +337,8 @@ def run_abbe(pd: AbbePlanData, masks_dev, out=None, peak=None, stream=None, engi
     n = pd.plan.n
     if engine not in ENGINES:
         raise ValueError(f"engine must be one of {ENGINES}, got {engine!r}")
+    if engine == "fused" and not fused_supported(n, int(pd.plan.L)):
+        engine = "plain"   # pupil wider than the grid allows a coarse grid for: full-grid GPU engine
     if out is None:
         out = torch.empty((pd.n_out, n, n), dtype=torch.float32, device=dev)
     if peak is None:

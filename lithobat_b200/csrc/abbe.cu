@@ -32,6 +32,10 @@ namespace litho {
 cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_per_clip, int n,
                                 int bm, float2* out, float scale, const float2* tw_inv,
                                 int num_sms, cudaStream_t st, int* status);
+bool wide_plan_ok(const LithoAbbePlan& p);
+int64_t wide_workspace_bytes(const LithoAbbePlan& p);
+int abbe_wide_run(const LithoAbbePlan& p, const void* blob, const void* table_in, const void* mask, float* image,
+                  float* peak, void* ws, cudaStream_t s, int num_sms, cudaEvent_t* ev);
 
 // ---------------------------------------------------------------------------
 // 1. pupil table: table[slot][comp][(dy+h)(2h+1) + dx+h], one block per slot,
@@ -523,6 +527,10 @@ struct AbbeLayout {
 
 static AbbeLayout abbe_layout(const LithoAbbePlan& p) {
   AbbeLayout l{};
+  if (p.L > 64) {  // wide engine (wide.cu); its status word is also at offset 0
+    l.total = wide_workspace_bytes(p);
+    return l;
+  }
   const int64_t Bm = 2 * p.bm + 1, side = 2 * p.h + 1, G = 4 * p.h + 1;
   int64_t off = 0;
   l.status = off;   off = align16(off + 16);
@@ -543,8 +551,11 @@ static int check_plan(const LithoAbbePlan* p) {
       p->n_pupils < 1 || p->h < 0 || p->bm < 0 || p->n_tab < 1 || p->n_tab > p->n_jobs)
     return LITHO_E_SIZE;
   if (p->ncomp_max != 1 && p->ncomp_max != 3) return LITHO_E_SIZE;
-  if (p->L != 32 && p->L != 64) return LITHO_E_UNSUPPORTED;
-  if (4 * p->h + 1 > p->L || p->h > (p->L == 32 ? kCoarseHMax32 : kCoarseHMax64)) return LITHO_E_BAND;
+  if (p->L == 32 || p->L == 64) {
+    if (4 * p->h + 1 > p->L || p->h > (p->L == 32 ? kCoarseHMax32 : kCoarseHMax64)) return LITHO_E_BAND;
+  } else if (!wide_plan_ok(*p)) {
+    return LITHO_E_UNSUPPORTED;
+  }
   if (p->bm < p->h) return LITHO_E_BAND;
   if (!(p->pixel_size > 0.0)) return LITHO_E_SIZE;
   const int64_t offs[6] = {p->off_jobs, p->off_pupils, p->off_items, p->off_out_items, p->off_norm,
@@ -593,6 +604,7 @@ static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* tab
   if ((int64_t)ws_bytes < l.total) return LITHO_E_WORKSPACE;
   if (p.n_items == 0 || p.n_jobs == 0) return LITHO_E_SIZE;
 
+  if (p.L > 64) return abbe_wide_run(p, blob, table_in, mask, image, peak, ws, s, num_sms_cached(), ev);
   const char* b = static_cast<const char*>(blob);
   const LithoJob* jobs = reinterpret_cast<const LithoJob*>(b + p.off_jobs);
   const LithoPupil* pupils = reinterpret_cast<const LithoPupil*>(b + p.off_pupils);
@@ -691,6 +703,7 @@ extern "C" int litho_coarse_image(const LithoAbbePlan* plan, const void* blob, c
   if (st) return st;
   if (!blob || !table || !mb || !bbox_out || !ws) return LITHO_E_NULL;
   const LithoAbbePlan& p = *plan;
+  if (p.L > 64) return LITHO_E_UNSUPPORTED;
   const AbbeLayout l = abbe_layout(p);
   if ((int64_t)ws_bytes < l.total) return LITHO_E_WORKSPACE;
   const char* b = static_cast<const char*>(blob);

@@ -175,6 +175,7 @@ k_row_band_tma(const void* __restrict__ in, int n_rows, int rows_per_clip, int n
 // ---------------------------------------------------------------------------
 struct BandGeo {
   int M, Lp, P, q, ld, Bm, npass, warps;
+  bool tb_smem;                                    // per-pass twiddle table in shared memory
   size_t y_per_warp, z_per_warp, off_y, off_z, total;
 };
 
@@ -190,7 +191,8 @@ __host__ __device__ inline BandGeo band_geo(int n, int bm, int warps) {
   g.warps = warps;
   g.y_per_warp = (size_t)g.P * 32 * g.ld;          // float2
   g.z_per_warp = (size_t)g.P * g.npass * 32;       // float2
-  g.off_y = (size_t)g.npass * 32 * g.M * 8;        // after the twiddle table
+  g.tb_smem = (size_t)g.npass * 32 * g.M * 8 <= 64 * 1024;
+  g.off_y = g.tb_smem ? (size_t)g.npass * 32 * g.M * 8 : 0;   // after the twiddle table
   g.off_z = g.off_y + (size_t)warps * g.y_per_warp * 8;
   g.total = g.off_z + (size_t)warps * g.z_per_warp * 8;
   return g;
@@ -211,10 +213,12 @@ k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int bm, 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float2* Y = bsm + g.off_y / 8 + warp * g.y_per_warp;   // [group][kp][b]
   float2* Z = bsm + g.off_z / 8 + warp * g.z_per_warp;   // [group][k + bm] (real pairs)
-  for (int j = threadIdx.x; j < npass * 32 * M; j += blockDim.x) {
-    const int p = j / (32 * M), kp = (j / M) & 31, b = j % M;
-    const int k = band_k(kp, p, bm);
-    TB[j] = k <= bm ? tw_inv[(-k * b) & (n - 1)] : make_float2(0.f, 0.f);
+  if (g.tb_smem) {
+    for (int j = threadIdx.x; j < npass * 32 * M; j += blockDim.x) {
+      const int p = j / (32 * M), kp = (j / M) & 31, b = j % M;
+      const int k = band_k(kp, p, bm);
+      TB[j] = k <= bm ? tw_inv[(-k * b) & (n - 1)] : make_float2(0.f, 0.f);
+    }
   }
   __syncthreads();
   const int pg = lane / Lp, bl = lane % Lp;
@@ -246,10 +250,18 @@ k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int bm, 
           }
           fft_reg<32, -1>(v);
         }
-        const float2* tb = TB + p * 32 * M + b;
         float2* yr = Y + pg * 32 * LD + b;
+        if (g.tb_smem) {
+          const float2* tb = TB + p * 32 * M + b;
 #pragma unroll
-        for (int kp = 0; kp < 32; ++kp) yr[kp * LD] = cmul(v[kp], tb[kp * M]);
+          for (int kp = 0; kp < 32; ++kp) yr[kp * LD] = cmul(v[kp], tb[kp * M]);
+        } else {  // wide bands: twiddles from the global table (L1-resident)
+#pragma unroll
+          for (int kp = 0; kp < 32; ++kp) {
+            const int k = band_k(kp, p, bm);
+            yr[kp * LD] = k <= bm ? cmul(v[kp], __ldg(tw_inv + ((-k * b) & (n - 1)))) : make_float2(0.f, 0.f);
+          }
+        }
       }
       __syncwarp();
       const int k = band_k(lane, p, bm);

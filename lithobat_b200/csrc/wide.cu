@@ -1,0 +1,316 @@
+// Abbe imaging for wide pupils: the band-limited engine on coarse grids of
+// L = 128 .. 1024 points (pupil half-width h >= 16 bins, e.g. EUV clips at
+// 512^2 and above), where one coherent system's L x L transform no longer
+// fits a warp's registers.
+//
+// Same mathematics as abbe.cu (expose/aerial_image.py:421-494 restated on
+// the smallest grid that holds |E|^2 exactly, L >= 4h + 1), with the two
+// passes of each coherent transform split across thread blocks:
+//   pass A (k_wide_cols): per transform and chunk of spectral columns kx, the
+//       inverse L-point FFT over ky of P M on the (2h+1)-row band -> T[kx][v]
+//       in global memory (L2-resident for a chunk of jobs);
+//   pass B (k_wide_rows): per work item and chunk of rows v, the inverse
+//       L-point FFT over kx of T[.][v] for every transform of the item and
+//       J(u, v) += w |e|^2 in shared memory -> the item's partial J;
+//   reduce (k_wide_reduce) in item order, F = FFT_L(J) / L^2 and the image
+//       band box B(g), |g| <= 2h (k_wide_box);
+//   synthesis: B scattered into an N x N spectrum, two outputs per complex
+//       inverse FFT (B is Hermitian, so each image is real), then the
+//       normalisation of aerial_image.py:217-241.
+// Transforms run in shared memory (fftsmem.cuh); every reduction has a fixed
+// order, so results are deterministic.
+#include "common.cuh"
+#include "fftsmem.cuh"
+
+namespace litho {
+
+cudaError_t plain_fft2(const void* in, bool in_real, float2* buf, long long planes, int n, int sign, float scale_rows,
+                       float scale_cols, const float2* tw, cudaStream_t st);
+cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_per_clip, int n, int bm,
+                                float2* out, float scale, const float2* tw_inv, int num_sms, cudaStream_t st,
+                                int* status);
+__global__ void k_pupil_table(const LithoJob* __restrict__ jobs, const int32_t* __restrict__ slots,
+                              const LithoPupil* __restrict__ pupils, int n_tab, int n, double pixel_size, int h,
+                              int ncomp_max, float2* __restrict__ table);
+__global__ void k_normalise(const float* __restrict__ blockmax, int nblk, const LithoNorm* __restrict__ norm,
+                            int n, float* __restrict__ image, float* __restrict__ peak, int apply_mode0);
+
+constexpr int kWideCols = 16;       // spectral columns per pass-A block
+constexpr int kWideRows = 16;       // coarse rows per pass-B block
+constexpr int kWideMaxBlk = 256;    // block maxima per output
+constexpr int64_t kWideTBudget = 512ll << 20;   // bytes of pass-A output per job chunk
+constexpr int kWideSpecPairs = 4;   // output pairs per synthesis chunk
+
+static int ilog2w(int n) {
+  int l = 0;
+  while ((1 << l) < n) ++l;
+  return l;
+}
+
+// Pass A. Grid (transform t of the chunk, column chunk). T[t][kx + h][v].
+__global__ void __launch_bounds__(256)
+k_wide_cols(const LithoJob* __restrict__ jobs, int j0, int ncomp_max, const float2* __restrict__ table, int h,
+            const float2* __restrict__ Mb, int bm, int L, int log2L, const float2* __restrict__ twL,
+            float2* __restrict__ T) {
+  extern __shared__ float2 wsm[];
+  float2* tw = wsm;
+  float2* s = wsm + L;  // [kWideCols][L]
+  const int t = blockIdx.x, c0 = blockIdx.y * kWideCols;
+  const int side = 2 * h + 1, npts = side * side, Bm = 2 * bm + 1;
+  const int j = j0 + t / ncomp_max, c = t % ncomp_max;
+  const LithoJob job = jobs[j];
+  if (c >= job.ncomp) return;
+  const int lines = (side - c0) < kWideCols ? (side - c0) : kWideCols;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twL[i];
+  for (int i = threadIdx.x; i < lines * L; i += blockDim.x) s[i] = make_float2(0.f, 0.f);
+  __syncthreads();
+  const float2* tp = table + ((size_t)job.tab * ncomp_max + c) * npts;
+  const float2* m = Mb + (size_t)job.clip * Bm * Bm;
+  for (int id = threadIdx.x; id < lines * side; id += blockDim.x) {
+    const int r = id / side, di = id % side;
+    const int kx = c0 + r - h, d = di - h;
+    const int mx = job.cx + kx + bm, my = job.cy + d + bm;
+    if (mx >= 0 && mx < Bm && my >= 0 && my < Bm)
+      s[r * L + brev(d & (L - 1), log2L)] = cmul(__ldg(tp + di * side + (kx + h)), __ldg(m + (size_t)my * Bm + mx));
+  }
+  block_fft_lines<+1>(s, L, lines, L, tw);
+  float2* dst = T + ((size_t)t * side + c0) * L;
+  for (int i = threadIdx.x; i < lines * L; i += blockDim.x) dst[i] = s[i];
+}
+
+// Pass B. Grid (item, row chunk). Adds the item's transforms whose jobs lie
+// in [j0, j0 + nj) to partial[item][v][u].
+__global__ void __launch_bounds__(256)
+k_wide_rows(const LithoItem* __restrict__ items, const LithoJob* __restrict__ jobs, int j0, int nj, int ncomp_max,
+            int h, int L, int log2L, const float2* __restrict__ twL, const float2* __restrict__ T,
+            float* __restrict__ partial) {
+  extern __shared__ float2 wsm[];
+  float2* tw = wsm;
+  float2* s = wsm + L;                                             // [kWideRows][L]
+  float* J = reinterpret_cast<float*>(s + kWideRows * L);          // [kWideRows][L]
+  const LithoItem it = items[blockIdx.x];
+  const int jb = it.job_begin > j0 ? it.job_begin : j0;
+  const int je = it.job_end < j0 + nj ? it.job_end : j0 + nj;
+  if (jb >= je) return;
+  const int v0 = blockIdx.y * kWideRows, side = 2 * h + 1;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twL[i];
+  float* pj = partial + ((size_t)blockIdx.x * L + v0) * L;
+  for (int i = threadIdx.x; i < kWideRows * L; i += blockDim.x) J[i] = pj[i];
+  for (int j = jb; j < je; ++j) {
+    const LithoJob job = jobs[j];
+    const float w = (float)job.weight;
+    for (int c = 0; c < job.ncomp; ++c) {
+      const float2* Tt = T + (size_t)((j - j0) * ncomp_max + c) * side * L;
+      __syncthreads();  // previous transform's reads of s are done
+      for (int i = threadIdx.x; i < kWideRows * L; i += blockDim.x) s[i] = make_float2(0.f, 0.f);
+      __syncthreads();
+      for (int id = threadIdx.x; id < side * kWideRows; id += blockDim.x) {
+        const int ki = id / kWideRows, r = id % kWideRows;
+        s[r * L + brev((ki - h) & (L - 1), log2L)] = Tt[(size_t)ki * L + v0 + r];
+      }
+      block_fft_lines<+1>(s, L, kWideRows, L, tw);
+      for (int i = threadIdx.x; i < kWideRows * L; i += blockDim.x) J[i] = fmaf(w, cabs2(s[i]), J[i]);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kWideRows * L; i += blockDim.x) pj[i] = J[i];
+}
+
+// J[o] = sum of its items' partials, in item order.
+__global__ void k_wide_reduce(const int32_t* __restrict__ out_items, const float* __restrict__ partial, int LL,
+                              float* __restrict__ J) {
+  const int o = blockIdx.y;
+  const int i0 = out_items[o], i1 = out_items[o + 1];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < LL; i += gridDim.x * blockDim.x) {
+    float acc = 0.f;
+    for (int it = i0; it < i1; ++it) acc += partial[(size_t)it * LL + i];
+    J[(size_t)o * LL + i] = acc;
+  }
+}
+
+// Image band box B(g) = F(g mod L), |g| <= 2h (F already scaled by 1/L^2).
+__global__ void k_wide_box(const float2* __restrict__ F, int L, int h, float2* __restrict__ bbox) {
+  const int o = blockIdx.y, G = 4 * h + 1, g0 = 2 * h;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G * G; i += gridDim.x * blockDim.x) {
+    const int gy = i / G - g0, gx = i % G - g0;
+    bbox[(size_t)o * G * G + i] = F[((size_t)o * L + (gy & (L - 1))) * L + (gx & (L - 1))];
+  }
+}
+
+// spec[pair] = B_{2p} + i B_{2p+1} on the N x N grid (zero off the box).
+__global__ void k_wide_spec(const float2* __restrict__ bbox, int o0, int n_out, int h, int n,
+                            float2* __restrict__ spec) {
+  const int pr = blockIdx.y, G = 4 * h + 1, g0 = 2 * h;
+  const int oa = o0 + 2 * pr, ob = oa + 1;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G * G; i += gridDim.x * blockDim.x) {
+    const int gy = i / G - g0, gx = i % G - g0;
+    const float2 a = bbox[(size_t)oa * G * G + i];
+    const float2 b = ob < n_out ? bbox[(size_t)ob * G * G + i] : make_float2(0.f, 0.f);
+    spec[((size_t)pr * n + ((gy + n) % n)) * n + ((gx + n) % n)] = make_float2(a.x - b.y, a.y + b.x);
+  }
+}
+
+// image[o] = Re / Im of the pair's synthesis, times the mode-0 scale; block
+// maxima of the raw image.
+__global__ void k_wide_real(const float2* __restrict__ spec, int o0, int n_out, int n, const LithoNorm* __restrict__ norm,
+                            float* __restrict__ image, float* __restrict__ blockmax) {
+  __shared__ float red[32];
+  const int o = o0 + blockIdx.y, pr = blockIdx.y >> 1, im = blockIdx.y & 1;
+  if (o >= n_out) return;
+  const LithoNorm nm = norm[o];
+  const float sc = nm.mode == 1 ? 1.0f : nm.scale;
+  const size_t NN = (size_t)n * n;
+  const float2* sp = spec + (size_t)pr * NN;
+  float* dst = image + (size_t)o * NN;
+  float mx = 0.f;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < NN; i += (size_t)gridDim.x * blockDim.x) {
+    const float2 z = sp[i];
+    const float v = im ? z.y : z.x;
+    mx = fmaxf(mx, v);
+    dst[i] = v * sc;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = red[0];
+    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) m = fmaxf(m, red[i]);
+    blockmax[(size_t)o * gridDim.x + blockIdx.x] = m;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct WideLayout {
+  int64_t status, twN, twL, u1, mb, table, T, partial, J, F, bbox, spec, blockmax, total;
+  int jobs_per_chunk;
+};
+
+WideLayout wide_layout(const LithoAbbePlan& p) {
+  WideLayout l{};
+  const int64_t Bm = 2 * p.bm + 1, side = 2 * p.h + 1, G = 4 * p.h + 1, L = p.L, NN = (int64_t)p.n * p.n;
+  const int64_t per_job = (int64_t)p.ncomp_max * side * L * 8;
+  int64_t jc = kWideTBudget / per_job;
+  if (jc < 1) jc = 1;
+  if (jc > p.n_jobs) jc = p.n_jobs;
+  l.jobs_per_chunk = (int)jc;
+  const int64_t pairs = (p.n_out + 1) / 2 < kWideSpecPairs ? (p.n_out + 1) / 2 : kWideSpecPairs;
+  int64_t off = 0;
+  l.status = off;   off = align16(off + 16);
+  l.twN = off;      off = align16(off + (int64_t)p.n * 8);
+  l.twL = off;      off = align16(off + L * 8);
+  l.u1 = off;       off = align16(off + (int64_t)p.n_clips * Bm * p.n * 8);
+  l.mb = off;       off = align16(off + (int64_t)p.n_clips * Bm * Bm * 8);
+  l.table = off;    off = align16(off + (int64_t)p.n_tab * p.ncomp_max * side * side * 8);
+  l.T = off;        off = align16(off + jc * per_job);
+  l.partial = off;  off = align16(off + (int64_t)p.n_items * L * L * 4);
+  l.J = off;        off = align16(off + (int64_t)p.n_out * L * L * 4);
+  l.F = off;        off = align16(off + (int64_t)p.n_out * L * L * 8);
+  l.bbox = off;     off = align16(off + (int64_t)p.n_out * G * G * 8);
+  l.spec = off;     off = align16(off + pairs * NN * 8);
+  l.blockmax = off; off = align16(off + (int64_t)p.n_out * kWideMaxBlk * 4);
+  l.total = off;
+  return l;
+}
+
+// Is this plan one for the wide engine (valid L above 64)?
+bool wide_plan_ok(const LithoAbbePlan& p) {
+  return p.L >= 128 && p.L <= 1024 && (p.L & (p.L - 1)) == 0 && 4 * p.h + 1 <= p.L && p.L <= p.n &&
+         p.n <= 4096 && (p.n & (p.n - 1)) == 0 && p.bm >= p.h;
+}
+
+int64_t wide_workspace_bytes(const LithoAbbePlan& p) { return wide_layout(p).total; }
+
+int abbe_wide_run(const LithoAbbePlan& p, const void* blob, const void* table_in, const void* mask, float* image,
+                  float* peak, void* ws, cudaStream_t s, int num_sms, cudaEvent_t* ev) {
+  const WideLayout l = wide_layout(p);
+  const char* b = static_cast<const char*>(blob);
+  const LithoJob* jobs = reinterpret_cast<const LithoJob*>(b + p.off_jobs);
+  const LithoPupil* pupils = reinterpret_cast<const LithoPupil*>(b + p.off_pupils);
+  const LithoItem* items = reinterpret_cast<const LithoItem*>(b + p.off_items);
+  const int32_t* out_items = reinterpret_cast<const int32_t*>(b + p.off_out_items);
+  const LithoNorm* norm = reinterpret_cast<const LithoNorm*>(b + p.off_norm);
+  const int32_t* slots = reinterpret_cast<const int32_t*>(b + p.off_slots);
+  char* w = static_cast<char*>(ws);
+  int* status = reinterpret_cast<int*>(w + l.status);
+  float2* twN = reinterpret_cast<float2*>(w + l.twN);
+  float2* twL = reinterpret_cast<float2*>(w + l.twL);
+  float2* u1 = reinterpret_cast<float2*>(w + l.u1);
+  float2* mb = reinterpret_cast<float2*>(w + l.mb);
+  float2* table = table_in ? (float2*)table_in : reinterpret_cast<float2*>(w + l.table);
+  float2* T = reinterpret_cast<float2*>(w + l.T);
+  float* partial = reinterpret_cast<float*>(w + l.partial);
+  float* J = reinterpret_cast<float*>(w + l.J);
+  float2* F = reinterpret_cast<float2*>(w + l.F);
+  float2* bbox = reinterpret_cast<float2*>(w + l.bbox);
+  float2* spec = reinterpret_cast<float2*>(w + l.spec);
+  float* blockmax = reinterpret_cast<float*>(w + l.blockmax);
+  const int n = p.n, L = p.L, lgL = ilog2w(L), Bm = 2 * p.bm + 1, side = 2 * p.h + 1, G = 4 * p.h + 1;
+  const size_t NN = (size_t)n * n;
+  cudaError_t e;
+  auto mark = [&](int i) { if (ev) cudaEventRecord(ev[i], s); };
+
+  mark(0);
+  if ((e = cudaMemsetAsync(status, 0, sizeof(int), s)) != cudaSuccess) return (int)e;
+  k_twiddle_table<<<(n + 255) / 256, 256, 0, s>>>(twN, n, +1);
+  k_twiddle_table<<<(L + 255) / 256, 256, 0, s>>>(twL, L, +1);
+  if (!table_in)
+    k_pupil_table<<<p.n_tab, 128, 0, s>>>(jobs, slots, pupils, p.n_tab, n, p.pixel_size, p.h, p.ncomp_max, table);
+  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  mark(1);
+  e = launch_row_band_dft(mask, p.mask_complex != 0, p.n_clips * n, n, n, p.bm, u1, 1.0f, twN, num_sms, s, status);
+  if (e != cudaSuccess) return (int)e;
+  mark(2);
+  e = launch_row_band_dft(u1, true, p.n_clips * Bm, Bm, n, p.bm, mb, 1.0f / ((float)n * (float)n), twN, num_sms, s,
+                          status);
+  if (e != cudaSuccess) return (int)e;
+  mark(3);
+  // coarse passes, chunk by chunk of jobs
+  if ((e = cudaMemsetAsync(partial, 0, (size_t)p.n_items * L * L * 4, s)) != cudaSuccess) return (int)e;
+  const size_t smA = (size_t)(L + kWideCols * L) * 8;
+  const size_t smB = (size_t)(L + kWideRows * L) * 8 + (size_t)kWideRows * L * 4;
+  cudaFuncSetAttribute(k_wide_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA);
+  cudaFuncSetAttribute(k_wide_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB);
+  for (int j0 = 0; j0 < p.n_jobs; j0 += l.jobs_per_chunk) {
+    const int nj = (p.n_jobs - j0) < l.jobs_per_chunk ? (p.n_jobs - j0) : l.jobs_per_chunk;
+    dim3 ga(nj * p.ncomp_max, (side + kWideCols - 1) / kWideCols);
+    k_wide_cols<<<ga, 256, smA, s>>>(jobs, j0, p.ncomp_max, table, p.h, mb, p.bm, L, lgL, twL, T);
+    dim3 gb(p.n_items, L / kWideRows);
+    k_wide_rows<<<gb, 256, smB, s>>>(items, jobs, j0, nj, p.ncomp_max, p.h, L, lgL, twL, T, partial);
+    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  }
+  mark(4);
+  {
+    const int LL = L * L;
+    dim3 gr((LL + 255) / 256 < 1024 ? (LL + 255) / 256 : 1024, p.n_out);
+    k_wide_reduce<<<gr, 256, 0, s>>>(out_items, partial, LL, J);
+    e = plain_fft2(J, true, F, p.n_out, L, -1, 1.0f, 1.0f / ((float)L * (float)L), twL, s);
+    if (e != cudaSuccess) return (int)e;
+    dim3 gx((G * G + 255) / 256, p.n_out);
+    k_wide_box<<<gx, 256, 0, s>>>(F, L, p.h, bbox);
+    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  }
+  mark(5);
+  for (int o0 = 0; o0 < p.n_out; o0 += 2 * kWideSpecPairs) {
+    const int no = (p.n_out - o0) < 2 * kWideSpecPairs ? (p.n_out - o0) : 2 * kWideSpecPairs;
+    const int pairs = (no + 1) / 2;
+    if ((e = cudaMemsetAsync(spec, 0, (size_t)pairs * NN * 8, s)) != cudaSuccess) return (int)e;
+    dim3 gs((G * G + 255) / 256, pairs);
+    k_wide_spec<<<gs, 256, 0, s>>>(bbox, o0, p.n_out, p.h, n, spec);
+    e = plain_fft2(nullptr, false, spec, pairs, n, +1, 1.0f, 1.0f, twN, s);
+    if (e != cudaSuccess) return (int)e;
+    dim3 gw(kWideMaxBlk, no);
+    k_wide_real<<<gw, 256, 0, s>>>(spec, o0, p.n_out, n, norm, image, blockmax);
+    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  }
+  mark(6);
+  dim3 gn((unsigned)((NN + 255) / 256 < 512 ? (NN + 255) / 256 : 512), p.n_out);
+  k_normalise<<<gn, 256, 0, s>>>(blockmax, kWideMaxBlk, norm, n, image, peak, 0);
+  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  mark(7);
+  return LITHO_OK;
+}
+
+}  // namespace litho

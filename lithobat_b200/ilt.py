@@ -29,6 +29,7 @@ from .config import optics_view
 from .hopkins import SOCSKernels
 
 N_PART = 64   # partial-sum blocks per clip for costs / pattern errors
+KERNEL_HMAX_FUSED = 15   # widest kernel band (bins) of the on-chip SOCS adjoint
 
 
 def gaussian_weights(sigma: float, truncate: float = 4.0) -> np.ndarray:
@@ -258,7 +259,10 @@ def stages(kernels: SOCSKernels, n_clips: int, engine: str = "fused") -> _Stages
     if st is None or st.k is not kernels:
         if len(_STAGES) > 16:
             _STAGES.clear()
-        st = (_Stages if engine == "fused" else _PlainStages)(kernels, n_clips)
+        # the on-chip SOCS adjoint covers kernel bands up to 15 bins (a 64-point
+        # coarse grid); wider bands run both directions on the full grid
+        fused = engine == "fused" and kernels.halfwidth <= KERNEL_HMAX_FUSED
+        st = (_Stages if fused else _PlainStages)(kernels, n_clips)
         _STAGES[key] = st
     return st
 

@@ -279,8 +279,39 @@ def main():
     cost, gk, signed, perr = objk(m)
     save("ilt_imm_128_k24", optics=o4, grid=g4, theta=theta, target=target.astype(np.uint8),
          beta=4.0, cost=cost, grad=gk, signed=signed, perr=perr)
+    wide()
     print("done")
 
 
+def wide():
+    """EUV cases whose pupil is wider than 15 bins (coarse grids above 64)."""
+    _import_reference()
+    from litho_sim.core.config import GridConfig, OpticsConfig
+    from litho_sim.expose import SOCSKernels, compute_aerial_image
+    from litho_sim.expose.source import Source
+
+    # 256^2 at 2.5 nm: pupil radius 15.6 bins (h = 16)
+    g = GridConfig(n_pixels=256, pixel_size=2.5e-9)
+    o = OpticsConfig(wavelength=13.5e-9, NA=0.33, source_grid=21, defocus=20e-9,
+                     zernike_coeffs={5: 0.01, 8: -0.008},
+                     source_spec=Source.dipole(0.9, 0.6, opening_deg=60).to_dict())
+    m = manhattan_clip(np.random.default_rng(31), 256, 2.5e-9, n_rect=(10, 20), width_nm=(20, 80))
+    raw, peak, clear = compute_aerial_image(m, o, g, return_raw=True)
+    save("euv_wide_256", optics=o, grid=g, mask=m.astype(np.uint8), raw=raw, peak=peak, clear=clear)
+
+    # SOCS with a 31-bin kernel band (128^2 at 5 nm), 24 kernels
+    g = GridConfig(n_pixels=128, pixel_size=5e-9)
+    o = OpticsConfig(wavelength=13.5e-9, NA=0.33, source_grid=15, normalisation="clear",
+                     source_spec=Source.dipole(0.9, 0.6, opening_deg=60).to_dict())
+    k = SOCSKernels.build(o, g, tol=0.0, max_kernels=24)
+    m = manhattan_clip(np.random.default_rng(32), 128, 5e-9, n_rect=(6, 12), width_nm=(20, 80))
+    r = k.raw(m)
+    save("socs_euv_wide_128_k24", optics=o, grid=g, mask=m.astype(np.uint8), weights=k.weights,
+         clear=k.clear, n_band=k.n_band, raw=r[0], peak=r[1])
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["wide"]:
+        wide()
+    else:
+        main()
