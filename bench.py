@@ -288,33 +288,48 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU (reference algorithm) timing
 # ---------------------------------------------------------------------------
-def cpu_sample_seconds(n_src: int = 12, repeats: int = 2) -> tuple[float, int, int]:
-    """Median seconds of the FP64 numpy Abbe sum over the first n_src source
-    points of the workload (one image); returns (t, n_src, S_total)."""
-    from oracle import litho_oracle as O
-    o = optics_c3()
-    S = len(O.source_points(o))
-    mask = masks_c3(1, 1)[0].astype(np.complex128)
+class CpuAbbeSample:
+    """The FP64 numpy Abbe sum (the reference algorithm, restated in the
+    oracle) over the first k source points of one workload image."""
 
-    class G:
-        n_pixels, pixel_size = N, PX
-    planes = [(o.defocus, o.image_index)]
-    O.abbe_sum(mask, o, G, planes, source_subset=range(2))  # warm the FFT plans
-    ts = []
-    for _ in range(repeats):
+    def __init__(self):
+        from oracle import litho_oracle as O
+        self.O = O
+        self.o = optics_c3()
+        self.S = len(O.source_points(self.o))
+        self.mask = masks_c3(1, 1)[0].astype(np.complex128)
+
+        class G:
+            n_pixels, pixel_size = N, PX
+        self.G = G
+        self.planes = [(self.o.defocus, self.o.image_index)]
+        self(2)  # warm the FFT plans
+
+    def __call__(self, k: int) -> float:
         t0 = time.perf_counter()
-        O.abbe_sum(mask, o, G, planes, source_subset=range(n_src))
-        ts.append(time.perf_counter() - t0)
-    return statistics.median(ts), n_src, S
+        self.O.abbe_sum(self.mask, self.o, self.G, self.planes, source_subset=range(k))
+        return time.perf_counter() - t0
+
+
+def cpu_sample_seconds(n_src: int = 12, repeats: int = 2) -> tuple[float, int, int]:
+    """Median seconds of the CPU Abbe sum over the first n_src source points
+    of one workload image; returns (t, n_src, S_total)."""
+    smp = CpuAbbeSample()
+    return statistics.median(smp(n_src) for _ in range(repeats)), n_src, smp.S
 
 
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    smp = CpuAbbeSample()
+    # source points per step: the whole run stays near 150 s of CPU work
+    t1 = smp(2) / 2.0
+    k = int(max(1, min(12, 150.0 / max(1, args.warmup + args.steps) / max(t1, 1e-3))))
+    S = smp.S
     vals = []
     for i in range(args.warmup + args.steps):
-        t, k, S = cpu_sample_seconds(repeats=1)
+        t = smp(k)
         if i >= args.warmup:
             vals.append(1.0 / (t * S / k))
     v = statistics.median(vals)
