@@ -107,7 +107,8 @@ typedef struct LithoAbbePlan {
     int32_t n_pupils;
     int32_t h;            /* half-width of a source point's disc, bins      */
     int32_t bm;           /* half-width of the mask band, bins              */
-    int32_t L;            /* coarse grid side (>= 4h+1, power of two)       */
+    int32_t L;            /* coarse grid side (>= 4h+1, power of two): 32 or */
+                          /* 64 on chip; 128..1024 (<= n) wide-pupil engine */
     int32_t mask_complex; /* 0: float32 masks, 1: complex64 masks           */
     int32_t ncomp_max;    /* 1 or 3                                         */
     int32_t n_tab;        /* pupil-table slots (max LithoJob.tab + 1)       */
@@ -186,7 +187,9 @@ int litho_abbe(const LithoAbbePlan* plan, const void* plan_blob_dev,
 /* litho_abbe() run `reps` times with CUDA events between its stages, for
  * measurement. stage_ms[0..6] receives the mean milliseconds of: pupil
  * table, mask band rows, mask band columns, coarse accumulation, coarse
- * reduction, synthesis, normalisation. Synchronises the stream. */
+ * reduction, then the peak pass and the writing synthesis pass (on grids
+ * without the pair-FFT synthesis, and on the wide-pupil engine: synthesis,
+ * then normalisation). Synchronises the stream. */
 int litho_abbe_profile(const LithoAbbePlan* plan, const void* plan_blob_dev,
                        const void* table_dev /* NULL: built each run */, const void* mask_dev, float* image_dev, float* peak_dev,
                        void* workspace_dev, size_t workspace_bytes, cudaStream_t stream,
