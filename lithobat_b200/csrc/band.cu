@@ -201,7 +201,7 @@ __host__ __device__ inline BandGeo band_geo(int n, int bm, int warps) {
 // M = N / 32 is a template constant, so every shared-memory offset below is
 // an immediate; the twiddle table is laid out per (pass, register kp, residue
 // b) with zeros where band_k(kp, pass) falls outside the band.
-template <bool CPLX, int M>
+template <bool CPLX, int M, bool TBS>
 __global__ void __launch_bounds__(256, 2)
 k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int bm, float2* __restrict__ out,
             float scale, const float2* __restrict__ tw_inv) {
@@ -213,7 +213,7 @@ k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int bm, 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float2* Y = bsm + g.off_y / 8 + warp * g.y_per_warp;   // [group][kp][b]
   float2* Z = bsm + g.off_z / 8 + warp * g.z_per_warp;   // [group][k + bm] (real pairs)
-  if (g.tb_smem) {
+  if (TBS) {
     for (int j = threadIdx.x; j < npass * 32 * M; j += blockDim.x) {
       const int p = j / (32 * M), kp = (j / M) & 31, b = j % M;
       const int k = band_k(kp, p, bm);
@@ -251,7 +251,7 @@ k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int bm, 
           fft_reg<32, -1>(v);
         }
         float2* yr = Y + pg * 32 * LD + b;
-        if (g.tb_smem) {
+        if (TBS) {
           const float2* tb = TB + p * 32 * M + b;
 #pragma unroll
           for (int kp = 0; kp < 32; ++kp) yr[kp * LD] = cmul(v[kp], tb[kp * M]);
@@ -325,8 +325,15 @@ static cudaError_t launch_band_rows_m(const void* in, int n_rows, int rows_per_c
   const int per_sm = (int)((227 * 1024) / g.total) >= 2 ? 2 : 1;
   long long blocks = (n_iter + warps - 1) / warps;
   if (blocks > (long long)num_sms * per_sm) blocks = (long long)num_sms * per_sm;
-  cudaFuncSetAttribute(k_band_rows<CPLX, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.total);
-  k_band_rows<CPLX, M><<<(int)blocks, warps * 32, g.total, st>>>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv);
+  if (g.tb_smem) {
+    cudaFuncSetAttribute(k_band_rows<CPLX, M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.total);
+    k_band_rows<CPLX, M, true><<<(int)blocks, warps * 32, g.total, st>>>(in, n_rows, rows_per_clip, bm, out, scale,
+                                                                         tw_inv);
+  } else {  // wide bands: a separate instantiation, so the common path keeps its registers
+    cudaFuncSetAttribute(k_band_rows<CPLX, M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.total);
+    k_band_rows<CPLX, M, false><<<(int)blocks, warps * 32, g.total, st>>>(in, n_rows, rows_per_clip, bm, out, scale,
+                                                                          tw_inv);
+  }
   return cudaGetLastError();
 }
 
