@@ -99,8 +99,8 @@ class _Stages:
     def mask_box(self, masks):
         return self.band(masks, self.h, 1.0 / (self.n * self.n))
 
-    def image(self, mbox):
-        """Raw SOCS intensity (C, N, N) from the mask band boxes."""
+    def image_box(self, mbox):
+        """Band box (C, (4h+1)^2) of the raw SOCS intensity from the mask band boxes."""
         torch, L = self.torch, self.L
         nb = C.c_size_t(0)
         nat.check("litho_abbe_workspace", L.litho_abbe_workspace(C.byref(self.pd.plan), C.byref(nb)))
@@ -110,7 +110,11 @@ class _Stages:
         nat.check("litho_coarse_image", L.litho_coarse_image(
             C.byref(self.pd.plan), self.blob.data_ptr(), self.table.data_ptr(), mbox.data_ptr(), bbox.data_ptr(),
             ws.data_ptr(), ws.numel(), self.stream()))
-        return self.synth(bbox, 2 * self.h, False)
+        return bbox
+
+    def image(self, mbox):
+        """Raw SOCS intensity (C, N, N) from the mask band boxes."""
+        return self.synth(self.image_box(mbox), 2 * self.h, False)
 
     def fields(self, mbox):
         """(C, K, N, N) complex64 coherent fields E_k = F^-1(phi_k F(m))."""
@@ -120,8 +124,13 @@ class _Stages:
 
     def adjoint(self, sens, scale: float = 1.0, mbox=None, field_boxes=None):
         """d/dm of sum_x sens(x) I(x): (C, N, N) float32 (opc/ilt.py:262-266)."""
-        torch, L = self.torch, self.L
         gbox = self.band(sens, 2 * self.h, scale / (self.n * self.n))
+        return self.synth(self.adjoint_box(gbox, mbox, field_boxes), self.h, False)
+
+    def adjoint_box(self, gbox, mbox=None, field_boxes=None):
+        """Band box (C, (2h+1)^2) of the mask gradient from the band box of
+        scale * dJ/dI on |g| <= 2h (already divided by N^2)."""
+        torch, L = self.torch, self.L
         nb = C.c_size_t(0)
         nat.check("litho_socs_adjoint_workspace", L.litho_socs_adjoint_workspace(
             self.C, self.pd.plan.n_items, self.h, C.byref(nb)))
@@ -132,7 +141,58 @@ class _Stages:
             None if mbox is None else mbox.data_ptr(),
             None if field_boxes is None else field_boxes.data_ptr(), gbox.data_ptr(), hbox.data_ptr(),
             ws.data_ptr(), ws.numel(), self.stream()))
-        return self.synth(hbox, self.h, False)
+        return hbox
+
+    # -- fused per-pixel passes (no blur, smoothing or penalties) ------------
+    def fused_ok(self, p) -> bool:
+        return (p.sigma_px < 1e-3 and p.smooth_px < 1e-3 and p.weight_tv == 0.0 and p.weight_discrete == 0.0
+                and bool(self.L.litho_ilt_rows_supported(self.n, 2 * self.h, 2 * self.h))
+                and bool(self.L.litho_ilt_rows_supported(self.n, self.h, self.h)))
+
+    def _rows_ws(self):
+        nb = C.c_size_t(0)
+        nat.check("litho_ilt_rows_workspace", self.L.litho_ilt_rows_workspace(self.n, C.byref(nb)))
+        return self.ws("rows", nb.value)
+
+    def band_columns(self, rows, bm: int, scale: float):
+        out = self.torch.empty((self.C, (2 * bm + 1) ** 2), dtype=self.torch.complex64, device=self.dev)
+        ws = self._rows_ws()
+        nat.check("litho_band_columns", self.L.litho_band_columns(
+            rows.data_ptr(), self.C, self.n, bm, float(scale), out.data_ptr(), ws.data_ptr(), ws.numel(),
+            self.stream()))
+        return out
+
+    def objective_fused(self, mbox, target, scale, level, sign, steepness, want_signed=True):
+        """The objective from the mask band boxes without per-pixel images:
+        (cost (C,), gradient band box (C, (2h+1)^2), signed or None, perr (C,))."""
+        torch, L = self.torch, self.L
+        h2 = 2 * self.h
+        bbox = self.image_box(mbox)
+        rows = torch.empty((self.C, 2 * h2 + 1, self.n), dtype=torch.complex64, device=self.dev)
+        nblk = self.n // 64
+        cpart = torch.empty((self.C, nblk), dtype=torch.float64, device=self.dev)
+        ppart = torch.empty((self.C, nblk), dtype=torch.int32, device=self.dev)
+        signed = torch.empty((self.C, self.n, self.n), dtype=torch.float32, device=self.dev) if want_signed else None
+        a = steepness / max(abs(level), 1e-12)
+        ws = self._rows_ws()
+        nat.check("litho_ilt_objective_rows", L.litho_ilt_objective_rows(
+            bbox.data_ptr(), h2, self.C, self.n, target.data_ptr(), float(scale), float(level), float(sign),
+            float(a), None if signed is None else signed.data_ptr(), cpart.data_ptr(), ppart.data_ptr(), h2,
+            rows.data_ptr(), ws.data_ptr(), ws.numel(), self.stream()))
+        gbox = self.band_columns(rows, h2, float(scale) / (self.n * self.n))
+        hbox = self.adjoint_box(gbox, mbox)
+        return cpart.sum(dim=1) / float(self.n * self.n), hbox, signed, ppart.sum(dim=1)
+
+    def update_fused(self, hbox, theta, m1, m2, beta, beta_next, step, b1, b2, eps, it):
+        """dJ/dm from its band box -> dJ/dtheta -> Adam (in place on theta, m1,
+        m2) -> the next mask's band box."""
+        rows = self.torch.empty((self.C, 2 * self.h + 1, self.n), dtype=self.torch.complex64, device=self.dev)
+        ws = self._rows_ws()
+        nat.check("litho_ilt_update_rows", self.L.litho_ilt_update_rows(
+            hbox.data_ptr(), self.h, self.C, self.n, theta.data_ptr(), m1.data_ptr(), m2.data_ptr(), float(beta),
+            float(beta_next), float(step), float(b1), float(b2), float(eps), int(it), None, self.h, rows.data_ptr(),
+            ws.data_ptr(), ws.numel(), self.stream()))
+        return self.band_columns(rows, self.h, 1.0 / (self.n * self.n))
 
     # -- elementwise ----------------------------------------------------------
     def blur(self, x, sigma_px: float):
@@ -461,9 +521,16 @@ class IltBatch:
 
     state: theta, Adam moments (float32), the current mask and gradient.
     ``step()`` is one iteration of opc/ilt.py:576-596: grad_theta, Adam, the
-    beta anneal, mask_of and the objective (SOCS forward + adjoint)."""
+    beta anneal, mask_of and the objective (SOCS forward + adjoint).
 
-    def __init__(self, kernels: SOCSKernels, targets, theta0, params: IltParams, engine: str = "fused"):
+    Without blurs, smoothing or penalties (the common ILT setting) the step
+    runs fused: the per-pixel image, dJ/dI, gradient and mask are never
+    written to memory (csrc/ilt_rows.cu); ``mask`` and ``grad_m`` are then
+    formed on demand from theta and the gradient's band box. ``fused=False``
+    forces the stage-by-stage path."""
+
+    def __init__(self, kernels: SOCSKernels, targets, theta0, params: IltParams, engine: str = "fused",
+                 fused: bool | None = None):
         self.st = stages(kernels, int(theta0.shape[0]), engine)
         torch = self.st.torch
         n = self.st.n
@@ -474,24 +541,55 @@ class IltBatch:
         self.m2 = torch.zeros_like(self.theta)
         self.beta = float(params.beta)
         self.it = 0
-        self.mask = self.st.mask_of(self.theta, self.beta, params.smooth_px)
-        self.cost, self.grad_m, self.signed, self.perr = self._objective(self.mask)
+        can = type(self.st) is _Stages and self.st.fused_ok(params)
+        self.fused = can if fused is None else (bool(fused) and can)
+        self._mask = self.st.mask_of(self.theta, self.beta, params.smooth_px)
+        self._grad_m = None
+        if self.fused:
+            self.mbox = self.st.mask_box(self._mask)
+            self.cost, self.hbox, self.signed, self.perr = self._objective_fused(True)
+        else:
+            self.cost, self._grad_m, self.signed, self.perr = self._objective(self._mask)
 
     def _objective(self, mask, want_signed=True):
         p = self.p
         return self.st.objective(mask, self.target, p.scale, p.level, p.sigma_px, p.sign, p.steepness,
                                  p.weight_tv, p.weight_discrete, want_signed=want_signed)
 
+    def _objective_fused(self, want_signed):
+        p = self.p
+        return self.st.objective_fused(self.mbox, self.target, p.scale, p.level, p.sign, p.steepness, want_signed)
+
+    @property
+    def mask(self):
+        if self._mask is None:
+            self._mask = self.st.mask_of(self.theta, self.beta, self.p.smooth_px)
+        return self._mask
+
+    @property
+    def grad_m(self):
+        if self._grad_m is None:
+            self._grad_m = self.st.synth(self.hbox, self.st.h, False)
+        return self._grad_m
+
     def step(self, want_signed: bool = True):
         p = self.p
         self.it += 1
+        if self.fused:
+            beta_next = self.beta * p.growth
+            self.mbox = self.st.update_fused(self.hbox, self.theta, self.m1, self.m2, self.beta, beta_next, p.step,
+                                             p.b1, p.b2, p.eps, self.it)
+            self.beta = beta_next
+            self._mask = self._grad_m = None
+            self.cost, self.hbox, self.signed, self.perr = self._objective_fused(want_signed)
+            return self.cost
         gt = self.st.grad_theta(self.grad_m, self.mask, self.beta, p.smooth_px)
         nat.check("litho_ilt_adam", self.st.L.litho_ilt_adam(
             gt.data_ptr(), gt.numel(), float(p.step), float(p.b1), float(p.b2), float(p.eps), self.it,
             self.theta.data_ptr(), self.m1.data_ptr(), self.m2.data_ptr(), self.st.stream()))
         self.beta *= p.growth
-        self.mask = self.st.mask_of(self.theta, self.beta, p.smooth_px)
-        self.cost, self.grad_m, self.signed, self.perr = self._objective(self.mask, want_signed)
+        self._mask = self.st.mask_of(self.theta, self.beta, p.smooth_px)
+        self.cost, self._grad_m, self.signed, self.perr = self._objective(self._mask, want_signed)
         return self.cost
 
 
