@@ -130,36 +130,35 @@ def bench_ilt(args, torch, dev, world, max_over_ranks, barrier) -> dict:
     # stage times of one step (events on the launching stream)
     st = b.st
     nat_ = __import__("lithobat_b200._native", fromlist=["x"])
-    if b.fused:
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(7)]
+    if b.fast:
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(8)]
         th, m1, m2 = b.theta.clone(), b.m1.clone(), b.m2.clone()
-        h2 = 2 * st.h
-        rows_m = torch.empty((nclip, 2 * st.h + 1, N), dtype=torch.complex64, device=dev)
-        rows_s = torch.empty((nclip, 2 * h2 + 1, N), dtype=torch.complex64, device=dev)
-        cpart = torch.empty((nclip, N // 64), dtype=torch.float64, device=dev)
-        ppart = torch.empty((nclip, N // 64), dtype=torch.int32, device=dev)
-        ws = st._rows_ws()
+        mk = torch.empty_like(th)
+        cpart = torch.empty((nclip, 64), dtype=torch.float64, device=dev)
+        ppart = torch.empty((nclip, 64), dtype=torch.int32, device=dev)
         ev[0].record()
-        nat_.check("update", st.L.litho_ilt_update_rows(
-            b.hbox.data_ptr(), st.h, nclip, N, th.data_ptr(), m1.data_ptr(), m2.data_ptr(), b.beta, b.beta, 0.4,
-            0.9, 0.999, 1e-8, 5, None, st.h, rows_m.data_ptr(), ws.data_ptr(), ws.numel(), st.stream()))
+        gm = st.synth(b.hbox, st.h, False)
         ev[1].record()
-        mbox = st.band_columns(rows_m, st.h, 1.0 / (N * N))
+        nat_.check("update", st.L.litho_ilt_update(gm.data_ptr(), gm.numel(), b.beta, b.beta, 0.4, 0.9, 0.999, 1e-8,
+                                                   5, th.data_ptr(), m1.data_ptr(), m2.data_ptr(), mk.data_ptr(),
+                                                   st.stream()))
         ev[2].record()
-        bbox = st.image_box(mbox)
+        mbox = st.mask_box(mk)
         ev[3].record()
-        nat_.check("objective", st.L.litho_ilt_objective_rows(
-            bbox.data_ptr(), h2, nclip, N, b.target.data_ptr(), float(params.scale), 0.3, 1.0, 50.0, None,
-            cpart.data_ptr(), ppart.data_ptr(), h2, rows_s.data_ptr(), ws.data_ptr(), ws.numel(), st.stream()))
+        raw = st.image(mbox)
         ev[4].record()
-        gbox = st.band_columns(rows_s, h2, float(params.scale) / (N * N))
+        dfield = torch.empty_like(raw)
+        nat_.check("obj", st.L.litho_ilt_objective(raw.data_ptr(), b.target.data_ptr(), nclip, N,
+                                                   float(params.scale), 0.3, 1.0, 50.0, dfield.data_ptr(), None,
+                                                   cpart.data_ptr(), ppart.data_ptr(), 64, st.stream()))
         ev[5].record()
-        st.adjoint_box(gbox, mbox)
+        gbox = st.band(dfield, 2 * st.h, float(params.scale) / (N * N))
         ev[6].record()
+        st.adjoint_box(gbox, mbox)
+        ev[7].record()
         torch.cuda.synchronize()
-        names = ["update_rows: gradient synthesis, dJ/dtheta, Adam, next mask band rows", "mask_band_columns",
-                 "coarse_image: per-kernel fields, sum lambda|e|^2, image band box",
-                 "objective_rows: image synthesis, resist, dJ/dI band rows", "sensitivity_band_columns",
+        names = ["gradient_synthesis", "theta_grad+adam+mask", "mask_band_spectrum",
+                 "coarse_image_and_synthesis", "objective", "sensitivity_band_spectrum",
                  "adjoint: dJ/dI on the 64 grid, per-kernel adjoint, gradient band box"]
     else:
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(9)]
@@ -230,7 +229,7 @@ def bench_ilt(args, torch, dev, world, max_over_ranks, barrier) -> dict:
     return {
         "metric": "ILT gradient steps/s @1024^2 (clip-steps)", "value": value, "unit": "clip-steps/s",
         "ms_per_step": ms / args.steps, "clips_per_step": nclip, "workload": ILT_WORKLOAD,
-        "kernels": len(k), "socs_build_ms": build_ms, "fused_rows": bool(b.fused), "stages_ms": stages,
+        "kernels": len(k), "socs_build_ms": build_ms, "fast_step": bool(b.fast), "stages_ms": stages,
         "plain": plain,
         "e2e": {"value": world * nclip * args.steps / (e2e_ms / 1000.0), "unit": "clip-steps/s",
                 "h2d_bytes_per_step": 2 * nclip * NN * 4 // args.steps, "d2h_bytes_per_step":

@@ -339,6 +339,13 @@ int litho_ilt_mask(const float* field_dev, long long count, float beta, float* m
 int litho_ilt_theta_grad(const float* grad_m_dev, const float* mask_dev, long long count, float beta,
                          float* q_dev, cudaStream_t stream);
 
+/* dJ/dtheta, Adam and the next mask in one pass (opc/ilt.py:381-389,
+ * 587-591, 368-378, without smoothing): m = sigmoid(beta theta),
+ * q = g beta m (1 - m), Adam step `it` on theta (m1, m2 in place), mask =
+ * sigmoid(beta_next theta). count a multiple of 4, 16-byte aligned arrays. */
+int litho_ilt_update(const float* g_dev, long long count, float beta, float beta_next, float step, float b1,
+                     float b2, float eps, int it, float* theta_dev, float* m1_dev, float* m2_dev, float* mask_dev,
+                     cudaStream_t stream);
 /* One Adam step at iteration it >= 1 (opc/ilt.py:582-591), in place. */
 int litho_ilt_adam(const float* g_dev, long long count, float step, float b1, float b2, float eps,
                    int it, float* theta_dev, float* m1_dev, float* m2_dev, cudaStream_t stream);
@@ -348,39 +355,6 @@ int litho_ilt_adam(const float* g_dev, long long count, float step, float b1, fl
  * (opc/ilt.py:_blur, :274-289). tmp_dev: scratch of the input's size. */
 int litho_gaussian_blur(const float* in_dev, float* out_dev, float* tmp_dev, int n_fields, int n,
                         const float* weights_dev, int radius, cudaStream_t stream);
-
-/* ---- fused per-pixel passes of an ILT step (no blur, smoothing, penalties) ----
- * Replace, for opc/ilt.py:576-596 with sigma_px = smooth = weight_tv =
- * weight_discrete = 0, the chain synthesis -> _Objective's resist and dJ/dI
- * (:313-336) -> band spectrum of dJ/dI, and the chain synthesis of dJ/dm ->
- * _grad_theta (:381-389) -> Adam (:587-591) -> _mask_of (:368-378) -> band
- * spectrum of the next mask, each as one pass over pixel rows that writes no
- * per-pixel image. Row-pass band output: [field][2 bm + 1][n] complex; finish
- * it with litho_band_columns(). n in {256, 512, 1024}, box half-width
- * g0 <= 31, 2 bm + 1 <= 64 (litho_ilt_rows_supported). */
-int litho_ilt_rows_workspace(int n, size_t* bytes);
-int litho_ilt_rows_supported(int n, int g0, int bm);
-/* image_box: [field][(2 g0 + 1)^2] band box of the raw SOCS intensity
- * (litho_coarse_image). cost_part / perr_part: [field][n / 64] partial sums
- * of (z - t)^2 and of pattern errors; signed_out (optional): sign (scale I -
- * level). The band rows are those of dJ/dI (not yet multiplied by scale). */
-int litho_ilt_objective_rows(const void* image_box_dev, int g0, int n_fields, int n, const float* target_dev,
-                             float scale, float level, float sign, float steepness_a, float* signed_out_dev,
-                             double* cost_part_dev, unsigned int* perr_part_dev, int bm, void* band_rows_dev,
-                             void* workspace_dev, size_t workspace_bytes, cudaStream_t stream);
-/* grad_box: [field][(2 g0 + 1)^2] band box of dJ/dm (litho_socs_adjoint).
- * Updates theta, m1, m2 in place (Adam step `it`, bias-corrected), writes
- * the band rows of sigmoid(beta_next theta) and, if mask_out is not NULL,
- * that mask itself. */
-int litho_ilt_update_rows(const void* grad_box_dev, int g0, int n_fields, int n, float* theta_dev, float* m1_dev,
-                          float* m2_dev, float beta, float beta_next, float step, float b1, float b2, float eps,
-                          int it, float* mask_out_dev, int bm, void* band_rows_dev, void* workspace_dev,
-                          size_t workspace_bytes, cudaStream_t stream);
-/* Column pass of a band spectrum whose row pass is done: band rows
- * [field][2 bm + 1][n] -> box [field][(2 bm + 1)^2], times scale. Workspace:
- * litho_ilt_rows_workspace(n). */
-int litho_band_columns(const void* band_rows_dev, int n_fields, int n, int bm, float scale, void* box_out_dev,
-                       void* workspace_dev, size_t workspace_bytes, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

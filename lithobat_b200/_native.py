@@ -119,13 +119,7 @@ def lib():
         "litho_ilt_theta_grad": [vp, vp, C.c_longlong, f32, vp, vp],
         "litho_ilt_adam": [vp, C.c_longlong, f32, f32, f32, f32, i32, vp, vp, vp, vp],
         "litho_gaussian_blur": [vp, vp, vp, i32, i32, vp, i32, vp],
-        "litho_ilt_rows_workspace": [i32, C.POINTER(C.c_size_t)],
-        "litho_ilt_rows_supported": [i32, i32, i32],
-        "litho_ilt_objective_rows": [vp, i32, i32, i32, vp, f32, f32, f32, f32, vp, vp, vp, i32, vp, vp, C.c_size_t,
-                                     vp],
-        "litho_ilt_update_rows": [vp, i32, i32, i32, vp, vp, vp, f32, f32, f32, f32, f32, f32, i32, vp, i32, vp, vp,
-                                  C.c_size_t, vp],
-        "litho_band_columns": [vp, i32, i32, i32, f32, vp, vp, C.c_size_t, vp],
+        "litho_ilt_update": [vp, C.c_longlong, f32, f32, f32, f32, f32, f32, i32, vp, vp, vp, vp, vp],
         "litho_plain_socs_workspace": [i32, i32, C.POINTER(sz)],
         "litho_plain_socs_forward": [vp, i32, i32, i32, vp, vp, vp, vp, i32, vp, vp, vp, sz, vp],
         "litho_plain_socs_adjoint": [vp, vp, i32, i32, i32, vp, vp, vp, vp, i32, vp, vp, sz, vp],

@@ -342,21 +342,34 @@ k_coarse_reduce(const int32_t* __restrict__ out_items, const float* __restrict__
     J[idx] = (s0 + s1) + (s2 + s3);
   }
   __syncthreads();
-  for (int id = threadIdx.x; id < L * G; id += blockDim.x) {
-    const int u = id / G, gy = id % G - g0;
+  // this block's rows gy of the box: [r0, r1) (grid.y splits an output when
+  // there are too few outputs to fill the GPU)
+  const int per = (G + gridDim.y - 1) / gridDim.y;
+  const int r0 = blockIdx.y * per, r1 = (r0 + per) < G ? (r0 + per) : G;
+  const int nr = r1 - r0;
+  for (int id = threadIdx.x; id < L * nr; id += blockDim.x) {
+    const int u = id / nr, gyi = r0 + id % nr, gy = gyi - g0;
     float2 acc = make_float2(0.f, 0.f);
     for (int v = 0; v < L; ++v) acc = cadd(acc, cscale(tw[(gy * v) & msk], J[v * L + u]));
-    R[u * G + (gy + g0)] = acc;
+    R[u * G + gyi] = acc;
   }
   __syncthreads();
   const float inv = 1.0f / (float)LL;
   float2* B = Bout + (size_t)o * G * G;
-  for (int id = threadIdx.x; id < G * G; id += blockDim.x) {
-    const int gyi = id / G, gx = id % G - g0;
+  for (int id = threadIdx.x; id < nr * G; id += blockDim.x) {
+    const int gyi = r0 + id / G, gx = id % G - g0;
     float2 acc = make_float2(0.f, 0.f);
     for (int u = 0; u < L; ++u) acc = cadd(acc, cmul(R[u * G + gyi], tw[(gx * u) & msk]));
     B[gyi * G + (gx + g0)] = cscale(acc, inv);
   }
+}
+
+// Blocks per output of k_coarse_reduce: split the box rows when the outputs
+// alone would leave most SMs idle.
+static unsigned reduce_split(int n_out, int G) {
+  int s = 1;
+  while (s < 8 && (long long)n_out * s < 2 * 148 && s * 2 <= G) s *= 2;
+  return (unsigned)s;
 }
 
 // ---------------------------------------------------------------------------
@@ -660,7 +673,7 @@ static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* tab
   mark(4);
   const size_t sm_red = (size_t)p.L * p.L * 4 + (size_t)p.L * G * 8 + (size_t)p.L * 8;
   cudaFuncSetAttribute(k_coarse_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_red);
-  k_coarse_reduce<<<p.n_out, 1024, sm_red, s>>>(out_items, partial, p.L, p.h, bbox);
+  k_coarse_reduce<<<dim3(p.n_out, reduce_split(p.n_out, G)), 1024, sm_red, s>>>(out_items, partial, p.L, p.h, bbox);
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
   mark(5);
   if (synth_pairs_ok(p.n, 2 * p.h)) {
@@ -727,7 +740,8 @@ extern "C" int litho_coarse_image(const LithoAbbePlan* plan, const void* blob, c
   if (e != cudaSuccess) return (int)e;
   const size_t sm_red = (size_t)p.L * p.L * 4 + (size_t)p.L * G * 8 + (size_t)p.L * 8;
   cudaFuncSetAttribute(k_coarse_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_red);
-  k_coarse_reduce<<<p.n_out, 1024, sm_red, s>>>(out_items, partial, p.L, p.h, static_cast<float2*>(bbox_out));
+  k_coarse_reduce<<<dim3(p.n_out, reduce_split(p.n_out, G)), 1024, sm_red, s>>>(out_items, partial, p.L, p.h,
+                                                                                 static_cast<float2*>(bbox_out));
   e = cudaGetLastError();
   return e == cudaSuccess ? LITHO_OK : (int)e;
 }

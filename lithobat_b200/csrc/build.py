@@ -74,7 +74,10 @@ def build(force: bool = False, verbose_ptxas: bool = False, quiet: bool = False)
                 if (verbose_ptxas or r.stderr.strip()) and not quiet:
                     sys.stderr.write(f"--- {s.name}\n{r.stderr}")
     objs = [BUILD / (s.stem + ".o") for s in srcs]
-    if jobs or not OUT.exists() or OUT.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+    orphans = [o for o in BUILD.glob("*.o") if o not in objs]   # objects of removed sources
+    for o in orphans:
+        o.unlink()
+    if jobs or orphans or not OUT.exists() or OUT.stat().st_mtime < max(o.stat().st_mtime for o in objs):
         cmd = [cc, *ARCH, "-shared", "-o", str(OUT), *map(str, objs), "-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

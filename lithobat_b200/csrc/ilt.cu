@@ -288,9 +288,7 @@ __global__ void k_ilt_objective(const float* __restrict__ img, const float* __re
   double cost = 0.0;
   unsigned int perr = 0;
   const long long base = (long long)blockIdx.y * npix;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < npix;
-       k += (long long)gridDim.x * blockDim.x) {
-    const long long i = base + k;
+  auto one = [&](long long i) -> void {
     const float fld = img[i] * scale;
     const float s = sign * (fld - level);
     const float z = sigmoid_clipped(a * s);
@@ -300,6 +298,35 @@ __global__ void k_ilt_objective(const float* __restrict__ img, const float* __re
     dfield[i] = sign * (inv_npix2 * r * (a * z * (1.0f - z)));
     if (signed_out) signed_out[i] = s;
     perr += ((s > 0.f) != (t > 0.5f)) ? 1u : 0u;
+  };
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if ((npix & 3) == 0 && ((base & 3) == 0) && (((uintptr_t)img | (uintptr_t)target | (uintptr_t)dfield) & 15) == 0 &&
+      (!signed_out || ((uintptr_t)signed_out & 15) == 0)) {
+    // four pixels per thread per iteration with 16-byte loads and stores
+    const long long n4 = npix >> 2;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n4; k += stride) {
+      const long long i = base + 4 * k;
+      const float4 iv = *reinterpret_cast<const float4*>(img + i);
+      const float4 tv = *reinterpret_cast<const float4*>(target + i);
+      const float ii[4] = {iv.x, iv.y, iv.z, iv.w}, tt[4] = {tv.x, tv.y, tv.z, tv.w};
+      float d[4], sg[4];
+      float c4 = 0.f;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float s = sign * (ii[q] * scale - level);
+        const float z = sigmoid_clipped(a * s);
+        const float r = z - tt[q];
+        c4 = fmaf(r, r, c4);
+        d[q] = sign * (inv_npix2 * r * (a * z * (1.0f - z)));
+        sg[q] = s;
+        perr += ((s > 0.f) != (tt[q] > 0.5f)) ? 1u : 0u;
+      }
+      cost += (double)c4;
+      *reinterpret_cast<float4*>(dfield + i) = make_float4(d[0], d[1], d[2], d[3]);
+      if (signed_out) *reinterpret_cast<float4*>(signed_out + i) = make_float4(sg[0], sg[1], sg[2], sg[3]);
+    }
+  } else {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < npix; k += stride) one(base + k);
   }
   for (int o = 16; o > 0; o >>= 1) {
     cost += __shfl_xor_sync(0xffffffffu, cost, o);
@@ -319,6 +346,37 @@ __global__ void k_ilt_objective(const float* __restrict__ img, const float* __re
     }
     cost_part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = c;
     perr_part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = p;
+  }
+}
+
+// One ILT update per pixel (opc/ilt.py:381-389, 587-591, 368-378 without
+// smoothing): m = sigmoid(beta theta), q = g beta m (1 - m), Adam on theta,
+// mask = sigmoid(beta_next theta). Four pixels per thread per iteration.
+__global__ void k_ilt_update(const float* __restrict__ g, long long total, float beta, float beta_next, float step,
+                             float b1, float b2, float eps, float c1, float c2, float* __restrict__ theta,
+                             float* __restrict__ m1, float* __restrict__ m2, float* __restrict__ mask) {
+  const long long n4 = total >> 2, stride = (long long)gridDim.x * blockDim.x;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n4; k += stride) {
+    const long long i = 4 * k;
+    const float4 gv = *reinterpret_cast<const float4*>(g + i);
+    const float4 tv = *reinterpret_cast<const float4*>(theta + i);
+    const float4 av = *reinterpret_cast<const float4*>(m1 + i);
+    const float4 vv = *reinterpret_cast<const float4*>(m2 + i);
+    float gg[4] = {gv.x, gv.y, gv.z, gv.w}, th[4] = {tv.x, tv.y, tv.z, tv.w};
+    float a1[4] = {av.x, av.y, av.z, av.w}, a2[4] = {vv.x, vv.y, vv.z, vv.w}, mk[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float m = sigmoid_clipped(beta * th[q]);
+      const float gi = gg[q] * (beta * m * (1.f - m));
+      a1[q] = b1 * a1[q] + (1.f - b1) * gi;
+      a2[q] = b2 * a2[q] + (1.f - b2) * gi * gi;
+      th[q] -= step * (a1[q] / c1) / (sqrtf(a2[q] / c2) + eps);
+      mk[q] = sigmoid_clipped(beta_next * th[q]);
+    }
+    *reinterpret_cast<float4*>(theta + i) = make_float4(th[0], th[1], th[2], th[3]);
+    *reinterpret_cast<float4*>(m1 + i) = make_float4(a1[0], a1[1], a1[2], a1[3]);
+    *reinterpret_cast<float4*>(m2 + i) = make_float4(a2[0], a2[1], a2[2], a2[3]);
+    *reinterpret_cast<float4*>(mask + i) = make_float4(mk[0], mk[1], mk[2], mk[3]);
   }
 }
 
@@ -600,6 +658,19 @@ extern "C" int litho_ilt_adam(const float* g, long long count, float step, float
   const float c1 = (float)(1.0 - pow((double)b1, it)), c2 = (float)(1.0 - pow((double)b2, it));
   k_ilt_adam<<<grid_for(count, 256, sms_here() * 16), 256, 0, s>>>(g, count, step, b1, b2, eps, c1, c2, theta, m1,
                                                                    m2);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+extern "C" int litho_ilt_update(const float* g, long long count, float beta, float beta_next, float step, float b1,
+                                float b2, float eps, int it, float* theta, float* m1, float* m2, float* mask,
+                                cudaStream_t s) {
+  if (!g || !theta || !m1 || !m2 || !mask) return LITHO_E_NULL;
+  if (count < 0 || (count & 3) || it < 1) return LITHO_E_SIZE;
+  if (((uintptr_t)g | (uintptr_t)theta | (uintptr_t)m1 | (uintptr_t)m2 | (uintptr_t)mask) & 15) return LITHO_E_ALIGN;
+  const float c1 = (float)(1.0 - pow((double)b1, it)), c2 = (float)(1.0 - pow((double)b2, it));
+  k_ilt_update<<<grid_for(count / 4, 256, sms_here() * 16), 256, 0, s>>>(g, count, beta, beta_next, step, b1, b2,
+                                                                         eps, c1, c2, theta, m1, m2, mask);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? LITHO_OK : (int)e;
 }

@@ -143,56 +143,40 @@ class _Stages:
             ws.data_ptr(), ws.numel(), self.stream()))
         return hbox
 
-    # -- fused per-pixel passes (no blur, smoothing or penalties) ------------
-    def fused_ok(self, p) -> bool:
+    # -- the fast step (no blur, smoothing or penalties) --------------------
+    def fast_ok(self, p) -> bool:
         return (p.sigma_px < 1e-3 and p.smooth_px < 1e-3 and p.weight_tv == 0.0 and p.weight_discrete == 0.0
-                and bool(self.L.litho_ilt_rows_supported(self.n, 2 * self.h, 2 * self.h))
-                and bool(self.L.litho_ilt_rows_supported(self.n, self.h, self.h)))
+                and self.n % 4 == 0)
 
-    def _rows_ws(self):
-        nb = C.c_size_t(0)
-        nat.check("litho_ilt_rows_workspace", self.L.litho_ilt_rows_workspace(self.n, C.byref(nb)))
-        return self.ws("rows", nb.value)
-
-    def band_columns(self, rows, bm: int, scale: float):
-        out = self.torch.empty((self.C, (2 * bm + 1) ** 2), dtype=self.torch.complex64, device=self.dev)
-        ws = self._rows_ws()
-        nat.check("litho_band_columns", self.L.litho_band_columns(
-            rows.data_ptr(), self.C, self.n, bm, float(scale), out.data_ptr(), ws.data_ptr(), ws.numel(),
-            self.stream()))
-        return out
-
-    def objective_fused(self, mbox, target, scale, level, sign, steepness, want_signed=True):
-        """The objective from the mask band boxes without per-pixel images:
-        (cost (C,), gradient band box (C, (2h+1)^2), signed or None, perr (C,))."""
+    def objective_split(self, mbox, target, scale, level, sign, steepness, want_signed=True):
+        """The objective from the mask band boxes, keeping only band boxes
+        between steps: (cost (C,), gradient band box (C, (2h+1)^2), signed or
+        None, perr (C,)). Synthesis of the image, the per-pixel resist, the
+        band of dJ/dI, the adjoint to the gradient's band box."""
         torch, L = self.torch, self.L
-        h2 = 2 * self.h
-        bbox = self.image_box(mbox)
-        rows = torch.empty((self.C, 2 * h2 + 1, self.n), dtype=torch.complex64, device=self.dev)
-        nblk = self.n // 64
-        cpart = torch.empty((self.C, nblk), dtype=torch.float64, device=self.dev)
-        ppart = torch.empty((self.C, nblk), dtype=torch.int32, device=self.dev)
-        signed = torch.empty((self.C, self.n, self.n), dtype=torch.float32, device=self.dev) if want_signed else None
+        raw = self.image(mbox)
         a = steepness / max(abs(level), 1e-12)
-        ws = self._rows_ws()
-        nat.check("litho_ilt_objective_rows", L.litho_ilt_objective_rows(
-            bbox.data_ptr(), h2, self.C, self.n, target.data_ptr(), float(scale), float(level), float(sign),
-            float(a), None if signed is None else signed.data_ptr(), cpart.data_ptr(), ppart.data_ptr(), h2,
-            rows.data_ptr(), ws.data_ptr(), ws.numel(), self.stream()))
-        gbox = self.band_columns(rows, h2, float(scale) / (self.n * self.n))
+        dfield = torch.empty_like(raw)
+        signed = torch.empty_like(raw) if want_signed else None
+        cpart = torch.empty((self.C, N_PART), dtype=torch.float64, device=self.dev)
+        ppart = torch.empty((self.C, N_PART), dtype=torch.int32, device=self.dev)
+        nat.check("litho_ilt_objective", L.litho_ilt_objective(
+            raw.data_ptr(), target.data_ptr(), self.C, self.n, float(scale), float(level), float(sign), float(a),
+            dfield.data_ptr(), None if signed is None else signed.data_ptr(), cpart.data_ptr(), ppart.data_ptr(),
+            N_PART, self.stream()))
+        gbox = self.band(dfield, 2 * self.h, float(scale) / (self.n * self.n))
         hbox = self.adjoint_box(gbox, mbox)
         return cpart.sum(dim=1) / float(self.n * self.n), hbox, signed, ppart.sum(dim=1)
 
-    def update_fused(self, hbox, theta, m1, m2, beta, beta_next, step, b1, b2, eps, it):
-        """dJ/dm from its band box -> dJ/dtheta -> Adam (in place on theta, m1,
-        m2) -> the next mask's band box."""
-        rows = self.torch.empty((self.C, 2 * self.h + 1, self.n), dtype=self.torch.complex64, device=self.dev)
-        ws = self._rows_ws()
-        nat.check("litho_ilt_update_rows", self.L.litho_ilt_update_rows(
-            hbox.data_ptr(), self.h, self.C, self.n, theta.data_ptr(), m1.data_ptr(), m2.data_ptr(), float(beta),
-            float(beta_next), float(step), float(b1), float(b2), float(eps), int(it), None, self.h, rows.data_ptr(),
-            ws.data_ptr(), ws.numel(), self.stream()))
-        return self.band_columns(rows, self.h, 1.0 / (self.n * self.n))
+    def update_split(self, hbox, theta, m1, m2, beta, beta_next, step, b1, b2, eps, it):
+        """dJ/dm from its band box -> dJ/dtheta -> Adam (theta, m1, m2 in
+        place) -> the next mask; returns (its band box, the mask)."""
+        g = self.synth(hbox, self.h, False)
+        mask = self.torch.empty_like(theta)
+        nat.check("litho_ilt_update", self.L.litho_ilt_update(
+            g.data_ptr(), g.numel(), float(beta), float(beta_next), float(step), float(b1), float(b2), float(eps),
+            int(it), theta.data_ptr(), m1.data_ptr(), m2.data_ptr(), mask.data_ptr(), self.stream()))
+        return self.mask_box(mask), mask
 
     # -- elementwise ----------------------------------------------------------
     def blur(self, x, sigma_px: float):
@@ -524,13 +508,12 @@ class IltBatch:
     beta anneal, mask_of and the objective (SOCS forward + adjoint).
 
     Without blurs, smoothing or penalties (the common ILT setting) the step
-    runs fused: the per-pixel image, dJ/dI, gradient and mask are never
-    written to memory (csrc/ilt_rows.cu); ``mask`` and ``grad_m`` are then
-    formed on demand from theta and the gradient's band box. ``fused=False``
-    forces the stage-by-stage path."""
+    keeps the gradient as its band box between steps and does dJ/dtheta,
+    Adam and the next mask in one pixel pass (``fast``); ``grad_m`` is then
+    synthesised on demand. ``fast=False`` forces the stage-by-stage path."""
 
     def __init__(self, kernels: SOCSKernels, targets, theta0, params: IltParams, engine: str = "fused",
-                 fused: bool | None = None):
+                 fast: bool | None = None):
         self.st = stages(kernels, int(theta0.shape[0]), engine)
         torch = self.st.torch
         n = self.st.n
@@ -541,13 +524,13 @@ class IltBatch:
         self.m2 = torch.zeros_like(self.theta)
         self.beta = float(params.beta)
         self.it = 0
-        can = type(self.st) is _Stages and self.st.fused_ok(params)
-        self.fused = can if fused is None else (bool(fused) and can)
+        can = type(self.st) is _Stages and self.st.fast_ok(params)
+        self.fast = can if fast is None else (bool(fast) and can)
         self._mask = self.st.mask_of(self.theta, self.beta, params.smooth_px)
         self._grad_m = None
-        if self.fused:
+        if self.fast:
             self.mbox = self.st.mask_box(self._mask)
-            self.cost, self.hbox, self.signed, self.perr = self._objective_fused(True)
+            self.cost, self.hbox, self.signed, self.perr = self._objective_fast(True)
         else:
             self.cost, self._grad_m, self.signed, self.perr = self._objective(self._mask)
 
@@ -556,9 +539,9 @@ class IltBatch:
         return self.st.objective(mask, self.target, p.scale, p.level, p.sigma_px, p.sign, p.steepness,
                                  p.weight_tv, p.weight_discrete, want_signed=want_signed)
 
-    def _objective_fused(self, want_signed):
+    def _objective_fast(self, want_signed):
         p = self.p
-        return self.st.objective_fused(self.mbox, self.target, p.scale, p.level, p.sign, p.steepness, want_signed)
+        return self.st.objective_split(self.mbox, self.target, p.scale, p.level, p.sign, p.steepness, want_signed)
 
     @property
     def mask(self):
@@ -575,13 +558,13 @@ class IltBatch:
     def step(self, want_signed: bool = True):
         p = self.p
         self.it += 1
-        if self.fused:
+        if self.fast:
             beta_next = self.beta * p.growth
-            self.mbox = self.st.update_fused(self.hbox, self.theta, self.m1, self.m2, self.beta, beta_next, p.step,
-                                             p.b1, p.b2, p.eps, self.it)
+            self.mbox, self._mask = self.st.update_split(self.hbox, self.theta, self.m1, self.m2, self.beta,
+                                                         beta_next, p.step, p.b1, p.b2, p.eps, self.it)
             self.beta = beta_next
-            self._mask = self._grad_m = None
-            self.cost, self.hbox, self.signed, self.perr = self._objective_fused(want_signed)
+            self._grad_m = None
+            self.cost, self.hbox, self.signed, self.perr = self._objective_fast(want_signed)
             return self.cost
         gt = self.st.grad_theta(self.grad_m, self.mask, self.beta, p.smooth_px)
         nat.check("litho_ilt_adam", self.st.L.litho_ilt_adam(
