@@ -238,6 +238,62 @@ def bench_ilt(args, torch, dev, world, max_over_ranks, barrier) -> dict:
     }
 
 
+UNEVEN_WORKLOAD = ("uneven EUV batch: 256 seeded Manhattan clips, sizes 256^2/512^2/1024^2/2048^2 at weights "
+                   "4:3:2:1, 2 nm pixels, lambda 13.5 nm NA 0.33, dipole 0.6-0.9 +-30 deg (source_grid 43)")
+
+
+def uneven_optics():
+    import lithobat_b200 as lb
+    from lithobat_b200.source import Source
+    return lb.OpticsConfig(wavelength=13.5e-9, NA=0.33, source_grid=43,
+                           source_spec=Source.dipole(0.9, 0.6, opening_deg=60).to_dict())
+
+
+def bench_uneven(args, torch, dev, world, max_over_ranks, barrier) -> dict:
+    """Images/s of the uneven batch: one CUDA-graph replay per batch, work-item
+    sizes tuned per grid size on first use."""
+    import lithobat_b200 as lb
+    from lithobat_b200 import patterns
+    from lithobat_b200.uneven import UnevenAbbe
+    rank = int(os.environ.get("RANK", "0"))
+    rng = np.random.default_rng(700 + rank)
+    count = args.uneven_clips
+    sizes = list(rng.choice([256, 512, 1024, 2048], size=count, p=[0.4, 0.3, 0.2, 0.1]))
+    o = uneven_optics()
+    masks = [torch.from_numpy(patterns.manhattan_clip(rng, int(n), 2e-9, n_rect=(20, 60),
+                                                      width_nm=(20.0, 80.0)).astype(np.float32)).to(dev)
+             for n in sizes]
+    t0 = time.perf_counter()
+    run = UnevenAbbe(sizes, o, 2e-9, tune=True, graph=True)
+    setup_s = time.perf_counter() - t0
+    run.load(masks)
+    for _ in range(max(1, args.warmup)):
+        run.run()
+    torch.cuda.synchronize()
+    barrier()
+    steps = max(1, min(args.steps, 20))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        run.run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / steps)
+    # agreement with one-clip-at-a-time imaging on one clip of each size
+    imgs = run(masks)
+    worst = 0.0
+    for n in sorted(set(sizes)):
+        i = sizes.index(n)
+        ref = lb.compute_aerial_batch(masks[i][None], o, lb.GridConfig(n_pixels=int(n), pixel_size=2e-9))[0][0, 0]
+        worst = max(worst, float((imgs[i].double() - ref.double()).abs().max() / ref.double().abs().max()))
+    return {"metric": "uneven-batch Abbe images/s", "value": world * count / (ms / 1000.0), "unit": "images/s",
+            "ms_per_batch": ms, "steps": steps, "workload": UNEVEN_WORKLOAD, "clips": count,
+            "clips_per_size": {int(n): int(sum(1 for x in sizes if x == n)) for n in sorted(set(sizes))},
+            "source_points": len(lb.source_points(o)), "graph_replay": run.graph is not None,
+            "tuned_items_per_block": {int(k): v["items_per_block"] for k, v in run.tuned.items()},
+            "setup_and_tuning_s": setup_s, "max_rel_diff_vs_single_clip": worst}
+
+
 def cpu_ilt_seconds() -> tuple[float, int]:
     """FP64 numpy objective (forward + adjoint) of one clip of the ILT workload, K = 24."""
     from oracle import litho_oracle as O
@@ -541,6 +597,8 @@ def run_ours(args) -> None:
                        "images_per_step": E2E_IMAGES}
     if "ilt" not in args.skip:
         line["ilt"] = bench_ilt(args, torch, dev, world, max_over_ranks, barrier)
+    if "uneven" not in args.skip:
+        line["uneven"] = bench_uneven(args, torch, dev, world, max_over_ranks, barrier)
     if rank == 0 and world == 1 and not args.no_cpu:
         t, k, S = cpu_sample_seconds()
         cv = 1.0 / (t * S / k)
@@ -565,8 +623,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--images", type=int, default=IMAGES_PER_STEP,
                     help="images per step (a small value makes a profiling case)")
-    ap.add_argument("--skip", default="", help="comma list of phases to skip: plain,e2e,profile,cpu,ilt,iltplain")
+    ap.add_argument("--skip", default="", help="comma list of phases to skip: plain,e2e,profile,cpu,ilt,iltplain,uneven")
     ap.add_argument("--ilt-clips", type=int, default=ILT_CLIPS, help="clips per ILT step")
+    ap.add_argument("--uneven-clips", type=int, default=256, help="clips in the uneven-size batch")
     args = ap.parse_args()
     args.skip = set(x for x in args.skip.split(",") if x)
     if "cpu" in args.skip:
