@@ -356,6 +356,18 @@ int litho_ilt_adam(const float* g_dev, long long count, float step, float b1, fl
 int litho_gaussian_blur(const float* in_dev, float* out_dev, float* tmp_dev, int n_fields, int n,
                         const float* weights_dev, int radius, cudaStream_t stream);
 
+/* ---- process-window helpers ----
+ * The dose axis of a dose-focus sweep (analysis/process_window.py:285-290):
+ * out[f][d] = raw[f] * normalisation_scale(mode, peak[f], clear[f], dose[d])
+ * (expose/aerial_image.py:217-241); mode 0 none, 1 peak, 2 clear. raw:
+ * [n_planes][npix] raw Abbe sums (litho_abbe with scale 1); out:
+ * [n_planes][n_doses][npix]; peak/clear: device [n_planes]; doses: device. */
+int litho_dose_stack(const float* raw_dev, const float* peak_dev, const float* clear_dev, int mode, int n_planes,
+                     long long npix, const float* doses_dev, int n_doses, float* out_dev, cudaStream_t stream);
+/* x = min(max(x, lo), hi) in place: the clip after PEB diffusion
+ * (bake/peb.py:65-66). */
+int litho_clamp(float* x_dev, long long count, float lo, float hi, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

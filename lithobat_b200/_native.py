@@ -120,6 +120,8 @@ def lib():
         "litho_ilt_adam": [vp, C.c_longlong, f32, f32, f32, f32, i32, vp, vp, vp, vp],
         "litho_gaussian_blur": [vp, vp, vp, i32, i32, vp, i32, vp],
         "litho_ilt_update": [vp, C.c_longlong, f32, f32, f32, f32, f32, f32, i32, vp, vp, vp, vp, vp],
+        "litho_dose_stack": [vp, vp, vp, i32, i32, C.c_longlong, vp, i32, vp, vp],
+        "litho_clamp": [vp, C.c_longlong, f32, f32, vp],
         "litho_plain_socs_workspace": [i32, i32, C.POINTER(sz)],
         "litho_plain_socs_forward": [vp, i32, i32, i32, vp, vp, vp, vp, i32, vp, vp, vp, sz, vp],
         "litho_plain_socs_adjoint": [vp, vp, i32, i32, i32, vp, vp, vp, vp, i32, vp, vp, sz, vp],

@@ -563,6 +563,42 @@ def blur(a, sigma_px):
     return gaussian_filter(a, sigma=sigma_px)
 
 
+def apply_peb(pac_map, diffusion_sigma, pixel_size):
+    """bake/peb.py:24-70 — Gaussian PEB diffusion (scipy, reflect), clipped to [0, 1]."""
+    a = np.asarray(pac_map)
+    if a.ndim != 2:
+        raise ValueError(f"apply_peb expects a 2-D (ny, nx) map, got ndim={a.ndim}")
+    if diffusion_sigma < 0:
+        raise ValueError(f"diffusion_sigma must be >= 0, got {diffusion_sigma!r}")
+    if pixel_size <= 0:
+        raise ValueError(f"pixel_size must be > 0, got {pixel_size!r}")
+    sigma_px = diffusion_sigma / pixel_size
+    if sigma_px < 1e-3:
+        return a.copy()
+    return np.clip(gaussian_filter(a.astype(np.float64), sigma=sigma_px), 0.0, 1.0)
+
+
+def dose_focus_images(mask, optics, grid, doses, defoci_nm, normalisation="clear"):
+    """analysis/process_window.py:215-300 (the imaging part of sweep_dose_focus):
+    one Abbe sum per defocus, each dose a rescale of the raw sum. (F, D, N, N)."""
+    import copy
+
+    def _with(o, **kw):
+        c = copy.copy(o)
+        for k, v in kw.items():
+            setattr(c, k, v)
+        return c
+    base = optics
+    if normalisation is not None and normalisation != getattr(optics, "normalisation", "peak"):
+        base = _with(optics, normalisation=normalisation)
+    out = []
+    for d_nm in defoci_nm:
+        local = _with(base, defocus=d_nm * 1e-9)
+        raw, peak, clear = compute_aerial_image(mask, local, grid, return_raw=True)
+        out.append([raw * normalisation_scale(base.normalisation, peak, clear, dose) for dose in doses])
+    return np.array(out)
+
+
 def objective(k: SOCS, target, mask, scale, level, sigma_px, sign, steepness,
               weight_tv=0.0, weight_discrete=0.0):
     """opc/ilt.py:311-360 — (cost, grad, signed, pattern_error)."""

@@ -280,6 +280,7 @@ def main():
     save("ilt_imm_128_k24", optics=o4, grid=g4, theta=theta, target=target.astype(np.uint8),
          beta=4.0, cost=cost, grad=gk, signed=signed, perr=perr)
     wide()
+    next_rows()
     print("done")
 
 
@@ -310,8 +311,37 @@ def wide():
          clear=k.clear, n_band=k.n_band, raw=r[0], peak=r[1])
 
 
+def next_rows():
+    """Rows beyond the imaging core: PEB diffusion (bake/peb.py) and the
+    imaging part of the dose-focus sweep (analysis/process_window.py)."""
+    _import_reference()
+    import dataclasses
+
+    from litho_sim.bake.peb import apply_peb
+    from litho_sim.core.config import GridConfig, OpticsConfig
+    from litho_sim.expose import compute_aerial_image, normalisation_scale
+    rng = np.random.default_rng(41)
+    pac = rng.random((96, 96))
+    save("peb_small", pac=pac, sigma=np.array([7e-9, 0.0]), px=np.array(4e-9),
+         out=apply_peb(pac, 7e-9, 4e-9), out0=apply_peb(pac, 0.0, 4e-9))
+    g = GridConfig(n_pixels=64, pixel_size=4e-9)
+    o = OpticsConfig(NA=0.93, source_type="annular", sigma_inner=0.5, sigma_outer=0.85, source_grid=11,
+                     normalisation="clear")
+    m = manhattan_clip(np.random.default_rng(42), 64, 4e-9, n_rect=(4, 8), width_nm=(40, 120))
+    defoci, doses = [-60.0, 0.0, 45.0], [0.8, 1.0, 1.25]
+    stack = []
+    for d_nm in defoci:
+        local = dataclasses.replace(o, defocus=d_nm * 1e-9)
+        raw, peak, clear = compute_aerial_image(m, local, g, return_raw=True)
+        stack.append([raw * normalisation_scale(o.normalisation, peak, clear, dose) for dose in doses])
+    save("dose_focus_64", optics=o, grid=g, mask=m.astype(np.uint8), defoci=np.array(defoci),
+         doses=np.array(doses), stack=np.array(stack))
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["wide"]:
         wide()
+    elif sys.argv[1:] == ["next"]:
+        next_rows()
     else:
         main()

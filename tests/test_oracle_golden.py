@@ -143,3 +143,21 @@ def test_ilt_mid_size_objective():
     assert cost == pytest.approx(float(a["cost"]), rel=1e-10)
     np.testing.assert_allclose(g, a["grad"], rtol=0, atol=1e-9 * np.abs(a["grad"]).max())
     assert perr == int(a["perr"])
+
+
+def test_peb_matches_reference():
+    a = load_golden("peb_small")[0]
+    np.testing.assert_allclose(O.apply_peb(a["pac"], 7e-9, 4e-9), a["out"], rtol=0, atol=1e-14)
+    np.testing.assert_array_equal(O.apply_peb(a["pac"], 0.0, 4e-9), a["out0"])
+    with pytest.raises(ValueError):
+        O.apply_peb(a["pac"][None], 7e-9, 4e-9)
+    with pytest.raises(ValueError):
+        O.apply_peb(a["pac"], -1e-9, 4e-9)
+
+
+def test_dose_focus_images_match_reference():
+    a, od, gd = load_golden("dose_focus_64")
+    o, g = ns_optics(od), ns_grid(gd)
+    st = O.dose_focus_images(a["mask"].astype(np.float64), o, g, list(a["doses"]), list(a["defoci"]),
+                             normalisation=None)
+    np.testing.assert_allclose(st, a["stack"], rtol=0, atol=1e-12 * float(np.abs(a["stack"]).max()))
