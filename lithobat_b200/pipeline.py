@@ -1,0 +1,92 @@
+"""Host-to-host imaging of a stream of mask batches with the copies overlapped.
+
+A caller whose masks live in host memory (the reference's numpy callers:
+opc/model.py, analysis/process_window.py, the CLI) pays the host link for every
+batch: 8 bytes per complex mask pixel in, 4 bytes per image pixel out. Run one
+batch at a time and the GPU idles while the link works. ``AbbePipeline`` keeps
+``depth`` device slots and three CUDA streams: while batch i is imaged, batch
+i+1 is uploaded and batch i-1 downloaded, ordered by events, so a stream of
+batches runs at the link's pace rather than at link + compute.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+from . import _native as nat
+from .aerial import fused_supported, plan_abbe, pupil_table
+from .config import optics_view
+
+
+class AbbePipeline:
+    """Images batches of ``batch`` clips (one optics, one grid) from pinned
+    host tensors into pinned host tensors.
+
+    ``run(inputs, outputs)``: inputs[i] (batch, N, N) float32 or complex64
+    pinned CPU tensors, outputs[i] (batch, N, N) float32 pinned CPU tensors
+    (the same tensor may appear several times in either list; an output is
+    complete once ``run`` returns)."""
+
+    def __init__(self, optics, grid, batch: int, mask_complex: bool, dose: float = 1.0, return_raw: bool = False,
+                 depth: int = 2, device=None):
+        torch = nat.require_cuda()
+        self.torch, self.L = torch, nat.lib()
+        self.dev = device if device is not None else torch.device("cuda", torch.cuda.current_device())
+        v = optics_view(optics)
+        self.n = n = int(grid.n_pixels)
+        self.batch = int(batch)
+        self.complex = bool(mask_complex)
+        self.pd = plan_abbe([v] * self.batch, n, float(grid.pixel_size), [[(v.defocus, v.image_index)]] * self.batch,
+                            float(dose), bool(return_raw), self.complex)
+        if not fused_supported(n, int(self.pd.plan.L)):
+            raise NotImplementedError("the pipeline runs the band-limited engines only")
+        self.pd._blob_dev = torch.from_numpy(self.pd.blob).to(self.dev)
+        self.table = pupil_table(self.pd, self.dev, nat.stream_ptr(torch, self.dev))
+        nb = C.c_size_t(0)
+        nat.check("litho_abbe_workspace", self.L.litho_abbe_workspace(C.byref(self.pd.plan), C.byref(nb)))
+        self.ws = torch.empty(max(nb.value, 256), dtype=torch.uint8, device=self.dev)
+        dt = torch.complex64 if self.complex else torch.float32
+        self.depth = max(2, int(depth))
+        self.d_in = [torch.empty((self.batch, n, n), dtype=dt, device=self.dev) for _ in range(self.depth)]
+        self.d_out = [torch.empty((self.batch, n, n), dtype=torch.float32, device=self.dev) for _ in range(self.depth)]
+        self.d_peak = [torch.empty((self.batch,), dtype=torch.float32, device=self.dev) for _ in range(self.depth)]
+        self.s_in = torch.cuda.Stream(device=self.dev)
+        self.s_run = torch.cuda.Stream(device=self.dev)
+        self.s_out = torch.cuda.Stream(device=self.dev)
+
+    def run(self, inputs, outputs) -> None:
+        torch, L = self.torch, self.L
+        if len(inputs) != len(outputs):
+            raise ValueError(f"{len(inputs)} input batches for {len(outputs)} outputs")
+        ev = torch.cuda.Event
+        read_done = [None] * self.depth    # compute finished reading d_in[slot]
+        sent = [None] * self.depth         # download of d_out[slot] finished
+        for i, (hin, hout) in enumerate(zip(inputs, outputs)):
+            k = i % self.depth
+            with torch.cuda.stream(self.s_in):
+                if read_done[k] is not None:
+                    self.s_in.wait_event(read_done[k])
+                self.d_in[k].copy_(hin, non_blocking=True)
+                loaded = ev()
+                loaded.record(self.s_in)
+            with torch.cuda.stream(self.s_run):
+                self.s_run.wait_event(loaded)
+                if sent[k] is not None:
+                    self.s_run.wait_event(sent[k])
+                nat.check("litho_abbe_tabled", L.litho_abbe_tabled(
+                    C.byref(self.pd.plan), self.pd._blob_dev.data_ptr(), self.table.data_ptr(),
+                    self.d_in[k].data_ptr(), self.d_out[k].data_ptr(), self.d_peak[k].data_ptr(),
+                    self.ws.data_ptr(), self.ws.numel(), int(self.s_run.cuda_stream)))
+                done = ev()
+                done.record(self.s_run)
+                read_done[k] = done
+            with torch.cuda.stream(self.s_out):
+                self.s_out.wait_event(done)
+                hout.copy_(self.d_out[k], non_blocking=True)
+                fin = ev()
+                fin.record(self.s_out)
+                sent[k] = fin
+        self.s_out.synchronize()
+
+
+__all__ = ["AbbePipeline"]
