@@ -466,10 +466,10 @@ int synth_blocks_for(int n) { return (n + kSynthRows - 1) / kSynthRows; }
 
 // Real synthesis of n_fields Hermitian boxes of side G into n x n images.
 cudaError_t launch_synth_real(const float2* box, int G, int n, int n_fields, const float2* tw, const LithoNorm* norm,
-                              float* out, float* blockmax, cudaStream_t s) {
+                              float* out, float* blockmax, cudaStream_t s, float2* cbuf) {
   const int gh = G / 2;
   if (!norm && synth_pairs_ok(n, gh))
-    return launch_synth_pairs(box, gh, n, n_fields, tw, nullptr, out, nullptr, blockmax, s, nullptr);
+    return launch_synth_pairs(box, gh, n, n_fields, tw, nullptr, out, nullptr, blockmax, s, nullptr, cbuf);
   const size_t sm = (size_t)n * 8 + (size_t)kSynthRows * (gh + 1) * 8 + (size_t)G * G * 8;
   cudaFuncSetAttribute(k_synth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   dim3 gs((n + kSynthRows - 1) / kSynthRows, n_fields);
@@ -534,7 +534,7 @@ __global__ void k_normalise(const float* __restrict__ blockmax, int nblk, const 
 static int synth_blocks(int n) { return (n + kSynthRows - 1) / kSynthRows; }
 
 struct AbbeLayout {
-  int64_t status, tw, u1, mb, table, partial, bbox, blockmax, total;
+  int64_t status, tw, u1, mb, table, partial, bbox, blockmax, cbuf, total;
 };
 
 
@@ -554,6 +554,8 @@ static AbbeLayout abbe_layout(const LithoAbbePlan& p) {
   l.partial = off;  off = align16(off + (int64_t)p.n_items * p.L * p.L * 4);
   l.bbox = off;     off = align16(off + (int64_t)p.n_out * G * G * 8);
   l.blockmax = off; off = align16(off + (int64_t)p.n_out * synth_blocks(p.n) * 4);
+  l.cbuf = off;
+  if (synth_pairs_ok(p.n, 2 * p.h)) off = align16(off + synth_cols_bytes(p.n_out, p.n, 2 * p.h));
   l.total = off;
   return l;
 }
@@ -678,7 +680,8 @@ static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* tab
   mark(5);
   if (synth_pairs_ok(p.n, 2 * p.h)) {
     // peak pass (peak-normalised outputs), then the writing pass
-    e = launch_synth_pairs(bbox, 2 * p.h, p.n, p.n_out, tw, norm, image, peak, blockmax, s, ev ? ev[6] : nullptr);
+    e = launch_synth_pairs(bbox, 2 * p.h, p.n, p.n_out, tw, norm, image, peak, blockmax, s, ev ? ev[6] : nullptr,
+                           reinterpret_cast<float2*>(w + l.cbuf));
     if (e != cudaSuccess) return (int)e;
   } else {
     const int gh = G / 2;

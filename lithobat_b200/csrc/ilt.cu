@@ -23,7 +23,8 @@ cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_
                                 float2* out, float scale, const float2* tw_inv, int num_sms, cudaStream_t st,
                                 int* status);
 cudaError_t launch_synth_real(const float2* box, int G, int n, int n_fields, const float2* tw, const LithoNorm* norm,
-                              float* out, float* blockmax, cudaStream_t s);
+                              float* out, float* blockmax, cudaStream_t s, float2* cbuf);
+int64_t synth_cols_bytes(int n_out, int n, int g0);
 int synth_blocks_for(int n);
 
 // ---------------------------------------------------------------------------
@@ -538,7 +539,10 @@ extern "C" int litho_band_spectrum(const void* in, int is_complex, int n_fields,
 extern "C" int litho_band_synthesis_workspace(int n_fields, int n, size_t* bytes) {
   if (!bytes) return LITHO_E_NULL;
   if (n_fields < 1 || n < 2) return LITHO_E_SIZE;
-  *bytes = (size_t)(align16((int64_t)n * 8) + align16((int64_t)n_fields * synth_blocks_for(n) * 4));
+  // twiddles, block maxima, and the whole-image column buffer for the widest
+  // box the pair synthesis takes (half-width 31)
+  *bytes = (size_t)(align16((int64_t)n * 8) + align16((int64_t)n_fields * synth_blocks_for(n) * 4) +
+                    align16(synth_cols_bytes(n_fields, n, 31)));
   return LITHO_OK;
 }
 
@@ -561,8 +565,11 @@ extern "C" int litho_band_synthesis(const void* box, int n_fields, int n, int h,
     k_synth_complex<<<g, 256, sm, s>>>(static_cast<const float2*>(box), h, n, tw, static_cast<float2*>(out));
     e = cudaGetLastError();
   } else {
+    float2* cbuf = h <= 31 ? reinterpret_cast<float2*>(static_cast<char*>(ws) + align16((int64_t)n * 8) +
+                                                       align16((int64_t)n_fields * synth_blocks_for(n) * 4))
+                           : nullptr;
     e = launch_synth_real(static_cast<const float2*>(box), 2 * h + 1, n, n_fields, tw, nullptr,
-                          static_cast<float*>(out), blockmax, s);
+                          static_cast<float*>(out), blockmax, s, cbuf);
   }
   return e == cudaSuccess ? LITHO_OK : (int)e;
 }

@@ -57,11 +57,56 @@ bool synth_pairs_ok(int n, int g0) {
 // PASS 0: block maxima only, for peak-normalised outputs (others return).
 // PASS 1: write raw * scale (scale / peak for peak-normalised outputs) and
 //         the block maxima of the raw image.
+// Column stage for whole images, done once ahead of both synthesis passes:
+// C[o][gx][y] = sum_gy B(gx, gy) w^(gy y) for gx = 0..g0 and every row y,
+// by the same residue method as the row stage (y = b + M a, a 32-point FFT
+// per residue). One warp per (output, gx).
+constexpr int kColWarps = 8;
+
+__global__ void __launch_bounds__(kColWarps * 32, 2)
+k_synth_cols(const float2* __restrict__ Bbox, int g0, int n, const float2* __restrict__ tw_inv,
+             float2* __restrict__ Cg) {
+  extern __shared__ float2 cols_tb[];                   // [g][b] = w^(g b), g = 0..g0
+  __shared__ float2 col[kColWarps][2 * kSyG0Max + 2];   // B(gx, gy + g0) of each warp's column
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int o = blockIdx.y, gx = blockIdx.x * kColWarps + warp;
+  const int gp = g0 + 1, G = 2 * g0 + 1, M = n >> 5, nmask = n - 1;
+  for (int j = threadIdx.x; j < gp * M; j += blockDim.x) {
+    const int g = j / M, b = j % M;
+    cols_tb[j] = __ldg(tw_inv + ((g * b) & nmask));
+  }
+  if (gx < gp) {
+    const float2* bc = Bbox + (size_t)o * G * G + gx + g0;
+    for (int i = lane; i < G; i += 32) col[warp][i] = bc[(size_t)i * G];
+  }
+  __syncthreads();
+  if (gx >= gp) return;
+  const float2* cw = col[warp] + g0;
+  float2* dst = Cg + ((size_t)o * gp + gx) * n;
+  for (int b = lane; b < M; b += 32) {
+    float2 Q[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) Q[i] = make_float2(0.f, 0.f);
+    Q[0] = cw[0];
+#pragma unroll
+    for (int g = 1; g <= kSyG0Max; ++g) {
+      if (g <= g0) {
+        const float2 t = cols_tb[g * M + b];
+        Q[g & 31] = cadd(Q[g & 31], cmul(cw[g], t));
+        Q[(-g) & 31] = cadd(Q[(-g) & 31], cmulc(cw[-g], t));
+      }
+    }
+    fft_reg<32, +1>(Q);
+#pragma unroll
+    for (int a = 0; a < 32; ++a) dst[b + M * a] = Q[a];
+  }
+}
+
 template <int PASS>
 __global__ void __launch_bounds__(kSyWarps * 32, 2)
 k_synth_pairs(const float2* __restrict__ Bbox, int g0, int n, const float2* __restrict__ tw_inv,
               const LithoNorm* __restrict__ norm, const float* __restrict__ peak, float* __restrict__ image,
-              float* __restrict__ blockmax) {
+              float* __restrict__ blockmax, const float2* __restrict__ Cg) {
   extern __shared__ __align__(16) unsigned char sy_raw[];
   const SynthSmem L = synth_smem(n, g0);
   const int o = blockIdx.y, y0 = blockIdx.x * kSyRows;
@@ -73,21 +118,34 @@ k_synth_pairs(const float2* __restrict__ Bbox, int g0, int n, const float2* __re
   float2* B = reinterpret_cast<float2*>(sy_raw + L.off_b);     // [gy + g0][gx + g0]
   __shared__ float red[kSyWarps];
   const int M = L.M, G = L.G, gp = L.gp, nmask = n - 1;
-  for (int j = threadIdx.x; j < n; j += blockDim.x) tw[j] = tw_inv[j];
-  const float2* Bo = Bbox + (size_t)o * G * G;
-  for (int j = threadIdx.x; j < G * G; j += blockDim.x) B[j] = Bo[j];
-  __syncthreads();
-  for (int j = threadIdx.x; j < gp * M; j += blockDim.x) {
-    const int g = j / M, b = j % M;
-    TB[j] = tw[(g * b) & nmask];
-  }
-  // column stage for the block's rows
-  for (int id = threadIdx.x; id < kSyRows * gp; id += blockDim.x) {
-    const int r = id / gp, gx = id % gp, y = y0 + r;
-    float2 acc = make_float2(0.f, 0.f);
-    const float2* bc = B + gx + g0;
-    for (int gy = -g0; gy <= g0; ++gy) acc = cadd(acc, cmul(bc[(gy + g0) * G], tw[(gy * y) & nmask]));
-    C[id] = acc;
+  if (Cg) {
+    // column stage done ahead (k_synth_cols): C[o][gx][y] -> C[row][gx]
+    for (int j = threadIdx.x; j < gp * M; j += blockDim.x) {
+      const int g = j / M, b = j % M;
+      TB[j] = __ldg(tw_inv + ((g * b) & nmask));
+    }
+    const float2* cs = Cg + (size_t)o * gp * n + y0;
+    for (int id = threadIdx.x; id < kSyRows * gp; id += blockDim.x) {
+      const int gx = id / kSyRows, r = id % kSyRows;
+      C[r * gp + gx] = __ldg(cs + (size_t)gx * n + r);
+    }
+  } else {
+    for (int j = threadIdx.x; j < n; j += blockDim.x) tw[j] = tw_inv[j];
+    const float2* Bo = Bbox + (size_t)o * G * G;
+    for (int j = threadIdx.x; j < G * G; j += blockDim.x) B[j] = Bo[j];
+    __syncthreads();
+    for (int j = threadIdx.x; j < gp * M; j += blockDim.x) {
+      const int g = j / M, b = j % M;
+      TB[j] = tw[(g * b) & nmask];
+    }
+    // column stage for the block's rows
+    for (int id = threadIdx.x; id < kSyRows * gp; id += blockDim.x) {
+      const int r = id / gp, gx = id % gp, y = y0 + r;
+      float2 acc = make_float2(0.f, 0.f);
+      const float2* bc = B + gx + g0;
+      for (int gy = -g0; gy <= g0; ++gy) acc = cadd(acc, cmul(bc[(gy + g0) * G], tw[(gy * y) & nmask]));
+      C[id] = acc;
+    }
   }
   __syncthreads();
 
@@ -171,25 +229,36 @@ int synth_pairs_blocks(int n) { return n / kSyRows; }
 // Synthesis of n_out Hermitian boxes of side 2 g0 + 1 into n x n images with
 // the normalisation of `norm` (nullptr: scale 1), the raw peaks into `peak`
 // (may be nullptr when norm is) and `mid` (optional) recorded between the
-// peak pass and the writing pass. Requires synth_pairs_ok(n, g0).
+// peak pass and the writing pass. cbuf (optional, n_out x (g0 + 1) x n
+// complex): the column stage then runs once for whole images ahead of both
+// passes. Requires synth_pairs_ok(n, g0).
 cudaError_t launch_synth_pairs(const float2* box, int g0, int n, int n_out, const float2* tw, const LithoNorm* norm,
-                               float* image, float* peak, float* blockmax, cudaStream_t s, cudaEvent_t mid) {
+                               float* image, float* peak, float* blockmax, cudaStream_t s, cudaEvent_t mid,
+                               float2* cbuf) {
   const SynthSmem L = synth_smem(n, g0);
   const dim3 grid(n / kSyRows, n_out);
   const int pk_blocks = (n_out + 7) / 8;
   cudaError_t e;
+  if (cbuf) {
+    const size_t smc = (size_t)(g0 + 1) * (n >> 5) * 8;
+    k_synth_cols<<<dim3((g0 + 1 + kColWarps - 1) / kColWarps, n_out), kColWarps * 32, smc, s>>>(box, g0, n, tw,
+                                                                                               cbuf);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   if (norm) {
     if (!peak) return cudaErrorInvalidValue;
     cudaFuncSetAttribute(k_synth_pairs<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
-    k_synth_pairs<0><<<grid, kSyWarps * 32, L.total, s>>>(box, g0, n, tw, norm, peak, image, blockmax);
+    k_synth_pairs<0><<<grid, kSyWarps * 32, L.total, s>>>(box, g0, n, tw, norm, peak, image, blockmax, cbuf);
     k_peak<<<pk_blocks, 256, 0, s>>>(blockmax, grid.x, norm, n_out, 1, peak);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   if (mid) cudaEventRecord(mid, s);
   cudaFuncSetAttribute(k_synth_pairs<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total);
-  k_synth_pairs<1><<<grid, kSyWarps * 32, L.total, s>>>(box, g0, n, tw, norm, peak, image, blockmax);
+  k_synth_pairs<1><<<grid, kSyWarps * 32, L.total, s>>>(box, g0, n, tw, norm, peak, image, blockmax, cbuf);
   if (peak) k_peak<<<pk_blocks, 256, 0, s>>>(blockmax, grid.x, norm, n_out, norm ? 0 : -1, peak);
   return cudaGetLastError();
 }
+
+int64_t synth_cols_bytes(int n_out, int n, int g0) { return (int64_t)n_out * (g0 + 1) * n * 8; }
 
 }  // namespace litho

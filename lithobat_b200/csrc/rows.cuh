@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 #include "../../include/litho_b200.h"
 
@@ -12,6 +13,9 @@ namespace litho {
 bool synth_pairs_ok(int n, int g0);
 int synth_pairs_blocks(int n);
 cudaError_t launch_synth_pairs(const float2* box, int g0, int n, int n_out, const float2* tw, const LithoNorm* norm,
-                               float* image, float* peak, float* blockmax, cudaStream_t s, cudaEvent_t mid);
+                               float* image, float* peak, float* blockmax, cudaStream_t s, cudaEvent_t mid,
+                               float2* cbuf);
+// Bytes of the whole-image column buffer of launch_synth_pairs.
+int64_t synth_cols_bytes(int n_out, int n, int g0);
 
 }  // namespace litho
