@@ -100,10 +100,14 @@ __host__ __device__ inline C32Smem c32_smem(int h, int bm) {
   return g;
 }
 
+// H: the pupil half-width as a compile-time constant (instantiated for 0..7),
+// so the band tests and the pruned FFTs' zero masks fold away.
+template <int H>
 __global__ void __launch_bounds__(kCoarseWarps * 32, 4)
 k_coarse32(const LithoItem* __restrict__ items, const LithoJob* __restrict__ jobs,
-           const float2* __restrict__ table, int h, int ncomp_max, const float2* __restrict__ Mb,
+           const float2* __restrict__ table, int ncomp_max, const float2* __restrict__ Mb,
            int bm, float* __restrict__ partial) {
+  constexpr int h = H;
   extern __shared__ __align__(16) unsigned char c32_raw[];
   const C32Smem g = c32_smem(h, bm);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -138,7 +142,7 @@ k_coarse32(const LithoItem* __restrict__ items, const LithoJob* __restrict__ job
 #pragma unroll
   for (int u = 0; u < 32; ++u) J[u] = 0.f;
   const int half = lane >> 4, col = lane & 15;
-  constexpr uint64_t kNZ = band_mask32(kCoarseHMax32);
+  constexpr uint64_t kNZ = band_mask32(H);
   for (int pp = warp; pp < n_pairs; pp += kCoarseWarps) {
     cp_async_wait_all();
     __syncwarp();
@@ -199,6 +203,31 @@ k_coarse32(const LithoItem* __restrict__ items, const LithoJob* __restrict__ job
 #pragma unroll
     for (int wp = 0; wp < kCoarseWarps; ++wp) s += js[wp * 1024 + idx];
     dst[idx] = s;  // idx = v * 32 + u  (row = y, column = x)
+  }
+}
+
+template <int H>
+static cudaError_t launch_coarse32_h(int n_items, size_t sm, cudaStream_t s, const LithoItem* items,
+                                     const LithoJob* jobs, const float2* table, int ncomp_max, const float2* mb,
+                                     int bm, float* partial) {
+  cudaFuncSetAttribute(k_coarse32<H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_coarse32<H><<<n_items, kCoarseWarps * 32, sm, s>>>(items, jobs, table, ncomp_max, mb, bm, partial);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_coarse32(int h, int n_items, size_t sm, cudaStream_t s, const LithoItem* items,
+                                   const LithoJob* jobs, const float2* table, int ncomp_max, const float2* mb,
+                                   int bm, float* partial) {
+  switch (h) {
+    case 0: return launch_coarse32_h<0>(n_items, sm, s, items, jobs, table, ncomp_max, mb, bm, partial);
+    case 1: return launch_coarse32_h<1>(n_items, sm, s, items, jobs, table, ncomp_max, mb, bm, partial);
+    case 2: return launch_coarse32_h<2>(n_items, sm, s, items, jobs, table, ncomp_max, mb, bm, partial);
+    case 3: return launch_coarse32_h<3>(n_items, sm, s, items, jobs, table, ncomp_max, mb, bm, partial);
+    case 4: return launch_coarse32_h<4>(n_items, sm, s, items, jobs, table, ncomp_max, mb, bm, partial);
+    case 5: return launch_coarse32_h<5>(n_items, sm, s, items, jobs, table, ncomp_max, mb, bm, partial);
+    case 6: return launch_coarse32_h<6>(n_items, sm, s, items, jobs, table, ncomp_max, mb, bm, partial);
+    case 7: return launch_coarse32_h<7>(n_items, sm, s, items, jobs, table, ncomp_max, mb, bm, partial);
+    default: return cudaErrorInvalidValue;
   }
 }
 
@@ -662,9 +691,8 @@ static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* tab
   mark(3);
   if (p.L == 32) {
     const size_t sm_coarse = c32_smem(p.h, p.bm).total;
-    cudaFuncSetAttribute(k_coarse32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_coarse);
-    k_coarse32<<<p.n_items, kCoarseWarps * 32, sm_coarse, s>>>(items, jobs, table, p.h, p.ncomp_max, mb, p.bm,
-                                                                partial);
+    e = launch_coarse32(p.h, p.n_items, sm_coarse, s, items, jobs, table, p.ncomp_max, mb, p.bm, partial);
+    if (e != cudaSuccess) return (int)e;
   } else {
     const size_t sm_coarse = coarse64_smem();
     cudaFuncSetAttribute(k_coarse64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_coarse);
@@ -730,9 +758,9 @@ extern "C" int litho_coarse_image(const LithoAbbePlan* plan, const void* blob, c
   const int G = 4 * p.h + 1;
   if (p.L == 32) {
     const size_t sm = c32_smem(p.h, p.bm).total;
-    cudaFuncSetAttribute(k_coarse32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_coarse32<<<p.n_items, kCoarseWarps * 32, sm, s>>>(items, jobs, static_cast<const float2*>(table), p.h,
-                                                        p.ncomp_max, static_cast<const float2*>(mb), p.bm, partial);
+    const cudaError_t e32 = launch_coarse32(p.h, p.n_items, sm, s, items, jobs, static_cast<const float2*>(table),
+                                            p.ncomp_max, static_cast<const float2*>(mb), p.bm, partial);
+    if (e32 != cudaSuccess) return (int)e32;
   } else {
     const size_t sm = coarse64_smem();
     cudaFuncSetAttribute(k_coarse64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
