@@ -36,6 +36,8 @@ bool wide_plan_ok(const LithoAbbePlan& p);
 int64_t wide_workspace_bytes(const LithoAbbePlan& p);
 int abbe_wide_run(const LithoAbbePlan& p, const void* blob, const void* table_in, const void* mask, float* image,
                   float* peak, void* ws, cudaStream_t s, int num_sms, cudaEvent_t* ev);
+int wide_coarse_box(const LithoAbbePlan& p, const void* blob, const float2* table, const float2* mb, float2* bbox_out,
+                    void* ws, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // 1. pupil table: table[slot][comp][(dy+h)(2h+1) + dx+h], one block per slot,
@@ -747,7 +749,11 @@ extern "C" int litho_coarse_image(const LithoAbbePlan* plan, const void* blob, c
   if (st) return st;
   if (!blob || !table || !mb || !bbox_out || !ws) return LITHO_E_NULL;
   const LithoAbbePlan& p = *plan;
-  if (p.L > 64) return LITHO_E_UNSUPPORTED;
+  if (p.L > 64) {
+    if ((int64_t)ws_bytes < wide_workspace_bytes(p)) return LITHO_E_WORKSPACE;
+    return wide_coarse_box(p, blob, static_cast<const float2*>(table), static_cast<const float2*>(mb),
+                           static_cast<float2*>(bbox_out), ws, s);
+  }
   const AbbeLayout l = abbe_layout(p);
   if ((int64_t)ws_bytes < l.total) return LITHO_E_WORKSPACE;
   const char* b = static_cast<const char*>(blob);

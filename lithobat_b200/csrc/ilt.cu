@@ -25,6 +25,14 @@ cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_
 cudaError_t launch_synth_real(const float2* box, int G, int n, int n_fields, const float2* tw, const LithoNorm* norm,
                               float* out, float* blockmax, cudaStream_t s, float2* cbuf);
 int64_t synth_cols_bytes(int n_out, int n, int g0);
+bool synth_pairs_ok(int n, int g0);
+bool wide_adjoint_ok(int h);
+int64_t wide_adjoint_ws(int n_clips, int h);
+int wide_socs_adjoint(const LithoAbbePlan& p, const void* blob, const float2* table, const float2* mask_box,
+                      const float2* sens_box, float2* grad_box, void* ws, cudaStream_t s);
+int64_t wide_synth_spec_bytes(int n_fields, int n);
+cudaError_t wide_synth_real(const float2* box, int g0, int n, int n_fields, float* out, float2* spec,
+                            const float2* twN, cudaStream_t s);
 int synth_blocks_for(int n);
 
 // ---------------------------------------------------------------------------
@@ -539,10 +547,11 @@ extern "C" int litho_band_spectrum(const void* in, int is_complex, int n_fields,
 extern "C" int litho_band_synthesis_workspace(int n_fields, int n, size_t* bytes) {
   if (!bytes) return LITHO_E_NULL;
   if (n_fields < 1 || n < 2) return LITHO_E_SIZE;
-  // twiddles, block maxima, and the whole-image column buffer for the widest
-  // box the pair synthesis takes (half-width 31)
+  // twiddles, block maxima, the whole-image column buffer for the widest box
+  // the pair synthesis takes (half-width 31), and the spectrum buffer the
+  // synthesis of wider boxes uses
   *bytes = (size_t)(align16((int64_t)n * 8) + align16((int64_t)n_fields * synth_blocks_for(n) * 4) +
-                    align16(synth_cols_bytes(n_fields, n, 31)));
+                    align16(synth_cols_bytes(n_fields, n, 31)) + align16(wide_synth_spec_bytes(n_fields, n)));
   return LITHO_OK;
 }
 
@@ -565,11 +574,17 @@ extern "C" int litho_band_synthesis(const void* box, int n_fields, int n, int h,
     k_synth_complex<<<g, 256, sm, s>>>(static_cast<const float2*>(box), h, n, tw, static_cast<float2*>(out));
     e = cudaGetLastError();
   } else {
-    float2* cbuf = h <= 31 ? reinterpret_cast<float2*>(static_cast<char*>(ws) + align16((int64_t)n * 8) +
-                                                       align16((int64_t)n_fields * synth_blocks_for(n) * 4))
-                           : nullptr;
-    e = launch_synth_real(static_cast<const float2*>(box), 2 * h + 1, n, n_fields, tw, nullptr,
-                          static_cast<float*>(out), blockmax, s, cbuf);
+    char* wb = static_cast<char*>(ws) + align16((int64_t)n * 8) + align16((int64_t)n_fields * synth_blocks_for(n) * 4);
+    if (!synth_pairs_ok(n, h) && h > 31 && n >= 32 && n <= 4096 && (n & (n - 1)) == 0 &&
+        2 * h + 1 <= n) {
+      // boxes too wide for the pair synthesis: scatter and one inverse FFT per two fields
+      float2* spec = reinterpret_cast<float2*>(wb + align16(synth_cols_bytes(n_fields, n, 31)));
+      e = wide_synth_real(static_cast<const float2*>(box), h, n, n_fields, static_cast<float*>(out), spec, tw, s);
+    } else {
+      float2* cbuf = h <= 31 ? reinterpret_cast<float2*>(wb) : nullptr;
+      e = launch_synth_real(static_cast<const float2*>(box), 2 * h + 1, n, n_fields, tw, nullptr,
+                            static_cast<float*>(out), blockmax, s, cbuf);
+    }
   }
   return e == cudaSuccess ? LITHO_OK : (int)e;
 }
@@ -581,7 +596,12 @@ static int64_t adj_ws(int n_clips, int n_items, int h) {
 
 extern "C" int litho_socs_adjoint_workspace(int n_clips, int n_items, int h, size_t* bytes) {
   if (!bytes) return LITHO_E_NULL;
-  if (n_clips < 1 || n_items < 1 || h < 0 || h > kAdjHMax) return LITHO_E_SIZE;
+  if (n_clips < 1 || n_items < 1 || h < 0) return LITHO_E_SIZE;
+  if (h > kAdjHMax) {
+    if (!wide_adjoint_ok(h)) return LITHO_E_SIZE;
+    *bytes = (size_t)wide_adjoint_ws(n_clips, h);
+    return LITHO_OK;
+  }
   *bytes = (size_t)adj_ws(n_clips, n_items, h);
   return LITHO_OK;
 }
@@ -595,7 +615,14 @@ extern "C" int litho_socs_adjoint(const LithoAbbePlan* plan, const void* blob, c
   if (!plan || !blob || !table || !sens_box || !grad_box_out || !ws) return LITHO_E_NULL;
   if (!mask_box && !field_box) return LITHO_E_NULL;
   const LithoAbbePlan& p = *plan;
-  if (p.h < 0 || p.h > kAdjHMax || p.n_clips < 1 || p.n_items < 1 || p.bm != p.h) return LITHO_E_SIZE;
+  if (p.h < 0 || p.n_clips < 1 || p.n_items < 1 || p.bm != p.h) return LITHO_E_SIZE;
+  if (p.h > kAdjHMax) {   // kernel bands wider than the 64-point grid: coarse grids of 128..1024
+    if (!wide_adjoint_ok(p.h)) return LITHO_E_SIZE;
+    if (!mask_box) return LITHO_E_NULL;
+    if ((int64_t)ws_bytes < wide_adjoint_ws(p.n_clips, p.h)) return LITHO_E_WORKSPACE;
+    return wide_socs_adjoint(p, blob, static_cast<const float2*>(table), static_cast<const float2*>(mask_box),
+                             static_cast<const float2*>(sens_box), static_cast<float2*>(grad_box_out), ws, s);
+  }
   if ((int64_t)ws_bytes < adj_ws(p.n_clips, p.n_items, p.h)) return LITHO_E_WORKSPACE;
   const char* b = static_cast<const char*>(blob);
   const LithoJob* jobs = reinterpret_cast<const LithoJob*>(b + p.off_jobs);

@@ -138,9 +138,9 @@ __global__ void k_wide_box(const float2* __restrict__ F, int L, int h, float2* _
 }
 
 // spec[pair] = B_{2p} + i B_{2p+1} on the N x N grid (zero off the box).
-__global__ void k_wide_spec(const float2* __restrict__ bbox, int o0, int n_out, int h, int n,
+__global__ void k_wide_spec(const float2* __restrict__ bbox, int o0, int n_out, int g0, int n,
                             float2* __restrict__ spec) {
-  const int pr = blockIdx.y, G = 4 * h + 1, g0 = 2 * h;
+  const int pr = blockIdx.y, G = 2 * g0 + 1;
   const int oa = o0 + 2 * pr, ob = oa + 1;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G * G; i += gridDim.x * blockDim.x) {
     const int gy = i / G - g0, gx = i % G - g0;
@@ -157,7 +157,7 @@ __global__ void k_wide_real(const float2* __restrict__ spec, int o0, int n_out, 
   __shared__ float red[32];
   const int o = o0 + blockIdx.y, pr = blockIdx.y >> 1, im = blockIdx.y & 1;
   if (o >= n_out) return;
-  const LithoNorm nm = norm[o];
+  const LithoNorm nm = norm ? norm[o] : LithoNorm{0, 1.0f};
   const float sc = nm.mode == 1 ? 1.0f : nm.scale;
   const size_t NN = (size_t)n * n;
   const float2* sp = spec + (size_t)pr * NN;
@@ -173,10 +173,112 @@ __global__ void k_wide_real(const float2* __restrict__ spec, int o0, int n_out, 
   for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && blockmax) {
     float m = red[0];
     for (int i = 1; i < (int)(blockDim.x >> 5); ++i) m = fmaxf(m, red[i]);
     blockmax[(size_t)o * gridDim.x + blockIdx.x] = m;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// SOCS adjoint on wide coarse grids (the ILT gradient for kernel bands wider
+// than 15 bins; opc/ilt.py:262-266 restated as in ilt.cu's file comment):
+//   e_k = IFFT_L(phi_k M)  (pass A, k_wide_cols, then the row inverse below)
+//   Y_k = FFT_L(e_k g_L) / L^2 on |f| <= h,  g_L = IFFT_L(sens band box)
+//   A(f) = sum_k lambda_k conj(phi_k(f)) Y_k(f),  H(f) = A(f) + conj A(-f).
+// ---------------------------------------------------------------------------
+
+// g_L: the (4h+1)^2 sensitivity box scattered onto the L x L grid.
+__global__ void k_wide_scatter_box(const float2* __restrict__ box, int g0, int L, float2* __restrict__ grid) {
+  const int c = blockIdx.y, G = 2 * g0 + 1;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G * G; i += gridDim.x * blockDim.x) {
+    const int gy = i / G - g0, gx = i % G - g0;
+    grid[((size_t)c * L + (gy & (L - 1))) * L + (gx & (L - 1))] = box[(size_t)c * G * G + i];
+  }
+}
+
+// Pass B of the adjoint. Grid (transform t of the chunk, chunk of `lines`
+// rows v): e(., v) = inverse over kx of T[t][.][v]; times g_L(., v); forward
+// over u; the band fx in [-h, h] -> T2[t][fx + h][v].
+__global__ void __launch_bounds__(256)
+k_wide_adj_rows(const LithoJob* __restrict__ jobs, int j0, int h, int L, int log2L, int lines,
+                const float2* __restrict__ twL, const float2* __restrict__ T, const float2* __restrict__ gL,
+                float2* __restrict__ T2) {
+  extern __shared__ float2 wsm[];
+  float2* tw = wsm;
+  float2* s1 = wsm + L;                 // [lines][L]
+  float2* s2 = s1 + (size_t)lines * L;  // [lines][L]
+  const int t = blockIdx.x, v0 = blockIdx.y * lines, side = 2 * h + 1;
+  const LithoJob job = jobs[j0 + t];
+  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twL[i];
+  for (int i = threadIdx.x; i < lines * L; i += blockDim.x) s1[i] = make_float2(0.f, 0.f);
+  __syncthreads();
+  const float2* Tt = T + (size_t)t * side * L;
+  for (int id = threadIdx.x; id < side * lines; id += blockDim.x) {
+    const int ki = id / lines, r = id % lines;
+    s1[r * L + brev((ki - h) & (L - 1), log2L)] = Tt[(size_t)ki * L + v0 + r];
+  }
+  block_fft_lines<+1>(s1, L, lines, L, tw);   // e(u, v) in natural order
+  const float2* g = gL + (size_t)job.clip * L * L;
+  for (int i = threadIdx.x; i < lines * L; i += blockDim.x) {
+    const int r = i / L, u = i % L;
+    s2[r * L + brev(u, log2L)] = cmul(s1[i], __ldg(g + (size_t)(v0 + r) * L + u));
+  }
+  block_fft_lines<-1>(s2, L, lines, L, tw);
+  float2* dst = T2 + (size_t)t * side * L;
+  for (int id = threadIdx.x; id < side * lines; id += blockDim.x) {
+    const int fi = id / lines, r = id % lines;
+    dst[(size_t)fi * L + v0 + r] = s2[r * L + ((fi - h) & (L - 1))];
+  }
+}
+
+// Pass C. Grid (transform t, chunk of kWideCols columns fx): forward over v of
+// T2[t][fx][.], the band fy in [-h, h], weighted: Yt[t][fy + h][fx + h] =
+// lambda conj(phi(fx, fy)) Y / L^2.
+__global__ void __launch_bounds__(256)
+k_wide_adj_cols(const LithoJob* __restrict__ jobs, int j0, const float2* __restrict__ table, int h, int L,
+                int log2L, const float2* __restrict__ twL, const float2* __restrict__ T2, float2* __restrict__ Yt) {
+  extern __shared__ float2 wsm[];
+  float2* tw = wsm;
+  float2* sl = wsm + L;  // [kWideCols][L]
+  const int t = blockIdx.x, c0 = blockIdx.y * kWideCols, side = 2 * h + 1, npts = side * side;
+  const LithoJob job = jobs[j0 + t];
+  const int lines = (side - c0) < kWideCols ? (side - c0) : kWideCols;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twL[i];
+  const float2* src = T2 + ((size_t)t * side + c0) * L;
+  for (int i = threadIdx.x; i < lines * L; i += blockDim.x) {
+    const int r = i / L, v = i % L;
+    sl[r * L + brev(v, log2L)] = src[i];
+  }
+  block_fft_lines<-1>(sl, L, lines, L, tw);
+  const float2* ph = table + (size_t)job.tab * npts;
+  const float sc = (float)job.weight / ((float)L * (float)L);
+  float2* dst = Yt + (size_t)t * npts;
+  for (int id = threadIdx.x; id < lines * side; id += blockDim.x) {
+    const int r = id / side, fyi = id % side, fxi = c0 + r;
+    const float2 y = sl[r * L + ((fyi - h) & (L - 1))];
+    dst[fyi * side + fxi] = cscale(cmulc(y, __ldg(ph + fyi * side + fxi)), sc);
+  }
+}
+
+// A[clip] += Yt[t] for the chunk's transforms, in job order.
+__global__ void k_wide_adj_acc(const LithoJob* __restrict__ jobs, int j0, int nj, int npts,
+                               const float2* __restrict__ Yt, float2* __restrict__ A) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += gridDim.x * blockDim.x) {
+    for (int t = 0; t < nj; ++t) {
+      const int c = jobs[j0 + t].clip;
+      A[(size_t)c * npts + i] = cadd(A[(size_t)c * npts + i], Yt[(size_t)t * npts + i]);
+    }
+  }
+}
+
+// H(f) = A(f) + conj A(-f).
+__global__ void k_wide_adj_final(const float2* __restrict__ A, int h, float2* __restrict__ H) {
+  const int c = blockIdx.y, side = 2 * h + 1, npts = side * side;
+  for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < npts; id += gridDim.x * blockDim.x) {
+    const int fy = id / side, fx = id % side;
+    const int mid = (2 * h - fy) * side + (2 * h - fx);
+    H[(size_t)c * npts + id] = cadd(A[(size_t)c * npts + id], cconj(A[(size_t)c * npts + mid]));
   }
 }
 
@@ -298,7 +400,7 @@ int abbe_wide_run(const LithoAbbePlan& p, const void* blob, const void* table_in
     const int pairs = (no + 1) / 2;
     if ((e = cudaMemsetAsync(spec, 0, (size_t)pairs * NN * 8, s)) != cudaSuccess) return (int)e;
     dim3 gs((G * G + 255) / 256, pairs);
-    k_wide_spec<<<gs, 256, 0, s>>>(bbox, o0, p.n_out, p.h, n, spec);
+    k_wide_spec<<<gs, 256, 0, s>>>(bbox, o0, p.n_out, 2 * p.h, n, spec);
     e = plain_fft2(nullptr, false, spec, pairs, n, +1, 1.0f, 1.0f, twN, s);
     if (e != cudaSuccess) return (int)e;
     dim3 gw(kWideMaxBlk, no);
@@ -311,6 +413,153 @@ int abbe_wide_run(const LithoAbbePlan& p, const void* blob, const void* table_in
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
   mark(7);
   return LITHO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// wide pieces for the SOCS / ILT stages
+// ---------------------------------------------------------------------------
+static int wide_L_for(int h) {
+  int L = 32;
+  while (L < 4 * h + 1) L *= 2;
+  return L;
+}
+
+bool wide_adjoint_ok(int h) { return h >= 1 && wide_L_for(h) >= 128 && wide_L_for(h) <= 1024; }
+
+static int adj_lines(int L) { return L >= 1024 ? 8 : 16; }
+static int64_t adj_jobs_per_chunk(int h) {
+  const int64_t side = 2 * h + 1, L = wide_L_for(h);
+  int64_t jc = kWideTBudget / (side * L * 8 * 2 + side * side * 8);
+  return jc < 1 ? 1 : jc;
+}
+
+struct WideAdjLayout {
+  int64_t twL, gL, T, T2, Yt, A, total;
+  int jobs_per_chunk;
+};
+
+static WideAdjLayout wide_adj_layout(int n_clips, int h) {
+  WideAdjLayout l{};
+  const int64_t side = 2 * h + 1, L = wide_L_for(h), jc = adj_jobs_per_chunk(h);
+  l.jobs_per_chunk = (int)jc;
+  int64_t off = 0;
+  l.twL = off; off = align16(off + L * 8);
+  l.gL = off;  off = align16(off + (int64_t)n_clips * L * L * 8);
+  l.T = off;   off = align16(off + jc * side * L * 8);
+  l.T2 = off;  off = align16(off + jc * side * L * 8);
+  l.Yt = off;  off = align16(off + jc * side * side * 8);
+  l.A = off;   off = align16(off + (int64_t)n_clips * side * side * 8);
+  l.total = off;
+  return l;
+}
+
+int64_t wide_adjoint_ws(int n_clips, int h) { return wide_adj_layout(n_clips, h).total; }
+
+// The SOCS adjoint band box for a plan with one job per (clip, kernel):
+// mask_box [clip][(2h+1)^2] (scaled 1/N^2), sens_box [clip][(4h+1)^2] (scale/N^2).
+int wide_socs_adjoint(const LithoAbbePlan& p, const void* blob, const float2* table, const float2* mask_box,
+                      const float2* sens_box, float2* grad_box, void* ws, cudaStream_t s) {
+  const int h = p.h, L = wide_L_for(h), lgL = ilog2w(L), side = 2 * h + 1, npts = side * side;
+  const WideAdjLayout l = wide_adj_layout(p.n_clips, h);
+  const LithoJob* jobs = reinterpret_cast<const LithoJob*>(static_cast<const char*>(blob) + p.off_jobs);
+  char* w = static_cast<char*>(ws);
+  float2* twL = reinterpret_cast<float2*>(w + l.twL);
+  float2* gL = reinterpret_cast<float2*>(w + l.gL);
+  float2* T = reinterpret_cast<float2*>(w + l.T);
+  float2* T2 = reinterpret_cast<float2*>(w + l.T2);
+  float2* Yt = reinterpret_cast<float2*>(w + l.Yt);
+  float2* A = reinterpret_cast<float2*>(w + l.A);
+  cudaError_t e;
+  k_twiddle_table<<<(L + 255) / 256, 256, 0, s>>>(twL, L, +1);
+  if ((e = cudaMemsetAsync(gL, 0, (size_t)p.n_clips * L * L * 8, s)) != cudaSuccess) return (int)e;
+  if ((e = cudaMemsetAsync(A, 0, (size_t)p.n_clips * npts * 8, s)) != cudaSuccess) return (int)e;
+  const int G = 4 * h + 1;
+  k_wide_scatter_box<<<dim3((G * G + 255) / 256, p.n_clips), 256, 0, s>>>(sens_box, 2 * h, L, gL);
+  e = plain_fft2(nullptr, false, gL, p.n_clips, L, +1, 1.0f, 1.0f, twL, s);
+  if (e != cudaSuccess) return (int)e;
+  const int lines = adj_lines(L);
+  const size_t smA = (size_t)(L + kWideCols * L) * 8;
+  const size_t smB = (size_t)(L + 2 * lines * L) * 8;
+  cudaFuncSetAttribute(k_wide_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA);
+  cudaFuncSetAttribute(k_wide_adj_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB);
+  cudaFuncSetAttribute(k_wide_adj_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA);
+  for (int j0 = 0; j0 < p.n_jobs; j0 += l.jobs_per_chunk) {
+    const int nj = (p.n_jobs - j0) < l.jobs_per_chunk ? (p.n_jobs - j0) : l.jobs_per_chunk;
+    const dim3 gc(nj, (side + kWideCols - 1) / kWideCols);
+    k_wide_cols<<<gc, 256, smA, s>>>(jobs, j0, 1, table, h, mask_box, h, L, lgL, twL, T);
+    k_wide_adj_rows<<<dim3(nj, L / lines), 256, smB, s>>>(jobs, j0, h, L, lgL, lines, twL, T, gL, T2);
+    k_wide_adj_cols<<<gc, 256, smA, s>>>(jobs, j0, table, h, L, lgL, twL, T2, Yt);
+    k_wide_adj_acc<<<(npts + 255) / 256, 256, 0, s>>>(jobs, j0, nj, npts, Yt, A);
+    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  }
+  k_wide_adj_final<<<dim3((npts + 255) / 256, p.n_clips), 256, 0, s>>>(A, h, grad_box);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+// The image band box of litho_coarse_image on a wide plan.
+int wide_coarse_box(const LithoAbbePlan& p, const void* blob, const float2* table, const float2* mb, float2* bbox_out,
+                    void* ws, cudaStream_t s) {
+  const WideLayout l = wide_layout(p);
+  const char* b = static_cast<const char*>(blob);
+  const LithoJob* jobs = reinterpret_cast<const LithoJob*>(b + p.off_jobs);
+  const LithoItem* items = reinterpret_cast<const LithoItem*>(b + p.off_items);
+  const int32_t* out_items = reinterpret_cast<const int32_t*>(b + p.off_out_items);
+  char* w = static_cast<char*>(ws);
+  float2* twL = reinterpret_cast<float2*>(w + l.twL);
+  float2* T = reinterpret_cast<float2*>(w + l.T);
+  float* partial = reinterpret_cast<float*>(w + l.partial);
+  float* J = reinterpret_cast<float*>(w + l.J);
+  float2* F = reinterpret_cast<float2*>(w + l.F);
+  const int L = p.L, lgL = ilog2w(L), side = 2 * p.h + 1, G = 4 * p.h + 1;
+  cudaError_t e;
+  k_twiddle_table<<<(L + 255) / 256, 256, 0, s>>>(twL, L, +1);
+  if ((e = cudaMemsetAsync(partial, 0, (size_t)p.n_items * L * L * 4, s)) != cudaSuccess) return (int)e;
+  const size_t smA = (size_t)(L + kWideCols * L) * 8;
+  const size_t smB = (size_t)(L + kWideRows * L) * 8 + (size_t)kWideRows * L * 4;
+  cudaFuncSetAttribute(k_wide_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA);
+  cudaFuncSetAttribute(k_wide_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB);
+  for (int j0 = 0; j0 < p.n_jobs; j0 += l.jobs_per_chunk) {
+    const int nj = (p.n_jobs - j0) < l.jobs_per_chunk ? (p.n_jobs - j0) : l.jobs_per_chunk;
+    k_wide_cols<<<dim3(nj * p.ncomp_max, (side + kWideCols - 1) / kWideCols), 256, smA, s>>>(
+        jobs, j0, p.ncomp_max, table, p.h, mb, p.bm, L, lgL, twL, T);
+    k_wide_rows<<<dim3(p.n_items, L / kWideRows), 256, smB, s>>>(items, jobs, j0, nj, p.ncomp_max, p.h, L, lgL, twL,
+                                                                  T, partial);
+    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  }
+  const int LL = L * L;
+  k_wide_reduce<<<dim3((LL + 255) / 256 < 1024 ? (LL + 255) / 256 : 1024, p.n_out), 256, 0, s>>>(out_items, partial,
+                                                                                                 LL, J);
+  e = plain_fft2(J, true, F, p.n_out, L, -1, 1.0f, 1.0f / ((float)L * (float)L), twL, s);
+  if (e != cudaSuccess) return (int)e;
+  k_wide_box<<<dim3((G * G + 255) / 256, p.n_out), 256, 0, s>>>(F, L, p.h, bbox_out);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+// Real synthesis of n_fields Hermitian boxes of half-width g0 (any width) by
+// scattering two boxes into one complex N x N spectrum and one inverse FFT.
+// spec: kWideSpecPairs x n x n complex; twN: exp(+2 pi i j / n).
+int64_t wide_synth_spec_bytes(int n_fields, int n) {
+  const int64_t pairs = (n_fields + 1) / 2 < kWideSpecPairs ? (n_fields + 1) / 2 : kWideSpecPairs;
+  return pairs * (int64_t)n * n * 8;
+}
+
+cudaError_t wide_synth_real(const float2* box, int g0, int n, int n_fields, float* out, float2* spec,
+                            const float2* twN, cudaStream_t s) {
+  const size_t NN = (size_t)n * n;
+  const int G = 2 * g0 + 1;
+  cudaError_t e;
+  for (int o0 = 0; o0 < n_fields; o0 += 2 * kWideSpecPairs) {
+    const int no = (n_fields - o0) < 2 * kWideSpecPairs ? (n_fields - o0) : 2 * kWideSpecPairs;
+    const int pairs = (no + 1) / 2;
+    if ((e = cudaMemsetAsync(spec, 0, (size_t)pairs * NN * 8, s)) != cudaSuccess) return e;
+    k_wide_spec<<<dim3((G * G + 255) / 256, pairs), 256, 0, s>>>(box, o0, n_fields, g0, n, spec);
+    if ((e = plain_fft2(nullptr, false, spec, pairs, n, +1, 1.0f, 1.0f, twN, s)) != cudaSuccess) return e;
+    k_wide_real<<<dim3(kWideMaxBlk, no), 256, 0, s>>>(spec, o0, n_fields, n, nullptr, out, nullptr);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace litho

@@ -32,6 +32,16 @@ N_PART = 64   # partial-sum blocks per clip for costs / pattern errors
 KERNEL_HMAX_FUSED = 15   # widest kernel band (bins) of the on-chip SOCS adjoint
 
 
+def band_limited_ok(n: int, h: int) -> bool:
+    """Can the band-limited ILT stages serve kernels of half-width h on an
+    n x n grid (on chip up to 15 bins, else a coarse grid of 128..1024 <= n)?"""
+    if h <= KERNEL_HMAX_FUSED:
+        return True
+    from .aerial import coarse_grid
+    L = coarse_grid(h)
+    return 128 <= L <= 1024 and L <= n <= 4096 and (n & (n - 1)) == 0
+
+
 def gaussian_weights(sigma: float, truncate: float = 4.0) -> np.ndarray:
     """scipy.ndimage's 1-D Gaussian (order 0): radius int(truncate sigma + 0.5),
     exp(-x^2 / (2 sigma^2)) normalised to unit sum, in float64."""
@@ -303,9 +313,10 @@ def stages(kernels: SOCSKernels, n_clips: int, engine: str = "fused") -> _Stages
     if st is None or st.k is not kernels:
         if len(_STAGES) > 16:
             _STAGES.clear()
-        # the on-chip SOCS adjoint covers kernel bands up to 15 bins (a 64-point
-        # coarse grid); wider bands run both directions on the full grid
-        fused = engine == "fused" and kernels.halfwidth <= KERNEL_HMAX_FUSED
+        # the band-limited stages cover kernel bands up to 15 bins on chip (a
+        # 64-point coarse grid) and wider ones on coarse grids of 128..1024
+        # points; bands wider than that run both directions on the full grid
+        fused = engine == "fused" and band_limited_ok(int(kernels.grid.n_pixels), kernels.halfwidth)
         st = (_Stages if fused else _PlainStages)(kernels, n_clips)
         _STAGES[key] = st
     return st
@@ -359,9 +370,26 @@ def socs_gradient(kernels: SOCSKernels, fields, sensitivity):
         grad = st.adjoint(g, mbox=mbox)[0]
     else:
         fl = fields if _is_torch(fields) else torch.from_numpy(np.asarray(fields).astype(np.complex64)).to(st.dev)
+        if st.h > KERNEL_HMAX_FUSED:
+            # wide kernel bands: the coarse-grid adjoint recomputes the fields from
+            # the mask, which these fields do not come with; use them directly
+            grad = _plain_adjoint(stages(kernels, 1, "plain"), fl.reshape(-1, 1, st.n, st.n).contiguous(), g)[0]
+            return grad if _is_torch(sensitivity) else grad.cpu().numpy().astype(np.float64)
         fb = st.band(fl.reshape(-1, st.n, st.n).contiguous(), st.h, 1.0 / (st.n * st.n))
         grad = st.adjoint(g, field_boxes=fb)[0]
     return grad if _is_torch(sensitivity) else grad.cpu().numpy().astype(np.float64)
+
+
+def _plain_adjoint(pst, fields, sens):
+    """Full-grid SOCS adjoint of given fields (K, C, N, N) complex64: (C, N, N)."""
+    torch, L = pst.torch, pst.L
+    grad = torch.empty(sens.shape, dtype=torch.float32, device=pst.dev)
+    ws = pst._pws()
+    nat.check("litho_plain_socs_adjoint", L.litho_plain_socs_adjoint(
+        fields.data_ptr(), sens.data_ptr(), pst.C, pst.n, len(pst.k), pst.phi.data_ptr(), pst.lam,
+        pst.bkx.data_ptr(), pst.bky.data_ptr(), pst.phi.shape[1], grad.data_ptr(), ws.data_ptr(), ws.numel(),
+        pst.stream()))
+    return grad
 
 
 @dataclass

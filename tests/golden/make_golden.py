@@ -310,6 +310,15 @@ def wide():
     save("socs_euv_wide_128_k24", optics=o, grid=g, mask=m.astype(np.uint8), weights=k.weights,
          clear=k.clear, n_band=k.n_band, raw=r[0], peak=r[1])
 
+    # the SOCS adjoint with those kernels (opc/ilt.py:235-266), the wide-band ILT gradient
+    from litho_sim.opc.ilt import socs_fields, socs_gradient
+    rng = np.random.default_rng(33)
+    mask = rng.random((128, 128))
+    sens = rng.standard_normal((128, 128))
+    fields, inten = socs_fields(k, mask)
+    save("ilt_euv_wide_128_k24", optics=o, grid=g, mask=mask, sens=sens, intensity=inten,
+         grad=socs_gradient(k, fields, sens))
+
 
 def next_rows():
     """Rows beyond the imaging core: PEB diffusion (bake/peb.py) and the
