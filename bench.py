@@ -22,6 +22,7 @@ bounded sample of source points, and prints the same line for it.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import math
 import os
@@ -286,7 +287,39 @@ def bench_uneven(args, torch, dev, world, max_over_ranks, barrier) -> dict:
         i = sizes.index(n)
         ref = lb.compute_aerial_batch(masks[i][None], o, lb.GridConfig(n_pixels=int(n), pixel_size=2e-9))[0][0, 0]
         worst = max(worst, float((imgs[i].double() - ref.double()).abs().max() / ref.double().abs().max()))
+    ilt_line = None
+    if "unevenilt" not in args.skip:
+        from lithobat_b200 import ilt
+        from lithobat_b200.uneven import UnevenIlt
+        o_ilt = dataclasses.replace(o, normalisation="clear")
+        th = [0.5 * torch.randn((int(n), int(n)), device=dev, generator=torch.Generator(device=dev).manual_seed(
+            900 + i)) for i, n in enumerate(sizes)]
+        t1 = time.perf_counter()
+        uni = UnevenIlt([m for m in masks], th, o_ilt, 2e-9,
+                        lambda k: ilt.IltParams(scale=1.0 / k.clear, level=0.3, steepness=15.0, step=0.2, beta=4.0),
+                        max_kernels=24)
+        torch.cuda.synchronize()
+        build_s = time.perf_counter() - t1
+        for _ in range(2):
+            uni.step()
+        torch.cuda.synchronize()
+        c0 = float(sum(float(c) for c in uni.step()))
+        n_steps = 20
+        e0.record()
+        for _ in range(n_steps):
+            uni.step()
+        e1.record()
+        torch.cuda.synchronize()
+        ims = max_over_ranks(e0.elapsed_time(e1) / n_steps)
+        c1 = float(sum(float(c) for c in uni.step()))
+        ilt_line = {"metric": "uneven-batch ILT clip-steps/s", "value": world * count / (ims / 1000.0),
+                    "unit": "clip-steps/s", "ms_per_step": ims, "steps": n_steps, "kernels": 24,
+                    "socs_build_and_setup_s": build_s, "band_limited_groups": {
+                        int(n): bool(b.fast) for n, _i, _k, b in uni.groups},
+                    "total_cost_before_after": [c0, c1]}
+        del uni
     return {"metric": "uneven-batch Abbe images/s", "value": world * count / (ms / 1000.0), "unit": "images/s",
+            "ilt": ilt_line,
             "ms_per_batch": ms, "steps": steps, "workload": UNEVEN_WORKLOAD, "clips": count,
             "clips_per_size": {int(n): int(sum(1 for x in sizes if x == n)) for n in sorted(set(sizes))},
             "source_points": len(lb.source_points(o)), "graph_replay": run.graph is not None,
@@ -629,7 +662,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--images", type=int, default=IMAGES_PER_STEP,
                     help="images per step (a small value makes a profiling case)")
-    ap.add_argument("--skip", default="", help="comma list of phases to skip: plain,e2e,profile,cpu,ilt,iltplain,uneven")
+    ap.add_argument("--skip", default="", help="comma list of phases to skip: plain,e2e,profile,cpu,ilt,iltplain,uneven,unevenilt")
     ap.add_argument("--ilt-clips", type=int, default=ILT_CLIPS, help="clips per ILT step")
     ap.add_argument("--uneven-clips", type=int, default=256, help="clips in the uneven-size batch")
     args = ap.parse_args()

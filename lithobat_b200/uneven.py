@@ -1,4 +1,5 @@
-"""Uneven batches: clips of several sizes imaged by one CUDA-graph replay.
+"""Uneven batches: clips of several sizes imaged by one CUDA-graph replay,
+and ILT over clips of several sizes.
 
 The reference images clips one call at a time, whatever their size
 (expose/aerial_image.py:502-548). Here the clips of a batch are grouped by
@@ -184,6 +185,58 @@ class UnevenAbbe:
         return out
 
 
+class UnevenIlt:
+    """ILT of a batch of clips of mixed sizes (one optics, one pixel size):
+    the clips are grouped by grid size, each group has its own SOCS kernels
+    (built once, on the device) and is stepped as one ``IltBatch``.
+
+    targets, theta0: lists of (N_i, N_i) arrays or device tensors, in batch
+    order. params(kernels) -> IltParams for a group (its normalisation scale
+    depends on the group's kernels)."""
+
+    def __init__(self, targets, theta0, optics, pixel_size: float, params, *, max_kernels: int | None = 24,
+                 tol: float = 0.0):
+        from .config import GridConfig
+        from .hopkins import SOCSKernels
+        from .ilt import IltBatch
+        torch = nat.require_cuda()
+        self.torch = torch
+        if len(targets) != len(theta0):
+            raise ValueError(f"{len(targets)} targets for {len(theta0)} initial fields")
+        self.sizes = [int(np.shape(t)[-1]) for t in targets]
+        by_n: dict = {}
+        for i, n in enumerate(self.sizes):
+            by_n.setdefault(n, []).append(i)
+        self.groups = []
+        for n in sorted(by_n):
+            idx = by_n[n]
+            k = SOCSKernels.build(optics, GridConfig(n_pixels=n, pixel_size=pixel_size), tol=tol,
+                                  max_kernels=max_kernels)
+
+            def stack(xs):
+                ts = [x if isinstance(x, torch.Tensor) else torch.from_numpy(np.asarray(x, dtype=np.float32))
+                      for x in xs]
+                return torch.stack([t.to(torch.float32).cuda() for t in ts])
+            b = IltBatch(k, stack([targets[i] for i in idx]), stack([theta0[i] for i in idx]), params(k))
+            self.groups.append((n, idx, k, b))
+
+    def step(self, want_signed: bool = False):
+        """One ILT iteration of every clip; returns the costs in batch order (device)."""
+        cost = [None] * len(self.sizes)
+        for _n, idx, _k, b in self.groups:
+            c = b.step(want_signed=want_signed)
+            for j, i in enumerate(idx):
+                cost[i] = c[j]
+        return cost
+
+    def theta(self):
+        out = [None] * len(self.sizes)
+        for _n, idx, _k, b in self.groups:
+            for j, i in enumerate(idx):
+                out[i] = b.theta[j]
+        return out
+
+
 def compute_aerial_uneven(masks, optics, pixel_size: float, dose: float = 1.0, return_raw: bool = False):
     """Images of clips of mixed sizes in one call (one CUDA-graph replay);
     numpy in -> list of numpy float64 out, torch in -> list of torch float32."""
@@ -196,4 +249,4 @@ def compute_aerial_uneven(masks, optics, pixel_size: float, dose: float = 1.0, r
     return [im.clone() if t else im.cpu().numpy().astype(np.float64) for im, t in zip(imgs, is_t)]
 
 
-__all__ = ["UnevenAbbe", "compute_aerial_uneven", "ITEM_CANDIDATES"]
+__all__ = ["UnevenAbbe", "UnevenIlt", "compute_aerial_uneven", "ITEM_CANDIDATES"]

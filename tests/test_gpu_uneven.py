@@ -61,3 +61,34 @@ def test_uneven_function_numpy_in_numpy_out(lb):
         g = lb.GridConfig(n_pixels=c.shape[0], pixel_size=2e-9)
         ref = lb.compute_aerial_image(c.astype(np.float64), o, g, return_raw=True)[0]
         assert float(np.abs(im - ref).max() / np.abs(ref).max()) <= TOL
+
+
+def test_uneven_ilt_groups_and_steps(lb):
+    """Mixed sizes: 128^2 (kernel band on chip) and 256^2 (wide band) at 2 nm
+    EUV; each group's step equals its own IltBatch step, costs fall."""
+    import torch
+    from lithobat_b200 import ilt
+    from lithobat_b200.uneven import UnevenIlt
+    o = lb.OpticsConfig(wavelength=13.5e-9, NA=0.33, source_grid=15, normalisation="clear",
+                        source_spec=__import__("lithobat_b200.source", fromlist=["Source"]).Source.dipole(
+                            0.9, 0.6, opening_deg=60).to_dict())
+    sizes = [256, 128, 128]
+    tg = _clips(7, sizes)
+    rng = np.random.default_rng(8)
+    th = [0.5 * rng.standard_normal((n, n)).astype(np.float32) for n in sizes]
+
+    def params(k):
+        return ilt.IltParams(scale=1.0 / k.clear, level=0.3, steepness=15.0, step=0.1, beta=4.0)
+    u = UnevenIlt(tg, th, o, 2e-9, params, max_kernels=12)
+    assert [g[0] for g in u.groups] == [128, 256]
+    assert u.groups[0][2].halfwidth <= 15 < u.groups[1][2].halfwidth
+    c0 = [float(c) for c in u.step()]
+    for _ in range(4):
+        c = [float(x) for x in u.step()]
+    assert all(b < a for a, b in zip(c0, c))
+    # the 256^2 group against its own batch
+    k = u.groups[1][2]
+    b = ilt.IltBatch(k, torch.from_numpy(tg[0][None]).cuda(), torch.from_numpy(th[0][None]).cuda(), params(k))
+    for _ in range(5):
+        b.step(want_signed=False)
+    assert float((b.theta[0] - u.theta()[0]).abs().max()) < 1e-5
