@@ -95,6 +95,26 @@ typedef struct LithoNorm {
     float scale;          /* mode 0: the factor; mode 1: the dose           */
 } LithoNorm;
 
+/* The blank under a reflective (EUV) mask, for mask_model="multilayer"
+ * (expose/m3d/provider.py:MultilayerSpectra, :190-295). The spectrum of
+ * source point (fsx, fsy) at order frequency (FX, FY) is multiplied by the
+ * blank's reflection r(theta), sin(theta) = |(tilt lambda fs / m + chief ray)
+ * + lambda F / m| (provider.py:72-126, :260-264); the multiply is folded into
+ * the pupil table. r is the linear interpolation, in theta, of |r| and of the
+ * unwrapped arg r on an ascending angle table (clamped at its ends); orders
+ * with sin(theta) > 1 get 0. One entry per LithoPupil when a plan sets
+ * `mirrored`. */
+typedef struct LithoMirror {
+    double wavelength;    /* m                                              */
+    double reduction;     /* mask-to-wafer demagnification                  */
+    double tilt_sign;     /* source offset -> mask-side sine sign (-1)      */
+    double sin_cx, sin_cy;/* chief-ray direction sines at the mask          */
+    int32_t n_theta;      /* table length (>= 2); 0: thin mask, no multiply */
+    int32_t pad;
+    int64_t off_table;    /* bytes from the start of the LithoMirror array  */
+                          /* to double[3][n_theta]: theta (rad), |r|, arg r */
+} LithoMirror;            /* 56 bytes */
+
 /* Geometry and counts of one Abbe batch. All clips share the grid. The
  * device "plan blob" holds the job/pupil/item/norm arrays at the byte
  * offsets given here (each 16-byte aligned). */
@@ -115,6 +135,9 @@ typedef struct LithoAbbePlan {
     double pixel_size;    /* m                                              */
     int64_t off_jobs, off_pupils, off_items, off_out_items, off_norm;
     int64_t off_slots;    /* int32[n_tab]: a job that owns each table slot  */
+    int32_t mirrored;     /* 1: LithoMirror[n_pupils] at off_mirrors        */
+    int32_t pad_m;
+    int64_t off_mirrors;
 } LithoAbbePlan;
 
 /* ---- library ----------------------------------------------------------- */
@@ -126,7 +149,7 @@ const char* litho_status_string(int status);
 int litho_version(void);
 
 /* sizeof() of the public structs, in declaration order: LithoPupil,
- * LithoJob, LithoItem, LithoNorm, LithoAbbePlan. Writes min(n, 5) values;
+ * LithoJob, LithoItem, LithoNorm, LithoAbbePlan, LithoMirror. Writes min(n, 6) values;
  * returns how many structs the ABI has. For binding generators. */
 int litho_abi_sizes(int32_t* out, int n);
 

@@ -59,10 +59,16 @@ class AbbePlan(C.Structure):
         ("pixel_size", C.c_double),
         ("off_jobs", C.c_int64), ("off_pupils", C.c_int64), ("off_items", C.c_int64),
         ("off_out_items", C.c_int64), ("off_norm", C.c_int64), ("off_slots", C.c_int64),
+        ("mirrored", C.c_int32), ("pad_m", C.c_int32), ("off_mirrors", C.c_int64),
     ]
 
 
-assert C.sizeof(AbbePlan) == 104
+MIRROR_DTYPE = np.dtype([
+    ("wavelength", "<f8"), ("reduction", "<f8"), ("tilt_sign", "<f8"), ("sin_cx", "<f8"), ("sin_cy", "<f8"),
+    ("n_theta", "<i4"), ("pad", "<i4"), ("off_table", "<i8"),
+], align=True)
+
+assert C.sizeof(AbbePlan) == 120 and MIRROR_DTYPE.itemsize == 56
 
 _lib = None
 

@@ -26,6 +26,7 @@ import numpy as np
 
 from . import _native as nat
 from .config import IMAGING_MODELS, NORMALISATIONS, optics_view
+from . import multilayer
 from .pupil import clear_throughput, jones_states
 from .source import source_points
 
@@ -85,10 +86,10 @@ def _validate_view(v) -> None:
         raise ValueError(f"imaging_model must be 'scalar' or 'vector', got '{v.imaging_model}'")
     if v.normalisation.lower() not in NORMALISATIONS:
         raise ValueError(f"normalisation must be 'peak', 'clear' or 'none', got '{v.normalisation}'")
-    if v.mask_model.lower() != "thin":
+    if v.mask_model.lower() not in ("thin", "multilayer"):
         raise ValueError(
-            f"mask_model={v.mask_model!r}: this engine images thin (Kirchhoff) masks only; "
-            "thick-mask spectra are outside the accelerated path")
+            f"mask_model={v.mask_model!r}: this engine images thin (Kirchhoff) masks, on their own or on "
+            "a multilayer mirror; rigorous (FDTD) near fields are outside the accelerated path")
 
 
 _PLANS: dict = {}
@@ -126,8 +127,15 @@ def _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, ite
     slot_reps: list[np.ndarray] = []
     n_tab = 0
     n_jobs = 0
+    mirror_rows = np.zeros(C * P, dtype=nat.MIRROR_DTYPE)
+    mirror_tabs: list = []       # distinct reflection tables, in first-use order
     for c, v in enumerate(views):
         _validate_view(v)
+        mirror, m_scale = None, None
+        if v.mask_model.lower() == "multilayer":
+            mirror = multilayer.mirror_table(multilayer.stack_for(v), v.wavelength)
+            if not any(t is mirror for t in mirror_tabs):
+                mirror_tabs.append(mirror)
         vector = v.imaging_model.lower() == "vector"
         vec_any |= vector
         exact = v.exact_defocus or vector
@@ -135,6 +143,10 @@ def _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, ite
         S = len(src)
         if S == 0:
             raise ValueError("the source has no points")
+        if mirror is not None:
+            m_scale = multilayer.clear_scales(v, src)
+            cxs, cys = multilayer.chief_ray_sines(v)
+            m_idx = next(i for i, t in enumerate(mirror_tabs) if t is mirror)
         _, hc = disc_halfwidth(v.NA, v.wavelength, n, pixel_size)
         h = max(h, hc)
         zern = np.zeros(21)
@@ -158,7 +170,10 @@ def _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, ite
             pupils[k]["vector"] = int(vector)
             pupils[k]["obliquity"] = int(v.obliquity)
             pupils[k]["has_zernike"] = int(bool(np.any(zern != 0.0)))
-            clears[k] = clear_throughput(src, v, float(n_img), vector)
+            clears[k] = clear_throughput(src, v, float(n_img), vector, m_scale)
+            if mirror is not None:
+                mirror_rows[k] = (v.wavelength, v.reduction, multilayer.SOURCE_TILT_SIGN, cxs, cys,
+                                  mirror.theta.size, m_idx, 0)
             m = S * nst
             skey = (vkey, float(dz), float(n_img))
             base = slot_of_state.get(skey)
@@ -211,14 +226,39 @@ def _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, ite
             else:
                 norm[k] = (0, normalisation_scale(v.normalisation, 1.0, clears[k], dose))
     bm = int(max(np.abs(jobs["cx"]).max(), np.abs(jobs["cy"]).max())) + h
-    blob, offs = nat.blob([jobs, pupils, items, out_items, norm, slots])
+    arrays = [jobs, pupils, items, out_items, norm, slots]
+    if mirror_tabs:
+        arrays.append(_mirror_segment(mirror_rows, mirror_tabs))
+    blob, offs = nat.blob(arrays)
     plan = nat.AbbePlan(
         n=n, n_clips=C, n_out=n_out, n_jobs=n_jobs, n_items=len(items), n_pupils=len(pupils),
         h=h, bm=bm, L=L, mask_complex=int(mask_complex), ncomp_max=3 if vec_any else 1, n_tab=n_tab,
         pixel_size=pixel_size, off_jobs=offs[0], off_pupils=offs[1], off_items=offs[2],
-        off_out_items=offs[3], off_norm=offs[4], off_slots=offs[5])
+        off_out_items=offs[3], off_norm=offs[4], off_slots=offs[5],
+        mirrored=int(bool(mirror_tabs)), off_mirrors=offs[6] if mirror_tabs else 0)
     transforms = int(np.sum(jobs["ncomp"]))
     return AbbePlanData(plan, blob, clears, n_out, n_jobs, transforms)
+
+
+def _mirror_segment(rows: np.ndarray, tabs: list) -> np.ndarray:
+    """LithoMirror[n_pupils] followed by each distinct reflection table
+    (float64 theta, |r|, arg r), 16-byte aligned; rows' ``pad`` field holds
+    the table index on entry and is cleared here."""
+    head = (rows.nbytes + 15) & ~15
+    offs, size = [], head
+    for t in tabs:
+        offs.append(size)
+        size += (3 * t.theta.size * 8 + 15) & ~15
+    seg = np.zeros(size, dtype=np.uint8)
+    out = rows.copy()
+    for k in range(out.size):
+        if out[k]["n_theta"]:
+            out[k]["off_table"] = offs[int(out[k]["pad"])]
+        out[k]["pad"] = 0
+    seg[:rows.nbytes] = out.view(np.uint8)
+    for o, t in zip(offs, tabs):
+        seg[o:o + 3 * t.theta.size * 8] = np.concatenate([t.theta, t.mag, t.phase]).astype("<f8").view(np.uint8)
+    return seg
 
 
 def plan_from_table(n: int, pixel_size: float, n_clips: int, weights, h: int, mask_complex: bool,

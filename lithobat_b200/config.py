@@ -69,6 +69,12 @@ class OpticsConfig:
     obliquity: bool = True
     normalisation: str = "peak"
     mask_model: str = "thin"
+    reduction: float = 4.0
+    chief_ray_deg: float = 0.0
+    chief_ray_axis: str = "x"
+    mask_stack: dict[str, Any] | None = None
+    mask_geometry: dict[str, Any] | None = None
+    m3d_angles: int = 3
 
     def __post_init__(self) -> None:
         o = "OpticsConfig"
@@ -91,6 +97,10 @@ class OpticsConfig:
         _choice(o, "polarisation", self.polarisation, POLARISATIONS)
         _choice(o, "normalisation", self.normalisation, NORMALISATIONS)
         _choice(o, "mask_model", self.mask_model, MASK_MODELS)
+        _choice(o, "chief_ray_axis", self.chief_ray_axis, ("x", "y"))
+        _bounded(o, "reduction", self.reduction, 0.0, lo_open=True)
+        _bounded(o, "chief_ray_deg", self.chief_ray_deg, -90.0, 90.0)
+        _bounded(o, "m3d_angles", self.m3d_angles, 1)
         for j, c in (self.zernike_coeffs or {}).items():
             if not isinstance(j, int) or isinstance(j, bool) or j < 1:
                 raise ValueError(f"{o}.zernike_coeffs keys are Noll indices (int ≥ 1), got {j!r}")
@@ -153,6 +163,14 @@ class OpticsView:
     obliquity: bool
     normalisation: str
     mask_model: str
+    reduction: float = 4.0
+    chief_ray_deg: float = 0.0
+    chief_ray_axis: str = "x"
+    mask_stack: str | None = None   # the stack spec as sorted JSON (hashable)
+
+    def mask_stack_spec(self) -> dict | None:
+        import json
+        return None if self.mask_stack is None else json.loads(self.mask_stack)
 
     @property
     def zernike_coeffs(self) -> dict[int, float]:
@@ -186,4 +204,15 @@ def optics_view(optics) -> OpticsView:
         imaging_model=str(g("imaging_model", "scalar")), polarisation=str(g("polarisation", "unpolarised")),
         obliquity=bool(g("obliquity", True)), normalisation=str(g("normalisation", "peak")),
         mask_model=str(g("mask_model", "thin")),
+        reduction=float(g("reduction", 4.0)), chief_ray_deg=float(g("chief_ray_deg", 0.0)),
+        chief_ray_axis=str(g("chief_ray_axis", "x")), mask_stack=_stack_json(g("mask_stack", None)),
     )
+
+
+def _stack_json(spec) -> str | None:
+    if spec is None:
+        return None
+    import json
+    if hasattr(spec, "to_spec"):
+        spec = spec.to_spec()
+    return json.dumps(spec, sort_keys=True, default=str)

@@ -43,13 +43,22 @@ int wide_coarse_box(const LithoAbbePlan& p, const void* blob, const float2* tabl
 // 1. pupil table: table[slot][comp][(dy+h)(2h+1) + dx+h], one block per slot,
 //    evaluated for the slot's representative job.
 // ---------------------------------------------------------------------------
+// mirrors (nullptr for thin masks): the blank's reflection per order is
+// multiplied in (mask_model="multilayer", expose/m3d/provider.py:280-281).
 __global__ void k_pupil_table(const LithoJob* __restrict__ jobs, const int32_t* __restrict__ slots,
-                              const LithoPupil* __restrict__ pupils, int n_tab, int n, double pixel_size, int h,
-                              int ncomp_max, float2* __restrict__ table) {
+                              const LithoPupil* __restrict__ pupils, const LithoMirror* __restrict__ mirrors,
+                              int n_tab, int n, double pixel_size, int h, int ncomp_max,
+                              float2* __restrict__ table) {
   const int t = blockIdx.x;
   if (t >= n_tab) return;
   const LithoJob job = jobs[slots[t]];
   const LithoPupil P = pupils[job.pupil];
+  LithoMirror M{};
+  const double* mtab = nullptr;
+  if (mirrors) {
+    M = mirrors[job.pupil];
+    mtab = reinterpret_cast<const double*>(reinterpret_cast<const char*>(mirrors) + M.off_table);
+  }
   const int side = 2 * h + 1, npts = side * side;
   const double val = ddiv(1.0, dmul((double)n, pixel_size));
   const double kmax = ddiv(P.NA, P.wavelength);
@@ -61,10 +70,29 @@ __global__ void k_pupil_table(const LithoJob* __restrict__ jobs, const int32_t* 
     if (bin_valid(kx, n) && bin_valid(ky, n)) {
       double fx, fy;
       const double rho = aperture_rho(kx, ky, val, job.fsx, job.fsy, kmax, fx, fy);
-      if (rho <= 1.0) pupil_values(P, rho, fx, fy, job.jx, job.jy, v);
+      if (rho <= 1.0) {
+        if (M.n_theta >= 2) {
+          double rr, ri;
+          mirror_reflection(M, mtab, bin_freq(kx, val), bin_freq(ky, val), job.fsx, job.fsy, rr, ri);
+          pupil_values_scaled(P, rho, fx, fy, job.jx, job.jy, rr, ri, v);
+        } else {
+          pupil_values(P, rho, fx, fy, job.jx, job.jy, v);
+        }
+      }
     }
     for (int c = 0; c < ncomp_max; ++c) out[(size_t)c * npts + p] = v[c];
   }
+}
+
+// The pupil table of a plan (every engine builds it the same way).
+cudaError_t launch_pupil_table(const LithoAbbePlan& p, const void* blob, float2* table, cudaStream_t s) {
+  const char* b = static_cast<const char*>(blob);
+  const LithoMirror* mirrors = p.mirrored ? reinterpret_cast<const LithoMirror*>(b + p.off_mirrors) : nullptr;
+  k_pupil_table<<<p.n_tab, 128, 0, s>>>(reinterpret_cast<const LithoJob*>(b + p.off_jobs),
+                                         reinterpret_cast<const int32_t*>(b + p.off_slots),
+                                         reinterpret_cast<const LithoPupil*>(b + p.off_pupils), mirrors, p.n_tab,
+                                         p.n, p.pixel_size, p.h, p.ncomp_max, table);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
@@ -604,10 +632,11 @@ static int check_plan(const LithoAbbePlan* p) {
   }
   if (p->bm < p->h) return LITHO_E_BAND;
   if (!(p->pixel_size > 0.0)) return LITHO_E_SIZE;
-  const int64_t offs[6] = {p->off_jobs, p->off_pupils, p->off_items, p->off_out_items, p->off_norm,
-                           p->off_slots};
-  for (int i = 0; i < 6; ++i)
+  const int64_t offs[7] = {p->off_jobs, p->off_pupils, p->off_items, p->off_out_items, p->off_norm,
+                           p->off_slots, p->mirrored ? p->off_mirrors : 0};
+  for (int i = 0; i < 7; ++i)
     if (offs[i] < 0 || (offs[i] & 15)) return LITHO_E_ALIGN;
+  if (p->mirrored != 0 && p->mirrored != 1) return LITHO_E_SIZE;
   return LITHO_OK;
 }
 
@@ -653,11 +682,9 @@ static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* tab
   if (p.L > 64) return abbe_wide_run(p, blob, table_in, mask, image, peak, ws, s, num_sms_cached(), ev);
   const char* b = static_cast<const char*>(blob);
   const LithoJob* jobs = reinterpret_cast<const LithoJob*>(b + p.off_jobs);
-  const LithoPupil* pupils = reinterpret_cast<const LithoPupil*>(b + p.off_pupils);
   const LithoItem* items = reinterpret_cast<const LithoItem*>(b + p.off_items);
   const int32_t* out_items = reinterpret_cast<const int32_t*>(b + p.off_out_items);
   const LithoNorm* norm = reinterpret_cast<const LithoNorm*>(b + p.off_norm);
-  const int32_t* slots = reinterpret_cast<const int32_t*>(b + p.off_slots);
 
   char* w = static_cast<char*>(ws);
   int* status = reinterpret_cast<int*>(w + l.status);
@@ -678,9 +705,7 @@ static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* tab
   if ((e = cudaMemsetAsync(status, 0, sizeof(int), s)) != cudaSuccess) return (int)e;
   k_twiddle_table<<<(p.n + 255) / 256, 256, 0, s>>>(tw, p.n, +1);
   if (!table_in)
-    k_pupil_table<<<p.n_tab, 128, 0, s>>>(jobs, slots, pupils, p.n_tab, p.n, p.pixel_size, p.h, p.ncomp_max,
-                                           table);
-  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+    if ((e = launch_pupil_table(p, blob, table, s)) != cudaSuccess) return (int)e;
   mark(1);
   // mask band spectrum: rows then columns, 1/N^2 folded into the second pass
   e = launch_row_band_dft(mask, p.mask_complex != 0, p.n_clips * p.n, p.n, p.n, p.bm, u1, 1.0f, tw, sms, s,
@@ -809,13 +834,7 @@ extern "C" int litho_abbe_pupil_table(const LithoAbbePlan* plan, const void* blo
   if (st) return st;
   if (!blob || !table) return LITHO_E_NULL;
   if (((uintptr_t)blob & 15) || ((uintptr_t)table & 7)) return LITHO_E_ALIGN;
-  const LithoAbbePlan& p = *plan;
-  const char* b = static_cast<const char*>(blob);
-  k_pupil_table<<<p.n_tab, 128, 0, s>>>(reinterpret_cast<const LithoJob*>(b + p.off_jobs),
-                                         reinterpret_cast<const int32_t*>(b + p.off_slots),
-                                         reinterpret_cast<const LithoPupil*>(b + p.off_pupils), p.n_tab, p.n,
-                                         p.pixel_size, p.h, p.ncomp_max, static_cast<float2*>(table));
-  const cudaError_t e = cudaGetLastError();
+  const cudaError_t e = launch_pupil_table(*plan, blob, static_cast<float2*>(table), s);
   return e == cudaSuccess ? LITHO_OK : (int)e;
 }
 

@@ -174,9 +174,7 @@ cudaError_t plain_fft2(const void* in, bool in_real, float2* buf, long long plan
 using namespace litho;
 
 namespace litho {
-__global__ void k_pupil_table(const LithoJob* __restrict__ jobs, const int32_t* __restrict__ slots,
-                              const LithoPupil* __restrict__ pupils, int n_tab, int n, double pixel_size, int h,
-                              int ncomp_max, float2* __restrict__ table);
+cudaError_t launch_pupil_table(const LithoAbbePlan& p, const void* blob, float2* table, cudaStream_t s);
 __global__ void k_normalise(const float* __restrict__ blockmax, int nblk, const LithoNorm* __restrict__ norm,
                             int n, float* __restrict__ image, float* __restrict__ peak, int apply_mode0);
 }
@@ -208,10 +206,11 @@ static int check_plain(const LithoAbbePlan* p, int batch) {
     return LITHO_E_SIZE;
   if (p->ncomp_max != 1 && p->ncomp_max != 3) return LITHO_E_SIZE;
   if (!(p->pixel_size > 0.0)) return LITHO_E_SIZE;
-  const int64_t offs[6] = {p->off_jobs, p->off_pupils, p->off_items, p->off_out_items, p->off_norm,
-                           p->off_slots};
-  for (int i = 0; i < 6; ++i)
+  const int64_t offs[7] = {p->off_jobs, p->off_pupils, p->off_items, p->off_out_items, p->off_norm,
+                           p->off_slots, p->mirrored ? p->off_mirrors : 0};
+  for (int i = 0; i < 7; ++i)
     if (offs[i] < 0 || (offs[i] & 15)) return LITHO_E_ALIGN;
+  if (p->mirrored != 0 && p->mirrored != 1) return LITHO_E_SIZE;
   return LITHO_OK;
 }
 
@@ -234,7 +233,6 @@ extern "C" int litho_abbe_plain(const LithoAbbePlan* plan, int batch, const void
   if ((int64_t)ws_bytes < l.total) return LITHO_E_WORKSPACE;
   const char* b = static_cast<const char*>(blob);
   const LithoJob* jobs = reinterpret_cast<const LithoJob*>(b + p.off_jobs);
-  const LithoPupil* pupils = reinterpret_cast<const LithoPupil*>(b + p.off_pupils);
   const LithoNorm* norm = reinterpret_cast<const LithoNorm*>(b + p.off_norm);
   char* w = static_cast<char*>(ws);
   float2* tw = reinterpret_cast<float2*>(w + l.tw);
@@ -247,8 +245,7 @@ extern "C" int litho_abbe_plain(const LithoAbbePlan* plan, int batch, const void
   cudaError_t e;
 
   k_twiddle_table<<<(n + 255) / 256, 256, 0, s>>>(tw, n, +1);
-  const int32_t* slots = reinterpret_cast<const int32_t*>(b + p.off_slots);
-  k_pupil_table<<<p.n_tab, 128, 0, s>>>(jobs, slots, pupils, p.n_tab, n, p.pixel_size, p.h, p.ncomp_max, table);
+  if ((e = launch_pupil_table(p, blob, table, s)) != cudaSuccess) return (int)e;
   // full mask spectrum / N^2 (the inverse below is unnormalised)
   e = plain_fft2(mask, p.mask_complex == 0, mfull, p.n_clips, n, -1, 1.0f, 1.0f / ((float)n * (float)n), tw, s);
   if (e != cudaSuccess) return (int)e;

@@ -87,20 +87,10 @@ __device__ __forceinline__ double pupil_phase(const LithoPupil& P, double rho, d
   return W;
 }
 
-// Coherent pupil value(s) at an in-aperture point. (fx, fy) is the diffracted
-// ray's frequency minus the source offset; rho its normalised radius.
-// Scalar: out[0] = exp(iW). Vector: out[c] = exp(iW) * V_c, c = x, y, z.
-__device__ __forceinline__ void pupil_values(const LithoPupil& P, double rho, double fx, double fy,
-                                             double jx, double jy, float2* out) {
-  const double r = sqrt(fx * fx + fy * fy);
-  double cp = 1.0, sp = 0.0;  // atan2(0, 0) = 0
-  if (r > 0.0) {
-    cp = fx / r;
-    sp = fy / r;
-  }
-  const double W = pupil_phase(P, rho, cp, sp);
-  double sW, cW;
-  sincos(W, &sW, &cW);
+// (cW, sW): the scalar factor exp(iW) (times the mask blank's reflection in
+// the multilayer model); the vector components multiply it.
+__device__ __forceinline__ void pupil_components(const LithoPupil& P, double rho, double cp, double sp, double jx,
+                                                 double jy, double cW, double sW, float2* out) {
   if (!P.vector) {
     out[0] = make_float2((float)cW, (float)sW);
     return;
@@ -123,6 +113,40 @@ __device__ __forceinline__ void pupil_values(const LithoPupil& P, double rho, do
   out[2] = make_float2((float)(cW * vz), (float)(sW * vz));
 }
 
+__device__ __forceinline__ void pupil_direction(double fx, double fy, double& cp, double& sp) {
+  const double r = sqrt(fx * fx + fy * fy);
+  cp = 1.0;
+  sp = 0.0;  // atan2(0, 0) = 0
+  if (r > 0.0) {
+    cp = fx / r;
+    sp = fy / r;
+  }
+}
+
+// Coherent pupil value(s) at an in-aperture point. (fx, fy) is the diffracted
+// ray's frequency minus the source offset; rho its normalised radius.
+// Scalar: out[0] = exp(iW). Vector: out[c] = exp(iW) * V_c, c = x, y, z.
+__device__ __forceinline__ void pupil_values(const LithoPupil& P, double rho, double fx, double fy,
+                                             double jx, double jy, float2* out) {
+  double cp, sp;
+  pupil_direction(fx, fy, cp, sp);
+  const double W = pupil_phase(P, rho, cp, sp);
+  double sW, cW;
+  sincos(W, &sW, &cW);
+  pupil_components(P, rho, cp, sp, jx, jy, cW, sW, out);
+}
+
+// pupil_values times the complex factor (rr + i ri).
+__device__ __forceinline__ void pupil_values_scaled(const LithoPupil& P, double rho, double fx, double fy,
+                                                    double jx, double jy, double rr, double ri, float2* out) {
+  double cp, sp;
+  pupil_direction(fx, fy, cp, sp);
+  const double W = pupil_phase(P, rho, cp, sp);
+  double sW, cW;
+  sincos(W, &sW, &cW);
+  pupil_components(P, rho, cp, sp, jx, jy, cW * rr - sW * ri, cW * ri + sW * rr, out);
+}
+
 // Exact aperture test of expose/aerial_image.py:_pupil_geometry (:131-138):
 // rho = sqrt((FX - fsx)^2 + (FY - fsy)^2) / (NA / lambda) <= 1, with FX the
 // numpy fftfreq value of bin kx. Returns rho (> 1 when outside) and the
@@ -133,6 +157,54 @@ __device__ __forceinline__ double aperture_rho(int kx, int ky, double val, doubl
   fy = dsub(bin_freq(ky, val), fsy);
   const double r2 = dadd(dmul(fx, fx), dmul(fy, fy));
   return ddiv(dsqrt(r2), kmax);
+}
+
+// Reflection of the mask blank for the order at frequency (FX, FY) under
+// source offset (fsx, fsy) (expose/m3d/provider.py:252-270): sin theta =
+// |(tilt lambda fs / m + chief ray) + lambda F / m|, then |r| and arg r
+// interpolated linearly in theta = asin(min(sin theta, 1)) on the ascending
+// table, held at its end values outside it; 0 when sin theta > 1.
+__device__ __forceinline__ void mirror_reflection(const LithoMirror& M, const double* __restrict__ tab, double FX,
+                                                  double FY, double fsx, double fsy, double& re, double& im) {
+  const double lam = M.wavelength, m = M.reduction;
+  const double sx0 = dadd(ddiv(dmul(dmul(M.tilt_sign, lam), fsx), m), M.sin_cx);
+  const double sy0 = dadd(ddiv(dmul(dmul(M.tilt_sign, lam), fsy), m), M.sin_cy);
+  const double sx = dadd(sx0, ddiv(dmul(lam, FX), m));
+  const double sy = dadd(sy0, ddiv(dmul(lam, FY), m));
+  const double st = dsqrt(dadd(dmul(sx, sx), dmul(sy, sy)));
+  if (!(st <= 1.0)) {
+    re = 0.0;
+    im = 0.0;
+    return;
+  }
+  const double th = asin(fmax(st, 0.0));
+  const int nt = M.n_theta;
+  const double* xp = tab;
+  const double* mag = tab + nt;
+  const double* ph = tab + 2 * nt;
+  double a, p;
+  if (th <= xp[0]) {
+    a = mag[0];
+    p = ph[0];
+  } else if (th >= xp[nt - 1]) {
+    a = mag[nt - 1];
+    p = ph[nt - 1];
+  } else {
+    // bisection for xp[j] <= th < xp[j + 1]
+    int lo = 0, hi = nt - 1;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (xp[mid] <= th) lo = mid; else hi = mid;
+    }
+    const double dx = dsub(th, xp[lo]);
+    const double span = dsub(xp[lo + 1], xp[lo]);
+    a = dadd(dmul(ddiv(dsub(mag[lo + 1], mag[lo]), span), dx), mag[lo]);
+    p = dadd(dmul(ddiv(dsub(ph[lo + 1], ph[lo]), span), dx), ph[lo]);
+  }
+  double sp, cp;
+  sincos(p, &sp, &cp);
+  re = a * cp;
+  im = a * sp;
 }
 
 }  // namespace litho

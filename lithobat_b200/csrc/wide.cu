@@ -29,9 +29,7 @@ cudaError_t plain_fft2(const void* in, bool in_real, float2* buf, long long plan
 cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_per_clip, int n, int bm,
                                 float2* out, float scale, const float2* tw_inv, int num_sms, cudaStream_t st,
                                 int* status);
-__global__ void k_pupil_table(const LithoJob* __restrict__ jobs, const int32_t* __restrict__ slots,
-                              const LithoPupil* __restrict__ pupils, int n_tab, int n, double pixel_size, int h,
-                              int ncomp_max, float2* __restrict__ table);
+cudaError_t launch_pupil_table(const LithoAbbePlan& p, const void* blob, float2* table, cudaStream_t s);
 __global__ void k_normalise(const float* __restrict__ blockmax, int nblk, const LithoNorm* __restrict__ norm,
                             int n, float* __restrict__ image, float* __restrict__ peak, int apply_mode0);
 
@@ -330,11 +328,9 @@ int abbe_wide_run(const LithoAbbePlan& p, const void* blob, const void* table_in
   const WideLayout l = wide_layout(p);
   const char* b = static_cast<const char*>(blob);
   const LithoJob* jobs = reinterpret_cast<const LithoJob*>(b + p.off_jobs);
-  const LithoPupil* pupils = reinterpret_cast<const LithoPupil*>(b + p.off_pupils);
   const LithoItem* items = reinterpret_cast<const LithoItem*>(b + p.off_items);
   const int32_t* out_items = reinterpret_cast<const int32_t*>(b + p.off_out_items);
   const LithoNorm* norm = reinterpret_cast<const LithoNorm*>(b + p.off_norm);
-  const int32_t* slots = reinterpret_cast<const int32_t*>(b + p.off_slots);
   char* w = static_cast<char*>(ws);
   int* status = reinterpret_cast<int*>(w + l.status);
   float2* twN = reinterpret_cast<float2*>(w + l.twN);
@@ -358,8 +354,7 @@ int abbe_wide_run(const LithoAbbePlan& p, const void* blob, const void* table_in
   if ((e = cudaMemsetAsync(status, 0, sizeof(int), s)) != cudaSuccess) return (int)e;
   k_twiddle_table<<<(n + 255) / 256, 256, 0, s>>>(twN, n, +1);
   k_twiddle_table<<<(L + 255) / 256, 256, 0, s>>>(twL, L, +1);
-  if (!table_in)
-    k_pupil_table<<<p.n_tab, 128, 0, s>>>(jobs, slots, pupils, p.n_tab, n, p.pixel_size, p.h, p.ncomp_max, table);
+  if (!table_in && (e = launch_pupil_table(p, blob, table, s)) != cudaSuccess) return (int)e;
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
   mark(1);
   e = launch_row_band_dft(mask, p.mask_complex != 0, p.n_clips * n, n, n, p.bm, u1, 1.0f, twN, num_sms, s, status);

@@ -43,13 +43,16 @@ def vector_coefficients(rho, phi, jx, jy, sin_theta_max, obliquity=True):
     return v * np.sqrt(ct) if obliquity else v
 
 
-def clear_throughput(src, view, n_image: float, vector: bool) -> float:
-    """What an unpatterned thin mask images to, for one plane.
+def clear_throughput(src, view, n_image: float, vector: bool, scale=None) -> float:
+    """What an unpatterned mask images to, for one plane.
 
     Scalar: sum of the weights of source points whose pupil passes DC.
     Vector: sum over those points and their states of w * |V(DC)|^2.
     The DC test is the reference's exact one: rho = sqrt((0 - fsx)^2 +
-    (0 - fsy)^2) / (NA / lambda) <= 1, in float64.
+    (0 - fsy)^2) / (NA / lambda) <= 1, in float64. ``scale`` (per source
+    point): what the blank returns there, |r|^2 for a mirror (the
+    reference's clear_scale, expose/aerial_image.py:431-438); None for a thin
+    mask (1).
     """
     k_max = view.NA / view.wavelength
     gx = 0.0 - src.fx
@@ -57,12 +60,15 @@ def clear_throughput(src, view, n_image: float, vector: bool) -> float:
     rho = np.sqrt(gx ** 2 + gy ** 2) / k_max
     inside = rho <= 1.0
     if not vector:
-        return float(np.sum(src.weight * inside.astype(np.float64)))
+        if scale is None:
+            return float(np.sum(src.weight * inside.astype(np.float64)))
+        return float(np.sum(src.weight * inside.astype(np.float64) * np.asarray(scale, dtype=np.float64)))
     total = 0.0
     phi = np.arctan2(gy, gx)
     stm = view.NA / n_image
     for s in np.nonzero(inside)[0]:
         for jx, jy, wp in jones_states(view.polarisation, float(src.phi[s])):
             V = vector_coefficients(rho[s], phi[s], jx, jy, stm, view.obliquity)
-            total += float(src.weight[s]) * wp * float(np.sum(V ** 2))
+            cs = 1.0 if scale is None else float(scale[s])
+            total += float(src.weight[s]) * wp * float(np.sum(V ** 2)) * cs
     return total

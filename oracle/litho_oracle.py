@@ -334,6 +334,112 @@ def normalisation_scale(mode, peak, clear, dose=1.0):
     raise ValueError(f"normalisation must be 'peak', 'clear' or 'none', got '{mode}'")
 
 
+# ---------------------------------------------------------------------------
+# The EUV blank as a Bragg mirror (mask_model="multilayer")
+# ---------------------------------------------------------------------------
+
+# expose/m3d/materials.py:58-82 (n + ik, k > 0 absorbing)
+_MASK_N = {
+    13.5e-9: {"vacuum": 1.0 + 0.0j, "Si": 0.99931 + 0.00182j, "Mo": 0.92108 + 0.00644j,
+              "Ru": 0.88651 + 0.01710j, "TaBN": 0.94900 + 0.03120j, "TaBO": 0.97000 + 0.02500j,
+              "Ta": 0.94270 + 0.04170j, "SiO2": 0.97800 + 0.01070j},
+    193e-9: {"vacuum": 1.0 + 0.0j, "air": 1.0 + 0.0j, "quartz": 1.5603 + 0.0j, "Cr": 0.84 + 1.65j,
+             "CrON": 1.95 + 1.05j, "MoSi": 2.343 + 0.586j},
+}
+# expose/m3d/multilayer.py:72-77 defaults; stack.py:178-187 presets (the parts the blank uses)
+_ML_DEFAULT = {"n_bilayers": 40, "period": 6.94e-9, "gamma": 0.4, "cap_material": "Ru",
+               "cap_thickness": 2.5e-9, "substrate": "Si"}
+
+
+def _mask_n(name, lam):
+    """materials.py:85-102."""
+    for w, table in _MASK_N.items():
+        if abs(w - lam) <= 1e-11:
+            return table[name]
+    raise KeyError(f"No mask-material table at {lam * 1e9:.3f} nm")
+
+
+def blank_films(optics):
+    """The blank's (indices, thicknesses): stack.py:106-132 + multilayer.py:86-110;
+    raises for a transmissive stack as provider.py:536-542."""
+    lam = optics.wavelength
+    spec = _opt(optics, "mask_stack", None)
+    if spec is None:                                   # stack.py:160-169: preset by wavelength
+        reflective = abs(lam - 13.5e-9) < 1e-11
+        ml = dict(_ML_DEFAULT) if reflective else None
+    elif not spec:                                     # stack.py:147-149: empty spec = defaults
+        reflective, ml = True, dict(_ML_DEFAULT)
+    else:                                              # stack.py:150-152
+        reflective = spec.get("regime", "euv_reflective") == "euv_reflective"
+        ml_spec = spec.get("multilayer", None)
+        ml = {**_ML_DEFAULT, **ml_spec} if ml_spec else None
+        if reflective and ml is None:
+            raise ValueError("regime='euv_reflective' needs a multilayer")
+    if not reflective:
+        raise ValueError("mask_model='multilayer' describes the Bragg mirror under an EUV mask, "
+                         "but the stack regime is 'duv_transmissive'.")
+    t_mo = ml["period"] * ml["gamma"]
+    t_si = ml["period"] - t_mo
+    n = [_mask_n("vacuum", lam), _mask_n(ml["cap_material"], lam)]
+    d = [0.0, ml["cap_thickness"]]
+    for _ in range(ml["n_bilayers"]):
+        n += [_mask_n("Si", lam), _mask_n("Mo", lam)]
+        d += [t_si, t_mo]
+    n.append(_mask_n(ml["substrate"], lam))
+    d.append(0.0)
+    return np.asarray(n, dtype=complex), np.asarray(d, dtype=np.float64)
+
+
+def films_reflection(n_stored, d, lam, theta0, pol):
+    """coat/films.py:168-227 — one angle, characteristic matrices multiplied
+    top-down, r = (eta_0 - C/B) / (eta_0 + C/B)."""
+    n = np.conj(np.asarray(n_stored, dtype=complex))
+    sin0 = n[0] * np.sin(theta0)
+    cos_t = np.sqrt(1.0 - (sin0 / n) ** 2)
+    eta = n * cos_t if pol == "s" else n / cos_t
+    M = np.eye(2, dtype=complex)
+    for j in range(1, len(n) - 1):
+        delta = 2.0 * np.pi * n[j] * cos_t[j] * d[j] / lam
+        M = M @ np.array([[np.cos(delta), 1j * np.sin(delta) / eta[j]],
+                          [1j * eta[j] * np.sin(delta), np.cos(delta)]], dtype=complex)
+    b, c = M @ np.array([1.0, eta[-1]], dtype=complex)
+    Y = c / b
+    return complex((eta[0] - Y) / (eta[0] + Y))
+
+
+def mirror_table(optics):
+    """provider.py:237-250 — (theta, |r|, unwrapped arg r) of the mean s/p reflection."""
+    n, d = blank_films(optics)
+    lam = optics.wavelength
+    theta = np.linspace(0.0, np.deg2rad(25.0), 501)
+    rs = np.array([films_reflection(n, d, lam, float(t), "s") for t in theta])
+    rp = np.array([films_reflection(n, d, lam, float(t), "p") for t in theta])
+    r = 0.5 * (rs + rp)
+    return theta, np.abs(r), np.unwrap(np.angle(r))
+
+
+def mirror_reflection(table, sin_theta):
+    """provider.py:252-264."""
+    theta_t, mag_t, ph_t = table
+    prop = sin_theta <= 1.0
+    th = np.arcsin(np.clip(sin_theta, 0.0, 1.0))
+    r = np.interp(th, theta_t, mag_t) * np.exp(1j * np.interp(th, theta_t, ph_t))
+    return np.where(prop, r, 0.0).astype(np.complex128)
+
+
+def mask_side_sines(fsx, fsy, optics):
+    """provider.py:72-126."""
+    lam, m = optics.wavelength, _opt(optics, "reduction", 4.0)
+    sx = SOURCE_TILT_SIGN * lam * fsx / m
+    sy = SOURCE_TILT_SIGN * lam * fsy / m
+    cra = math.sin(math.radians(_opt(optics, "chief_ray_deg", 0.0)))
+    if _opt(optics, "chief_ray_axis", "x").lower() == "x":
+        sx += cra
+    else:
+        sy += cra
+    return sx, sy
+
+
 def abbe_sum(mask, optics, grid, planes, source_subset=None):
     """aerial_image.py:351-494 (thin mask) — raw (P,n,n), peak (P,), clear (P,).
 
@@ -357,6 +463,13 @@ def abbe_sum(mask, optics, grid, planes, source_subset=None):
     src = source_points(optics)
     M = np.fft.fft2(np.asarray(mask).astype(np.complex128))     # m3d/provider.py:177-178
     FX, FY = make_freq_grid(n, grid.pixel_size)
+    mmodel = _opt(optics, "mask_model", "thin").lower()
+    if mmodel not in ("thin", "multilayer"):
+        raise ValueError(f"oracle images thin and multilayer masks, got mask_model={mmodel!r}")
+    mirror = mirror_table(optics) if mmodel == "multilayer" else None
+    if mirror is not None:                                     # provider.py:222-225
+        doff_x = lam * FX / _opt(optics, "reduction", 4.0)
+        doff_y = lam * FY / _opt(optics, "reduction", 4.0)
     k_max = NA / lam
 
     P = len(planes)
@@ -386,6 +499,12 @@ def abbe_sum(mask, optics, grid, planes, source_subset=None):
     for s in order:
         w_s = float(src.weight[s])
         fsx, fsy = float(src.fx[s]), float(src.fy[s])
+        M_s, clear_scale = M, 1.0
+        if mirror is not None:                                 # provider.py:266-295
+            sx0, sy0 = mask_side_sines(fsx, fsy, optics)
+            sx, sy = sx0 + doff_x, sy0 + doff_y
+            M_s = M * mirror_reflection(mirror, np.sqrt(sx * sx + sy * sy))
+            clear_scale = float(abs(mirror_reflection(mirror, np.array([math.hypot(sx0, sy0)]))[0]) ** 2)
         gx, gy = FX - fsx, FY - fsy
         RHO = np.sqrt(gx ** 2 + gy ** 2) / k_max                 # aerial_image.py:136
         PHI = np.arctan2(gy, gx) if need_phi else None
@@ -393,7 +512,7 @@ def abbe_sum(mask, optics, grid, planes, source_subset=None):
         idx = np.nonzero(inside)
         rho_in = RHO[idx]
         phi_in = None if PHI is None else PHI[idx]
-        M_in = M[idx]
+        M_in = M_s[idx]
         dc_in = float(inside[0, 0])
         states = jones_states(optics.polarisation, float(src.phi[s])) if vector else None
         for p, (dz, n_img) in enumerate(planes):
@@ -403,7 +522,7 @@ def abbe_sum(mask, optics, grid, planes, source_subset=None):
                 spec = np.zeros((n, n), dtype=np.complex128)
                 spec[idx] = coh
                 push(spec, p, w_s)
-                clear[p] += w_s * dc_in
+                clear[p] += w_s * dc_in * clear_scale
                 continue
             for jx, jy, wp in states:
                 V = vector_coefficients(rho_in, phi_in, jx, jy, NA / n_img,
@@ -414,7 +533,7 @@ def abbe_sum(mask, optics, grid, planes, source_subset=None):
                     push(spec, p, w_s * wp)
                 if dc_in:
                     at = np.nonzero((idx[0] == 0) & (idx[1] == 0))[0][0]
-                    clear[p] += (w_s * wp) * sum(abs(c[at]) ** 2 for c in V)
+                    clear[p] += (w_s * wp) * sum(abs(c[at]) ** 2 for c in V) * clear_scale
     flush()
     peak = aerial.reshape(P, -1).max(axis=1)
     return aerial, peak, clear

@@ -347,8 +347,74 @@ def next_rows():
          doses=np.array(doses), stack=np.array(stack))
 
 
+def multilayer():
+    """The EUV blank as a Bragg mirror (mask_model="multilayer",
+    expose/m3d/provider.py:190-295): images, the reflection table, the
+    clear-field factors and the reflection at chosen direction sines."""
+    _import_reference()
+    import dataclasses
+
+    from litho_sim.core.config import GridConfig, OpticsConfig
+    from litho_sim.expose import compute_aerial_image, compute_aerial_planes
+    from litho_sim.expose.m3d import MaskStack
+    from litho_sim.expose.m3d.provider import MultilayerSpectra
+    from litho_sim.expose.source import Source
+    from litho_sim.mask.patterns import lines_and_spaces
+
+    # the reference test's grating (tests/test_m3d.py:211-231): 32 nm half pitch at 2 nm
+    g = GridConfig(n_pixels=128, pixel_size=2e-9)
+    m = lines_and_spaces(128, 2e-9, pitch=64e-9, cd=32e-9)
+    base = OpticsConfig(wavelength=13.5e-9, NA=0.33, sigma_outer=0.6, source_grid=11, chief_ray_deg=6.0,
+                        reduction=4.0, normalisation="clear", mask_model="multilayer")
+    for name, o in (("ml_ls_128_cra6", base),
+                    ("ml_ls_128_cram6", dataclasses.replace(base, chief_ray_deg=-6.0)),
+                    ("ml_ls_128_thin", dataclasses.replace(base, mask_model="thin"))):
+        raw, peak, clear = compute_aerial_image(m, o, g, return_raw=True)
+        save(name, optics=o, grid=g, mask=m.astype(np.uint8), raw=raw, peak=peak, clear=clear)
+
+    # through focus (the best-focus shift, tests/test_m3d.py:258-278), one planes call
+    foci = np.linspace(-40e-9, 40e-9, 9)
+    planes = [(float(d), 1.0) for d in foci]
+    stack = compute_aerial_planes(m, base, g, planes)
+    save("ml_ls_128_focus", optics=base, grid=g, mask=m.astype(np.uint8), foci=foci, images=np.asarray(stack))
+
+    # a Manhattan clip: dipole, y chief ray, Zernikes, a custom stack, peak normalisation
+    g2 = GridConfig(n_pixels=256, pixel_size=2e-9)
+    o2 = OpticsConfig(wavelength=13.5e-9, NA=0.33, source_grid=17, chief_ray_deg=5.0, chief_ray_axis="y",
+                      defocus=15e-9, zernike_coeffs={7: 0.02, 9: -0.01}, mask_model="multilayer",
+                      mask_stack={"regime": "euv_reflective", "absorber": "TaBN", "absorber_thickness": 60e-9,
+                                  "substrate": "SiO2",
+                                  "multilayer": {"n_bilayers": 30, "period": 7.0e-9, "gamma": 0.42}},
+                      source_spec=Source.dipole(0.9, 0.6, opening_deg=60).to_dict())
+    m2 = manhattan_clip(np.random.default_rng(51), 256, 2e-9, n_rect=(10, 20), width_nm=(20, 80))
+    raw, peak, clear = compute_aerial_image(m2, o2, g2, return_raw=True)
+    save("ml_dipole_256", optics=o2, grid=g2, mask=m2.astype(np.uint8), raw=raw, peak=peak, clear=clear)
+
+    # wide pupil (512^2 at 2 nm: coarse grid 128), vector TE model
+    g3 = GridConfig(n_pixels=512, pixel_size=2e-9)
+    o3 = OpticsConfig(wavelength=13.5e-9, NA=0.33, source_type="annular", sigma_inner=0.5, sigma_outer=0.8,
+                      source_grid=9, chief_ray_deg=6.0, mask_model="multilayer", imaging_model="vector",
+                      polarisation="te", normalisation="clear")
+    m3 = manhattan_clip(np.random.default_rng(52), 512, 2e-9, n_rect=(20, 40), width_nm=(20, 80))
+    raw, peak, clear = compute_aerial_image(m3, o3, g3, return_raw=True)
+    save("ml_vector_512", optics=o3, grid=g3, mask=m3.astype(np.uint8), raw=raw.astype(np.float32), peak=peak,
+         clear=clear)
+
+    # the reflection itself: table, clear factors, values at chosen sines
+    stack = MaskStack.for_wavelength(13.5e-9)
+    sp = MultilayerSpectra(np.ones((128, 128)), base, g, stack)
+    sines = np.array([0.0, 0.02, 0.05, 0.1045, 0.15, 0.2, 0.3, 0.5, 1.0, 1.4, 12.0])
+    fs = np.array([[0.0, 0.0], [1.2e6, -0.7e6], [-2.0e6, 1.5e6], [4.0e6, 0.0]])
+    save("ml_reflection", theta=sp._theta, mag=sp._mag, phase=sp._phase, sines=sines,
+         r=sp._reflection(sines), fs=fs, clear_intensity=np.array([sp.clear_intensity(a, b) for a, b in fs]),
+         blank_s_6deg=np.array(stack.blank_reflection(13.5e-9, np.radians(6.0), "s")),
+         blank_p_9deg=np.array(stack.blank_reflection(13.5e-9, np.radians(9.0), "p")))
+
+
 if __name__ == "__main__":
-    if sys.argv[1:] == ["wide"]:
+    if sys.argv[1:] == ["multilayer"]:
+        multilayer()
+    elif sys.argv[1:] == ["wide"]:
         wide()
     elif sys.argv[1:] == ["next"]:
         next_rows()

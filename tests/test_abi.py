@@ -28,8 +28,8 @@ def test_struct_sizes_match_the_python_layouts():
     out = (C.c_int32 * 16)()
     k = L.litho_abi_sizes(out, 16)
     sizes = list(out)[:k]
-    assert sizes[:5] == [nat.PUPIL_DTYPE.itemsize, nat.JOB_DTYPE.itemsize, nat.ITEM_DTYPE.itemsize,
-                         nat.NORM_DTYPE.itemsize, C.sizeof(nat.AbbePlan)]
+    assert sizes[:6] == [nat.PUPIL_DTYPE.itemsize, nat.JOB_DTYPE.itemsize, nat.ITEM_DTYPE.itemsize,
+                         nat.NORM_DTYPE.itemsize, C.sizeof(nat.AbbePlan), nat.MIRROR_DTYPE.itemsize]
 
 
 def test_status_strings():
