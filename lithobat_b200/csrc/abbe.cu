@@ -523,10 +523,17 @@ k_synth(const float2* __restrict__ Bbox, int G, int n, const float2* __restrict_
 
 int synth_blocks_for(int n) { return (n + kSynthRows - 1) / kSynthRows; }
 
+static int num_sms_cached();
+
 // Real synthesis of n_fields Hermitian boxes of side G into n x n images.
+// cbuf: max(synth_mma_bytes, synth_cols_bytes) of workspace for the tensor-core
+// or pair synthesis (nullptr: the direct kernel).
 cudaError_t launch_synth_real(const float2* box, int G, int n, int n_fields, const float2* tw, const LithoNorm* norm,
-                              float* out, float* blockmax, cudaStream_t s, float2* cbuf) {
+                              float* out, float* blockmax, cudaStream_t s, float2* cbuf, int* status) {
   const int gh = G / 2;
+  if (!norm && cbuf && status && synth_mma_pick(n_fields, n, gh))
+    return launch_synth_mma(box, gh, n, n_fields, tw, nullptr, out, nullptr, blockmax, s, nullptr, cbuf, status,
+                            num_sms_cached());
   if (!norm && synth_pairs_ok(n, gh))
     return launch_synth_pairs(box, gh, n, n_fields, tw, nullptr, out, nullptr, blockmax, s, nullptr, cbuf);
   const size_t sm = (size_t)n * 8 + (size_t)kSynthRows * (gh + 1) * 8 + (size_t)G * G * 8;
@@ -614,7 +621,8 @@ static AbbeLayout abbe_layout(const LithoAbbePlan& p) {
   l.bbox = off;     off = align16(off + (int64_t)p.n_out * G * G * 8);
   l.blockmax = off; off = align16(off + (int64_t)p.n_out * synth_blocks(p.n) * 4);
   l.cbuf = off;
-  if (synth_pairs_ok(p.n, 2 * p.h)) off = align16(off + synth_cols_bytes(p.n_out, p.n, 2 * p.h));
+  if (synth_mma_pick(p.n_out, p.n, 2 * p.h)) off = align16(off + synth_mma_bytes(p.n_out, p.n, 2 * p.h));
+  else if (synth_pairs_ok(p.n, 2 * p.h)) off = align16(off + synth_cols_bytes(p.n_out, p.n, 2 * p.h));
   l.total = off;
   return l;
 }
@@ -733,8 +741,12 @@ static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* tab
   k_coarse_reduce<<<dim3(p.n_out, reduce_split(p.n_out, G)), 1024, sm_red, s>>>(out_items, partial, p.L, p.h, bbox);
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
   mark(5);
-  if (synth_pairs_ok(p.n, 2 * p.h)) {
-    // peak pass (peak-normalised outputs), then the writing pass
+  if (synth_mma_pick(p.n_out, p.n, 2 * p.h)) {
+    // peak pass (peak-normalised outputs), then the writing pass, on the tensor cores
+    e = launch_synth_mma(bbox, 2 * p.h, p.n, p.n_out, tw, norm, image, peak, blockmax, s, ev ? ev[6] : nullptr,
+                         w + l.cbuf, status, sms);
+    if (e != cudaSuccess) return (int)e;
+  } else if (synth_pairs_ok(p.n, 2 * p.h)) {
     e = launch_synth_pairs(bbox, 2 * p.h, p.n, p.n_out, tw, norm, image, peak, blockmax, s, ev ? ev[6] : nullptr,
                            reinterpret_cast<float2*>(w + l.cbuf));
     if (e != cudaSuccess) return (int)e;

@@ -15,6 +15,8 @@
 // and grad(x) = sum_f H(f) exp(2 pi i f.x / N) with H(f) = A(f) + conj(A(-f)),
 // one band-limited synthesis (csrc/abbe.cu k_synth). Scale: M = F(m) / N^2,
 // G band = F(G) / N^2, as the band-spectrum stage produces them.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace litho {
@@ -23,7 +25,9 @@ cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_
                                 float2* out, float scale, const float2* tw_inv, int num_sms, cudaStream_t st,
                                 int* status);
 cudaError_t launch_synth_real(const float2* box, int G, int n, int n_fields, const float2* tw, const LithoNorm* norm,
-                              float* out, float* blockmax, cudaStream_t s, float2* cbuf);
+                              float* out, float* blockmax, cudaStream_t s, float2* cbuf, int* status);
+bool synth_mma_ok(int n, int g0);
+int64_t synth_mma_bytes(int n_out, int n, int g0);
 int64_t synth_cols_bytes(int n_out, int n, int g0);
 bool synth_pairs_ok(int n, int g0);
 bool wide_adjoint_ok(int h);
@@ -544,14 +548,25 @@ extern "C" int litho_band_spectrum(const void* in, int is_complex, int n_fields,
   return e == cudaSuccess ? LITHO_OK : (int)e;
 }
 
+// status word, twiddles, block maxima, then one region for the synthesis
+// engine in use: the operand planes of the tensor-core synthesis or the column
+// buffer of the pair synthesis (boxes up to half-width 31), or the spectrum of
+// the synthesis of wider boxes
+static int64_t band_synth_region(int n_fields, int n) {
+  int64_t r = align16(synth_cols_bytes(n_fields, n, 31));
+  if (synth_mma_ok(n, 31)) r = std::max(r, align16(synth_mma_bytes(n_fields, n, 31)));
+  return std::max(r, align16(wide_synth_spec_bytes(n_fields, n)));
+}
+
+static int64_t band_synth_ws(int n_fields, int n) {
+  return align16(16) + align16((int64_t)n * 8) + align16((int64_t)n_fields * synth_blocks_for(n) * 4) +
+         band_synth_region(n_fields, n);
+}
+
 extern "C" int litho_band_synthesis_workspace(int n_fields, int n, size_t* bytes) {
   if (!bytes) return LITHO_E_NULL;
   if (n_fields < 1 || n < 2) return LITHO_E_SIZE;
-  // twiddles, block maxima, the whole-image column buffer for the widest box
-  // the pair synthesis takes (half-width 31), and the spectrum buffer the
-  // synthesis of wider boxes uses
-  *bytes = (size_t)(align16((int64_t)n * 8) + align16((int64_t)n_fields * synth_blocks_for(n) * 4) +
-                    align16(synth_cols_bytes(n_fields, n, 31)) + align16(wide_synth_spec_bytes(n_fields, n)));
+  *bytes = (size_t)band_synth_ws(n_fields, n);
   return LITHO_OK;
 }
 
@@ -562,10 +577,14 @@ extern "C" int litho_band_synthesis(const void* box, int n_fields, int n, int h,
   size_t need = 0;
   litho_band_synthesis_workspace(n_fields, n, &need);
   if (ws_bytes < need) return LITHO_E_WORKSPACE;
-  float2* tw = static_cast<float2*>(ws);
-  float* blockmax = reinterpret_cast<float*>(static_cast<char*>(ws) + align16((int64_t)n * 8));
+  if ((uintptr_t)ws & 15) return LITHO_E_ALIGN;
+  char* w0 = static_cast<char*>(ws);
+  int* status = reinterpret_cast<int*>(w0);
+  float2* tw = reinterpret_cast<float2*>(w0 + align16(16));
+  float* blockmax = reinterpret_cast<float*>(w0 + align16(16) + align16((int64_t)n * 8));
+  cudaError_t e = cudaMemsetAsync(status, 0, sizeof(int), s);
+  if (e != cudaSuccess) return (int)e;
   k_twiddle_table<<<(n + 255) / 256, 256, 0, s>>>(tw, n, +1);
-  cudaError_t e;
   if (complex_out) {
     const int side = 2 * h + 1;
     const size_t sm = (size_t)n * 8 + (size_t)kCsRows * side * 8;
@@ -574,16 +593,16 @@ extern "C" int litho_band_synthesis(const void* box, int n_fields, int n, int h,
     k_synth_complex<<<g, 256, sm, s>>>(static_cast<const float2*>(box), h, n, tw, static_cast<float2*>(out));
     e = cudaGetLastError();
   } else {
-    char* wb = static_cast<char*>(ws) + align16((int64_t)n * 8) + align16((int64_t)n_fields * synth_blocks_for(n) * 4);
+    char* wb = w0 + align16(16) + align16((int64_t)n * 8) + align16((int64_t)n_fields * synth_blocks_for(n) * 4);
     if (!synth_pairs_ok(n, h) && h > 31 && n >= 32 && n <= 4096 && (n & (n - 1)) == 0 &&
         2 * h + 1 <= n) {
-      // boxes too wide for the pair synthesis: scatter and one inverse FFT per two fields
-      float2* spec = reinterpret_cast<float2*>(wb + align16(synth_cols_bytes(n_fields, n, 31)));
-      e = wide_synth_real(static_cast<const float2*>(box), h, n, n_fields, static_cast<float*>(out), spec, tw, s);
+      // boxes too wide for the row synthesis: scatter and one inverse FFT per two fields
+      e = wide_synth_real(static_cast<const float2*>(box), h, n, n_fields, static_cast<float*>(out),
+                          reinterpret_cast<float2*>(wb), tw, s);
     } else {
       float2* cbuf = h <= 31 ? reinterpret_cast<float2*>(wb) : nullptr;
       e = launch_synth_real(static_cast<const float2*>(box), 2 * h + 1, n, n_fields, tw, nullptr,
-                            static_cast<float*>(out), blockmax, s, cbuf);
+                            static_cast<float*>(out), blockmax, s, cbuf, status);
     }
   }
   return e == cudaSuccess ? LITHO_OK : (int)e;

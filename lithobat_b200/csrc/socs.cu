@@ -21,6 +21,7 @@
 //                         the Rayleigh quotient with the exact A, so the
 //                         weights carry FP64 accuracy whatever the Gram's.
 #include "common.cuh"
+#include "tcgen05.cuh"
 #include "pupil.cuh"
 
 namespace litho {
@@ -78,33 +79,6 @@ constexpr int kGThreads = 128;
 constexpr uint32_t kGAtile = kGM * kGK * 4;  // bytes of one A plane (16 KiB)
 constexpr uint32_t kGBtile = kGN * kGK * 4;  // bytes of one B plane (32 KiB)
 
-__device__ __forceinline__ uint32_t to_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
-
-// Canonical K-major no-swizzle descriptor (version 1 for sm_100).
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
-}
-
-__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                          uint32_t accumulate) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 // Value of row `row` (of the 2S rows of [X; Y]) at column k (< 2 ld).
 __device__ __forceinline__ double gram_operand(const double* Are, const double* Aim, int S, int ld, int row,

@@ -1,0 +1,410 @@
+// Band-limited synthesis of real images on the tcgen05 tensor cores.
+//
+// The last stage of the Abbe sum (expose/aerial_image.py:488-494) and of the
+// SOCS image and gradient (opc/ilt.py:227-232, 263-266) evaluates
+//     I(x, y) = sum_{|gx|,|gy| <= g0} B(gx, gy) w^(gx x + gy y),  w = exp(2 pi i / N),
+// for a Hermitian box B, so I is real. With the column stage
+//     C(gx, y) = sum_gy B(gx, gy) w^(gy y)   (gx = 0..g0),
+// the row stage is one real product per image:
+//     I(x, y) = sum_k Q[x][k] P[y][k],  K = 2 g0 + 1 terms,
+//     Q[x] = [1, cos(2 pi x / N), sin(2 pi x / N), cos(4 pi x / N), ...],
+//     P[y] = [Re C(0, y), 2 Re C(1, y), -2 Im C(1, y), 2 Re C(2, y), ...],
+// i.e. a GEMM with M = N = image side and K = 2 g0 + 1 (padded to Kp, a
+// multiple of 8). It runs as tcgen05.mma kind::tf32 with every operand split
+// into TF32 hi + lo planes and three products per K step (hi hi + hi lo +
+// lo hi): about 2^-22 relative error per product, FP32 accumulation in TMEM.
+//
+// Kernels:
+//   k_synth_pplanes : P for every output and row (column sums by 32-point
+//                     FFTs over residues), written in the MMA's shared-memory
+//                     layout so each nt x Kp tile is one bulk copy;
+//   k_synth_qplanes : Q for every x (the same for all outputs);
+//   k_synth_mma     : persistent, one CTA per SM; a CTA takes (output, row
+//                     tile) units and sweeps the x tiles: one thread loads
+//                     operand tiles (cp.async.bulk, double-buffered), one
+//                     thread issues the MMAs into two TMEM accumulators, four
+//                     warps drain the accumulators (tcgen05.ld), scale, store
+//                     coalesced rows of the image and keep the maxima.
+// Peak normalisation needs the peak before the scaled image is written:
+// pass 0 computes only the maxima, pass 1 writes. Every wait is bounded and a
+// wait that gives up reports LITHO_E_TIMEOUT through the status word.
+#include <type_traits>
+
+#include "common.cuh"
+#include "rows.cuh"
+#include "tcgen05.cuh"
+
+namespace litho {
+
+constexpr int kSmMT = 128;       // x rows per tile (MMA M)
+constexpr int kSmG0Max = 31;     // box half-width limit (K = 2 g0 + 1 <= 63)
+constexpr int kSmDrainWarps = 4;  // warp w drains TMEM lanes 32 w .. 32 w + 31
+constexpr int kSmThreads = (kSmDrainWarps + 2) * 32;  // + one loading warp and one MMA warp
+
+
+__host__ __device__ inline int smma_kp(int g0) { return (2 * g0 + 1 + 7) & ~7; }
+// rows per tile (MMA N): two A and two B buffers stay within 192 KiB
+__host__ __device__ inline int smma_nt(int kp) { return kp <= 32 ? 256 : (kp <= 48 ? 128 : 64); }
+__host__ __device__ inline uint32_t smma_a_bytes(int kp) { return (uint32_t)kSmMT * kp * 8; }
+__host__ __device__ inline uint32_t smma_b_bytes(int kp) { return (uint32_t)smma_nt(kp) * kp * 8; }
+// byte offset of element (row, k) in one plane of a tile of R rows: K-major
+// core matrices (8 rows x 16 bytes), 16-byte K chunks R * 16 bytes apart
+__host__ __device__ inline uint32_t smma_off(int R, int row, int k) {
+  return (uint32_t)((k >> 2) * (R * 16) + row * 16 + (k & 3) * 4);
+}
+
+bool synth_mma_ok(int n, int g0) {
+  return g0 >= 0 && g0 <= kSmG0Max && n >= 256 && n <= 4096 && (n & (n - 1)) == 0;
+}
+
+// Worth it when there are enough 128 x 256 output tiles to keep every SM's
+// MMA and drain pipeline busy (about 16 per SM); smaller batches use the
+// pair synthesis, whose fixed costs are lower.
+bool synth_mma_pick(int n_out, int n, int g0) {
+  return synth_mma_ok(n, g0) && (int64_t)n_out * (n / 256) * (n / kSmMT) >= 16 * 148;
+}
+
+int64_t synth_mma_bytes(int n_out, int n, int g0) {
+  const int kp = smma_kp(g0);
+  return align16((int64_t)n_out * n * kp * 8) + align16((int64_t)n * kp * 8);
+}
+
+// P planes: [output][row tile][hi | lo][chunk][row][4] (row tile of nt rows).
+// The column sums C(gx, y) come from 32-point FFTs over residues: with
+// N = 32 M and y = b + M a, C(gx, b + M a) = sum_r w32^(r a) S_b(r),
+// S_b(r) = sum_{gy = r mod 32} B(gx, gy) w^(gy b), one FFT per residue b held
+// in a lane's registers. One warp per (output, gx); the gx = 0 warp also
+// writes the zero padding K <= k < Kp.
+constexpr int kPpWarps = 8;
+
+__device__ __forceinline__ void p_put(uint32_t* tile, int nt, int kp, int row, int k, float v) {
+  const uint32_t h = to_tf32(v);
+  const uint32_t o = smma_off(nt, row, k) >> 2;
+  tile[o] = h;
+  tile[(size_t)nt * kp + o] = to_tf32(v - __uint_as_float(h));
+}
+
+__global__ void __launch_bounds__(kPpWarps * 32)
+k_synth_pplanes(const float2* __restrict__ Bbox, int g0, int n, const float2* __restrict__ tw_inv, int kp, int nt,
+                uint32_t* __restrict__ planes) {
+  extern __shared__ float2 pp_tb[];                     // [g][b] = w^(g b), g = 0..g0
+  __shared__ float2 col[kPpWarps][2 * kSmG0Max + 2];    // B(gx, gy + g0) of each warp's column
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int o = blockIdx.y, gx = blockIdx.x * kPpWarps + warp;
+  const int gp = g0 + 1, G = 2 * g0 + 1, M = n >> 5, nmask = n - 1;
+  for (int j = threadIdx.x; j < gp * M; j += blockDim.x) {
+    const int g = j / M, b = j % M;
+    pp_tb[j] = __ldg(tw_inv + ((g * b) & nmask));
+  }
+  if (gx < gp) {
+    const float2* bc = Bbox + (size_t)o * G * G + gx + g0;
+    for (int i = lane; i < G; i += 32) col[warp][i] = bc[(size_t)i * G];
+  }
+  __syncthreads();
+  if (gx >= gp) return;
+  const float2* cw = col[warp] + g0;
+  uint32_t* base = planes + (size_t)o * (n / nt) * ((size_t)nt * kp * 2);
+  for (int b = lane; b < M; b += 32) {
+    float2 Q[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) Q[i] = make_float2(0.f, 0.f);
+    Q[0] = cw[0];
+#pragma unroll
+    for (int g = 1; g <= kSmG0Max; ++g) {
+      if (g <= g0) {
+        const float2 t = pp_tb[g * M + b];
+        Q[g & 31] = cadd(Q[g & 31], cmul(cw[g], t));
+        Q[(-g) & 31] = cadd(Q[(-g) & 31], cmulc(cw[-g], t));
+      }
+    }
+    fft_reg<32, +1>(Q);
+#pragma unroll
+    for (int a = 0; a < 32; ++a) {
+      const int y = b + M * a, row = y % nt;
+      uint32_t* tile = base + (size_t)(y / nt) * ((size_t)nt * kp * 2);
+      if (gx == 0) {
+        p_put(tile, nt, kp, row, 0, Q[a].x);
+        for (int k = G; k < kp; ++k) p_put(tile, nt, kp, row, k, 0.f);
+      } else {
+        p_put(tile, nt, kp, row, 2 * gx - 1, 2.f * Q[a].x);
+        p_put(tile, nt, kp, row, 2 * gx, -2.f * Q[a].y);
+      }
+    }
+  }
+}
+
+// Q planes: [x tile][hi | lo][chunk][row][4], identical for every output.
+__global__ void __launch_bounds__(kSmMT)
+k_synth_qplanes(const float2* __restrict__ tw, int g0, int n, int kp, uint32_t* __restrict__ planes) {
+  const int x = blockIdx.x * kSmMT + threadIdx.x;
+  const int K = 2 * g0 + 1, nmask = n - 1;
+  uint32_t* hi = planes + (size_t)blockIdx.x * kSmMT * kp * 2;
+  uint32_t* lo = hi + (size_t)kSmMT * kp;
+  for (int c = 0; c < kp / 4; ++c) {
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int k = 4 * c + q;
+      float f = 0.f;
+      if (k == 0) {
+        f = 1.f;
+      } else if (k < K) {
+        const int g = (k + 1) >> 1;
+        const float2 w = tw[(g * x) & nmask];
+        f = (k & 1) ? w.x : w.y;
+      }
+      h[q] = to_tf32(f);
+      l[q] = to_tf32(f - __uint_as_float(h[q]));
+    }
+    const uint32_t o = smma_off(kSmMT, threadIdx.x, 4 * c) >> 2;
+    *reinterpret_cast<uint4*>(hi + o) = make_uint4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<uint4*>(lo + o) = make_uint4(l[0], l[1], l[2], l[3]);
+  }
+}
+
+// PASS 0: maxima of peak-normalised outputs only (others skipped).
+// PASS 1: every output: image = raw * scale (scale / peak for peak-normalised
+//         outputs) and the maxima of the raw image.
+// blockmax[o][row tile][x range][warp]: the maximum over each drain warp's part.
+// N: the image side as a compile-time constant (the drain's store offsets
+// become immediates).
+template <int PASS, int N>
+__global__ void __launch_bounds__(kSmThreads, 1)
+k_synth_mma(const uint32_t* __restrict__ pplanes, const uint32_t* __restrict__ qplanes, int n_out, int kp,
+            int xsplit, const LithoNorm* __restrict__ norm, const float* __restrict__ peak, float* __restrict__ image,
+            float* __restrict__ blockmax, int* __restrict__ status) {
+  extern __shared__ __align__(1024) unsigned char sm_raw[];
+  __shared__ uint64_t bar_bfull[2], bar_bempty[2], bar_afull[2], bar_aempty[2], bar_accfull[2], bar_accempty[2];
+  __shared__ uint64_t bar_drain;
+  __shared__ uint32_t s_tmem;
+  __shared__ volatile int s_fail;
+  const int nt = smma_nt(kp);
+  const uint32_t abytes = smma_a_bytes(kp), bbytes = smma_b_bytes(kp);
+  unsigned char* bufB0 = sm_raw;
+  unsigned char* bufA0 = sm_raw + 2 * bbytes;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int n = N;
+  const int yt_per = n / nt, xt_per = n / kSmMT, xper = xt_per / xsplit;
+  const int n_units = n_out * yt_per * xsplit;  // unit: (output, row tile, x range of xper tiles)
+  const uint32_t tcols = 2u * (uint32_t)nt;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(tcols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (threadIdx.x == 0) {
+    s_fail = 0;
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&bar_bfull[b], 1);
+      mbar_init(&bar_bempty[b], 1);
+      mbar_init(&bar_afull[b], 1);
+      mbar_init(&bar_aempty[b], 1);
+      mbar_init(&bar_accfull[b], 1);
+      mbar_init(&bar_accempty[b], kSmDrainWarps * 32);
+    }
+    mbar_init(&bar_drain, 1);
+    fence_mbar_init();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+
+  auto live = [&](int u) -> bool {
+    if (PASS == 1) return true;
+    return norm != nullptr && norm[u / (yt_per * xsplit)].mode == 1;
+  };
+
+  if (warp == kSmDrainWarps) {
+    // ---- operand loads ----------------------------------------------------
+    if (lane == 0) {
+      int i = 0, a = 0;
+      bool ok = true;
+      for (int u = blockIdx.x; u < n_units && ok; u += gridDim.x) {
+        if (!live(u)) continue;
+        const int ib = i & 1;
+        if (i >= 2 && !mbar_wait(&bar_bempty[ib], ((i >> 1) - 1) & 1)) { ok = false; break; }
+        mbar_expect_tx(&bar_bfull[ib], bbytes);
+        bulk_g2s(bufB0 + ib * bbytes, pplanes + (size_t)(u / xsplit) * (bbytes >> 2), bbytes, &bar_bfull[ib]);
+        ++i;
+        for (int j = (u % xsplit) * xper; j < (u % xsplit + 1) * xper; ++j) {
+          const int ab = a & 1;
+          if (s_fail || (a >= 2 && !mbar_wait(&bar_aempty[ab], ((a >> 1) - 1) & 1))) { ok = false; break; }
+          mbar_expect_tx(&bar_afull[ab], abytes);
+          bulk_g2s(bufA0 + ab * abytes, qplanes + (size_t)j * (abytes >> 2), abytes, &bar_afull[ab]);
+          ++a;
+        }
+      }
+      if (!ok) s_fail = 1;
+      // let the last copy into each buffer land before the block can exit
+      for (int k = 1; k <= 2; ++k) {
+        if (i - k >= 0) mbar_wait(&bar_bfull[(i - k) & 1], ((i - k) >> 1) & 1);
+        if (a - k >= 0) mbar_wait(&bar_afull[(a - k) & 1], ((a - k) >> 1) & 1);
+      }
+    }
+  } else if (warp == kSmDrainWarps + 1) {
+    // ---- MMA issue --------------------------------------------------------
+    if (lane == 0) {
+      const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(nt >> 3) << 17) |
+                             ((uint32_t)(kSmMT >> 4) << 24);
+      int i = 0, a = 0, c = 0;
+      bool ok = true;
+      for (int u = blockIdx.x; u < n_units && ok; u += gridDim.x) {
+        if (!live(u)) continue;
+        const int ib = i & 1;
+        if (!mbar_wait(&bar_bfull[ib], (i >> 1) & 1)) { ok = false; break; }
+        const uint32_t bh0 = smem_u32(bufB0 + ib * bbytes), bl0 = bh0 + (bbytes >> 1);
+        for (int j = 0; j < xper; ++j) {
+          const int ab = a & 1, cb = c & 1;
+          if (s_fail || !mbar_wait(&bar_afull[ab], (a >> 1) & 1) ||
+              (c >= 2 && !mbar_wait(&bar_accempty[cb], ((c >> 1) - 1) & 1))) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t ah0 = smem_u32(bufA0 + ab * abytes), al0 = ah0 + (abytes >> 1);
+          const uint32_t d = tmem + (uint32_t)(cb * nt);
+          for (int s = 0; s < kp / 8; ++s) {
+            const uint32_t ao = (uint32_t)s * 2 * (kSmMT * 16), bo = (uint32_t)s * 2 * (nt * 16);
+            const uint64_t ah = umma_desc(ah0 + ao, kSmMT * 16, 128), al = umma_desc(al0 + ao, kSmMT * 16, 128);
+            const uint64_t bh = umma_desc(bh0 + bo, nt * 16, 128), bl = umma_desc(bl0 + bo, nt * 16, 128);
+            umma_tf32(d, ah, bh, idesc, s > 0 ? 1u : 0u);
+            umma_tf32(d, ah, bl, idesc, 1u);
+            umma_tf32(d, al, bh, idesc, 1u);
+          }
+          umma_commit(&bar_accfull[cb]);
+          umma_commit(&bar_aempty[ab]);
+          if (j == xper - 1) umma_commit(&bar_bempty[ib]);
+          ++a;
+          ++c;
+        }
+        ++i;
+      }
+      if (!ok) s_fail = 1;
+      if (c > 0) {  // every MMA this thread issued has completed before TMEM is released
+        umma_commit(&bar_drain);
+        mbar_wait(&bar_drain, 0);
+      }
+    }
+  } else {
+    // ---- accumulator drain (warps 0-3: TMEM lanes 32 w .. 32 w + 31) -------
+    // Each store instruction writes 32 consecutive x of one image row (128
+    // bytes, coalesced); the offsets of the 32 rows of a chunk are immediates.
+    int c = 0;
+    bool ok = true;
+    for (int u = blockIdx.x; u < n_units && ok; u += gridDim.x) {
+      if (!live(u)) continue;
+      const int tile = u / xsplit, xs = u % xsplit;
+      const int o = tile / yt_per, y0 = (tile % yt_per) * nt;
+      float sc = 1.f;
+      bool want_max = true;   // the writing pass of a peak-normalised output has its peak already
+      if (PASS == 1) {
+        const LithoNorm nm = norm ? norm[o] : LithoNorm{0, 1.0f};
+        sc = nm.scale;
+        if (nm.mode == 1) {
+          const float pk = peak[o];
+          sc = pk > 0.f ? nm.scale / pk : nm.scale;
+          want_max = false;
+        }
+      }
+      float mx = 0.f;
+      float* img = image + (size_t)o * n * n;
+      for (int j = xs * xper; j < (xs + 1) * xper; ++j) {
+        const int cb = c & 1;
+        if (s_fail || !mbar_wait(&bar_accfull[cb], (c >> 1) & 1)) { ok = false; break; }
+        tc_fence_after();
+        const int x = j * kSmMT + warp * 32 + lane;
+        const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cb * nt);
+        for (int c0 = 0; c0 < nt; c0 += 32) {
+          uint32_t r[32];
+          tmem_ld32(ta + (uint32_t)c0, r);
+          tmem_ld_wait();
+          if (PASS == 0 || want_max) {
+#pragma unroll
+            for (int q = 0; q < 32; ++q) mx = fmaxf(mx, __uint_as_float(r[q]));
+          }
+          if (PASS == 1) {
+            float* dst = img + (size_t)(y0 + c0) * N + x;
+#pragma unroll
+            for (int q = 0; q < 32; ++q) __stcs(dst + q * N, __uint_as_float(r[q]) * sc);
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(&bar_accempty[cb]);
+        ++c;
+      }
+      if (!ok) break;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      if (lane == 0) blockmax[(size_t)u * kSmDrainWarps + warp] = mx;
+    }
+    if (!ok) s_fail = 1;
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (s_fail && threadIdx.x == 0) atomicExch(status, LITHO_E_TIMEOUT);
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tcols));
+}
+
+__global__ void k_peak(const float* __restrict__ blockmax, int nblk, const LithoNorm* __restrict__ norm, int n_out,
+                       int which, float* __restrict__ peak);
+
+// Synthesis of n_out Hermitian boxes of side 2 g0 + 1 into n x n images, with
+// the normalisation of `norm` (nullptr: scale 1), the raw peaks into `peak`
+// (may be nullptr when norm is) and `mid` (optional) recorded between the
+// peak pass and the writing pass. planes: synth_mma_bytes(n_out, n, g0) of
+// workspace. Requires synth_mma_ok(n, g0).
+cudaError_t launch_synth_mma(const float2* box, int g0, int n, int n_out, const float2* tw, const LithoNorm* norm,
+                             float* image, float* peak, float* blockmax, cudaStream_t s, cudaEvent_t mid,
+                             void* planes, int* status, int num_sms) {
+  const int kp = smma_kp(g0), nt = smma_nt(kp);
+  uint32_t* pp = static_cast<uint32_t*>(planes);
+  uint32_t* qp = reinterpret_cast<uint32_t*>(static_cast<char*>(planes) + align16((int64_t)n_out * n * kp * 8));
+  cudaError_t e;
+  const size_t smp = (size_t)(g0 + 1) * (n >> 5) * 8;
+  cudaFuncSetAttribute(k_synth_pplanes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp);
+  k_synth_pplanes<<<dim3((g0 + 1 + kPpWarps - 1) / kPpWarps, n_out), kPpWarps * 32, smp, s>>>(box, g0, n, tw, kp,
+                                                                                             nt, pp);
+  k_synth_qplanes<<<n / kSmMT, kSmMT, 0, s>>>(tw, g0, n, kp, qp);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const size_t smm = 2 * (size_t)(smma_a_bytes(kp) + smma_b_bytes(kp));
+  // split the x tiles of a (output, row tile) over blocks when there are
+  // fewer of those than SMs (at most nt / 32 ways, so the block maxima fit
+  // in n / 8 floats per output)
+  int xsplit = 1;
+  const int tiles = n_out * (n / nt);
+  while (tiles * xsplit < num_sms && xsplit * 2 <= n / kSmMT && xsplit * 2 <= nt / 32) xsplit *= 2;
+  const int units = tiles * xsplit;
+  const int grid = units < num_sms ? units : num_sms;
+  const int nblk = (n / nt) * xsplit * kSmDrainWarps;
+  const int pk_blocks = (n_out + 7) / 8;
+  auto pass = [&](auto pass_c) -> cudaError_t {
+    constexpr int P = decltype(pass_c)::value;
+    switch (n) {
+#define LITHO_SMMA(NN)                                                                                           \
+  case NN:                                                                                                       \
+    cudaFuncSetAttribute(k_synth_mma<P, NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smm);             \
+    k_synth_mma<P, NN><<<grid, kSmThreads, smm, s>>>(pp, qp, n_out, kp, xsplit, norm, peak, image, blockmax,     \
+                                                      status);                                                   \
+    break;
+      LITHO_SMMA(256) LITHO_SMMA(512) LITHO_SMMA(1024) LITHO_SMMA(2048) LITHO_SMMA(4096)
+#undef LITHO_SMMA
+      default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+  };
+  if (norm) {
+    if (!peak) return cudaErrorInvalidValue;
+    if ((e = pass(std::integral_constant<int, 0>{})) != cudaSuccess) return e;
+    k_peak<<<pk_blocks, 256, 0, s>>>(blockmax, nblk, norm, n_out, 1, peak);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  if (mid) cudaEventRecord(mid, s);
+  if ((e = pass(std::integral_constant<int, 1>{})) != cudaSuccess) return e;
+  if (peak) k_peak<<<pk_blocks, 256, 0, s>>>(blockmax, nblk, norm, n_out, norm ? 0 : -1, peak);
+  return cudaGetLastError();
+}
+
+}  // namespace litho

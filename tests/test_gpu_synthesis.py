@@ -1,0 +1,80 @@
+"""Band-limited synthesis through the C ABI (litho_band_synthesis) against
+numpy's inverse FFT of the same Hermitian box, over box half-widths, grid
+sizes and batch sizes that reach every synthesis engine: the tensor-core GEMM
+(large batches; K padded to 8, row tiles of 256, 128 and 64), the pair FFT,
+the direct kernel and the wide scatter + FFT.
+
+Bar: max |I_gpu - I_ref| / max |I_ref| <= 1e-5 (FP32 result; the tensor-core
+path splits operands into TF32 hi + lo).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def env():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from lithobat_b200 import _native as nat
+    return torch, nat
+
+
+def _hermitian_box(rng, h, n_fields):
+    G = 2 * h + 1
+    b = rng.standard_normal((n_fields, G, G)) + 1j * rng.standard_normal((n_fields, G, G))
+    g = np.arange(-h, h + 1)
+    b *= np.exp(-np.hypot(g[None, :, None], g[None, None, :]) / max(h, 1))[...]
+    b = 0.5 * (b + np.conj(b[:, ::-1, ::-1]))      # B(-g) = conj B(g)
+    b[:, h, h] = np.abs(b[:, h, h]) * 10
+    return b
+
+
+def _reference(box, n):
+    F, G, _ = box.shape
+    h = G // 2
+    spec = np.zeros((F, n, n), complex)
+    for iy, gy in enumerate(range(-h, h + 1)):
+        for ix, gx in enumerate(range(-h, h + 1)):
+            spec[:, gy % n, gx % n] += box[:, iy, ix]
+    return np.fft.ifft2(spec).real * n * n
+
+
+def _fields_for_tensor_cores(n):
+    """Fields that make the batch large enough for the tensor-core engine
+    (about 16 output tiles of 128 x 256 per SM)."""
+    return -(-16 * 148 // ((n // 256) * (n // 128)))
+
+
+@pytest.mark.parametrize("n,h,big", [(256, 0, True), (256, 3, True), (1024, 14, True), (512, 20, True),
+                                     (256, 31, True), (2048, 9, True), (4096, 5, True),
+                                     (256, 1, False), (1024, 14, False), (2048, 9, False),
+                                     (128, 7, False), (512, 40, False)])
+def test_band_synthesis_matches_numpy(env, n, h, big):
+    torch, nat = env
+    L = nat.lib()
+    rng = np.random.default_rng(n + h)
+    F = _fields_for_tensor_cores(n) if big else 3
+    box = _hermitian_box(rng, h, F)
+    check = sorted({0, F // 2, F - 1})
+    want = _reference(box[check], n)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    bx = torch.from_numpy(box.astype(np.complex64)).to(dev)
+    nb = C.c_size_t(0)
+    nat.check("litho_band_synthesis_workspace", L.litho_band_synthesis_workspace(F, n, C.byref(nb)))
+    ws = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+    out = torch.empty((F, n, n), dtype=torch.float32, device=dev)
+    nat.check("litho_band_synthesis", L.litho_band_synthesis(
+        bx.data_ptr(), F, n, h, 0, out.data_ptr(), ws.data_ptr(), ws.numel(), torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    assert int(ws[:4].view(torch.int32).item()) == 0          # no wait gave up
+    got = out[check].double().cpu().numpy()
+    err = float(np.abs(got - want).max() / np.abs(want).max())
+    assert err <= 1e-5, err
