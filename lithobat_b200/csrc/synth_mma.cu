@@ -15,9 +15,10 @@
 // lo hi): about 2^-22 relative error per product, FP32 accumulation in TMEM.
 //
 // Kernels:
-//   k_synth_pplanes : P for every output and row (column sums by 32-point
-//                     FFTs over residues), written in the MMA's shared-memory
-//                     layout so each nt x Kp tile is one bulk copy;
+//   k_synth_pplanes(_blk) : P for every output and row (column sums by
+//                     32-point FFTs over residues), written in the MMA's
+//                     shared-memory layout so each nt x Kp tile is one bulk
+//                     copy;
 //   k_synth_qplanes : Q for every x (the same for all outputs);
 //   k_synth_mma     : persistent, one CTA per SM; a CTA takes (output, row
 //                     tile) units and sweeps the x tiles: one thread loads
@@ -130,6 +131,77 @@ k_synth_pplanes(const float2* __restrict__ Bbox, int g0, int n, const float2* __
         p_put(tile, nt, kp, row, 2 * gx, -2.f * Q[a].y);
       }
     }
+  }
+}
+
+// The same planes with the column sums gathered per output in shared memory
+// first (C[gx][y] for all y), so each thread then writes whole 16-byte K
+// chunks of one row: one block per output, used when C fits in shared memory.
+constexpr int kPbWarps = 8;
+
+__host__ __device__ inline size_t pblk_smem(int n, int g0) {
+  const int gp = g0 + 1;
+  return (size_t)gp * n * 8 + (size_t)gp * (n >> 5) * 8 + (size_t)kPbWarps * (2 * kSmG0Max + 2) * 8;
+}
+
+__global__ void __launch_bounds__(kPbWarps * 32)
+k_synth_pplanes_blk(const float2* __restrict__ Bbox, int g0, int n, const float2* __restrict__ tw_inv, int kp,
+                    int nt, uint32_t* __restrict__ planes) {
+  extern __shared__ float2 pb_sm[];
+  const int gp = g0 + 1, G = 2 * g0 + 1, M = n >> 5, nmask = n - 1;
+  float2* Cs = pb_sm;                      // [gx][y]
+  float2* TB = Cs + (size_t)gp * n;        // [g][b] = w^(g b)
+  float2* colb = TB + (size_t)gp * M;      // [warp][gy + g0]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, o = blockIdx.x;
+  for (int j = threadIdx.x; j < gp * M; j += blockDim.x) {
+    const int g = j / M, b = j % M;
+    TB[j] = __ldg(tw_inv + ((g * b) & nmask));
+  }
+  __syncthreads();
+  float2* cw0 = colb + warp * (2 * kSmG0Max + 2);
+  for (int gx = warp; gx < gp; gx += kPbWarps) {
+    const float2* bc = Bbox + (size_t)o * G * G + gx + g0;
+    for (int i = lane; i < G; i += 32) cw0[i] = bc[(size_t)i * G];
+    __syncwarp();
+    const float2* cw = cw0 + g0;
+    for (int b = lane; b < M; b += 32) {
+      float2 Q[32];
+#pragma unroll
+      for (int i = 0; i < 32; ++i) Q[i] = make_float2(0.f, 0.f);
+      Q[0] = cw[0];
+#pragma unroll
+      for (int g = 1; g <= kSmG0Max; ++g) {
+        if (g <= g0) {
+          const float2 t = TB[g * M + b];
+          Q[g & 31] = cadd(Q[g & 31], cmul(cw[g], t));
+          Q[(-g) & 31] = cadd(Q[(-g) & 31], cmulc(cw[-g], t));
+        }
+      }
+      fft_reg<32, +1>(Q);
+#pragma unroll
+      for (int a = 0; a < 32; ++a) Cs[(size_t)gx * n + b + M * a] = Q[a];
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  const int K = G, nck = kp >> 2;
+  uint32_t* base = planes + (size_t)o * (n / nt) * ((size_t)nt * kp * 2);
+  for (int id = threadIdx.x; id < nck * n; id += blockDim.x) {
+    const int y = id % n, c = id / n;
+    uint32_t hv[4], lv[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int k = 4 * c + q;
+      float f = 0.f;
+      if (k == 0) f = Cs[y].x;
+      else if (k < K) f = (k & 1) ? 2.f * Cs[(size_t)((k + 1) >> 1) * n + y].x : -2.f * Cs[(size_t)(k >> 1) * n + y].y;
+      hv[q] = to_tf32(f);
+      lv[q] = to_tf32(f - __uint_as_float(hv[q]));
+    }
+    uint32_t* tile = base + (size_t)(y / nt) * ((size_t)nt * kp * 2);
+    const uint32_t off = smma_off(nt, y % nt, 4 * c) >> 2;
+    *reinterpret_cast<uint4*>(tile + off) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+    *reinterpret_cast<uint4*>(tile + (size_t)nt * kp + off) = make_uint4(lv[0], lv[1], lv[2], lv[3]);
   }
 }
 
@@ -363,10 +435,16 @@ cudaError_t launch_synth_mma(const float2* box, int g0, int n, int n_out, const 
   uint32_t* pp = static_cast<uint32_t*>(planes);
   uint32_t* qp = reinterpret_cast<uint32_t*>(static_cast<char*>(planes) + align16((int64_t)n_out * n * kp * 8));
   cudaError_t e;
-  const size_t smp = (size_t)(g0 + 1) * (n >> 5) * 8;
-  cudaFuncSetAttribute(k_synth_pplanes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp);
-  k_synth_pplanes<<<dim3((g0 + 1 + kPpWarps - 1) / kPpWarps, n_out), kPpWarps * 32, smp, s>>>(box, g0, n, tw, kp,
-                                                                                             nt, pp);
+  const size_t smb = pblk_smem(n, g0);
+  if (smb <= 200 * 1024) {
+    cudaFuncSetAttribute(k_synth_pplanes_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb);
+    k_synth_pplanes_blk<<<n_out, kPbWarps * 32, smb, s>>>(box, g0, n, tw, kp, nt, pp);
+  } else {
+    const size_t smp = (size_t)(g0 + 1) * (n >> 5) * 8;
+    cudaFuncSetAttribute(k_synth_pplanes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp);
+    k_synth_pplanes<<<dim3((g0 + 1 + kPpWarps - 1) / kPpWarps, n_out), kPpWarps * 32, smp, s>>>(box, g0, n, tw,
+                                                                                               kp, nt, pp);
+  }
   k_synth_qplanes<<<n / kSmMT, kSmMT, 0, s>>>(tw, g0, n, kp, qp);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const size_t smm = 2 * (size_t)(smma_a_bytes(kp) + smma_b_bytes(kp));
