@@ -10,25 +10,31 @@
 //     Q[x] = [1, cos(2 pi x / N), sin(2 pi x / N), cos(4 pi x / N), ...],
 //     P[y] = [Re C(0, y), 2 Re C(1, y), -2 Im C(1, y), 2 Re C(2, y), ...],
 // i.e. a GEMM with M = N = image side and K = 2 g0 + 1 (padded to Kp, a
-// multiple of 8). It runs as tcgen05.mma kind::tf32 with every operand split
-// into TF32 hi + lo planes and three products per K step (hi hi + hi lo +
-// lo hi): about 2^-22 relative error per product, FP32 accumulation in TMEM.
+// multiple of 16). It runs as tcgen05.mma kind::f16 with every operand split
+// into FP16 hi + lo planes and three products per K step (hi hi + hi lo +
+// lo hi), FP32 accumulation in TMEM: about 2^-22 of the largest term, the
+// accuracy of FP32 operands. P is scaled per output by a power of two so that
+// its bound 2 max_gx sum_gy |B(gx, gy)| stays below 2^14; the drain undoes it
+// exactly. FP16 runs the tensor cores at twice the TF32 rate with half the
+// operand bytes.
 //
 // Kernels:
 //   k_synth_pplanes(_blk) : P for every output and row (column sums by
 //                     32-point FFTs over residues), written in the MMA's
-//                     shared-memory layout so each nt x Kp tile is one bulk
-//                     copy;
+//                     shared-memory layout so each 256 x Kp tile is one bulk
+//                     copy, and the output's scale;
 //   k_synth_qplanes : Q for every x (the same for all outputs);
 //   k_synth_mma     : persistent, one CTA per SM; a CTA takes (output, row
-//                     tile) units and sweeps the x tiles: one thread loads
-//                     operand tiles (cp.async.bulk, double-buffered), one
-//                     thread issues the MMAs into two TMEM accumulators, four
-//                     warps drain the accumulators (tcgen05.ld), scale, store
-//                     coalesced rows of the image and keep the maxima.
+//                     tile, x range) units: one thread loads operand tiles
+//                     (cp.async.bulk, double-buffered), one thread issues the
+//                     MMAs into two TMEM accumulators, four warps drain the
+//                     accumulators (tcgen05.ld), scale, store coalesced rows
+//                     of the image and keep the maxima.
 // Peak normalisation needs the peak before the scaled image is written:
 // pass 0 computes only the maxima, pass 1 writes. Every wait is bounded and a
 // wait that gives up reports LITHO_E_TIMEOUT through the status word.
+#include <cuda_fp16.h>
+
 #include <type_traits>
 
 #include "common.cuh"
@@ -37,98 +43,138 @@
 
 namespace litho {
 
-constexpr int kSmMT = 128;       // x rows per tile (MMA M)
-constexpr int kSmG0Max = 31;     // box half-width limit (K = 2 g0 + 1 <= 63)
+constexpr int kSmMT = 128;        // x rows per tile (MMA M)
+constexpr int kSmNT = 256;        // image rows per tile (MMA N)
+constexpr int kSmG0Max = 31;      // box half-width limit (K = 2 g0 + 1 <= 63)
 constexpr int kSmDrainWarps = 4;  // warp w drains TMEM lanes 32 w .. 32 w + 31
 constexpr int kSmThreads = (kSmDrainWarps + 2) * 32;  // + one loading warp and one MMA warp
 
-
-__host__ __device__ inline int smma_kp(int g0) { return (2 * g0 + 1 + 7) & ~7; }
-// rows per tile (MMA N): two A and two B buffers stay within 192 KiB
-__host__ __device__ inline int smma_nt(int kp) { return kp <= 32 ? 256 : (kp <= 48 ? 128 : 64); }
-__host__ __device__ inline uint32_t smma_a_bytes(int kp) { return (uint32_t)kSmMT * kp * 8; }
-__host__ __device__ inline uint32_t smma_b_bytes(int kp) { return (uint32_t)smma_nt(kp) * kp * 8; }
+__host__ __device__ inline int smma_kp(int g0) { return (2 * g0 + 1 + 15) & ~15; }
+// bytes of one operand tile (hi and lo planes, FP16)
+__host__ __device__ inline uint32_t smma_a_bytes(int kp) { return (uint32_t)kSmMT * kp * 4; }
+__host__ __device__ inline uint32_t smma_b_bytes(int kp) { return (uint32_t)kSmNT * kp * 4; }
 // byte offset of element (row, k) in one plane of a tile of R rows: K-major
-// core matrices (8 rows x 16 bytes), 16-byte K chunks R * 16 bytes apart
+// core matrices (8 rows x 16 bytes = 8 FP16), 16-byte K chunks R * 16 bytes apart
 __host__ __device__ inline uint32_t smma_off(int R, int row, int k) {
-  return (uint32_t)((k >> 2) * (R * 16) + row * 16 + (k & 3) * 4);
+  return (uint32_t)((k >> 3) * (R * 16) + row * 16 + (k & 7) * 2);
 }
 
 bool synth_mma_ok(int n, int g0) {
-  return g0 >= 0 && g0 <= kSmG0Max && n >= 256 && n <= 4096 && (n & (n - 1)) == 0;
+  return g0 >= 0 && g0 <= kSmG0Max && n >= kSmNT && n <= 4096 && (n & (n - 1)) == 0;
 }
 
 // Worth it when there are enough 128 x 256 output tiles to keep every SM's
 // MMA and drain pipeline busy (about 16 per SM); smaller batches use the
 // pair synthesis, whose fixed costs are lower.
 bool synth_mma_pick(int n_out, int n, int g0) {
-  return synth_mma_ok(n, g0) && (int64_t)n_out * (n / 256) * (n / kSmMT) >= 16 * 148;
+  return synth_mma_ok(n, g0) && (int64_t)n_out * (n / kSmNT) * (n / kSmMT) >= 16 * 148;
 }
+
+// P planes, then Q planes, then the per-output inverse scales.
+static int64_t pplanes_bytes(int n_out, int n, int kp) { return align16((int64_t)n_out * n * kp * 4); }
+static int64_t qplanes_bytes(int n, int kp) { return align16((int64_t)n * kp * 4); }
 
 int64_t synth_mma_bytes(int n_out, int n, int g0) {
   const int kp = smma_kp(g0);
-  return align16((int64_t)n_out * n * kp * 8) + align16((int64_t)n * kp * 8);
+  return pplanes_bytes(n_out, n, kp) + qplanes_bytes(n, kp) + align16((int64_t)n_out * 4);
 }
 
-// P planes: [output][row tile][hi | lo][chunk][row][4] (row tile of nt rows).
+__device__ __forceinline__ void split_f16(float v, __half& hi, __half& lo) {
+  hi = __float2half_rn(v);
+  lo = __float2half_rn(v - __half2float(hi));
+}
+
+// Power-of-two scale for output o's P values, from the bound
+// |P_k(y)| <= 2 max_gx sum_gy |B(gx, gy)|, computed the same way in every
+// block. Contains a __syncthreads.
+__device__ float p_scale(const float2* __restrict__ Bo, int g0, float* red) {
+  const int G = 2 * g0 + 1;
+  if (threadIdx.x <= g0) {
+    float sum = 0.f;
+    for (int i = 0; i < G; ++i) {
+      const float2 b = Bo[(size_t)i * G + threadIdx.x + g0];
+      sum += sqrtf(b.x * b.x + b.y * b.y);
+    }
+    red[threadIdx.x] = sum;
+  }
+  __syncthreads();
+  float m = 0.f;
+  for (int i = 0; i <= g0; ++i) m = fmaxf(m, red[i]);
+  m *= 2.f;
+  if (!(m > 0.f) || !isfinite(m)) return 1.f;
+  int e;
+  frexpf(m, &e);               // m < 2^e
+  return ldexpf(1.f, 14 - e);  // scaled bound < 2^14
+}
+
+// P planes: [output][row tile][hi | lo][chunk][row][8] (row tile of 256 rows).
 // The column sums C(gx, y) come from 32-point FFTs over residues: with
 // N = 32 M and y = b + M a, C(gx, b + M a) = sum_r w32^(r a) S_b(r),
 // S_b(r) = sum_{gy = r mod 32} B(gx, gy) w^(gy b), one FFT per residue b held
-// in a lane's registers. One warp per (output, gx); the gx = 0 warp also
-// writes the zero padding K <= k < Kp.
+// in a lane's registers.
+__device__ __forceinline__ void column_fft(const float2* cw, const float2* TB, int g0, int M, int b,
+                                           float2 (&Q)[32]) {
+#pragma unroll
+  for (int i = 0; i < 32; ++i) Q[i] = make_float2(0.f, 0.f);
+  Q[0] = cw[0];
+#pragma unroll
+  for (int g = 1; g <= kSmG0Max; ++g) {
+    if (g <= g0) {
+      const float2 t = TB[g * M + b];
+      Q[g & 31] = cadd(Q[g & 31], cmul(cw[g], t));
+      Q[(-g) & 31] = cadd(Q[(-g) & 31], cmulc(cw[-g], t));
+    }
+  }
+  fft_reg<32, +1>(Q);
+}
+
+// One warp per (output, gx), scattered 2-byte stores; the gx = 0 warp also
+// writes the zero padding K <= k < Kp. For grids whose column sums do not fit
+// in shared memory.
 constexpr int kPpWarps = 8;
 
-__device__ __forceinline__ void p_put(uint32_t* tile, int nt, int kp, int row, int k, float v) {
-  const uint32_t h = to_tf32(v);
-  const uint32_t o = smma_off(nt, row, k) >> 2;
+__device__ __forceinline__ void p_put(__half* tile, int kp, int row, int k, float v) {
+  __half h, l;
+  split_f16(v, h, l);
+  const uint32_t o = smma_off(kSmNT, row, k) >> 1;
   tile[o] = h;
-  tile[(size_t)nt * kp + o] = to_tf32(v - __uint_as_float(h));
+  tile[(size_t)kSmNT * kp + o] = l;
 }
 
 __global__ void __launch_bounds__(kPpWarps * 32)
-k_synth_pplanes(const float2* __restrict__ Bbox, int g0, int n, const float2* __restrict__ tw_inv, int kp, int nt,
-                uint32_t* __restrict__ planes) {
+k_synth_pplanes(const float2* __restrict__ Bbox, int g0, int n, const float2* __restrict__ tw_inv, int kp,
+                __half* __restrict__ planes, float* __restrict__ inv_scale) {
   extern __shared__ float2 pp_tb[];                     // [g][b] = w^(g b), g = 0..g0
   __shared__ float2 col[kPpWarps][2 * kSmG0Max + 2];    // B(gx, gy + g0) of each warp's column
+  __shared__ float red[kSmG0Max + 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int o = blockIdx.y, gx = blockIdx.x * kPpWarps + warp;
   const int gp = g0 + 1, G = 2 * g0 + 1, M = n >> 5, nmask = n - 1;
+  const float2* Bo = Bbox + (size_t)o * G * G;
   for (int j = threadIdx.x; j < gp * M; j += blockDim.x) {
     const int g = j / M, b = j % M;
     pp_tb[j] = __ldg(tw_inv + ((g * b) & nmask));
   }
-  if (gx < gp) {
-    const float2* bc = Bbox + (size_t)o * G * G + gx + g0;
-    for (int i = lane; i < G; i += 32) col[warp][i] = bc[(size_t)i * G];
-  }
-  __syncthreads();
+  if (gx < gp)
+    for (int i = lane; i < G; i += 32) col[warp][i] = Bo[(size_t)i * G + gx + g0];
+  const float sc = p_scale(Bo, g0, red);
+  if (blockIdx.x == 0 && threadIdx.x == 0) inv_scale[o] = 1.f / sc;
   if (gx >= gp) return;
   const float2* cw = col[warp] + g0;
-  uint32_t* base = planes + (size_t)o * (n / nt) * ((size_t)nt * kp * 2);
+  __half* base = planes + (size_t)o * (n / kSmNT) * ((size_t)kSmNT * kp * 2);
   for (int b = lane; b < M; b += 32) {
     float2 Q[32];
-#pragma unroll
-    for (int i = 0; i < 32; ++i) Q[i] = make_float2(0.f, 0.f);
-    Q[0] = cw[0];
-#pragma unroll
-    for (int g = 1; g <= kSmG0Max; ++g) {
-      if (g <= g0) {
-        const float2 t = pp_tb[g * M + b];
-        Q[g & 31] = cadd(Q[g & 31], cmul(cw[g], t));
-        Q[(-g) & 31] = cadd(Q[(-g) & 31], cmulc(cw[-g], t));
-      }
-    }
-    fft_reg<32, +1>(Q);
+    column_fft(cw, pp_tb, g0, M, b, Q);
 #pragma unroll
     for (int a = 0; a < 32; ++a) {
-      const int y = b + M * a, row = y % nt;
-      uint32_t* tile = base + (size_t)(y / nt) * ((size_t)nt * kp * 2);
+      const int y = b + M * a, row = y % kSmNT;
+      __half* tile = base + (size_t)(y / kSmNT) * ((size_t)kSmNT * kp * 2);
       if (gx == 0) {
-        p_put(tile, nt, kp, row, 0, Q[a].x);
-        for (int k = G; k < kp; ++k) p_put(tile, nt, kp, row, k, 0.f);
+        p_put(tile, kp, row, 0, Q[a].x * sc);
+        for (int k = G; k < kp; ++k) p_put(tile, kp, row, k, 0.f);
       } else {
-        p_put(tile, nt, kp, row, 2 * gx - 1, 2.f * Q[a].x);
-        p_put(tile, nt, kp, row, 2 * gx, -2.f * Q[a].y);
+        p_put(tile, kp, row, 2 * gx - 1, 2.f * Q[a].x * sc);
+        p_put(tile, kp, row, 2 * gx, -2.f * Q[a].y * sc);
       }
     }
   }
@@ -146,77 +192,68 @@ __host__ __device__ inline size_t pblk_smem(int n, int g0) {
 
 __global__ void __launch_bounds__(kPbWarps * 32)
 k_synth_pplanes_blk(const float2* __restrict__ Bbox, int g0, int n, const float2* __restrict__ tw_inv, int kp,
-                    int nt, uint32_t* __restrict__ planes) {
+                    __half* __restrict__ planes, float* __restrict__ inv_scale) {
   extern __shared__ float2 pb_sm[];
+  __shared__ float red[kSmG0Max + 1];
   const int gp = g0 + 1, G = 2 * g0 + 1, M = n >> 5, nmask = n - 1;
   float2* Cs = pb_sm;                      // [gx][y]
   float2* TB = Cs + (size_t)gp * n;        // [g][b] = w^(g b)
   float2* colb = TB + (size_t)gp * M;      // [warp][gy + g0]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, o = blockIdx.x;
+  const float2* Bo = Bbox + (size_t)o * G * G;
   for (int j = threadIdx.x; j < gp * M; j += blockDim.x) {
     const int g = j / M, b = j % M;
     TB[j] = __ldg(tw_inv + ((g * b) & nmask));
   }
-  __syncthreads();
+  const float sc = p_scale(Bo, g0, red);
+  if (threadIdx.x == 0) inv_scale[o] = 1.f / sc;
   float2* cw0 = colb + warp * (2 * kSmG0Max + 2);
   for (int gx = warp; gx < gp; gx += kPbWarps) {
-    const float2* bc = Bbox + (size_t)o * G * G + gx + g0;
-    for (int i = lane; i < G; i += 32) cw0[i] = bc[(size_t)i * G];
+    for (int i = lane; i < G; i += 32) cw0[i] = Bo[(size_t)i * G + gx + g0];
     __syncwarp();
-    const float2* cw = cw0 + g0;
     for (int b = lane; b < M; b += 32) {
       float2 Q[32];
-#pragma unroll
-      for (int i = 0; i < 32; ++i) Q[i] = make_float2(0.f, 0.f);
-      Q[0] = cw[0];
-#pragma unroll
-      for (int g = 1; g <= kSmG0Max; ++g) {
-        if (g <= g0) {
-          const float2 t = TB[g * M + b];
-          Q[g & 31] = cadd(Q[g & 31], cmul(cw[g], t));
-          Q[(-g) & 31] = cadd(Q[(-g) & 31], cmulc(cw[-g], t));
-        }
-      }
-      fft_reg<32, +1>(Q);
+      column_fft(cw0 + g0, TB, g0, M, b, Q);
 #pragma unroll
       for (int a = 0; a < 32; ++a) Cs[(size_t)gx * n + b + M * a] = Q[a];
     }
     __syncwarp();
   }
   __syncthreads();
-  const int K = G, nck = kp >> 2;
-  uint32_t* base = planes + (size_t)o * (n / nt) * ((size_t)nt * kp * 2);
+  const int K = G, nck = kp >> 3;
+  __half* base = planes + (size_t)o * (n / kSmNT) * ((size_t)kSmNT * kp * 2);
   for (int id = threadIdx.x; id < nck * n; id += blockDim.x) {
     const int y = id % n, c = id / n;
-    uint32_t hv[4], lv[4];
+    __align__(16) __half hv[8];
+    __align__(16) __half lv[8];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int k = 4 * c + q;
+    for (int q = 0; q < 8; ++q) {
+      const int k = 8 * c + q;
       float f = 0.f;
       if (k == 0) f = Cs[y].x;
       else if (k < K) f = (k & 1) ? 2.f * Cs[(size_t)((k + 1) >> 1) * n + y].x : -2.f * Cs[(size_t)(k >> 1) * n + y].y;
-      hv[q] = to_tf32(f);
-      lv[q] = to_tf32(f - __uint_as_float(hv[q]));
+      split_f16(f * sc, hv[q], lv[q]);
     }
-    uint32_t* tile = base + (size_t)(y / nt) * ((size_t)nt * kp * 2);
-    const uint32_t off = smma_off(nt, y % nt, 4 * c) >> 2;
-    *reinterpret_cast<uint4*>(tile + off) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
-    *reinterpret_cast<uint4*>(tile + (size_t)nt * kp + off) = make_uint4(lv[0], lv[1], lv[2], lv[3]);
+    __half* tile = base + (size_t)(y / kSmNT) * ((size_t)kSmNT * kp * 2);
+    const uint32_t off = smma_off(kSmNT, y % kSmNT, 8 * c) >> 1;
+    *reinterpret_cast<uint4*>(tile + off) = *reinterpret_cast<const uint4*>(hv);
+    *reinterpret_cast<uint4*>(tile + (size_t)kSmNT * kp + off) = *reinterpret_cast<const uint4*>(lv);
   }
 }
 
-// Q planes: [x tile][hi | lo][chunk][row][4], identical for every output.
+// Q planes: [x tile][hi | lo][chunk][row][8], identical for every output.
 __global__ void __launch_bounds__(kSmMT)
-k_synth_qplanes(const float2* __restrict__ tw, int g0, int n, int kp, uint32_t* __restrict__ planes) {
+k_synth_qplanes(const float2* __restrict__ tw, int g0, int n, int kp, __half* __restrict__ planes) {
   const int x = blockIdx.x * kSmMT + threadIdx.x;
   const int K = 2 * g0 + 1, nmask = n - 1;
-  uint32_t* hi = planes + (size_t)blockIdx.x * kSmMT * kp * 2;
-  uint32_t* lo = hi + (size_t)kSmMT * kp;
-  for (int c = 0; c < kp / 4; ++c) {
-    uint32_t h[4], l[4];
+  __half* hi = planes + (size_t)blockIdx.x * kSmMT * kp * 2;
+  __half* lo = hi + (size_t)kSmMT * kp;
+  for (int c = 0; c < kp / 8; ++c) {
+    __align__(16) __half h[8];
+    __align__(16) __half l[8];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int k = 4 * c + q;
+    for (int q = 0; q < 8; ++q) {
+      const int k = 8 * c + q;
       float f = 0.f;
       if (k == 0) {
         f = 1.f;
@@ -225,13 +262,20 @@ k_synth_qplanes(const float2* __restrict__ tw, int g0, int n, int kp, uint32_t* 
         const float2 w = tw[(g * x) & nmask];
         f = (k & 1) ? w.x : w.y;
       }
-      h[q] = to_tf32(f);
-      l[q] = to_tf32(f - __uint_as_float(h[q]));
+      split_f16(f, h[q], l[q]);
     }
-    const uint32_t o = smma_off(kSmMT, threadIdx.x, 4 * c) >> 2;
-    *reinterpret_cast<uint4*>(hi + o) = make_uint4(h[0], h[1], h[2], h[3]);
-    *reinterpret_cast<uint4*>(lo + o) = make_uint4(l[0], l[1], l[2], l[3]);
+    const uint32_t o = smma_off(kSmMT, threadIdx.x, 8 * c) >> 1;
+    *reinterpret_cast<uint4*>(hi + o) = *reinterpret_cast<const uint4*>(h);
+    *reinterpret_cast<uint4*>(lo + o) = *reinterpret_cast<const uint4*>(l);
   }
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
 // PASS 0: maxima of peak-normalised outputs only (others skipped).
@@ -242,15 +286,16 @@ k_synth_qplanes(const float2* __restrict__ tw, int g0, int n, int kp, uint32_t* 
 // become immediates).
 template <int PASS, int N>
 __global__ void __launch_bounds__(kSmThreads, 1)
-k_synth_mma(const uint32_t* __restrict__ pplanes, const uint32_t* __restrict__ qplanes, int n_out, int kp,
-            int xsplit, const LithoNorm* __restrict__ norm, const float* __restrict__ peak, float* __restrict__ image,
-            float* __restrict__ blockmax, int* __restrict__ status) {
+k_synth_mma(const __half* __restrict__ pplanes, const __half* __restrict__ qplanes,
+            const float* __restrict__ inv_scale, int n_out, int kp, int xsplit, const LithoNorm* __restrict__ norm,
+            const float* __restrict__ peak, float* __restrict__ image, float* __restrict__ blockmax,
+            int* __restrict__ status) {
   extern __shared__ __align__(1024) unsigned char sm_raw[];
   __shared__ uint64_t bar_bfull[2], bar_bempty[2], bar_afull[2], bar_aempty[2], bar_accfull[2], bar_accempty[2];
   __shared__ uint64_t bar_drain;
   __shared__ uint32_t s_tmem;
   __shared__ volatile int s_fail;
-  const int nt = smma_nt(kp);
+  constexpr int nt = kSmNT;
   const uint32_t abytes = smma_a_bytes(kp), bbytes = smma_b_bytes(kp);
   unsigned char* bufB0 = sm_raw;
   unsigned char* bufA0 = sm_raw + 2 * bbytes;
@@ -298,13 +343,13 @@ k_synth_mma(const uint32_t* __restrict__ pplanes, const uint32_t* __restrict__ q
         const int ib = i & 1;
         if (i >= 2 && !mbar_wait(&bar_bempty[ib], ((i >> 1) - 1) & 1)) { ok = false; break; }
         mbar_expect_tx(&bar_bfull[ib], bbytes);
-        bulk_g2s(bufB0 + ib * bbytes, pplanes + (size_t)(u / xsplit) * (bbytes >> 2), bbytes, &bar_bfull[ib]);
+        bulk_g2s(bufB0 + ib * bbytes, pplanes + (size_t)(u / xsplit) * (bbytes >> 1), bbytes, &bar_bfull[ib]);
         ++i;
         for (int j = (u % xsplit) * xper; j < (u % xsplit + 1) * xper; ++j) {
           const int ab = a & 1;
           if (s_fail || (a >= 2 && !mbar_wait(&bar_aempty[ab], ((a >> 1) - 1) & 1))) { ok = false; break; }
           mbar_expect_tx(&bar_afull[ab], abytes);
-          bulk_g2s(bufA0 + ab * abytes, qplanes + (size_t)j * (abytes >> 2), abytes, &bar_afull[ab]);
+          bulk_g2s(bufA0 + ab * abytes, qplanes + (size_t)j * (abytes >> 1), abytes, &bar_afull[ab]);
           ++a;
         }
       }
@@ -318,8 +363,8 @@ k_synth_mma(const uint32_t* __restrict__ pplanes, const uint32_t* __restrict__ q
   } else if (warp == kSmDrainWarps + 1) {
     // ---- MMA issue --------------------------------------------------------
     if (lane == 0) {
-      const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(nt >> 3) << 17) |
-                             ((uint32_t)(kSmMT >> 4) << 24);
+      // D f32, A and B f16, both K-major, N = 256, M = 128
+      const uint32_t idesc = (1u << 4) | ((uint32_t)(nt >> 3) << 17) | ((uint32_t)(kSmMT >> 4) << 24);
       int i = 0, a = 0, c = 0;
       bool ok = true;
       for (int u = blockIdx.x; u < n_units && ok; u += gridDim.x) {
@@ -337,13 +382,13 @@ k_synth_mma(const uint32_t* __restrict__ pplanes, const uint32_t* __restrict__ q
           tc_fence_after();
           const uint32_t ah0 = smem_u32(bufA0 + ab * abytes), al0 = ah0 + (abytes >> 1);
           const uint32_t d = tmem + (uint32_t)(cb * nt);
-          for (int s = 0; s < kp / 8; ++s) {
+          for (int s = 0; s < kp / 16; ++s) {
             const uint32_t ao = (uint32_t)s * 2 * (kSmMT * 16), bo = (uint32_t)s * 2 * (nt * 16);
             const uint64_t ah = umma_desc(ah0 + ao, kSmMT * 16, 128), al = umma_desc(al0 + ao, kSmMT * 16, 128);
             const uint64_t bh = umma_desc(bh0 + bo, nt * 16, 128), bl = umma_desc(bl0 + bo, nt * 16, 128);
-            umma_tf32(d, ah, bh, idesc, s > 0 ? 1u : 0u);
-            umma_tf32(d, ah, bl, idesc, 1u);
-            umma_tf32(d, al, bh, idesc, 1u);
+            umma_f16(d, ah, bh, idesc, s > 0 ? 1u : 0u);
+            umma_f16(d, ah, bl, idesc, 1u);
+            umma_f16(d, al, bh, idesc, 1u);
           }
           umma_commit(&bar_accfull[cb]);
           umma_commit(&bar_aempty[ab]);
@@ -369,14 +414,15 @@ k_synth_mma(const uint32_t* __restrict__ pplanes, const uint32_t* __restrict__ q
       if (!live(u)) continue;
       const int tile = u / xsplit, xs = u % xsplit;
       const int o = tile / yt_per, y0 = (tile % yt_per) * nt;
-      float sc = 1.f;
-      bool want_max = true;   // the writing pass of a peak-normalised output has its peak already
+      const float inv = inv_scale[o];  // a power of two: exact
+      float sc = inv;
+      bool want_max = true;  // the writing pass of a peak-normalised output has its peak already
       if (PASS == 1) {
         const LithoNorm nm = norm ? norm[o] : LithoNorm{0, 1.0f};
-        sc = nm.scale;
+        sc = nm.scale * inv;
         if (nm.mode == 1) {
           const float pk = peak[o];
-          sc = pk > 0.f ? nm.scale / pk : nm.scale;
+          sc = (pk > 0.f ? nm.scale / pk : nm.scale) * inv;
           want_max = false;
         }
       }
@@ -409,7 +455,7 @@ k_synth_mma(const uint32_t* __restrict__ pplanes, const uint32_t* __restrict__ q
       if (!ok) break;
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-      if (lane == 0) blockmax[(size_t)u * kSmDrainWarps + warp] = mx;
+      if (lane == 0) blockmax[(size_t)u * kSmDrainWarps + warp] = mx * inv;
     }
     if (!ok) s_fail = 1;
   }
@@ -431,32 +477,34 @@ __global__ void k_peak(const float* __restrict__ blockmax, int nblk, const Litho
 cudaError_t launch_synth_mma(const float2* box, int g0, int n, int n_out, const float2* tw, const LithoNorm* norm,
                              float* image, float* peak, float* blockmax, cudaStream_t s, cudaEvent_t mid,
                              void* planes, int* status, int num_sms) {
-  const int kp = smma_kp(g0), nt = smma_nt(kp);
-  uint32_t* pp = static_cast<uint32_t*>(planes);
-  uint32_t* qp = reinterpret_cast<uint32_t*>(static_cast<char*>(planes) + align16((int64_t)n_out * n * kp * 8));
+  const int kp = smma_kp(g0);
+  char* pb = static_cast<char*>(planes);
+  __half* pp = reinterpret_cast<__half*>(pb);
+  __half* qp = reinterpret_cast<__half*>(pb + pplanes_bytes(n_out, n, kp));
+  float* inv = reinterpret_cast<float*>(pb + pplanes_bytes(n_out, n, kp) + qplanes_bytes(n, kp));
   cudaError_t e;
   const size_t smb = pblk_smem(n, g0);
   if (smb <= 200 * 1024) {
     cudaFuncSetAttribute(k_synth_pplanes_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb);
-    k_synth_pplanes_blk<<<n_out, kPbWarps * 32, smb, s>>>(box, g0, n, tw, kp, nt, pp);
+    k_synth_pplanes_blk<<<n_out, kPbWarps * 32, smb, s>>>(box, g0, n, tw, kp, pp, inv);
   } else {
     const size_t smp = (size_t)(g0 + 1) * (n >> 5) * 8;
     cudaFuncSetAttribute(k_synth_pplanes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp);
     k_synth_pplanes<<<dim3((g0 + 1 + kPpWarps - 1) / kPpWarps, n_out), kPpWarps * 32, smp, s>>>(box, g0, n, tw,
-                                                                                               kp, nt, pp);
+                                                                                               kp, pp, inv);
   }
   k_synth_qplanes<<<n / kSmMT, kSmMT, 0, s>>>(tw, g0, n, kp, qp);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const size_t smm = 2 * (size_t)(smma_a_bytes(kp) + smma_b_bytes(kp));
   // split the x tiles of a (output, row tile) over blocks when there are
-  // fewer of those than SMs (at most nt / 32 ways, so the block maxima fit
-  // in n / 8 floats per output)
+  // fewer of those than SMs (at most 8 ways, so the block maxima fit in
+  // n / 8 floats per output)
   int xsplit = 1;
-  const int tiles = n_out * (n / nt);
-  while (tiles * xsplit < num_sms && xsplit * 2 <= n / kSmMT && xsplit * 2 <= nt / 32) xsplit *= 2;
+  const int tiles = n_out * (n / kSmNT);
+  while (tiles * xsplit < num_sms && xsplit * 2 <= n / kSmMT && xsplit * 2 <= kSmNT / 32) xsplit *= 2;
   const int units = tiles * xsplit;
   const int grid = units < num_sms ? units : num_sms;
-  const int nblk = (n / nt) * xsplit * kSmDrainWarps;
+  const int nblk = (n / kSmNT) * xsplit * kSmDrainWarps;
   const int pk_blocks = (n_out + 7) / 8;
   auto pass = [&](auto pass_c) -> cudaError_t {
     constexpr int P = decltype(pass_c)::value;
@@ -464,8 +512,8 @@ cudaError_t launch_synth_mma(const float2* box, int g0, int n, int n_out, const 
 #define LITHO_SMMA(NN)                                                                                           \
   case NN:                                                                                                       \
     cudaFuncSetAttribute(k_synth_mma<P, NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smm);             \
-    k_synth_mma<P, NN><<<grid, kSmThreads, smm, s>>>(pp, qp, n_out, kp, xsplit, norm, peak, image, blockmax,     \
-                                                      status);                                                   \
+    k_synth_mma<P, NN><<<grid, kSmThreads, smm, s>>>(pp, qp, inv, n_out, kp, xsplit, norm, peak, image,          \
+                                                      blockmax, status);                                         \
     break;
       LITHO_SMMA(256) LITHO_SMMA(512) LITHO_SMMA(1024) LITHO_SMMA(2048) LITHO_SMMA(4096)
 #undef LITHO_SMMA

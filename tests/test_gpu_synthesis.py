@@ -1,11 +1,11 @@
 """Band-limited synthesis through the C ABI (litho_band_synthesis) against
 numpy's inverse FFT of the same Hermitian box, over box half-widths, grid
 sizes and batch sizes that reach every synthesis engine: the tensor-core GEMM
-(large batches; K padded to 8, row tiles of 256, 128 and 64), the pair FFT,
+(large batches; K padded to 16), the pair FFT,
 the direct kernel and the wide scatter + FFT.
 
 Bar: max |I_gpu - I_ref| / max |I_ref| <= 1e-5 (FP32 result; the tensor-core
-path splits operands into TF32 hi + lo).
+path splits operands into FP16 hi + lo).
 """
 
 from __future__ import annotations
