@@ -6,10 +6,10 @@
 // Same mathematics as abbe.cu (expose/aerial_image.py:421-494 restated on
 // the smallest grid that holds |E|^2 exactly, L >= 4h + 1), with the two
 // passes of each coherent transform split across thread blocks:
-//   pass A (k_wide_cols): per transform and chunk of spectral columns kx, the
-//       inverse L-point FFT over ky of P M on the (2h+1)-row band -> T[kx][v]
-//       in global memory (L2-resident for a chunk of jobs);
-//   pass B (k_wide_rows): per work item and chunk of rows v, the inverse
+//   pass A (k_wide_cols_w): per transform and chunk of spectral columns kx,
+//       the inverse L-point FFT over ky of P M on the (2h+1)-row band ->
+//       T[kx][v] in global memory (L2-resident for a chunk of jobs);
+//   pass B (k_wide_rows_w): per work item and chunk of rows v, the inverse
 //       L-point FFT over kx of T[.][v] for every transform of the item and
 //       J(u, v) += w |e|^2 in shared memory -> the item's partial J;
 //   reduce (k_wide_reduce) in item order, F = FFT_L(J) / L^2 and the image
@@ -17,10 +17,12 @@
 //   synthesis: B scattered into an N x N spectrum, two outputs per complex
 //       inverse FFT (B is Hermitian, so each image is real), then the
 //       normalisation of aerial_image.py:217-241.
-// Transforms run in shared memory (fftsmem.cuh); every reduction has a fixed
-// order, so results are deterministic.
+// Passes A and B run warp-per-line register FFTs (fftwarp.cuh); the adjoint
+// passes and the L x L transforms run in shared memory (fftsmem.cuh). Every
+// reduction has a fixed order, so results are deterministic.
 #include "common.cuh"
 #include "fftsmem.cuh"
+#include "fftwarp.cuh"
 
 namespace litho {
 
@@ -34,7 +36,6 @@ __global__ void k_normalise(const float* __restrict__ blockmax, int nblk, const 
                             int n, float* __restrict__ image, float* __restrict__ peak, int apply_mode0);
 
 constexpr int kWideCols = 16;       // spectral columns per pass-A block
-constexpr int kWideRows = 16;       // coarse rows per pass-B block
 constexpr int kWideMaxBlk = 256;    // block maxima per output
 constexpr int64_t kWideTBudget = 512ll << 20;   // bytes of pass-A output per job chunk
 constexpr int kWideSpecPairs = 4;   // output pairs per synthesis chunk
@@ -76,42 +77,137 @@ k_wide_cols(const LithoJob* __restrict__ jobs, int j0, int ncomp_max, const floa
   for (int i = threadIdx.x; i < lines * L; i += blockDim.x) dst[i] = s[i];
 }
 
-// Pass B. Grid (item, row chunk). Adds the item's transforms whose jobs lie
-// in [j0, j0 + nj) to partial[item][v][u].
-__global__ void __launch_bounds__(256)
-k_wide_rows(const LithoItem* __restrict__ items, const LithoJob* __restrict__ jobs, int j0, int nj, int ncomp_max,
-            int h, int L, int log2L, const float2* __restrict__ twL, const float2* __restrict__ T,
-            float* __restrict__ partial) {
+// Register-FFT forms of passes A and B (fftwarp.cuh): a warp transforms
+// 32 / R lines of L = 32 R points at once; kWfWarps warps per block.
+constexpr int kWfWarps = 8;
+
+// twiddles, the warps' transpose buffers, then (pass B) the warps' J rows
+__host__ __device__ inline size_t wf_smem(int L) {
+  return (size_t)L * 8 + (size_t)kWfWarps * 32 * kTbLd * 8 + (size_t)kWfWarps * 32 * 32 * 4;
+}
+
+// Pass A. Grid (transform t of the chunk, chunk of kWfWarps * LPW columns).
+template <int L>
+__global__ void __launch_bounds__(kWfWarps * 32, 2)
+k_wide_cols_w(const LithoJob* __restrict__ jobs, int j0, int ncomp_max, const float2* __restrict__ table, int h,
+              const float2* __restrict__ Mb, int bm, const float2* __restrict__ twL, float2* __restrict__ T) {
+  constexpr int R = L / 32, LPW = 32 / R;
   extern __shared__ float2 wsm[];
   float2* tw = wsm;
-  float2* s = wsm + L;                                             // [kWideRows][L]
-  float* J = reinterpret_cast<float*>(s + kWideRows * L);          // [kWideRows][L]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* tb = wsm + L + warp * 32 * kTbLd;
+  const int t = blockIdx.x;
+  const int side = 2 * h + 1, npts = side * side, Bm = 2 * bm + 1;
+  const int j = j0 + t / ncomp_max, c = t % ncomp_max;
+  const LithoJob job = jobs[j];
+  if (c >= job.ncomp) return;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twL[i];
+  __syncthreads();
+  const int col0 = (blockIdx.y * kWfWarps + warp) * LPW;
+  if (col0 >= side) return;
+  const float2* tp = table + ((size_t)job.tab * ncomp_max + c) * npts;
+  const float2* m = Mb + (size_t)job.clip * Bm * Bm;
+  float2 x[32];
+#pragma unroll
+  for (int l = 0; l < LPW; ++l) {
+    const int kxi = col0 + l;
+    const int mx = job.cx + (kxi - h) + bm;
+    const bool col_ok = kxi < side && mx >= 0 && mx < Bm;
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int i = lane + 32 * q;
+      const int ky = i <= h ? i : i - L;  // in [-h, h] when i <= h or i >= L - h
+      float2 v = make_float2(0.f, 0.f);
+      const int my = job.cy + ky + bm;
+      if (col_ok && (i <= h || i >= L - h) && my >= 0 && my < Bm)
+        v = cmul(__ldg(tp + (ky + h) * side + kxi), __ldg(m + (size_t)my * Bm + mx));
+      x[l * R + q] = v;
+    }
+  }
+  warp_fft_lines<L, +1>(x, tb, tw);
+  const int kxi = col0 + lane / R;
+  if (kxi < side) {
+    float2* dst = T + ((size_t)t * side + kxi) * L + lane % R;
+#pragma unroll
+    for (int s = 0; s < 32; ++s) dst[R * s] = x[s];
+  }
+}
+
+// Pass B. Grid (item, chunk of kWfWarps * LPW rows v). Adds the item's
+// transforms whose jobs lie in [j0, j0 + nj) to partial[item][v][u]; each
+// warp keeps its rows' J in shared memory across the transforms.
+template <int L>
+__global__ void __launch_bounds__(kWfWarps * 32, 2)
+k_wide_rows_w(const LithoItem* __restrict__ items, const LithoJob* __restrict__ jobs, int j0, int nj,
+              int ncomp_max, int h, const float2* __restrict__ twL, const float2* __restrict__ T,
+              float* __restrict__ partial) {
+  constexpr int R = L / 32, LPW = 32 / R;
+  extern __shared__ float2 wsm[];
+  float2* tw = wsm;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* tb = wsm + L + warp * 32 * kTbLd;
   const LithoItem it = items[blockIdx.x];
   const int jb = it.job_begin > j0 ? it.job_begin : j0;
   const int je = it.job_end < j0 + nj ? it.job_end : j0 + nj;
   if (jb >= je) return;
-  const int v0 = blockIdx.y * kWideRows, side = 2 * h + 1;
   for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twL[i];
-  float* pj = partial + ((size_t)blockIdx.x * L + v0) * L;
-  for (int i = threadIdx.x; i < kWideRows * L; i += blockDim.x) J[i] = pj[i];
-  for (int j = jb; j < je; ++j) {
-    const LithoJob job = jobs[j];
+  __syncthreads();
+  const int side = 2 * h + 1;
+  const int v0 = (blockIdx.y * kWfWarps + warp) * LPW;
+  float* pj = partial + ((size_t)blockIdx.x * L + v0 + lane / R) * L + lane % R;
+  float* J = reinterpret_cast<float*>(wsm + L + kWfWarps * 32 * kTbLd) + warp * 32 * 32 + lane;  // [s][lane]
+#pragma unroll
+  for (int s = 0; s < 32; ++s) J[s * 32] = pj[R * s];
+  for (int jj = jb; jj < je; ++jj) {
+    const LithoJob job = jobs[jj];
     const float w = (float)job.weight;
     for (int c = 0; c < job.ncomp; ++c) {
-      const float2* Tt = T + (size_t)((j - j0) * ncomp_max + c) * side * L;
-      __syncthreads();  // previous transform's reads of s are done
-      for (int i = threadIdx.x; i < kWideRows * L; i += blockDim.x) s[i] = make_float2(0.f, 0.f);
-      __syncthreads();
-      for (int id = threadIdx.x; id < side * kWideRows; id += blockDim.x) {
-        const int ki = id / kWideRows, r = id % kWideRows;
-        s[r * L + brev((ki - h) & (L - 1), log2L)] = Tt[(size_t)ki * L + v0 + r];
+      const float2* Tt = T + (size_t)((jj - j0) * ncomp_max + c) * side * L + v0;
+      float2 x[32];
+#pragma unroll
+      for (int l = 0; l < LPW; ++l) {
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int i = lane + 32 * q;
+          const int kx = i <= h ? i : i - L;
+          x[l * R + q] = (i <= h || i >= L - h) ? Tt[(size_t)(kx + h) * L + l] : make_float2(0.f, 0.f);
+        }
       }
-      block_fft_lines<+1>(s, L, kWideRows, L, tw);
-      for (int i = threadIdx.x; i < kWideRows * L; i += blockDim.x) J[i] = fmaf(w, cabs2(s[i]), J[i]);
+      warp_fft_lines<L, +1>(x, tb, tw);
+#pragma unroll
+      for (int s = 0; s < 32; ++s) J[s * 32] = fmaf(w, cabs2(x[s]), J[s * 32]);
     }
   }
-  __syncthreads();
-  for (int i = threadIdx.x; i < kWideRows * L; i += blockDim.x) pj[i] = J[i];
+#pragma unroll
+  for (int s = 0; s < 32; ++s) pj[R * s] = J[s * 32];
+}
+
+template <int L>
+static cudaError_t launch_wide_passes_l(const LithoAbbePlan& p, int j0, int nj, const LithoItem* items,
+                                        const LithoJob* jobs, const float2* table, const float2* mb,
+                                        const float2* twL, float2* T, float* partial, cudaStream_t s) {
+  constexpr int R = L / 32, LPW = 32 / R;
+  const int side = 2 * p.h + 1;
+  const size_t sm = wf_smem(L);
+  cudaFuncSetAttribute(k_wide_cols_w<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_wide_rows_w<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  dim3 ga(nj * p.ncomp_max, (side + kWfWarps * LPW - 1) / (kWfWarps * LPW));
+  k_wide_cols_w<L><<<ga, kWfWarps * 32, sm, s>>>(jobs, j0, p.ncomp_max, table, p.h, mb, p.bm, twL, T);
+  dim3 gb(p.n_items, L / (kWfWarps * LPW));
+  k_wide_rows_w<L><<<gb, kWfWarps * 32, sm, s>>>(items, jobs, j0, nj, p.ncomp_max, p.h, twL, T, partial);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_wide_passes(const LithoAbbePlan& p, int j0, int nj, const LithoItem* items,
+                                      const LithoJob* jobs, const float2* table, const float2* mb,
+                                      const float2* twL, float2* T, float* partial, cudaStream_t s) {
+  switch (p.L) {
+    case 128: return launch_wide_passes_l<128>(p, j0, nj, items, jobs, table, mb, twL, T, partial, s);
+    case 256: return launch_wide_passes_l<256>(p, j0, nj, items, jobs, table, mb, twL, T, partial, s);
+    case 512: return launch_wide_passes_l<512>(p, j0, nj, items, jobs, table, mb, twL, T, partial, s);
+    case 1024: return launch_wide_passes_l<1024>(p, j0, nj, items, jobs, table, mb, twL, T, partial, s);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 // J[o] = sum of its items' partials, in item order.
@@ -345,7 +441,7 @@ int abbe_wide_run(const LithoAbbePlan& p, const void* blob, const void* table_in
   float2* bbox = reinterpret_cast<float2*>(w + l.bbox);
   float2* spec = reinterpret_cast<float2*>(w + l.spec);
   float* blockmax = reinterpret_cast<float*>(w + l.blockmax);
-  const int n = p.n, L = p.L, lgL = ilog2w(L), Bm = 2 * p.bm + 1, side = 2 * p.h + 1, G = 4 * p.h + 1;
+  const int n = p.n, L = p.L, Bm = 2 * p.bm + 1, G = 4 * p.h + 1;
   const size_t NN = (size_t)n * n;
   cudaError_t e;
   auto mark = [&](int i) { if (ev) cudaEventRecord(ev[i], s); };
@@ -366,17 +462,9 @@ int abbe_wide_run(const LithoAbbePlan& p, const void* blob, const void* table_in
   mark(3);
   // coarse passes, chunk by chunk of jobs
   if ((e = cudaMemsetAsync(partial, 0, (size_t)p.n_items * L * L * 4, s)) != cudaSuccess) return (int)e;
-  const size_t smA = (size_t)(L + kWideCols * L) * 8;
-  const size_t smB = (size_t)(L + kWideRows * L) * 8 + (size_t)kWideRows * L * 4;
-  cudaFuncSetAttribute(k_wide_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA);
-  cudaFuncSetAttribute(k_wide_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB);
   for (int j0 = 0; j0 < p.n_jobs; j0 += l.jobs_per_chunk) {
     const int nj = (p.n_jobs - j0) < l.jobs_per_chunk ? (p.n_jobs - j0) : l.jobs_per_chunk;
-    dim3 ga(nj * p.ncomp_max, (side + kWideCols - 1) / kWideCols);
-    k_wide_cols<<<ga, 256, smA, s>>>(jobs, j0, p.ncomp_max, table, p.h, mb, p.bm, L, lgL, twL, T);
-    dim3 gb(p.n_items, L / kWideRows);
-    k_wide_rows<<<gb, 256, smB, s>>>(items, jobs, j0, nj, p.ncomp_max, p.h, L, lgL, twL, T, partial);
-    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+    if ((e = launch_wide_passes(p, j0, nj, items, jobs, table, mb, twL, T, partial, s)) != cudaSuccess) return (int)e;
   }
   mark(4);
   {
@@ -506,21 +594,13 @@ int wide_coarse_box(const LithoAbbePlan& p, const void* blob, const float2* tabl
   float* partial = reinterpret_cast<float*>(w + l.partial);
   float* J = reinterpret_cast<float*>(w + l.J);
   float2* F = reinterpret_cast<float2*>(w + l.F);
-  const int L = p.L, lgL = ilog2w(L), side = 2 * p.h + 1, G = 4 * p.h + 1;
+  const int L = p.L, G = 4 * p.h + 1;
   cudaError_t e;
   k_twiddle_table<<<(L + 255) / 256, 256, 0, s>>>(twL, L, +1);
   if ((e = cudaMemsetAsync(partial, 0, (size_t)p.n_items * L * L * 4, s)) != cudaSuccess) return (int)e;
-  const size_t smA = (size_t)(L + kWideCols * L) * 8;
-  const size_t smB = (size_t)(L + kWideRows * L) * 8 + (size_t)kWideRows * L * 4;
-  cudaFuncSetAttribute(k_wide_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA);
-  cudaFuncSetAttribute(k_wide_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB);
   for (int j0 = 0; j0 < p.n_jobs; j0 += l.jobs_per_chunk) {
     const int nj = (p.n_jobs - j0) < l.jobs_per_chunk ? (p.n_jobs - j0) : l.jobs_per_chunk;
-    k_wide_cols<<<dim3(nj * p.ncomp_max, (side + kWideCols - 1) / kWideCols), 256, smA, s>>>(
-        jobs, j0, p.ncomp_max, table, p.h, mb, p.bm, L, lgL, twL, T);
-    k_wide_rows<<<dim3(p.n_items, L / kWideRows), 256, smB, s>>>(items, jobs, j0, nj, p.ncomp_max, p.h, L, lgL, twL,
-                                                                  T, partial);
-    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+    if ((e = launch_wide_passes(p, j0, nj, items, jobs, table, mb, twL, T, partial, s)) != cudaSuccess) return (int)e;
   }
   const int LL = L * L;
   k_wide_reduce<<<dim3((LL + 255) / 256 < 1024 ? (LL + 255) / 256 : 1024, p.n_out), 256, 0, s>>>(out_items, partial,
