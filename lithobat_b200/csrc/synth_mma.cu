@@ -86,13 +86,15 @@ __device__ __forceinline__ void split_f16(float v, __half& hi, __half& lo) {
 
 // Power-of-two scale for output o's P values, from the bound
 // |P_k(y)| <= 2 max_gx sum_gy |B(gx, gy)|, computed the same way in every
-// block. Contains a __syncthreads.
-__device__ float p_scale(const float2* __restrict__ Bo, int g0, float* red) {
+// block. bs: the output's box staged in shared memory, complete before the
+// call; element (gy, gx) at bs[(gy + g0) * rs + (gx + g0) * cs]. Contains a
+// __syncthreads.
+__device__ float p_scale(const float2* bs, int g0, int rs, int cs, float* red) {
   const int G = 2 * g0 + 1;
   if (threadIdx.x <= g0) {
     float sum = 0.f;
     for (int i = 0; i < G; ++i) {
-      const float2 b = Bo[(size_t)i * G + threadIdx.x + g0];
+      const float2 b = bs[i * rs + (threadIdx.x + g0) * cs];
       sum += sqrtf(b.x * b.x + b.y * b.y);
     }
     red[threadIdx.x] = sum;
@@ -144,20 +146,23 @@ __device__ __forceinline__ void p_put(__half* tile, int kp, int row, int k, floa
 __global__ void __launch_bounds__(kPpWarps * 32)
 k_synth_pplanes(const float2* __restrict__ Bbox, int g0, int n, const float2* __restrict__ tw_inv, int kp,
                 __half* __restrict__ planes, float* __restrict__ inv_scale) {
-  extern __shared__ float2 pp_tb[];                     // [g][b] = w^(g b), g = 0..g0
+  extern __shared__ float2 pp_tb[];                     // [g][b] = w^(g b), g = 0..g0, then the box
   __shared__ float2 col[kPpWarps][2 * kSmG0Max + 2];    // B(gx, gy + g0) of each warp's column
   __shared__ float red[kSmG0Max + 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int o = blockIdx.y, gx = blockIdx.x * kPpWarps + warp;
   const int gp = g0 + 1, G = 2 * g0 + 1, M = n >> 5, nmask = n - 1;
   const float2* Bo = Bbox + (size_t)o * G * G;
+  float2* bs = pp_tb + (size_t)gp * M;                  // [gy + g0][gx + g0]
   for (int j = threadIdx.x; j < gp * M; j += blockDim.x) {
     const int g = j / M, b = j % M;
     pp_tb[j] = __ldg(tw_inv + ((g * b) & nmask));
   }
+  for (int j = threadIdx.x; j < G * G; j += blockDim.x) bs[j] = Bo[j];
+  __syncthreads();
   if (gx < gp)
-    for (int i = lane; i < G; i += 32) col[warp][i] = Bo[(size_t)i * G + gx + g0];
-  const float sc = p_scale(Bo, g0, red);
+    for (int i = lane; i < G; i += 32) col[warp][i] = bs[i * G + gx + g0];
+  const float sc = p_scale(bs, g0, G, 1, red);
   if (blockIdx.x == 0 && threadIdx.x == 0) inv_scale[o] = 1.f / sc;
   if (gx >= gp) return;
   const float2* cw = col[warp] + g0;
@@ -183,11 +188,11 @@ k_synth_pplanes(const float2* __restrict__ Bbox, int g0, int n, const float2* __
 // The same planes with the column sums gathered per output in shared memory
 // first (C[gx][y] for all y), so each thread then writes whole 16-byte K
 // chunks of one row: one block per output, used when C fits in shared memory.
-constexpr int kPbWarps = 8;
+constexpr int kPbWarps = 16;
 
 __host__ __device__ inline size_t pblk_smem(int n, int g0) {
   const int gp = g0 + 1;
-  return (size_t)gp * n * 8 + (size_t)gp * (n >> 5) * 8 + (size_t)kPbWarps * (2 * kSmG0Max + 2) * 8;
+  return (size_t)gp * n * 8 + (size_t)gp * (n >> 5) * 8 + (size_t)(2 * g0 + 1) * (2 * g0 + 1) * 8;
 }
 
 __global__ void __launch_bounds__(kPbWarps * 32)
@@ -198,26 +203,25 @@ k_synth_pplanes_blk(const float2* __restrict__ Bbox, int g0, int n, const float2
   const int gp = g0 + 1, G = 2 * g0 + 1, M = n >> 5, nmask = n - 1;
   float2* Cs = pb_sm;                      // [gx][y]
   float2* TB = Cs + (size_t)gp * n;        // [g][b] = w^(g b)
-  float2* colb = TB + (size_t)gp * M;      // [warp][gy + g0]
+  float2* bs = TB + (size_t)gp * M;        // the box, transposed: [gx + g0][gy + g0]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, o = blockIdx.x;
   const float2* Bo = Bbox + (size_t)o * G * G;
   for (int j = threadIdx.x; j < gp * M; j += blockDim.x) {
     const int g = j / M, b = j % M;
     TB[j] = __ldg(tw_inv + ((g * b) & nmask));
   }
-  const float sc = p_scale(Bo, g0, red);
+  for (int j = threadIdx.x; j < G * G; j += blockDim.x) bs[(j % G) * G + j / G] = Bo[j];
+  __syncthreads();
+  const float sc = p_scale(bs, g0, 1, G, red);
   if (threadIdx.x == 0) inv_scale[o] = 1.f / sc;
-  float2* cw0 = colb + warp * (2 * kSmG0Max + 2);
   for (int gx = warp; gx < gp; gx += kPbWarps) {
-    for (int i = lane; i < G; i += 32) cw0[i] = Bo[(size_t)i * G + gx + g0];
-    __syncwarp();
+    const float2* cw = bs + (gx + g0) * G + g0;  // B(gx, gy) at cw[gy]
     for (int b = lane; b < M; b += 32) {
       float2 Q[32];
-      column_fft(cw0 + g0, TB, g0, M, b, Q);
+      column_fft(cw, TB, g0, M, b, Q);
 #pragma unroll
       for (int a = 0; a < 32; ++a) Cs[(size_t)gx * n + b + M * a] = Q[a];
     }
-    __syncwarp();
   }
   __syncthreads();
   const int K = G, nck = kp >> 3;
@@ -488,7 +492,7 @@ cudaError_t launch_synth_mma(const float2* box, int g0, int n, int n_out, const 
     cudaFuncSetAttribute(k_synth_pplanes_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb);
     k_synth_pplanes_blk<<<n_out, kPbWarps * 32, smb, s>>>(box, g0, n, tw, kp, pp, inv);
   } else {
-    const size_t smp = (size_t)(g0 + 1) * (n >> 5) * 8;
+    const size_t smp = (size_t)(g0 + 1) * (n >> 5) * 8 + (size_t)(2 * g0 + 1) * (2 * g0 + 1) * 8;
     cudaFuncSetAttribute(k_synth_pplanes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smp);
     k_synth_pplanes<<<dim3((g0 + 1 + kPpWarps - 1) / kPpWarps, n_out), kPpWarps * 32, smp, s>>>(box, g0, n, tw,
                                                                                                kp, pp, inv);
