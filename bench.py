@@ -571,9 +571,9 @@ def run_ours(args) -> None:
         formula_bytes = NN * (16 * transforms + 24)  # dense two-pass FFT equivalent, per image
         line["config"]["pupil_table"] = f"built once per optics ({table_ms:.3f} ms), reused across steps"
         # DRAM bytes (read + write) of one launch, from an ncu capture of the
-        # 16-image case (134.25 MB read + 3.89 MB written) scaled by images per
+        # 96-image case (805.33 MB read + 9.52 MB written) scaled by images per
         # launch: traffic grows in proportion to the images processed
-        traffic = {"band_rows": (134.25e6 + 3.89e6) / 16 * B}.get(dom)
+        traffic = {"band_rows": (805.33e6 + 9.52e6) / 96 * B}.get(dom)
         line["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                             "frac": achieved / hbm, "traffic": traffic,
                             "peak_source": "measured" if not peaks.get("_fallback") else "fallback"}
