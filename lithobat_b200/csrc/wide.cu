@@ -35,47 +35,9 @@ cudaError_t launch_pupil_table(const LithoAbbePlan& p, const void* blob, float2*
 __global__ void k_normalise(const float* __restrict__ blockmax, int nblk, const LithoNorm* __restrict__ norm,
                             int n, float* __restrict__ image, float* __restrict__ peak, int apply_mode0);
 
-constexpr int kWideCols = 16;       // spectral columns per pass-A block
 constexpr int kWideMaxBlk = 256;    // block maxima per output
 constexpr int64_t kWideTBudget = 512ll << 20;   // bytes of pass-A output per job chunk
 constexpr int kWideSpecPairs = 4;   // output pairs per synthesis chunk
-
-static int ilog2w(int n) {
-  int l = 0;
-  while ((1 << l) < n) ++l;
-  return l;
-}
-
-// Pass A. Grid (transform t of the chunk, column chunk). T[t][kx + h][v].
-__global__ void __launch_bounds__(256)
-k_wide_cols(const LithoJob* __restrict__ jobs, int j0, int ncomp_max, const float2* __restrict__ table, int h,
-            const float2* __restrict__ Mb, int bm, int L, int log2L, const float2* __restrict__ twL,
-            float2* __restrict__ T) {
-  extern __shared__ float2 wsm[];
-  float2* tw = wsm;
-  float2* s = wsm + L;  // [kWideCols][L]
-  const int t = blockIdx.x, c0 = blockIdx.y * kWideCols;
-  const int side = 2 * h + 1, npts = side * side, Bm = 2 * bm + 1;
-  const int j = j0 + t / ncomp_max, c = t % ncomp_max;
-  const LithoJob job = jobs[j];
-  if (c >= job.ncomp) return;
-  const int lines = (side - c0) < kWideCols ? (side - c0) : kWideCols;
-  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twL[i];
-  for (int i = threadIdx.x; i < lines * L; i += blockDim.x) s[i] = make_float2(0.f, 0.f);
-  __syncthreads();
-  const float2* tp = table + ((size_t)job.tab * ncomp_max + c) * npts;
-  const float2* m = Mb + (size_t)job.clip * Bm * Bm;
-  for (int id = threadIdx.x; id < lines * side; id += blockDim.x) {
-    const int r = id / side, di = id % side;
-    const int kx = c0 + r - h, d = di - h;
-    const int mx = job.cx + kx + bm, my = job.cy + d + bm;
-    if (mx >= 0 && mx < Bm && my >= 0 && my < Bm)
-      s[r * L + brev(d & (L - 1), log2L)] = cmul(__ldg(tp + di * side + (kx + h)), __ldg(m + (size_t)my * Bm + mx));
-  }
-  block_fft_lines<+1>(s, L, lines, L, tw);
-  float2* dst = T + ((size_t)t * side + c0) * L;
-  for (int i = threadIdx.x; i < lines * L; i += blockDim.x) dst[i] = s[i];
-}
 
 // Register-FFT forms of passes A and B (fftwarp.cuh): a warp transforms
 // 32 / R lines of L = 32 R points at once; kWfWarps warps per block.
@@ -291,67 +253,133 @@ __global__ void k_wide_scatter_box(const float2* __restrict__ box, int g0, int L
   }
 }
 
-// Pass B of the adjoint. Grid (transform t of the chunk, chunk of `lines`
-// rows v): e(., v) = inverse over kx of T[t][.][v]; times g_L(., v); forward
-// over u; the band fx in [-h, h] -> T2[t][fx + h][v].
-__global__ void __launch_bounds__(256)
-k_wide_adj_rows(const LithoJob* __restrict__ jobs, int j0, int h, int L, int log2L, int lines,
-                const float2* __restrict__ twL, const float2* __restrict__ T, const float2* __restrict__ gL,
-                float2* __restrict__ T2) {
+// Register-FFT forms of the adjoint passes. Pass B of the adjoint, per warp
+// LPW rows v of one transform: the row inverse of T (as in pass B), times
+// g_L(., v), the forward transform of that product, the band fx in [-h, h]
+// -> T2[t][fx + h][v]. Between the two transforms the product goes through the
+// warp's buffer as LPW rows of pitch L + R, from the output layout of one
+// transform into the input layout of the next.
+template <int L>
+__global__ void __launch_bounds__(kWfWarps * 32, 2)
+k_wide_adj_rows_w(const LithoJob* __restrict__ jobs, int j0, int h, const float2* __restrict__ twL,
+                  const float2* __restrict__ T, const float2* __restrict__ gL, float2* __restrict__ T2) {
+  constexpr int R = L / 32, LPW = 32 / R, PITCH = L + R;
+  static_assert(LPW * PITCH <= 32 * kTbLd, "row buffer fits the transpose buffer");
   extern __shared__ float2 wsm[];
   float2* tw = wsm;
-  float2* s1 = wsm + L;                 // [lines][L]
-  float2* s2 = s1 + (size_t)lines * L;  // [lines][L]
-  const int t = blockIdx.x, v0 = blockIdx.y * lines, side = 2 * h + 1;
-  const LithoJob job = jobs[j0 + t];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* tb = wsm + L + warp * 32 * kTbLd;
   for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twL[i];
-  for (int i = threadIdx.x; i < lines * L; i += blockDim.x) s1[i] = make_float2(0.f, 0.f);
   __syncthreads();
-  const float2* Tt = T + (size_t)t * side * L;
-  for (int id = threadIdx.x; id < side * lines; id += blockDim.x) {
-    const int ki = id / lines, r = id % lines;
-    s1[r * L + brev((ki - h) & (L - 1), log2L)] = Tt[(size_t)ki * L + v0 + r];
+  const int t = blockIdx.x, side = 2 * h + 1;
+  const int v0 = (blockIdx.y * kWfWarps + warp) * LPW;
+  const LithoJob job = jobs[j0 + t];
+  const float2* Tt = T + (size_t)t * side * L + v0;
+  float2 x[32];
+#pragma unroll
+  for (int l = 0; l < LPW; ++l) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int i = lane + 32 * q;
+      const int kx = i <= h ? i : i - L;
+      x[l * R + q] = (i <= h || i >= L - h) ? Tt[(size_t)(kx + h) * L + l] : make_float2(0.f, 0.f);
+    }
   }
-  block_fft_lines<+1>(s1, L, lines, L, tw);   // e(u, v) in natural order
-  const float2* g = gL + (size_t)job.clip * L * L;
-  for (int i = threadIdx.x; i < lines * L; i += blockDim.x) {
-    const int r = i / L, u = i % L;
-    s2[r * L + brev(u, log2L)] = cmul(s1[i], __ldg(g + (size_t)(v0 + r) * L + u));
+  warp_fft_lines<L, +1>(x, tb, tw);  // lane: row v0 + lane / R, u = lane % R + R s
+  {
+    const int lp = lane / R, rp = lane % R;
+    const float2* g = gL + ((size_t)job.clip * L + v0 + lp) * L + rp;
+#pragma unroll
+    for (int sidx = 0; sidx < 32; ++sidx) tb[lp * PITCH + rp + R * sidx] = cmul(x[sidx], __ldg(g + R * sidx));
   }
-  block_fft_lines<-1>(s2, L, lines, L, tw);
-  float2* dst = T2 + (size_t)t * side * L;
-  for (int id = threadIdx.x; id < side * lines; id += blockDim.x) {
-    const int fi = id / lines, r = id % lines;
-    dst[(size_t)fi * L + v0 + r] = s2[r * L + ((fi - h) & (L - 1))];
+  __syncwarp();
+#pragma unroll
+  for (int l = 0; l < LPW; ++l) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) x[l * R + q] = tb[l * PITCH + lane + 32 * q];
+  }
+  __syncwarp();
+  warp_fft_lines<L, -1>(x, tb, tw);  // lane: row v0 + lane / R, fx = lane % R + R s (mod L)
+  const int lp = lane / R, rp = lane % R;
+  float2* dst = T2 + (size_t)t * side * L + v0 + lp;
+#pragma unroll
+  for (int sidx = 0; sidx < 32; ++sidx) {
+    const int f = rp + R * sidx;
+    const int fx = f <= h ? f : f - L;
+    if (f <= h || f >= L - h) dst[(size_t)(fx + h) * L] = x[sidx];
   }
 }
 
-// Pass C. Grid (transform t, chunk of kWideCols columns fx): forward over v of
-// T2[t][fx][.], the band fy in [-h, h], weighted: Yt[t][fy + h][fx + h] =
-// lambda conj(phi(fx, fy)) Y / L^2.
-__global__ void __launch_bounds__(256)
-k_wide_adj_cols(const LithoJob* __restrict__ jobs, int j0, const float2* __restrict__ table, int h, int L,
-                int log2L, const float2* __restrict__ twL, const float2* __restrict__ T2, float2* __restrict__ Yt) {
+// Pass C of the adjoint, per warp LPW columns fx of one transform: forward
+// over v of T2[t][fx][.], the band fy in [-h, h], weighted:
+// Yt[t][fy + h][fx + h] = lambda conj(phi(fx, fy)) Y / L^2.
+template <int L>
+__global__ void __launch_bounds__(kWfWarps * 32, 2)
+k_wide_adj_cols_w(const LithoJob* __restrict__ jobs, int j0, const float2* __restrict__ table, int h,
+                  const float2* __restrict__ twL, const float2* __restrict__ T2, float2* __restrict__ Yt) {
+  constexpr int R = L / 32, LPW = 32 / R;
   extern __shared__ float2 wsm[];
   float2* tw = wsm;
-  float2* sl = wsm + L;  // [kWideCols][L]
-  const int t = blockIdx.x, c0 = blockIdx.y * kWideCols, side = 2 * h + 1, npts = side * side;
-  const LithoJob job = jobs[j0 + t];
-  const int lines = (side - c0) < kWideCols ? (side - c0) : kWideCols;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* tb = wsm + L + warp * 32 * kTbLd;
   for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twL[i];
-  const float2* src = T2 + ((size_t)t * side + c0) * L;
-  for (int i = threadIdx.x; i < lines * L; i += blockDim.x) {
-    const int r = i / L, v = i % L;
-    sl[r * L + brev(v, log2L)] = src[i];
+  __syncthreads();
+  const int t = blockIdx.x, side = 2 * h + 1, npts = side * side;
+  const int c0 = (blockIdx.y * kWfWarps + warp) * LPW;
+  if (c0 >= side) return;
+  const LithoJob job = jobs[j0 + t];
+  const float2* src = T2 + (size_t)t * side * L;
+  float2 x[32];
+#pragma unroll
+  for (int l = 0; l < LPW; ++l) {
+    const int fxi = c0 + l;
+#pragma unroll
+    for (int q = 0; q < R; ++q)
+      x[l * R + q] = fxi < side ? src[(size_t)fxi * L + lane + 32 * q] : make_float2(0.f, 0.f);
   }
-  block_fft_lines<-1>(sl, L, lines, L, tw);
+  warp_fft_lines<L, -1>(x, tb, tw);  // lane: column c0 + lane / R, fy = lane % R + R s (mod L)
+  const int fxi = c0 + lane / R, rp = lane % R;
+  if (fxi >= side) return;
   const float2* ph = table + (size_t)job.tab * npts;
   const float sc = (float)job.weight / ((float)L * (float)L);
   float2* dst = Yt + (size_t)t * npts;
-  for (int id = threadIdx.x; id < lines * side; id += blockDim.x) {
-    const int r = id / side, fyi = id % side, fxi = c0 + r;
-    const float2 y = sl[r * L + ((fyi - h) & (L - 1))];
-    dst[fyi * side + fxi] = cscale(cmulc(y, __ldg(ph + fyi * side + fxi)), sc);
+#pragma unroll
+  for (int sidx = 0; sidx < 32; ++sidx) {
+    const int f = rp + R * sidx;
+    const int fy = f <= h ? f : f - L;
+    if (f <= h || f >= L - h) {
+      const int fyi = fy + h;
+      dst[fyi * side + fxi] = cscale(cmulc(x[sidx], __ldg(ph + fyi * side + fxi)), sc);
+    }
+  }
+}
+
+template <int L>
+static cudaError_t launch_wide_adjoint_l(int j0, int nj, const LithoJob* jobs, const float2* table, int h,
+                                         const float2* mask_box, const float2* twL, float2* T, const float2* gL,
+                                         float2* T2, float2* Yt, cudaStream_t s) {
+  constexpr int R = L / 32, LPW = 32 / R;
+  const int side = 2 * h + 1;
+  const size_t sm = wf_smem(L);
+  cudaFuncSetAttribute(k_wide_cols_w<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_wide_adj_rows_w<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_wide_adj_cols_w<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  const dim3 gc(nj, (side + kWfWarps * LPW - 1) / (kWfWarps * LPW));
+  k_wide_cols_w<L><<<gc, kWfWarps * 32, sm, s>>>(jobs, j0, 1, table, h, mask_box, h, twL, T);
+  k_wide_adj_rows_w<L><<<dim3(nj, L / (kWfWarps * LPW)), kWfWarps * 32, sm, s>>>(jobs, j0, h, twL, T, gL, T2);
+  k_wide_adj_cols_w<L><<<gc, kWfWarps * 32, sm, s>>>(jobs, j0, table, h, twL, T2, Yt);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_wide_adjoint(int L, int j0, int nj, const LithoJob* jobs, const float2* table, int h,
+                                       const float2* mask_box, const float2* twL, float2* T, const float2* gL,
+                                       float2* T2, float2* Yt, cudaStream_t s) {
+  switch (L) {
+    case 128: return launch_wide_adjoint_l<128>(j0, nj, jobs, table, h, mask_box, twL, T, gL, T2, Yt, s);
+    case 256: return launch_wide_adjoint_l<256>(j0, nj, jobs, table, h, mask_box, twL, T, gL, T2, Yt, s);
+    case 512: return launch_wide_adjoint_l<512>(j0, nj, jobs, table, h, mask_box, twL, T, gL, T2, Yt, s);
+    case 1024: return launch_wide_adjoint_l<1024>(j0, nj, jobs, table, h, mask_box, twL, T, gL, T2, Yt, s);
+    default: return cudaErrorInvalidValue;
   }
 }
 
@@ -509,7 +537,6 @@ static int wide_L_for(int h) {
 
 bool wide_adjoint_ok(int h) { return h >= 1 && wide_L_for(h) >= 128 && wide_L_for(h) <= 1024; }
 
-static int adj_lines(int L) { return L >= 1024 ? 8 : 16; }
 static int64_t adj_jobs_per_chunk(int h) {
   const int64_t side = 2 * h + 1, L = wide_L_for(h);
   int64_t jc = kWideTBudget / (side * L * 8 * 2 + side * side * 8);
@@ -542,7 +569,7 @@ int64_t wide_adjoint_ws(int n_clips, int h) { return wide_adj_layout(n_clips, h)
 // mask_box [clip][(2h+1)^2] (scaled 1/N^2), sens_box [clip][(4h+1)^2] (scale/N^2).
 int wide_socs_adjoint(const LithoAbbePlan& p, const void* blob, const float2* table, const float2* mask_box,
                       const float2* sens_box, float2* grad_box, void* ws, cudaStream_t s) {
-  const int h = p.h, L = wide_L_for(h), lgL = ilog2w(L), side = 2 * h + 1, npts = side * side;
+  const int h = p.h, L = wide_L_for(h), side = 2 * h + 1, npts = side * side;
   const WideAdjLayout l = wide_adj_layout(p.n_clips, h);
   const LithoJob* jobs = reinterpret_cast<const LithoJob*>(static_cast<const char*>(blob) + p.off_jobs);
   char* w = static_cast<char*>(ws);
@@ -560,18 +587,10 @@ int wide_socs_adjoint(const LithoAbbePlan& p, const void* blob, const float2* ta
   k_wide_scatter_box<<<dim3((G * G + 255) / 256, p.n_clips), 256, 0, s>>>(sens_box, 2 * h, L, gL);
   e = plain_fft2(nullptr, false, gL, p.n_clips, L, +1, 1.0f, 1.0f, twL, s);
   if (e != cudaSuccess) return (int)e;
-  const int lines = adj_lines(L);
-  const size_t smA = (size_t)(L + kWideCols * L) * 8;
-  const size_t smB = (size_t)(L + 2 * lines * L) * 8;
-  cudaFuncSetAttribute(k_wide_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA);
-  cudaFuncSetAttribute(k_wide_adj_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB);
-  cudaFuncSetAttribute(k_wide_adj_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA);
   for (int j0 = 0; j0 < p.n_jobs; j0 += l.jobs_per_chunk) {
     const int nj = (p.n_jobs - j0) < l.jobs_per_chunk ? (p.n_jobs - j0) : l.jobs_per_chunk;
-    const dim3 gc(nj, (side + kWideCols - 1) / kWideCols);
-    k_wide_cols<<<gc, 256, smA, s>>>(jobs, j0, 1, table, h, mask_box, h, L, lgL, twL, T);
-    k_wide_adj_rows<<<dim3(nj, L / lines), 256, smB, s>>>(jobs, j0, h, L, lgL, lines, twL, T, gL, T2);
-    k_wide_adj_cols<<<gc, 256, smA, s>>>(jobs, j0, table, h, L, lgL, twL, T2, Yt);
+    if ((e = launch_wide_adjoint(L, j0, nj, jobs, table, h, mask_box, twL, T, gL, T2, Yt, s)) != cudaSuccess)
+      return (int)e;
     k_wide_adj_acc<<<(npts + 255) / 256, 256, 0, s>>>(jobs, j0, nj, npts, Yt, A);
     if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
   }
