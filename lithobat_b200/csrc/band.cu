@@ -14,6 +14,7 @@
 // A warp covers 32/min(M,32) rows at a time, so every lane is busy for any
 // N that is a multiple of 32.
 #include "common.cuh"
+#include "fftwarp.cuh"
 
 namespace litho {
 
@@ -352,6 +353,113 @@ static cudaError_t launch_band_rows(const void* in, int n_rows, int rows_per_cli
   }
 }
 
+// Wide bands (the residue method's twiddle table outgrows shared memory):
+// full transforms of each row with the warp-per-line register FFT. With
+// SPLIT = N / L sub-sequences x_j(i) = x(j + SPLIT i) (L <= 1024 points each),
+//     U(k) = sum_j exp(-2 pi i j k / N) F_j(k mod L),
+// so a row costs SPLIT L-point FFTs; the band [-bm, bm] (2 bm + 1 <= L) meets
+// each residue k mod L at most once. The partial sums live in a per-warp
+// shared-memory array while the sub-transforms run.
+constexpr int kBfWarps = 4;
+
+__host__ __device__ inline size_t bandfft_smem(int L) {
+  return (size_t)L * 8 + (size_t)kBfWarps * 32 * kTbLd * 8 + (size_t)kBfWarps * 32 * 32 * 8;
+}
+
+template <bool CPLX, int L, int SPLIT>
+__global__ void __launch_bounds__(kBfWarps * 32)
+k_band_rows_fft(const void* __restrict__ in, int n_rows, int rows_per_clip, int bm, float2* __restrict__ out,
+                float scale, const float2* __restrict__ tw_inv) {
+  constexpr int R = L / 32, LPW = 32 / R, N = L * SPLIT;
+  extern __shared__ float2 bf_sm[];
+  float2* tw = bf_sm;  // exp(+2 pi i j / L)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* tb = bf_sm + L + warp * 32 * kTbLd;
+  float2* acc = bf_sm + L + kBfWarps * 32 * kTbLd + warp * 32 * 32;  // [s][lane]
+  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = tw_inv[SPLIT * i];
+  __syncthreads();
+  const int Bm = 2 * bm + 1;
+  const int lp = lane / R, rp = lane % R;
+  for (long long r0 = ((long long)blockIdx.x * kBfWarps + warp) * LPW; r0 < n_rows;
+       r0 += (long long)gridDim.x * kBfWarps * LPW) {
+#pragma unroll 1
+    for (int j = 0; j < SPLIT; ++j) {
+      float2 x[32];
+#pragma unroll
+      for (int l = 0; l < LPW; ++l) {
+        const long long row = r0 + l;
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const size_t e = (size_t)row * N + j + SPLIT * (lane + 32 * q);
+          float2 v = make_float2(0.f, 0.f);
+          if (row < n_rows) {
+            if (CPLX) v = __ldg(reinterpret_cast<const float2*>(in) + e);
+            else v.x = __ldg(reinterpret_cast<const float*>(in) + e);
+          }
+          x[l * R + q] = v;
+        }
+      }
+      warp_fft_lines<L, -1>(x, tb, tw);  // lane: row r0 + lp, k' = rp + R s
+#pragma unroll
+      for (int sidx = 0; sidx < 32; ++sidx) {
+        const int kp = rp + R * sidx;
+        const int k = kp <= bm ? kp : kp - L;  // the band value with residue kp, if any
+        float2 v = x[sidx];
+        if (SPLIT > 1 && j > 0) {
+          const float2 w = __ldg(tw_inv + ((j * k) & (N - 1)));
+          v = cmulc(v, w);  // times exp(-2 pi i j k / N)
+          v = cadd(v, acc[sidx * 32 + lane]);
+        }
+        acc[sidx * 32 + lane] = v;
+      }
+    }
+    const long long row = r0 + lp;
+    if (row >= n_rows) continue;
+    const long long clip = row / rows_per_clip, i = row % rows_per_clip;
+#pragma unroll
+    for (int sidx = 0; sidx < 32; ++sidx) {
+      const int kp = rp + R * sidx;
+      if (kp <= bm || kp >= L - bm) {
+        const int k = kp <= bm ? kp : kp - L;
+        out[((size_t)clip * Bm + (k + bm)) * rows_per_clip + i] = cscale(acc[sidx * 32 + lane], scale);
+      }
+    }
+  }
+}
+
+template <bool CPLX, int L, int SPLIT>
+static cudaError_t launch_band_fft_l(const void* in, int n_rows, int rows_per_clip, int bm, float2* out,
+                                     float scale, const float2* tw_inv, int num_sms, cudaStream_t st) {
+  constexpr int R = L / 32, LPW = 32 / R;
+  const size_t sm = bandfft_smem(L);
+  cudaFuncSetAttribute(k_band_rows_fft<CPLX, L, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  long long blocks = ((long long)n_rows + kBfWarps * LPW - 1) / (kBfWarps * LPW);
+  const long long cap = (long long)num_sms * 3;
+  if (blocks > cap) blocks = cap;
+  k_band_rows_fft<CPLX, L, SPLIT><<<(int)blocks, kBfWarps * 32, sm, st>>>(in, n_rows, rows_per_clip, bm, out, scale,
+                                                                          tw_inv);
+  return cudaGetLastError();
+}
+
+// N in {256 .. 4096} (power of two), 2 bm + 1 <= min(N, 1024).
+template <bool CPLX>
+static cudaError_t launch_band_fft(const void* in, int n_rows, int rows_per_clip, int n, int bm, float2* out,
+                                   float scale, const float2* tw_inv, int num_sms, cudaStream_t st) {
+  switch (n) {
+    case 256: return launch_band_fft_l<CPLX, 256, 1>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms, st);
+    case 512: return launch_band_fft_l<CPLX, 512, 1>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms, st);
+    case 1024: return launch_band_fft_l<CPLX, 1024, 1>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms, st);
+    case 2048: return launch_band_fft_l<CPLX, 1024, 2>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms, st);
+    case 4096: return launch_band_fft_l<CPLX, 1024, 4>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+static bool band_fft_ok(int n, int bm) {
+  const int L = n < 1024 ? n : 1024;
+  return n >= 256 && n <= 4096 && (n & (n - 1)) == 0 && 2 * bm + 1 <= L;
+}
+
 // Fallback for N not a multiple of 32: one thread per (row, k), direct sum.
 template <bool CPLX>
 __global__ void k_row_band_direct(const void* __restrict__ in, int n_rows, int rows_per_clip, int n,
@@ -388,7 +496,15 @@ cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_
                                 int num_sms, cudaStream_t st, int* status) {
   const int esz = cplx ? 8 : 4;
   const int M = n >> 5;
-  if (n >= 32 && n <= 2048 && (n & (n - 1)) == 0 && (cplx || (rows_per_clip % 2 == 0 && n_rows % 2 == 0))) {
+  const bool pow2 = n >= 32 && (n & (n - 1)) == 0;
+  const bool wide = pow2 && n >= 256 && (n > 2048 || !band_geo(n, bm, n <= 1024 ? 8 : 4).tb_smem);
+  if (wide && band_fft_ok(n, bm)) {
+    // wide bands: full row transforms (the residue method's twiddle table would not fit)
+    const cudaError_t e = cplx ? launch_band_fft<true>(in, n_rows, rows_per_clip, n, bm, out, scale, tw_inv, num_sms, st)
+                               : launch_band_fft<false>(in, n_rows, rows_per_clip, n, bm, out, scale, tw_inv, num_sms,
+                                                        st);
+    if (e != cudaSuccess) return e;
+  } else if (n >= 32 && n <= 2048 && (n & (n - 1)) == 0 && (cplx || (rows_per_clip % 2 == 0 && n_rows % 2 == 0))) {
     const cudaError_t e = cplx ? launch_band_rows<true>(in, n_rows, rows_per_clip, n, bm, out, scale, tw_inv, num_sms, st)
                                : launch_band_rows<false>(in, n_rows, rows_per_clip, n, bm, out, scale, tw_inv, num_sms,
                                                          st);

@@ -78,3 +78,33 @@ def test_band_synthesis_matches_numpy(env, n, h, big):
     got = out[check].double().cpu().numpy()
     err = float(np.abs(got - want).max() / np.abs(want).max())
     assert err <= 1e-5, err
+
+
+@pytest.mark.parametrize("n,bm,cplx", [(1024, 200, False), (1024, 300, True), (2048, 100, False),
+                                       (2048, 400, False), (2048, 250, True), (4096, 60, False), (256, 100, True)])
+def test_band_spectrum_matches_numpy(env, n, bm, cplx):
+    """litho_band_spectrum (rows, then columns of its own output) against
+    numpy's fft2 restricted to |kx|, |ky| <= bm, including bands wide enough
+    for the full-row transforms."""
+    torch, nat = env
+    L = nat.lib()
+    rng = np.random.default_rng(n + bm)
+    F = 2
+    x = rng.standard_normal((F, n, n))
+    if cplx:
+        x = x + 1j * rng.standard_normal((F, n, n))
+    k = np.arange(-bm, bm + 1) % n
+    want = np.fft.fft2(x)[:, k][:, :, k] / (n * n)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    xd = torch.from_numpy(x.astype(np.complex64 if cplx else np.float32)).to(dev)
+    nb = C.c_size_t(0)
+    nat.check("litho_band_spectrum_workspace", L.litho_band_spectrum_workspace(F, n, bm, C.byref(nb)))
+    ws = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+    out = torch.empty((F, (2 * bm + 1) ** 2), dtype=torch.complex64, device=dev)
+    nat.check("litho_band_spectrum", L.litho_band_spectrum(
+        xd.data_ptr(), int(cplx), F, n, bm, 1.0 / (n * n), out.data_ptr(), ws.data_ptr(), ws.numel(),
+        torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().astype(np.complex128).reshape(F, 2 * bm + 1, 2 * bm + 1)
+    err = float(np.abs(got - want).max() / np.abs(want).max())
+    assert err <= 1e-5, err
