@@ -14,12 +14,14 @@
 //       J(u, v) += w |e|^2 in shared memory -> the item's partial J;
 //   reduce (k_wide_reduce) in item order, F = FFT_L(J) / L^2 and the image
 //       band box B(g), |g| <= 2h (k_wide_box);
-//   synthesis: B scattered into an N x N spectrum, two outputs per complex
-//       inverse FFT (B is Hermitian, so each image is real), then the
+//   synthesis: two outputs per complex transform (B is Hermitian, so each
+//       image is real): a column stage over gy, then a row stage over gx that
+//       writes both images (k_wsyn_cols, k_wsyn_rows), then the
 //       normalisation of aerial_image.py:217-241.
-// Passes A and B run warp-per-line register FFTs (fftwarp.cuh); the adjoint
-// passes and the L x L transforms run in shared memory (fftsmem.cuh). Every
-// reduction has a fixed order, so results are deterministic.
+// Passes A and B, the adjoint passes and the synthesis run warp-per-line
+// register FFTs (fftwarp.cuh); the L x L transforms of J and g_L run in shared
+// memory (fftsmem.cuh). Every reduction has a fixed order, so results are
+// deterministic.
 #include "common.cuh"
 #include "fftsmem.cuh"
 #include "fftwarp.cuh"
@@ -193,46 +195,171 @@ __global__ void k_wide_box(const float2* __restrict__ F, int L, int h, float2* _
   }
 }
 
-// spec[pair] = B_{2p} + i B_{2p+1} on the N x N grid (zero off the box).
-__global__ void k_wide_spec(const float2* __restrict__ bbox, int o0, int n_out, int g0, int n,
-                            float2* __restrict__ spec) {
+// Synthesis of two outputs per complex transform with the warp register FFT:
+// Z = I_a + i I_b from the boxes' sum D = B_a + i B_b (B Hermitian, so each
+// image is real). Column stage: for every gx in [-g0, g0] the inverse N-point
+// transform over gy of D(gx, .) -> Cw[pair][gx + g0][y]; row stage: for every
+// y the inverse transform over gx of Cw[pair][.][y] -> the two images' rows.
+// N = SPLIT L (L <= 1024) by decimation in frequency: output x = SPLIT m + e
+// comes from the L-point transform of y_e(x') = w_N^(e x')
+// sum_t d(x' + t L) w_SPLIT^(e t).
+template <int L, int SPLIT, class Load>
+__device__ __forceinline__ void band_ifft_e(int e, int g0, const Load& ld, float2 (&x)[32], float2* tb,
+                                            const float2* tw, const float2* __restrict__ twN) {
+  constexpr int R = L / 32, LPW = 32 / R, N = L * SPLIT;
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int l = 0; l < LPW; ++l) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int xp = lane + 32 * q;
+      float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int t = 0; t < SPLIT; ++t) {
+        const int idx = xp + t * L;
+        if (idx <= g0 || idx >= N - g0) {
+          float2 v = ld(l, idx <= g0 ? idx : idx - N);
+          if (SPLIT > 1 && t > 0 && e > 0) v = cmul(v, __ldg(twN + ((e * t * L) & (N - 1))));
+          acc = cadd(acc, v);
+        }
+      }
+      if (SPLIT > 1 && e > 0) acc = cmul(acc, __ldg(twN + ((e * xp) & (N - 1))));
+      x[l * R + q] = acc;
+    }
+  }
+  warp_fft_lines<L, +1>(x, tb, tw);  // lane: line lane / R, output SPLIT (lane % R + R s) + e
+}
+
+template <int L, int SPLIT>
+__global__ void __launch_bounds__(kWfWarps * 32, 2)
+k_wsyn_cols(const float2* __restrict__ bbox, int o0, int n_out, int g0, const float2* __restrict__ twN,
+            float2* __restrict__ Cw) {
+  constexpr int R = L / 32, LPW = 32 / R, N = L * SPLIT;
+  extern __shared__ float2 wsm[];
+  float2* tw = wsm;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* tb = wsm + L + warp * 32 * kTbLd;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twN[SPLIT * i];
+  __syncthreads();
   const int pr = blockIdx.y, G = 2 * g0 + 1;
+  const int c0 = (blockIdx.x * kWfWarps + warp) * LPW;
+  if (c0 >= G) return;
   const int oa = o0 + 2 * pr, ob = oa + 1;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G * G; i += gridDim.x * blockDim.x) {
-    const int gy = i / G - g0, gx = i % G - g0;
-    const float2 a = bbox[(size_t)oa * G * G + i];
-    const float2 b = ob < n_out ? bbox[(size_t)ob * G * G + i] : make_float2(0.f, 0.f);
-    spec[((size_t)pr * n + ((gy + n) % n)) * n + ((gx + n) % n)] = make_float2(a.x - b.y, a.y + b.x);
+  const float2* Ba = bbox + (size_t)oa * G * G;
+  const float2* Bb = bbox + (size_t)ob * G * G;
+  const bool has_b = ob < n_out;
+  auto ld = [&](int l, int gy) -> float2 {
+    const int gxi = c0 + l;
+    if (gxi >= G) return make_float2(0.f, 0.f);
+    const float2 a = __ldg(Ba + (gy + g0) * G + gxi);
+    const float2 b = has_b ? __ldg(Bb + (gy + g0) * G + gxi) : make_float2(0.f, 0.f);
+    return make_float2(a.x - b.y, a.y + b.x);
+  };
+  const int gxi = c0 + lane / R;
+  float2* dst = Cw + ((size_t)pr * G + gxi) * N;
+  for (int e = 0; e < SPLIT; ++e) {
+    float2 x[32];
+    band_ifft_e<L, SPLIT>(e, g0, ld, x, tb, tw, twN);
+    if (gxi < G) {
+#pragma unroll
+      for (int sidx = 0; sidx < 32; ++sidx) dst[SPLIT * (lane % R + R * sidx) + e] = x[sidx];
+    }
   }
 }
 
-// image[o] = Re / Im of the pair's synthesis, times the mode-0 scale; block
-// maxima of the raw image.
-__global__ void k_wide_real(const float2* __restrict__ spec, int o0, int n_out, int n, const LithoNorm* __restrict__ norm,
-                            float* __restrict__ image, float* __restrict__ blockmax) {
-  __shared__ float red[32];
-  const int o = o0 + blockIdx.y, pr = blockIdx.y >> 1, im = blockIdx.y & 1;
-  if (o >= n_out) return;
-  const LithoNorm nm = norm ? norm[o] : LithoNorm{0, 1.0f};
-  const float sc = nm.mode == 1 ? 1.0f : nm.scale;
-  const size_t NN = (size_t)n * n;
-  const float2* sp = spec + (size_t)pr * NN;
-  float* dst = image + (size_t)o * NN;
-  float mx = 0.f;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < NN; i += (size_t)gridDim.x * blockDim.x) {
-    const float2 z = sp[i];
-    const float v = im ? z.y : z.x;
-    mx = fmaxf(mx, v);
-    dst[i] = v * sc;
-  }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+// Row stage, writing the images (times the mode-0 scale) and kWideMaxBlk block
+// maxima of each raw image (block b of the grid takes rows b, b + kWideMaxBlk,
+// ... in units of the block's kWfWarps * LPW rows).
+template <int L, int SPLIT>
+__global__ void __launch_bounds__(kWfWarps * 32, 2)
+k_wsyn_rows(const float2* __restrict__ Cw, int o0, int n_out, int g0, const float2* __restrict__ twN,
+            const LithoNorm* __restrict__ norm, float* __restrict__ image, float* __restrict__ blockmax) {
+  constexpr int R = L / 32, LPW = 32 / R, N = L * SPLIT;
+  extern __shared__ float2 wsm[];
+  __shared__ float red[2][kWfWarps];
+  float2* tw = wsm;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* tb = wsm + L + warp * 32 * kTbLd;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twN[SPLIT * i];
   __syncthreads();
-  if (threadIdx.x == 0 && blockmax) {
-    float m = red[0];
-    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) m = fmaxf(m, red[i]);
-    blockmax[(size_t)o * gridDim.x + blockIdx.x] = m;
+  const int pr = blockIdx.y, G = 2 * g0 + 1;
+  const int oa = o0 + 2 * pr, ob = oa + 1;
+  const bool has_b = ob < n_out;
+  const LithoNorm na = norm ? norm[oa] : LithoNorm{0, 1.0f};
+  const LithoNorm nb = (norm && has_b) ? norm[ob] : LithoNorm{0, 1.0f};
+  const float sa = na.mode == 1 ? 1.0f : na.scale, sb = nb.mode == 1 ? 1.0f : nb.scale;
+  const float2* Cp = Cw + (size_t)pr * G * N;
+  float* ia = image + (size_t)oa * N * N;
+  float* ib = image + (size_t)ob * N * N;
+  float mxa = 0.f, mxb = 0.f;
+  for (int y0 = (blockIdx.x * kWfWarps + warp) * LPW; y0 < N; y0 += kWideMaxBlk * kWfWarps * LPW) {
+    auto ld = [&](int l, int gx) -> float2 { return Cp[(size_t)(gx + g0) * N + y0 + l]; };
+    const int y = y0 + lane / R;
+    for (int e = 0; e < SPLIT; ++e) {
+      float2 x[32];
+      band_ifft_e<L, SPLIT>(e, g0, ld, x, tb, tw, twN);
+#pragma unroll
+      for (int sidx = 0; sidx < 32; ++sidx) {
+        const size_t off = (size_t)y * N + SPLIT * (lane % R + R * sidx) + e;
+        mxa = fmaxf(mxa, x[sidx].x);
+        ia[off] = x[sidx].x * sa;
+        if (has_b) {
+          mxb = fmaxf(mxb, x[sidx].y);
+          ib[off] = x[sidx].y * sb;
+        }
+      }
+    }
+  }
+  if (!blockmax) return;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    mxa = fmaxf(mxa, __shfl_xor_sync(0xffffffffu, mxa, off));
+    mxb = fmaxf(mxb, __shfl_xor_sync(0xffffffffu, mxb, off));
+  }
+  if (lane == 0) {
+    red[0][warp] = mxa;
+    red[1][warp] = mxb;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float a = red[0][0], b = red[1][0];
+    for (int i = 1; i < kWfWarps; ++i) {
+      a = fmaxf(a, red[0][i]);
+      b = fmaxf(b, red[1][i]);
+    }
+    blockmax[(size_t)oa * kWideMaxBlk + blockIdx.x] = a;
+    if (has_b) blockmax[(size_t)ob * kWideMaxBlk + blockIdx.x] = b;
+  }
+}
+
+template <int L, int SPLIT>
+static cudaError_t launch_wsyn_l(const float2* bbox, int o0, int n_out, int g0, int pairs, const float2* twN,
+                                 const LithoNorm* norm, float* image, float* blockmax, float2* Cw, cudaStream_t s) {
+  constexpr int R = L / 32, LPW = 32 / R;
+  const int G = 2 * g0 + 1;
+  const size_t sm = wf_smem(L);
+  cudaFuncSetAttribute(k_wsyn_cols<L, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_wsyn_rows<L, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_wsyn_cols<L, SPLIT><<<dim3((G + kWfWarps * LPW - 1) / (kWfWarps * LPW), pairs), kWfWarps * 32, sm, s>>>(
+      bbox, o0, n_out, g0, twN, Cw);
+  k_wsyn_rows<L, SPLIT><<<dim3(kWideMaxBlk, pairs), kWfWarps * 32, sm, s>>>(Cw, o0, n_out, g0, twN, norm, image,
+                                                                            blockmax);
+  return cudaGetLastError();
+}
+
+// Images o0 .. o0 + 2 pairs - 1 (clipped to n_out) from their boxes of
+// half-width g0 (2 g0 + 1 <= n); Cw: pairs x (2 g0 + 1) x n complex.
+static cudaError_t wide_synth_pairs_w(const float2* bbox, int o0, int n_out, int g0, int n, int pairs,
+                                      const float2* twN, const LithoNorm* norm, float* image, float* blockmax,
+                                      float2* Cw, cudaStream_t s) {
+  switch (n) {
+    case 128: return launch_wsyn_l<128, 1>(bbox, o0, n_out, g0, pairs, twN, norm, image, blockmax, Cw, s);
+    case 256: return launch_wsyn_l<256, 1>(bbox, o0, n_out, g0, pairs, twN, norm, image, blockmax, Cw, s);
+    case 512: return launch_wsyn_l<512, 1>(bbox, o0, n_out, g0, pairs, twN, norm, image, blockmax, Cw, s);
+    case 1024: return launch_wsyn_l<1024, 1>(bbox, o0, n_out, g0, pairs, twN, norm, image, blockmax, Cw, s);
+    case 2048: return launch_wsyn_l<1024, 2>(bbox, o0, n_out, g0, pairs, twN, norm, image, blockmax, Cw, s);
+    case 4096: return launch_wsyn_l<1024, 4>(bbox, o0, n_out, g0, pairs, twN, norm, image, blockmax, Cw, s);
+    default: return cudaErrorInvalidValue;
   }
 }
 
@@ -509,14 +636,8 @@ int abbe_wide_run(const LithoAbbePlan& p, const void* blob, const void* table_in
   for (int o0 = 0; o0 < p.n_out; o0 += 2 * kWideSpecPairs) {
     const int no = (p.n_out - o0) < 2 * kWideSpecPairs ? (p.n_out - o0) : 2 * kWideSpecPairs;
     const int pairs = (no + 1) / 2;
-    if ((e = cudaMemsetAsync(spec, 0, (size_t)pairs * NN * 8, s)) != cudaSuccess) return (int)e;
-    dim3 gs((G * G + 255) / 256, pairs);
-    k_wide_spec<<<gs, 256, 0, s>>>(bbox, o0, p.n_out, 2 * p.h, n, spec);
-    e = plain_fft2(nullptr, false, spec, pairs, n, +1, 1.0f, 1.0f, twN, s);
+    e = wide_synth_pairs_w(bbox, o0, p.n_out, 2 * p.h, n, pairs, twN, norm, image, blockmax, spec, s);
     if (e != cudaSuccess) return (int)e;
-    dim3 gw(kWideMaxBlk, no);
-    k_wide_real<<<gw, 256, 0, s>>>(spec, o0, p.n_out, n, norm, image, blockmax);
-    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
   }
   mark(6);
   dim3 gn((unsigned)((NN + 255) / 256 < 512 ? (NN + 255) / 256 : 512), p.n_out);
@@ -631,9 +752,10 @@ int wide_coarse_box(const LithoAbbePlan& p, const void* blob, const float2* tabl
   return e == cudaSuccess ? LITHO_OK : (int)e;
 }
 
-// Real synthesis of n_fields Hermitian boxes of half-width g0 (any width) by
-// scattering two boxes into one complex N x N spectrum and one inverse FFT.
-// spec: kWideSpecPairs x n x n complex; twN: exp(+2 pi i j / n).
+// Real synthesis of n_fields Hermitian boxes of half-width g0 (2 g0 + 1 <= n),
+// two boxes per complex transform by the column and row stages above.
+// spec: kWideSpecPairs x n x n complex (the column stage's buffer, which
+// needs kWideSpecPairs x (2 g0 + 1) x n); twN: exp(+2 pi i j / n).
 int64_t wide_synth_spec_bytes(int n_fields, int n) {
   const int64_t pairs = (n_fields + 1) / 2 < kWideSpecPairs ? (n_fields + 1) / 2 : kWideSpecPairs;
   return pairs * (int64_t)n * n * 8;
@@ -641,17 +763,12 @@ int64_t wide_synth_spec_bytes(int n_fields, int n) {
 
 cudaError_t wide_synth_real(const float2* box, int g0, int n, int n_fields, float* out, float2* spec,
                             const float2* twN, cudaStream_t s) {
-  const size_t NN = (size_t)n * n;
-  const int G = 2 * g0 + 1;
   cudaError_t e;
   for (int o0 = 0; o0 < n_fields; o0 += 2 * kWideSpecPairs) {
     const int no = (n_fields - o0) < 2 * kWideSpecPairs ? (n_fields - o0) : 2 * kWideSpecPairs;
     const int pairs = (no + 1) / 2;
-    if ((e = cudaMemsetAsync(spec, 0, (size_t)pairs * NN * 8, s)) != cudaSuccess) return e;
-    k_wide_spec<<<dim3((G * G + 255) / 256, pairs), 256, 0, s>>>(box, o0, n_fields, g0, n, spec);
-    if ((e = plain_fft2(nullptr, false, spec, pairs, n, +1, 1.0f, 1.0f, twN, s)) != cudaSuccess) return e;
-    k_wide_real<<<dim3(kWideMaxBlk, no), 256, 0, s>>>(spec, o0, n_fields, n, nullptr, out, nullptr);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = wide_synth_pairs_w(box, o0, n_fields, g0, n, pairs, twN, nullptr, out, nullptr, spec, s)) != cudaSuccess)
+      return e;
   }
   return cudaSuccess;
 }
