@@ -56,7 +56,8 @@ def _fields_for_tensor_cores(n):
 @pytest.mark.parametrize("n,h,big", [(256, 0, True), (256, 3, True), (1024, 14, True), (512, 20, True),
                                      (256, 31, True), (2048, 9, True), (4096, 5, True),
                                      (256, 1, False), (1024, 14, False), (2048, 9, False),
-                                     (128, 7, False), (512, 40, False)])
+                                     (128, 7, False), (512, 40, False), (1024, 100, False), (2048, 200, False),
+                                     (2048, 400, False), (256, 100, False)])
 def test_band_synthesis_matches_numpy(env, n, h, big):
     torch, nat = env
     L = nat.lib()
