@@ -369,6 +369,22 @@ int litho_ilt_theta_grad(const float* grad_m_dev, const float* mask_dev, long lo
 int litho_ilt_update(const float* g_dev, long long count, float beta, float beta_next, float step, float b1,
                      float b2, float eps, int it, float* theta_dev, float* m1_dev, float* m2_dev, float* mask_dev,
                      cudaStream_t stream);
+/* The step schedule of litho_ilt_update_sched(), in device memory, so that a
+ * step recorded once (a CUDA graph) can be replayed: each call first sets
+ * beta = beta_next, it = it + 1, beta_next = beta * growth, then runs
+ * litho_ilt_update() with those values (run_ilt's beta annealing and Adam
+ * counter, opc/ilt.py:582-596). Start it with beta = beta_next = the current
+ * sharpness and it = the number of steps already taken. */
+typedef struct LithoIltSched {
+    double beta, beta_next, growth;
+    int32_t it;
+    float c1, c2;         /* Adam bias corrections 1 - b1^it, 1 - b2^it     */
+    int32_t pad;
+} LithoIltSched;          /* 40 bytes */
+
+int litho_ilt_update_sched(const float* g_dev, long long count, LithoIltSched* sched_dev, float step, float b1,
+                           float b2, float eps, float* theta_dev, float* m1_dev, float* m2_dev, float* mask_dev,
+                           cudaStream_t stream);
 /* One Adam step at iteration it >= 1 (opc/ilt.py:582-591), in place. */
 int litho_ilt_adam(const float* g_dev, long long count, float step, float b1, float b2, float eps,
                    int it, float* theta_dev, float* m1_dev, float* m2_dev, cudaStream_t stream);

@@ -68,7 +68,12 @@ MIRROR_DTYPE = np.dtype([
     ("n_theta", "<i4"), ("pad", "<i4"), ("off_table", "<i8"),
 ], align=True)
 
-assert C.sizeof(AbbePlan) == 120 and MIRROR_DTYPE.itemsize == 56
+ILT_SCHED_DTYPE = np.dtype([
+    ("beta", "<f8"), ("beta_next", "<f8"), ("growth", "<f8"), ("it", "<i4"), ("c1", "<f4"), ("c2", "<f4"),
+    ("pad", "<i4"),
+], align=True)
+
+assert C.sizeof(AbbePlan) == 120 and MIRROR_DTYPE.itemsize == 56 and ILT_SCHED_DTYPE.itemsize == 40
 
 _lib = None
 
@@ -126,6 +131,7 @@ def lib():
         "litho_ilt_adam": [vp, C.c_longlong, f32, f32, f32, f32, i32, vp, vp, vp, vp],
         "litho_gaussian_blur": [vp, vp, vp, i32, i32, vp, i32, vp],
         "litho_ilt_update": [vp, C.c_longlong, f32, f32, f32, f32, f32, f32, i32, vp, vp, vp, vp, vp],
+        "litho_ilt_update_sched": [vp, C.c_longlong, vp, f32, f32, f32, f32, vp, vp, vp, vp, vp],
         "litho_dose_stack": [vp, vp, vp, i32, i32, C.c_longlong, vp, i32, vp, vp],
         "litho_clamp": [vp, C.c_longlong, f32, f32, vp],
         "litho_plain_socs_workspace": [i32, i32, C.POINTER(sz)],

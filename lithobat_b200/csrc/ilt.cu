@@ -365,9 +365,41 @@ __global__ void k_ilt_objective(const float* __restrict__ img, const float* __re
 // One ILT update per pixel (opc/ilt.py:381-389, 587-591, 368-378 without
 // smoothing): m = sigmoid(beta theta), q = g beta m (1 - m), Adam on theta,
 // mask = sigmoid(beta_next theta). Four pixels per thread per iteration.
+__device__ __forceinline__ void ilt_update_body(const float* __restrict__ g, long long total, float beta,
+                                                float beta_next, float step, float b1, float b2, float eps, float c1,
+                                                float c2, float* __restrict__ theta, float* __restrict__ m1,
+                                                float* __restrict__ m2, float* __restrict__ mask);
+
 __global__ void k_ilt_update(const float* __restrict__ g, long long total, float beta, float beta_next, float step,
                              float b1, float b2, float eps, float c1, float c2, float* __restrict__ theta,
                              float* __restrict__ m1, float* __restrict__ m2, float* __restrict__ mask) {
+  ilt_update_body(g, total, beta, beta_next, step, b1, b2, eps, c1, c2, theta, m1, m2, mask);
+}
+
+// The same step with beta, beta_next and the bias corrections read from a
+// device schedule (advanced by k_ilt_sched_advance just before).
+__global__ void k_ilt_update_s(const float* __restrict__ g, long long total, const LithoIltSched* __restrict__ sc,
+                               float step, float b1, float b2, float eps, float* __restrict__ theta,
+                               float* __restrict__ m1, float* __restrict__ m2, float* __restrict__ mask) {
+  ilt_update_body(g, total, (float)sc->beta, (float)sc->beta_next, step, b1, b2, eps, sc->c1, sc->c2, theta, m1, m2,
+                  mask);
+}
+
+__global__ void k_ilt_sched_advance(LithoIltSched* sc, double b1, double b2) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  LithoIltSched v = *sc;
+  v.beta = v.beta_next;
+  v.it += 1;
+  v.beta_next = v.beta * v.growth;
+  v.c1 = (float)(1.0 - pow(b1, (double)v.it));
+  v.c2 = (float)(1.0 - pow(b2, (double)v.it));
+  *sc = v;
+}
+
+__device__ __forceinline__ void ilt_update_body(const float* __restrict__ g, long long total, float beta,
+                                                float beta_next, float step, float b1, float b2, float eps, float c1,
+                                                float c2, float* __restrict__ theta, float* __restrict__ m1,
+                                                float* __restrict__ m2, float* __restrict__ mask) {
   const long long n4 = total >> 2, stride = (long long)gridDim.x * blockDim.x;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n4; k += stride) {
     const long long i = 4 * k;
@@ -724,6 +756,20 @@ extern "C" int litho_ilt_update(const float* g, long long count, float beta, flo
   const float c1 = (float)(1.0 - pow((double)b1, it)), c2 = (float)(1.0 - pow((double)b2, it));
   k_ilt_update<<<grid_for(count / 4, 256, sms_here() * 16), 256, 0, s>>>(g, count, beta, beta_next, step, b1, b2,
                                                                          eps, c1, c2, theta, m1, m2, mask);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+extern "C" int litho_ilt_update_sched(const float* g, long long count, LithoIltSched* sched, float step, float b1,
+                                      float b2, float eps, float* theta, float* m1, float* m2, float* mask,
+                                      cudaStream_t s) {
+  if (!g || !sched || !theta || !m1 || !m2 || !mask) return LITHO_E_NULL;
+  if (count < 0 || (count & 3)) return LITHO_E_SIZE;
+  if (((uintptr_t)g | (uintptr_t)theta | (uintptr_t)m1 | (uintptr_t)m2 | (uintptr_t)mask) & 15) return LITHO_E_ALIGN;
+  if ((uintptr_t)sched & 7) return LITHO_E_ALIGN;
+  k_ilt_sched_advance<<<1, 32, 0, s>>>(sched, (double)b1, (double)b2);
+  k_ilt_update_s<<<grid_for(count / 4, 256, sms_here() * 16), 256, 0, s>>>(g, count, sched, step, b1, b2, eps, theta,
+                                                                          m1, m2, mask);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? LITHO_OK : (int)e;
 }

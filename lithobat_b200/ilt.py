@@ -137,15 +137,17 @@ class _Stages:
         gbox = self.band(sens, 2 * self.h, scale / (self.n * self.n))
         return self.synth(self.adjoint_box(gbox, mbox, field_boxes), self.h, False)
 
-    def adjoint_box(self, gbox, mbox=None, field_boxes=None):
+    def adjoint_box(self, gbox, mbox=None, field_boxes=None, out=None):
         """Band box (C, (2h+1)^2) of the mask gradient from the band box of
-        scale * dJ/dI on |g| <= 2h (already divided by N^2)."""
+        scale * dJ/dI on |g| <= 2h (already divided by N^2); into ``out``
+        when given."""
         torch, L = self.torch, self.L
         nb = C.c_size_t(0)
         nat.check("litho_socs_adjoint_workspace", L.litho_socs_adjoint_workspace(
             self.C, self.pd.plan.n_items, self.h, C.byref(nb)))
         ws = self.ws("adjoint", nb.value)
-        hbox = torch.empty((self.C, self.side * self.side), dtype=torch.complex64, device=self.dev)
+        hbox = out if out is not None else torch.empty((self.C, self.side * self.side), dtype=torch.complex64,
+                                                       device=self.dev)
         nat.check("litho_socs_adjoint", L.litho_socs_adjoint(
             C.byref(self.pd.plan), self.blob.data_ptr(), self.table.data_ptr(),
             None if mbox is None else mbox.data_ptr(),
@@ -158,7 +160,7 @@ class _Stages:
         return (p.sigma_px < 1e-3 and p.smooth_px < 1e-3 and p.weight_tv == 0.0 and p.weight_discrete == 0.0
                 and self.n % 4 == 0)
 
-    def objective_split(self, mbox, target, scale, level, sign, steepness, want_signed=True):
+    def objective_split(self, mbox, target, scale, level, sign, steepness, want_signed=True, out_hbox=None):
         """The objective from the mask band boxes, keeping only band boxes
         between steps: (cost (C,), gradient band box (C, (2h+1)^2), signed or
         None, perr (C,)). Synthesis of the image, the per-pixel resist, the
@@ -175,7 +177,7 @@ class _Stages:
             dfield.data_ptr(), None if signed is None else signed.data_ptr(), cpart.data_ptr(), ppart.data_ptr(),
             N_PART, self.stream()))
         gbox = self.band(dfield, 2 * self.h, float(scale) / (self.n * self.n))
-        hbox = self.adjoint_box(gbox, mbox)
+        hbox = self.adjoint_box(gbox, mbox, out=out_hbox)
         return cpart.sum(dim=1) / float(self.n * self.n), hbox, signed, ppart.sum(dim=1)
 
     def update_split(self, hbox, theta, m1, m2, beta, beta_next, step, b1, b2, eps, it):
@@ -556,6 +558,7 @@ class IltBatch:
         self.fast = can if fast is None else (bool(fast) and can)
         self._mask = self.st.mask_of(self.theta, self.beta, params.smooth_px)
         self._grad_m = None
+        self._graph = None
         if self.fast:
             self.mbox = self.st.mask_box(self._mask)
             self.cost, self.hbox, self.signed, self.perr = self._objective_fast(True)
@@ -583,7 +586,63 @@ class IltBatch:
             self._grad_m = self.st.synth(self.hbox, self.st.h, False)
         return self._grad_m
 
+    def run(self, n_steps: int, graph: bool = True):
+        """``n_steps`` steps without the signed field; returns the last cost.
+
+        The fast step is recorded once as a CUDA graph (its beta annealing and
+        Adam counter kept in device memory, ``litho_ilt_update_sched``) and
+        replayed, which removes the launch gaps between its ~15 kernels; the
+        results are those of ``step()``. Other configurations step eagerly."""
+        n_steps = int(n_steps)
+        if n_steps <= 0:
+            return self.cost
+        if not (self.fast and graph):
+            for _ in range(n_steps):
+                self.step(want_signed=False)
+            return self.cost
+        if self._graph is None:
+            if self.it == 0:          # the first step allocates the stages' workspaces
+                self.step(want_signed=False)
+                n_steps -= 1
+            self._capture()
+        for _ in range(n_steps):
+            self._graph.replay()
+            self.it += 1
+            self.beta = self.beta * self.p.growth
+        self.signed = None
+        return self.cost
+
+    def _capture(self):
+        torch = self.st.torch
+        p = self.p
+        sched = np.zeros(1, dtype=nat.ILT_SCHED_DTYPE)
+        sched["beta"] = sched["beta_next"] = self.beta
+        sched["growth"] = p.growth
+        sched["it"] = self.it
+        self._sched = torch.from_numpy(sched.view(np.uint8)).to(self.st.dev)
+        hbox = torch.empty_like(self.hbox)
+        hbox.copy_(self.hbox)
+        self.hbox = hbox
+        torch.cuda.synchronize(self.st.dev)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            st = self.st
+            grad = st.synth(self.hbox, st.h, False)
+            mask = torch.empty_like(self.theta)
+            nat.check("litho_ilt_update_sched", st.L.litho_ilt_update_sched(
+                grad.data_ptr(), grad.numel(), self._sched.data_ptr(), float(p.step), float(p.b1), float(p.b2),
+                float(p.eps), self.theta.data_ptr(), self.m1.data_ptr(), self.m2.data_ptr(), mask.data_ptr(),
+                st.stream()))
+            mbox = st.mask_box(mask)
+            cost, _, _, perr = st.objective_split(mbox, self.target, p.scale, p.level, p.sign, p.steepness,
+                                                  want_signed=False, out_hbox=self.hbox)
+        self._graph = g
+        self._mask, self.mbox, self.cost, self.perr = mask, mbox, cost, perr
+        self._grad_m = None
+
     def step(self, want_signed: bool = True):
+        if self._graph is not None:
+            raise RuntimeError("this batch steps by graph replay (run()); make a new IltBatch to step eagerly")
         p = self.p
         self.it += 1
         if self.fast:

@@ -172,3 +172,34 @@ def test_plain_engine_gives_the_same_objective(lb):
     assert float(plain.cost[0]) == pytest.approx(float(a["cost"]), rel=1e-5)
     assert rel(plain.grad_m[0].cpu().numpy(), a["grad"]) <= TOL_G
     assert rel(fused.grad_m[0].cpu().numpy(), plain.grad_m[0].cpu().numpy().astype(np.float64)) <= TOL_G
+
+
+def test_graph_replayed_steps_match_eager_steps(lb):
+    """IltBatch.run replays the fast step as a CUDA graph with the beta
+    schedule and Adam counter in device memory; the iterates are those of
+    eager step() calls (here with beta annealing)."""
+    import torch
+    from lithobat_b200 import ilt
+    from lithobat_b200.patterns import manhattan_clip
+    o = lb.OpticsConfig(wavelength=193e-9, NA=1.35, n_immersion=1.44, source_type="annular", sigma_inner=0.5,
+                        sigma_outer=0.8, source_grid=11, normalisation="clear")
+    g = lb.GridConfig(n_pixels=256, pixel_size=2e-9)
+    k = lb.SOCSKernels.build(o, g, tol=0.0, max_kernels=12)
+    rng = np.random.default_rng(21)
+    tg = np.stack([manhattan_clip(rng, 256, 2e-9, n_rect=(4, 8), width_nm=(40, 120)) for _ in range(3)])
+    th = 0.5 * rng.standard_normal((3, 256, 256))
+    p = ilt.IltParams(scale=1.0 / k.clear, level=0.3, steepness=15.0, step=0.2, beta=4.0, growth=1.07)
+    a = ilt.IltBatch(k, tg, th, p)
+    b = ilt.IltBatch(k, tg, th, p)
+    assert a.fast
+    for _ in range(5):
+        a.step(want_signed=False)
+    b.run(2)
+    b.run(3)
+    torch.cuda.synchronize()
+    assert b._graph is not None and b.it == a.it == 5 and abs(b.beta - a.beta) < 1e-12
+    assert float((a.theta - b.theta).abs().max()) < 1e-6
+    assert float((a.mask - b.mask).abs().max()) < 1e-6
+    np.testing.assert_allclose(b.cost.cpu().numpy(), a.cost.cpu().numpy(), rtol=1e-6)
+    with pytest.raises(RuntimeError):
+        b.step()
