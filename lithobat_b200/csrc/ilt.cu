@@ -74,11 +74,17 @@ __global__ void k_gl64(const float2* __restrict__ Gb, int h, float2* __restrict_
 }
 
 // ---------------------------------------------------------------------------
-// Coarse adjoint, one warp per (clip, kernel) job; h <= 15.
+// Coarse adjoint, one pair of warps per (clip, kernel) job; h <= 15. The
+// two warps of a pair split each job's work in half (the even and odd
+// halves of the 64-point transforms in passes 1 and 3, the two halves of the
+// rows in pass 2), so a job's serial latency halves; a block holds two pairs.
 // ---------------------------------------------------------------------------
-constexpr int kAdjWarps = 2;
+constexpr int kAdjPairs = 2;
 constexpr int kAdjHMax = 15;
 constexpr int kAdjLd = 65;
+constexpr int kAdjXLd = 33;
+// per pair: T [31][kAdjLd], Xa and Xb [31][kAdjXLd], Aw [31][32] (complex)
+constexpr int kAdjPerPair = 31 * kAdjLd + 2 * 31 * kAdjXLd + 31 * 32;
 
 // 64-point forward DFT outputs X(k), k in [-h, h], of a full sequence held as
 // even (ev[i] = x(2i)) and odd (od[i] = x(2i+1)) halves:
@@ -88,30 +94,37 @@ __device__ __forceinline__ float2 combine64(const float2 (&ev)[32], const float2
   return cadd(ev[kk & 31], twiddle64<-1>(od[kk & 31], kk & 63));
 }
 
-__global__ void __launch_bounds__(kAdjWarps * 32)
+__device__ __forceinline__ void pair_sync(int pair) {
+  asm volatile("bar.sync %0, 64;" ::"r"(1 + pair) : "memory");
+}
+
+__global__ void __launch_bounds__(kAdjPairs * 64)
 k_coarse64_adjoint(const LithoItem* __restrict__ items, const LithoJob* __restrict__ jobs,
                    const float2* __restrict__ table, int h, const float2* __restrict__ Mb,
                    const float2* __restrict__ etab, const float2* __restrict__ gl, float2* __restrict__ partial) {
   extern __shared__ float2 adj_sm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pair = warp >> 1, role = warp & 1;
   const int side = 2 * h + 1, npts = side * side;
-  const int per_warp = 31 * kAdjLd + 31 * 32;
-  float2* T = adj_sm + warp * per_warp;          // [kx or fx][v], 31 x 65
-  float2* Aw = T + 31 * kAdjLd;                   // [fx][fy] accumulator, 31 x 32
+  float2* T = adj_sm + pair * kAdjPerPair;       // [kx or fx][v]
+  float2* Xa = T + 31 * kAdjLd;                   // pass 3: forward of the even v, per column
+  float2* Xb = Xa + 31 * kAdjXLd;                 // pass 3: forward of the odd v
+  float2* Aw = Xb + 31 * kAdjXLd;                 // [fx][fy] accumulator
   const LithoItem it = items[blockIdx.x];
   const int dx = lane - h;
   const bool col_live = lane < side;
-  for (int i = lane; i < 31 * 32; i += 32) Aw[i] = make_float2(0.f, 0.f);
-  __syncwarp();
+  for (int i = threadIdx.x & 63; i < 31 * 32; i += 64) Aw[i] = make_float2(0.f, 0.f);
+  pair_sync(pair);
   const float inv = 1.0f / 4096.0f;
-  for (int j = it.job_begin + warp; j < it.job_end; j += kAdjWarps) {
+  for (int j = it.job_begin + pair; j < it.job_end; j += kAdjPairs) {
     const LithoJob job = jobs[j];
     const float lam = (float)job.weight;
     const float2* tp = table + (size_t)job.tab * npts;
     const float2* m = Mb + (size_t)job.clip * npts;
     const float2* g = gl + (size_t)job.clip * 4096;
     float2 a[32], b[32];
-    // pass 1: columns kx = dx of E = phi M, inverse over ky
+    // pass 1: columns kx = dx of E = phi M, inverse over ky; role 0 the even
+    // outputs T(kx, 2v'), role 1 the odd ones T(kx, 2v'+1)
 #pragma unroll
     for (int i = 0; i < 32; ++i) a[i] = make_float2(0.f, 0.f);
     if (col_live) {
@@ -122,29 +135,23 @@ k_coarse64_adjoint(const LithoItem* __restrict__ items, const LithoJob* __restri
           a[d & 31] = etab ? __ldg(etab + (size_t)j * npts + p) : cmul(__ldg(tp + p), __ldg(m + p));
         }
     }
-    {
+    if (role == 1) {
 #pragma unroll
       for (int i = 0; i < 32; ++i) {
         const int d = i < 16 ? i : i - 32;
-        b[i] = twiddle64<+1>(a[i], d & 63);
+        a[i] = twiddle64<+1>(a[i], d & 63);
       }
-      fft_reg<32, +1>(a);
-      fft_reg<32, +1>(b);
     }
-    __syncwarp();
+    fft_reg<32, +1>(a);
     if (col_live) {
 #pragma unroll
-      for (int i = 0; i < 32; ++i) {
-        T[lane * kAdjLd + 2 * i] = a[i];
-        T[lane * kAdjLd + 2 * i + 1] = b[i];
-      }
+      for (int i = 0; i < 32; ++i) T[lane * kAdjLd + 2 * i + role] = a[i];
     }
-    __syncwarp();
-    // pass 2: rows v = lane, lane + 32: e(u, v) over kx, times g(u, v), then
+    pair_sync(pair);
+    // pass 2: rows v = lane + 32 role: e(u, v) over kx, times g(u, v), then
     // the forward DFT over u restricted to fx in [-h, h]; in place in T[., v].
-#pragma unroll 1
-    for (int half = 0; half < 2; ++half) {
-      const int v = lane + 32 * half;
+    {
+      const int v = lane + 32 * role;
 #pragma unroll
       for (int i = 0; i < 32; ++i) a[i] = make_float2(0.f, 0.f);
 #pragma unroll
@@ -165,40 +172,51 @@ k_coarse64_adjoint(const LithoItem* __restrict__ items, const LithoJob* __restri
       }
       fft_reg<32, -1>(a);
       fft_reg<32, -1>(b);
+      pair_sync(pair);   // every read of this job's pass-1 columns is done
 #pragma unroll
       for (int f = -kAdjHMax; f <= kAdjHMax; ++f)
         if (f >= -h && f <= h) T[(f + h) * kAdjLd + v] = combine64(a, b, f);
     }
-    __syncwarp();
-    // pass 3: lane = fx, forward over v restricted to fy in [-h, h]
+    pair_sync(pair);
+    // pass 3: lane = fx, forward over v restricted to fy in [-h, h]; role 0
+    // transforms the even v, role 1 the odd v, then each role combines half
+    // of the fy band
     if (col_live) {
       const float2* tr = T + lane * kAdjLd;
 #pragma unroll
-      for (int i = 0; i < 32; ++i) {
-        a[i] = tr[2 * i];
-        b[i] = tr[2 * i + 1];
-      }
+      for (int i = 0; i < 32; ++i) a[i] = tr[2 * i + role];
       fft_reg<32, -1>(a);
-      fft_reg<32, -1>(b);
+      float2* X = role ? Xb : Xa;
+#pragma unroll
+      for (int i = 0; i < 32; ++i) X[lane * kAdjXLd + i] = a[i];
+    }
+    pair_sync(pair);
+    if (col_live) {
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        a[i] = Xa[lane * kAdjXLd + i];
+        b[i] = Xb[lane * kAdjXLd + i];
+      }
       float2* arow = Aw + lane * 32;
 #pragma unroll
       for (int f = -kAdjHMax; f <= kAdjHMax; ++f)
-        if (f >= -h && f <= h) {
+        if (f >= -h && f <= h && (f > 0) == (role == 1)) {
           const float2 y = cscale(combine64(a, b, f), inv);
           const float2 ph = __ldg(tp + (f + h) * side + lane);   // phi(fx = dx, fy = f)
           const float2 acc = arow[f + h];
           arow[f + h] = cadd(acc, cscale(cmulc(y, ph), lam));    // lambda conj(phi) Y
         }
     }
-    __syncwarp();
+    pair_sync(pair);
   }
   __syncthreads();
-  // fixed-order sum over the block's warps -> partial[item][(fy+h) side + fx+h]
+  // fixed-order sum over the block's pairs -> partial[item][(fy+h) side + fx+h]
   float2* dst = partial + (size_t)blockIdx.x * npts;
   for (int id = threadIdx.x; id < npts; id += blockDim.x) {
     const int fy = id / side, fx = id % side;
     float2 s = make_float2(0.f, 0.f);
-    for (int wp = 0; wp < kAdjWarps; ++wp) s = cadd(s, adj_sm[wp * per_warp + 31 * kAdjLd + fx * 32 + fy]);
+    for (int pp = 0; pp < kAdjPairs; ++pp)
+      s = cadd(s, adj_sm[pp * kAdjPerPair + 31 * kAdjLd + 2 * 31 * kAdjXLd + fx * 32 + fy]);
     dst[id] = s;
   }
 }
@@ -684,9 +702,9 @@ extern "C" int litho_socs_adjoint(const LithoAbbePlan* plan, const void* blob, c
   k_gl64<<<dim3(p.n_clips, 64 / kGlRows), 256, 0, s>>>(static_cast<const float2*>(sens_box), p.h, gl);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
-  const size_t sm = (size_t)kAdjWarps * (31 * kAdjLd + 31 * 32) * sizeof(float2);
+  const size_t sm = (size_t)kAdjPairs * kAdjPerPair * sizeof(float2);
   cudaFuncSetAttribute(k_coarse64_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k_coarse64_adjoint<<<p.n_items, kAdjWarps * 32, sm, s>>>(items, jobs, static_cast<const float2*>(table), p.h,
+  k_coarse64_adjoint<<<p.n_items, kAdjPairs * 64, sm, s>>>(items, jobs, static_cast<const float2*>(table), p.h,
                                                             static_cast<const float2*>(mask_box),
                                                             static_cast<const float2*>(field_box), gl, part);
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
