@@ -184,12 +184,15 @@ k_coarse32(const LithoItem* __restrict__ items, const LithoJob* __restrict__ job
       if (t < n_t && col < side) {
         const LithoJob* jb = jobs + it.job_begin + t / ncomp;
         const int mx = __ldg(&jb->cx) + (col - h) + bm, cy = __ldg(&jb->cy);
+        // sqrt|w| rides in the field, so pass 2 accumulates |e|^2 without a multiply
+        const float sw = sqrtf(fabsf((float)__ldg(&jb->weight)));
         if (mx >= 0 && mx < Bm) {
           const float2* tp = TAB + half * npad + col;
 #pragma unroll
           for (int d = -kCoarseHMax32; d <= kCoarseHMax32; ++d) {
             const int my = cy + d + bm;
-            if (d >= -h && d <= h && my >= 0 && my < Bm) v[d & 31] = cmul(tp[(d + h) * side], msk[my * Bm + mx]);
+            if (d >= -h && d <= h && my >= 0 && my < Bm)
+              v[d & 31] = cmul(__fmul2_rn(tp[(d + h) * side], make_float2(sw, sw)), msk[my * Bm + mx]);
           }
         }
       }
@@ -214,9 +217,14 @@ k_coarse32(const LithoItem* __restrict__ items, const LithoJob* __restrict__ job
 #pragma unroll
       for (int d = -kCoarseHMax32; d <= kCoarseHMax32; ++d)
         if (d >= -h && d <= h) r[d & 31] = tc[(d + h) * kC32TLd];
-      fft_reg_sparse<32, +1, kNZ>(r);  // over kx: e(u, v = lane)
+      fft_reg_sparse<32, +1, kNZ>(r);  // over kx: sqrt|w| e(u, v = lane)
+      if (w >= 0.f) {  // warp-uniform: one transform per warp here
 #pragma unroll
-      for (int u = 0; u < 32; ++u) J[u] = fmaf(w, cabs2(r[u]), J[u]);
+        for (int u = 0; u < 32; ++u) J[u] = fmaf(r[u].x, r[u].x, fmaf(r[u].y, r[u].y, J[u]));
+      } else {
+#pragma unroll
+        for (int u = 0; u < 32; ++u) J[u] = fmaf(-r[u].x, r[u].x, fmaf(-r[u].y, r[u].y, J[u]));
+      }
     }
     __syncwarp();
   }
@@ -305,6 +313,7 @@ k_coarse64(const LithoItem* __restrict__ items, const LithoJob* __restrict__ job
   for (int j = it.job_begin + warp; j < it.job_end; j += kCoarse64Warps) {
     const LithoJob job = jobs[j];
     const float w = (float)job.weight;
+    const float sw = sqrtf(fabsf(w));  // carried in the field; the sign is applied in pass 2
     const float2* m = Mb + (size_t)job.clip * Bm * Bm;
     const int mx = job.cx + dx + bm;
     for (int c = 0; c < job.ncomp; ++c) {
@@ -317,7 +326,8 @@ k_coarse64(const LithoItem* __restrict__ items, const LithoJob* __restrict__ job
         for (int d = -kCoarseHMax64; d <= kCoarseHMax64; ++d) {
           const int my = job.cy + d + bm;
           if (d >= -h && d <= h && my >= 0 && my < Bm)
-            a[d & 31] = cmul(__ldg(tp + (d + h) * side + (dx + h)), __ldg(m + (size_t)my * Bm + mx));
+            a[d & 31] = cmul(__fmul2_rn(__ldg(tp + (d + h) * side + (dx + h)), make_float2(sw, sw)),
+                             __ldg(m + (size_t)my * Bm + mx));
         }
       }
       fft64_of_box(a, b);  // column kx = dx: T(kx, 2v') = a[v'], T(kx, 2v'+1) = b[v']
@@ -340,10 +350,11 @@ k_coarse64(const LithoItem* __restrict__ items, const LithoJob* __restrict__ job
           if (d >= -h && d <= h) a[d & 31] = T[(d + h) * kT64Ld + v];
         fft64_of_box(a, b);  // e(2u', v) = a[u'], e(2u'+1, v) = b[u']
         float* jr = Jw + v * kT64Ld;
+        const float sg = w >= 0.f ? 1.f : -1.f;
 #pragma unroll
         for (int i = 0; i < 32; ++i) {
-          jr[2 * i] = fmaf(w, cabs2(a[i]), jr[2 * i]);
-          jr[2 * i + 1] = fmaf(w, cabs2(b[i]), jr[2 * i + 1]);
+          jr[2 * i] = fmaf(sg * a[i].x, a[i].x, fmaf(sg * a[i].y, a[i].y, jr[2 * i]));
+          jr[2 * i + 1] = fmaf(sg * b[i].x, b[i].x, fmaf(sg * b[i].y, b[i].y, jr[2 * i + 1]));
         }
       }
     }

@@ -56,6 +56,42 @@ __device__ __forceinline__ float2 twiddle64(float2 b, int t) {
   return make_float2(b.x * c - b.y * s, b.x * s + b.y * c);
 }
 
+// One radix-2 butterfly (a, b) <- (a + w b, a - w b), w = exp(SIGN 2 pi i t / 64).
+// Component-wise sums run as packed FP32 pairs (__fadd2_rn / __ffma2_rn, one
+// instruction for both components). A non-trivial w is factored as
+// f (1 + i r) (|cos| >= |sin|: f = cos, r = tan) or f (r + i) (f = sin,
+// r = cot), |r| <= 1, so u = w b / f costs two FMAs and the scale by f rides
+// in the packed FMAs a +- f u. w = +-i keeps the swap-and-add form.
+template <int SIGN>
+__device__ __forceinline__ void bfly64(float2& a, float2& b, int t) {
+  t &= 63;
+  const float2 a0 = a;
+  if (t == 0 || t == 32) {
+    const float2 p = __fadd2_rn(a0, b), m = __fadd2_rn(a0, make_float2(-b.x, -b.y));
+    a = t == 0 ? p : m;
+    b = t == 0 ? m : p;
+    return;
+  }
+  if (t == 16 || t == 48) {
+    const float2 bw = twiddle64<SIGN>(b, t);
+    a = cadd(a0, bw);
+    b = csub(a0, bw);
+    return;
+  }
+  const float r = SIGN > 0 ? tw64_ratio(t) : -tw64_ratio(t);
+  float2 u;
+  float f;
+  if (tw64_cos_major(t)) {
+    u = make_float2(fmaf(-r, b.y, b.x), fmaf(r, b.x, b.y));
+    f = tw64_re(t);
+  } else {
+    u = make_float2(fmaf(r, b.x, -b.y), fmaf(r, b.y, b.x));
+    f = SIGN > 0 ? tw64_im(t) : -tw64_im(t);
+  }
+  a = __ffma2_rn(u, make_float2(f, f), a0);
+  b = __ffma2_rn(u, make_float2(-f, -f), a0);
+}
+
 template <int N, int SIGN>
 __device__ __forceinline__ void fft_reg(float2 (&v)[N]) {
   static_assert(N >= 2 && N <= 64 && (N & (N - 1)) == 0, "fft_reg: N in {2..64}");
@@ -74,12 +110,7 @@ __device__ __forceinline__ void fft_reg(float2 (&v)[N]) {
 #pragma unroll
     for (int base = 0; base < N; base += 2 * half) {
 #pragma unroll
-      for (int k = 0; k < half; ++k) {
-        const float2 a = v[base + k];
-        const float2 bw = twiddle64<SIGN>(v[base + k + half], k * (64 / (2 * half)));
-        v[base + k] = cadd(a, bw);
-        v[base + k + half] = csub(a, bw);
-      }
+      for (int k = 0; k < half; ++k) bfly64<SIGN>(v[base + k], v[base + k + half], k * (64 / (2 * half)));
     }
   }
 }
@@ -119,16 +150,12 @@ struct SparseStage {
             // both zero: stays zero
           } else if (zb) {
             v[base + k + HALF] = v[base + k];
-          } else {
+          } else if (za) {
             const float2 bw = twiddle64<SIGN>(v[base + k + HALF], k * (64 / (2 * HALF)));
-            if (za) {
-              v[base + k] = bw;
-              v[base + k + HALF] = make_float2(-bw.x, -bw.y);
-            } else {
-              const float2 a = v[base + k];
-              v[base + k] = cadd(a, bw);
-              v[base + k + HALF] = csub(a, bw);
-            }
+            v[base + k] = bw;
+            v[base + k + HALF] = make_float2(-bw.x, -bw.y);
+          } else {
+            bfly64<SIGN>(v[base + k], v[base + k + HALF], k * (64 / (2 * HALF)));
           }
         }
       }
