@@ -153,44 +153,61 @@ k_coarse32(const LithoItem* __restrict__ items, const LithoJob* __restrict__ job
   }
   const int n_t = (it.job_end - it.job_begin) * ncomp;
   const int n_pairs = (n_t + 1) >> 1;
-  auto fetch = [&](int pp) {
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      const int t = 2 * pp + half;
-      if (t < n_t) {
-        const int j = it.job_begin + t / ncomp, c = t % ncomp;
-        const float2* src = table + ((size_t)__ldg(&jobs[j].tab) * ncomp_max + c) * npts;
-        for (int e = lane; e < npts; e += 32) cp_async8(TAB + half * npad + e, src + e);
-      }
+  const int half = lane >> 4, col = lane & 15;
+  // This lane's transform t = 2 pp + half of a pair: its job's centre, weight
+  // and pupil-table offset (toff < 0: past the end). Loaded one pair ahead so
+  // the global loads overlap the current pair's transforms.
+  struct Rec {
+    int cx, cy, toff;
+    float w;
+  };
+  auto load_rec = [&](int pp) {
+    Rec r{0, 0, -1, 0.f};
+    const int t = 2 * pp + half;
+    if (pp < n_pairs && t < n_t) {
+      const int tj = div_ncomp(t, ncomp), c = t - tj * ncomp;
+      const LithoJob* jb = jobs + it.job_begin + tj;
+      r.cx = __ldg(&jb->cx);
+      r.cy = __ldg(&jb->cy);
+      r.w = (float)__ldg(&jb->weight);
+      r.toff = (__ldg(&jb->tab) * ncomp_max + c) * npts;
     }
+    return r;
+  };
+  // the pair's two pupil-table blocks into TAB (every lane copies part of both)
+  auto fetch = [&](const Rec& r) {
+    const int off[2] = {__shfl_sync(0xffffffffu, r.toff, 0), __shfl_sync(0xffffffffu, r.toff, 16)};
+#pragma unroll
+    for (int hf = 0; hf < 2; ++hf)
+      if (off[hf] >= 0)
+        for (int e = lane; e < npts; e += 32) cp_async8(TAB + hf * npad + e, table + off[hf] + e);
     cp_async_commit();
   };
-  if (warp < n_pairs) fetch(warp);
+  Rec cur = load_rec(warp);
+  if (warp < n_pairs) fetch(cur);
   __syncthreads();  // mask box staged
 
   float J[32];
 #pragma unroll
   for (int u = 0; u < 32; ++u) J[u] = 0.f;
-  const int half = lane >> 4, col = lane & 15;
   constexpr uint64_t kNZ = band_mask32(H);
   for (int pp = warp; pp < n_pairs; pp += kCoarseWarps) {
+    const Rec nxt = load_rec(pp + kCoarseWarps);
     cp_async_wait_all();
     __syncwarp();
     {
-      const int t = 2 * pp + half;
       float2 v[32];
 #pragma unroll
       for (int i = 0; i < 32; ++i) v[i] = make_float2(0.f, 0.f);
-      if (t < n_t && col < side) {
-        const LithoJob* jb = jobs + it.job_begin + t / ncomp;
-        const int mx = __ldg(&jb->cx) + (col - h) + bm, cy = __ldg(&jb->cy);
+      if (cur.toff >= 0 && col < side) {
+        const int mx = cur.cx + (col - h) + bm;
         // sqrt|w| rides in the field, so pass 2 accumulates |e|^2 without a multiply
-        const float sw = sqrtf(fabsf((float)__ldg(&jb->weight)));
+        const float sw = sqrtf(fabsf(cur.w));
         if (mx >= 0 && mx < Bm) {
           const float2* tp = TAB + half * npad + col;
 #pragma unroll
           for (int d = -kCoarseHMax32; d <= kCoarseHMax32; ++d) {
-            const int my = cy + d + bm;
+            const int my = cur.cy + d + bm;
             if (d >= -h && d <= h && my >= 0 && my < Bm)
               v[d & 31] = cmul(__fmul2_rn(tp[(d + h) * side], make_float2(sw, sw)), msk[my * Bm + mx]);
           }
@@ -204,12 +221,11 @@ k_coarse32(const LithoItem* __restrict__ items, const LithoJob* __restrict__ job
       }
     }
     __syncwarp();
-    if (pp + kCoarseWarps < n_pairs) fetch(pp + kCoarseWarps);  // TAB is free again
+    if (pp + kCoarseWarps < n_pairs) fetch(nxt);  // TAB is free again
 #pragma unroll
     for (int hh = 0; hh < 2; ++hh) {
-      const int t = 2 * pp + hh;
-      if (t >= n_t) break;
-      const float w = (float)__ldg(&jobs[it.job_begin + t / ncomp].weight);
+      if (2 * pp + hh >= n_t) break;
+      const float w = __shfl_sync(0xffffffffu, cur.w, 16 * hh);
       float2 r[32];
 #pragma unroll
       for (int i = 0; i < 32; ++i) r[i] = make_float2(0.f, 0.f);
@@ -227,6 +243,7 @@ k_coarse32(const LithoItem* __restrict__ items, const LithoJob* __restrict__ job
       }
     }
     __syncwarp();
+    cur = nxt;
   }
 
   // Fixed-order reduction of the warps' J into this block's partial.
@@ -650,6 +667,8 @@ static int check_plan(const LithoAbbePlan* p) {
     return LITHO_E_UNSUPPORTED;
   }
   if (p->bm < p->h) return LITHO_E_BAND;
+  // the coarse kernels address the pupil table with 32-bit element offsets
+  if ((int64_t)p->n_tab * p->ncomp_max * (2 * p->h + 1) * (2 * p->h + 1) >= ((int64_t)1 << 31)) return LITHO_E_SIZE;
   if (!(p->pixel_size > 0.0)) return LITHO_E_SIZE;
   const int64_t offs[7] = {p->off_jobs, p->off_pupils, p->off_items, p->off_out_items, p->off_norm,
                            p->off_slots, p->mirrored ? p->off_mirrors : 0};

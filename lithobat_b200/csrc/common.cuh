@@ -25,6 +25,12 @@ __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2
 __device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y; }
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 
+// t / n for a component count n in {1, 3} and 0 <= t < 2^31, without an
+// integer division (multiply-high by ceil(2^32 / 3)).
+__device__ __forceinline__ int div_ncomp(int t, int n) {
+  return n == 3 ? (int)__umulhi((unsigned)t, 0x55555556u) : t;
+}
+
 // ---------------------------------------------------------------------------
 // Register FFT: natural-order in and out, radix-2 decimation in time,
 // SIGN = +1 computes sum_k v_k exp(+2 pi i k j / N) (unnormalised inverse),

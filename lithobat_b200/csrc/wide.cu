@@ -62,7 +62,7 @@ k_wide_cols_w(const LithoJob* __restrict__ jobs, int j0, int ncomp_max, const fl
   float2* tb = wsm + L + warp * 32 * kTbLd;
   const int t = blockIdx.x;
   const int side = 2 * h + 1, npts = side * side, Bm = 2 * bm + 1;
-  const int j = j0 + t / ncomp_max, c = t % ncomp_max;
+  const int tj = div_ncomp(t, ncomp_max), j = j0 + tj, c = t - tj * ncomp_max;
   const LithoJob job = jobs[j];
   if (c >= job.ncomp) return;
   for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twL[i];
