@@ -28,11 +28,14 @@
 //                     tile, x range) units: one thread loads operand tiles
 //                     (cp.async.bulk, double-buffered), one thread issues the
 //                     MMAs into two TMEM accumulators, four warps drain the
-//                     accumulators (tcgen05.ld), scale, store coalesced rows
-//                     of the image and keep the maxima.
+//                     accumulators (tcgen05.ld), scale, stage 32 x 32 image
+//                     blocks in shared memory for 2-D tensor stores
+//                     (cp.async.bulk.tensor; coalesced row stores when no
+//                     tensor map can be made) and keep the maxima.
 // Peak normalisation needs the peak before the scaled image is written:
 // pass 0 computes only the maxima, pass 1 writes. Every wait is bounded and a
 // wait that gives up reports LITHO_E_TIMEOUT through the status word.
+#include <cuda.h>  // CUtensorMap (the encoder is fetched through the runtime)
 #include <cuda_fp16.h>
 
 #include <type_traits>
@@ -288,12 +291,20 @@ __device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64
 // blockmax[o][row tile][x range][warp]: the maximum over each drain warp's part.
 // N: the image side as a compile-time constant (the drain's store offsets
 // become immediates).
+// One 32 x 32 FP32 block (shared, row-major, 128-byte rows) to the image
+// tensor at element (x, y); x a multiple of 32.
+__device__ __forceinline__ void tma_store_block(const CUtensorMap* m, const void* src, int x, int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(m),
+               "r"(smem_u32(src)), "r"(x), "r"(y)
+               : "memory");
+}
+
 template <int PASS, int N>
 __global__ void __launch_bounds__(kSmThreads, 1)
 k_synth_mma(const __half* __restrict__ pplanes, const __half* __restrict__ qplanes,
             const float* __restrict__ inv_scale, int n_out, int kp, int xsplit, const LithoNorm* __restrict__ norm,
             const float* __restrict__ peak, float* __restrict__ image, float* __restrict__ blockmax,
-            int* __restrict__ status) {
+            int* __restrict__ status, const __grid_constant__ CUtensorMap tmap, int use_tmap) {
   extern __shared__ __align__(1024) unsigned char sm_raw[];
   __shared__ uint64_t bar_bfull[2], bar_bempty[2], bar_afull[2], bar_aempty[2], bar_accfull[2], bar_accempty[2];
   __shared__ uint64_t bar_drain;
@@ -410,8 +421,12 @@ k_synth_mma(const __half* __restrict__ pplanes, const __half* __restrict__ qplan
     }
   } else {
     // ---- accumulator drain (warps 0-3: TMEM lanes 32 w .. 32 w + 31) -------
-    // Each store instruction writes 32 consecutive x of one image row (128
-    // bytes, coalesced); the offsets of the 32 rows of a chunk are immediates.
+    // A chunk of 32 image rows x 32 x goes through this warp's shared-memory
+    // stage (two buffers) and out as one 2-D tensor store issued by lane 0,
+    // so the copy engine carries the image stores. Without a tensor map each
+    // store instruction writes 32 consecutive x of one row (128 bytes).
+    float* stage = reinterpret_cast<float*>(sm_raw + 2 * (abytes + bbytes)) + warp * 2 * 1024;
+    int sb = 0;
     int c = 0;
     bool ok = true;
     for (int u = blockIdx.x; u < n_units && ok; u += gridDim.x) {
@@ -446,7 +461,20 @@ k_synth_mma(const __half* __restrict__ pplanes, const __half* __restrict__ qplan
 #pragma unroll
             for (int q = 0; q < 32; ++q) mx = fmaxf(mx, __uint_as_float(r[q]));
           }
-          if (PASS == 1) {
+          if (PASS == 1 && use_tmap) {
+            float* sbuf = stage + sb * 1024;   // [row q][x]
+            if (lane == 0) bulk_wait_read<1>();  // the store out of sbuf (two chunks ago) has read it
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < 32; ++q) sbuf[q * 32 + lane] = __uint_as_float(r[q]) * sc;
+            fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) {
+              tma_store_block(&tmap, sbuf, x - lane, o * N + y0 + c0);
+              bulk_commit();
+            }
+            sb ^= 1;
+          } else if (PASS == 1) {
             float* dst = img + (size_t)(y0 + c0) * N + x;
 #pragma unroll
             for (int q = 0; q < 32; ++q) __stcs(dst + q * N, __uint_as_float(r[q]) * sc);
@@ -461,6 +489,7 @@ k_synth_mma(const __half* __restrict__ pplanes, const __half* __restrict__ qplan
       for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
       if (lane == 0) blockmax[(size_t)u * kSmDrainWarps + warp] = mx * inv;
     }
+    if (PASS == 1 && use_tmap && lane == 0) bulk_wait<0>();  // every store out of the stage is done
     if (!ok) s_fail = 1;
   }
 
@@ -472,6 +501,30 @@ k_synth_mma(const __half* __restrict__ pplanes, const __half* __restrict__ qplan
 
 __global__ void k_peak(const float* __restrict__ blockmax, int nblk, const LithoNorm* __restrict__ norm, int n_out,
                        int which, float* __restrict__ peak);
+
+// The n_out x n x n FP32 images as a 2-D tensor (n columns, n_out n rows)
+// stored in 32 x 32 blocks. False when the driver's encoder is unavailable or
+// refuses the layout (the drain then stores rows itself).
+static bool image_tmap(CUtensorMap* m, float* image, int n, int n_out) {
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static const Encode enc = []() -> Encode {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<Encode>(f);
+  }();
+  if (!enc || ((uintptr_t)image & 15) || (int64_t)n_out * n >= ((int64_t)1 << 31)) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)n_out * (cuuint64_t)n};
+  const cuuint64_t strides[1] = {(cuuint64_t)n * 4};
+  const cuuint32_t box[2] = {32, 32}, estride[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, image, dims, strides, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
 
 // Synthesis of n_out Hermitian boxes of side 2 g0 + 1 into n x n images, with
 // the normalisation of `norm` (nullptr: scale 1), the raw peaks into `peak`
@@ -499,7 +552,8 @@ cudaError_t launch_synth_mma(const float2* box, int g0, int n, int n_out, const 
   }
   k_synth_qplanes<<<n / kSmMT, kSmMT, 0, s>>>(tw, g0, n, kp, qp);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  const size_t smm = 2 * (size_t)(smma_a_bytes(kp) + smma_b_bytes(kp));
+  // operand buffers, then the drain warps' image stages (2 x 32 x 32 floats each)
+  const size_t smm = 2 * (size_t)(smma_a_bytes(kp) + smma_b_bytes(kp)) + (size_t)kSmDrainWarps * 2 * 1024 * 4;
   // split the x tiles of a (output, row tile) over blocks when there are
   // fewer of those than SMs (at most 8 ways, so the block maxima fit in
   // n / 8 floats per output)
@@ -510,6 +564,8 @@ cudaError_t launch_synth_mma(const float2* box, int g0, int n, int n_out, const 
   const int grid = units < num_sms ? units : num_sms;
   const int nblk = (n / kSmNT) * xsplit * kSmDrainWarps;
   const int pk_blocks = (n_out + 7) / 8;
+  CUtensorMap tmap{};
+  const int use_tmap = image_tmap(&tmap, image, n, n_out) ? 1 : 0;
   auto pass = [&](auto pass_c) -> cudaError_t {
     constexpr int P = decltype(pass_c)::value;
     switch (n) {
@@ -517,7 +573,7 @@ cudaError_t launch_synth_mma(const float2* box, int g0, int n, int n_out, const 
   case NN:                                                                                                       \
     cudaFuncSetAttribute(k_synth_mma<P, NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smm);             \
     k_synth_mma<P, NN><<<grid, kSmThreads, smm, s>>>(pp, qp, inv, n_out, kp, xsplit, norm, peak, image,          \
-                                                      blockmax, status);                                         \
+                                                      blockmax, status, tmap, P == 1 ? use_tmap : 0);           \
     break;
       LITHO_SMMA(256) LITHO_SMMA(512) LITHO_SMMA(1024) LITHO_SMMA(2048) LITHO_SMMA(4096)
 #undef LITHO_SMMA
