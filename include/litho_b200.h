@@ -349,6 +349,17 @@ int litho_ilt_objective(const float* img_dev, const float* target_dev, int n_fie
                         float* signed_out_dev, double* cost_part_dev, unsigned int* perr_part_dev,
                         int n_part, cudaStream_t stream);
 
+/* litho_ilt_objective() that also finishes the sums on the device: the last
+ * block of each field sums its partials in block order into cost_out[field]
+ * = sum (z - t)^2 / npix (the _Objective cost, opc/ilt.py:331) and
+ * perr_out[field] = the pattern-error count. counters_dev: n_fields words,
+ * zero before the first call; every call leaves them zero again. */
+int litho_ilt_objective_totals(const float* img_dev, const float* target_dev, int n_fields, int n, float scale,
+                               float level, float sign, float steepness_a, float* dfield_dev,
+                               float* signed_out_dev, double* cost_part_dev, unsigned int* perr_part_dev,
+                               int n_part, unsigned int* counters_dev, double* cost_out_dev,
+                               long long* perr_out_dev, cudaStream_t stream);
+
 /* TV (periodic neighbours) and discreteness penalties (opc/ilt.py:339-357):
  * adds their gradients to grad_dev and their costs to cost_part_dev. */
 int litho_ilt_penalties(const float* mask_dev, int n_fields, int n, float w_tv, float w_disc,

@@ -125,6 +125,8 @@ def lib():
         "litho_socs_adjoint_workspace": [i32, i32, i32, C.POINTER(sz)],
         "litho_socs_adjoint": [C.POINTER(AbbePlan), vp, vp, vp, vp, vp, vp, vp, sz, vp],
         "litho_ilt_objective": [vp, vp, i32, i32, f32, f32, f32, f32, vp, vp, vp, vp, i32, vp],
+        "litho_ilt_objective_totals": [vp, vp, i32, i32, f32, f32, f32, f32, vp, vp, vp, vp, i32, vp, vp, vp,
+                                       vp],
         "litho_ilt_penalties": [vp, i32, i32, f32, f32, vp, vp, i32, vp],
         "litho_ilt_mask": [vp, C.c_longlong, f32, vp, vp],
         "litho_ilt_theta_grad": [vp, vp, C.c_longlong, f32, vp, vp],

@@ -310,10 +310,16 @@ __device__ __forceinline__ float sigmoid_clipped(float s) {
 // Relaxed resist objective (opc/ilt.py:313-336), after the optional blur of
 // the image: fld = scale * img; signed = sign (fld - level);
 // z = sigmoid(a signed); resid = z - target; dfield = sign (2/npix) resid a z (1 - z).
+// TOTALS: the last block of each field to finish (counted in counters[field],
+// which it resets) also sums that field's partials in block order into
+// cost_out = sum / npix and perr_out.
+template <bool TOTALS>
 __global__ void k_ilt_objective(const float* __restrict__ img, const float* __restrict__ target, long long npix,
                                 float scale, float level, float sign, float a, float inv_npix2,
                                 float* __restrict__ dfield, float* __restrict__ signed_out,
-                                double* __restrict__ cost_part, unsigned int* __restrict__ perr_part) {
+                                double* __restrict__ cost_part, unsigned int* __restrict__ perr_part,
+                                unsigned int* __restrict__ counters, double* __restrict__ cost_out,
+                                long long* __restrict__ perr_out) {
   __shared__ double sc[32];
   __shared__ unsigned int sp[32];
   double cost = 0.0;
@@ -377,6 +383,28 @@ __global__ void k_ilt_objective(const float* __restrict__ img, const float* __re
     }
     cost_part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = c;
     perr_part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = p;
+  }
+  if (TOTALS) {
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+      __threadfence();  // this block's partials are visible before it is counted
+      last = atomicAdd(&counters[blockIdx.y], 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+      __threadfence();
+      const double* cp = cost_part + (size_t)blockIdx.y * gridDim.x;
+      const unsigned int* pq = perr_part + (size_t)blockIdx.y * gridDim.x;
+      double c = 0.0;
+      long long p = 0;
+      for (unsigned int b = 0; b < gridDim.x; ++b) {
+        c += __ldcg(cp + b);
+        p += __ldcg(pq + b);
+      }
+      cost_out[blockIdx.y] = c / (double)npix;
+      perr_out[blockIdx.y] = p;
+      counters[blockIdx.y] = 0u;
+    }
   }
 }
 
@@ -720,8 +748,26 @@ extern "C" int litho_ilt_objective(const float* img, const float* target, int n_
   if (n_fields < 1 || n < 1 || n_part < 1) return LITHO_E_SIZE;
   const double npix = (double)n * n;
   dim3 g(n_part, n_fields);
-  k_ilt_objective<<<g, 256, 0, s>>>(img, target, (long long)n * n, scale, level, sign, steepness_a,
-                                    (float)(2.0 / npix), dfield, signed_out, cost_part, perr_part);
+  k_ilt_objective<false><<<g, 256, 0, s>>>(img, target, (long long)n * n, scale, level, sign, steepness_a,
+                                           (float)(2.0 / npix), dfield, signed_out, cost_part, perr_part, nullptr,
+                                           nullptr, nullptr);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+extern "C" int litho_ilt_objective_totals(const float* img, const float* target, int n_fields, int n, float scale,
+                                          float level, float sign, float steepness_a, float* dfield,
+                                          float* signed_out, double* cost_part, unsigned int* perr_part, int n_part,
+                                          unsigned int* counters, double* cost_out, long long* perr_out,
+                                          cudaStream_t s) {
+  if (!img || !target || !dfield || !cost_part || !perr_part || !counters || !cost_out || !perr_out)
+    return LITHO_E_NULL;
+  if (n_fields < 1 || n < 1 || n_part < 1) return LITHO_E_SIZE;
+  const double npix = (double)n * n;
+  dim3 g(n_part, n_fields);
+  k_ilt_objective<true><<<g, 256, 0, s>>>(img, target, (long long)n * n, scale, level, sign, steepness_a,
+                                          (float)(2.0 / npix), dfield, signed_out, cost_part, perr_part, counters,
+                                          cost_out, perr_out);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? LITHO_OK : (int)e;
 }

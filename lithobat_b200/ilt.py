@@ -68,6 +68,7 @@ class _Stages:
         self.table = kernels.table()
         self._ws = {}
         self._blur = {}
+        self._obj_counters = None     # litho_ilt_objective_totals' per-field block counters
 
     def stream(self):
         return nat.stream_ptr(self.torch, self.dev)
@@ -172,13 +173,17 @@ class _Stages:
         signed = torch.empty_like(raw) if want_signed else None
         cpart = torch.empty((self.C, N_PART), dtype=torch.float64, device=self.dev)
         ppart = torch.empty((self.C, N_PART), dtype=torch.int32, device=self.dev)
-        nat.check("litho_ilt_objective", L.litho_ilt_objective(
+        if self._obj_counters is None:
+            self._obj_counters = torch.zeros((self.C,), dtype=torch.int32, device=self.dev)
+        cost = torch.empty((self.C,), dtype=torch.float64, device=self.dev)
+        perr = torch.empty((self.C,), dtype=torch.int64, device=self.dev)
+        nat.check("litho_ilt_objective_totals", L.litho_ilt_objective_totals(
             raw.data_ptr(), target.data_ptr(), self.C, self.n, float(scale), float(level), float(sign), float(a),
             dfield.data_ptr(), None if signed is None else signed.data_ptr(), cpart.data_ptr(), ppart.data_ptr(),
-            N_PART, self.stream()))
+            N_PART, self._obj_counters.data_ptr(), cost.data_ptr(), perr.data_ptr(), self.stream()))
         gbox = self.band(dfield, 2 * self.h, float(scale) / (self.n * self.n))
         hbox = self.adjoint_box(gbox, mbox, out=out_hbox)
-        return cpart.sum(dim=1) / float(self.n * self.n), hbox, signed, ppart.sum(dim=1)
+        return cost, hbox, signed, perr
 
     def update_split(self, hbox, theta, m1, m2, beta, beta_next, step, b1, b2, eps, it):
         """dJ/dm from its band box -> dJ/dtheta -> Adam (theta, m1, m2 in
