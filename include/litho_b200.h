@@ -360,6 +360,20 @@ int litho_ilt_objective_totals(const float* img_dev, const float* target_dev, in
                                int n_part, unsigned int* counters_dev, double* cost_out_dev,
                                long long* perr_out_dev, cudaStream_t stream);
 
+/* The raw SOCS image synthesised from its band box (side 2 g0 + 1 per field,
+ * as litho_band_synthesis) with the objective of litho_ilt_objective_totals()
+ * applied to every pixel as it is made, so the image itself is never stored:
+ * the image and objective halves of opc/ilt.py:_Objective (:313-336) on the
+ * band-limited image. Writes dfield, cost_out, perr_out (counters_dev as
+ * litho_ilt_objective_totals()); target_dev 16-byte aligned. The workspace
+ * query returns LITHO_E_UNSUPPORTED where the row-pair synthesis with its
+ * target stage does not apply (n a power of two in [256, 1024], g0 <= 31). */
+int litho_ilt_image_objective_workspace(int n_fields, int n, int g0, size_t* bytes);
+int litho_ilt_image_objective(const void* image_box_dev, int n_fields, int n, int g0, const float* target_dev,
+                              float scale, float level, float sign, float steepness_a, float* dfield_dev,
+                              unsigned int* counters_dev, double* cost_out_dev, long long* perr_out_dev,
+                              void* workspace, size_t ws_bytes, cudaStream_t stream);
+
 /* TV (periodic neighbours) and discreteness penalties (opc/ilt.py:339-357):
  * adds their gradients to grad_dev and their costs to cost_part_dev. */
 int litho_ilt_penalties(const float* mask_dev, int n_fields, int n, float w_tv, float w_disc,

@@ -17,6 +17,7 @@ LIB_PATH = Path(__file__).resolve().parent / "liblitho_b200.so"
 
 
 NOALLOC_SCRATCH_BYTES = 32 << 20   # LITHO_NOALLOC_SCRATCH_BYTES
+LITHO_E_UNSUPPORTED = -5           # a valid request this build does not serve
 
 
 class NativeUnavailable(RuntimeError):
@@ -125,6 +126,8 @@ def lib():
         "litho_socs_adjoint_workspace": [i32, i32, i32, C.POINTER(sz)],
         "litho_socs_adjoint": [C.POINTER(AbbePlan), vp, vp, vp, vp, vp, vp, vp, sz, vp],
         "litho_ilt_objective": [vp, vp, i32, i32, f32, f32, f32, f32, vp, vp, vp, vp, i32, vp],
+        "litho_ilt_image_objective_workspace": [i32, i32, i32, vp],
+        "litho_ilt_image_objective": [vp, i32, i32, i32, vp, f32, f32, f32, f32, vp, vp, vp, vp, vp, sz, vp],
         "litho_ilt_objective_totals": [vp, vp, i32, i32, f32, f32, f32, f32, vp, vp, vp, vp, i32, vp, vp, vp,
                                        vp],
         "litho_ilt_penalties": [vp, i32, i32, f32, f32, vp, vp, i32, vp],

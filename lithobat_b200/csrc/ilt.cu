@@ -18,6 +18,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "ilt_math.cuh"
 
 namespace litho {
 
@@ -30,6 +31,10 @@ bool synth_mma_ok(int n, int g0);
 int64_t synth_mma_bytes(int n_out, int n, int g0);
 int64_t synth_cols_bytes(int n_out, int n, int g0);
 bool synth_pairs_ok(int n, int g0);
+int synth_pairs_blocks(int n);
+bool synth_objective_ok(int n, int g0);
+cudaError_t launch_synth_objective(const float2* box, int g0, int n, int n_out, const float2* tw, float* blockmax,
+                                   float2* cbuf, const SynthObj& obj, cudaStream_t s);
 bool wide_adjoint_ok(int h);
 int64_t wide_adjoint_ws(int n_clips, int h);
 int wide_socs_adjoint(const LithoAbbePlan& p, const void* blob, const float2* table, const float2* mask_box,
@@ -302,11 +307,6 @@ k_synth_complex(const float2* __restrict__ box, int h, int n, const float2* __re
 // ---------------------------------------------------------------------------
 // Elementwise stages (n_fields x N x N, row-major).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float sigmoid_clipped(float s) {
-  s = fminf(fmaxf(s, -60.f), 60.f);
-  return 1.0f / (1.0f + expf(-s));
-}
-
 // Relaxed resist objective (opc/ilt.py:313-336), after the optional blur of
 // the image: fld = scale * img; signed = sign (fld - level);
 // z = sigmoid(a signed); resid = z - target; dfield = sign (2/npix) resid a z (1 - z).
@@ -349,15 +349,8 @@ __global__ void k_ilt_objective(const float* __restrict__ img, const float* __re
       float d[4], sg[4];
       float c4 = 0.f;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const float s = sign * (ii[q] * scale - level);
-        const float z = sigmoid_clipped(a * s);
-        const float r = z - tt[q];
-        c4 = fmaf(r, r, c4);
-        d[q] = sign * (inv_npix2 * r * (a * z * (1.0f - z)));
-        sg[q] = s;
-        perr += ((s > 0.f) != (tt[q] > 0.5f)) ? 1u : 0u;
-      }
+      for (int q = 0; q < 4; ++q)
+        d[q] = ilt_objective_pixel(ii[q], tt[q], scale, level, sign, a, inv_npix2, c4, perr, &sg[q]);
       cost += (double)c4;
       *reinterpret_cast<float4*>(dfield + i) = make_float4(d[0], d[1], d[2], d[3]);
       if (signed_out) *reinterpret_cast<float4*>(signed_out + i) = make_float4(sg[0], sg[1], sg[2], sg[3]);
@@ -769,6 +762,51 @@ extern "C" int litho_ilt_objective_totals(const float* img, const float* target,
                                           (float)(2.0 / npix), dfield, signed_out, cost_part, perr_part, counters,
                                           cost_out, perr_out);
   cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+// tw, block maxima, cost and pattern-error partials, then the column stage
+static int64_t image_obj_ws(int n_fields, int n, int g0) {
+  const int64_t nb = (int64_t)n_fields * synth_pairs_blocks(n);
+  return align16((int64_t)n * 8) + align16(nb * 4) + align16(nb * 8) + align16(nb * 4) +
+         align16(synth_cols_bytes(n_fields, n, g0));
+}
+
+extern "C" int litho_ilt_image_objective_workspace(int n_fields, int n, int g0, size_t* bytes) {
+  if (!bytes) return LITHO_E_NULL;
+  if (n_fields < 1 || n < 2 || g0 < 0) return LITHO_E_SIZE;
+  if (!synth_objective_ok(n, g0)) return LITHO_E_UNSUPPORTED;
+  *bytes = (size_t)image_obj_ws(n_fields, n, g0);
+  return LITHO_OK;
+}
+
+extern "C" int litho_ilt_image_objective(const void* image_box, int n_fields, int n, int g0, const float* target,
+                                         float scale, float level, float sign, float steepness_a, float* dfield,
+                                         unsigned int* counters, double* cost_out, long long* perr_out, void* ws,
+                                         size_t ws_bytes, cudaStream_t s) {
+  if (!image_box || !target || !dfield || !counters || !cost_out || !perr_out || !ws) return LITHO_E_NULL;
+  size_t need = 0;
+  const int st = litho_ilt_image_objective_workspace(n_fields, n, g0, &need);
+  if (st) return st;
+  if (ws_bytes < need) return LITHO_E_WORKSPACE;
+  if (((uintptr_t)ws | (uintptr_t)target) & 15) return LITHO_E_ALIGN;  // target rows are copied in 16-byte pieces
+  const int64_t nb = (int64_t)n_fields * synth_pairs_blocks(n);
+  char* w = static_cast<char*>(ws);
+  float2* tw = reinterpret_cast<float2*>(w);
+  w += align16((int64_t)n * 8);
+  float* blockmax = reinterpret_cast<float*>(w);
+  w += align16(nb * 4);
+  double* cpart = reinterpret_cast<double*>(w);
+  w += align16(nb * 8);
+  unsigned int* ppart = reinterpret_cast<unsigned int*>(w);
+  w += align16(nb * 4);
+  float2* cbuf = reinterpret_cast<float2*>(w);
+  k_twiddle_table<<<(n + 255) / 256, 256, 0, s>>>(tw, n, +1);
+  const double npix = (double)n * n;
+  const SynthObj obj{target, scale, level, sign, steepness_a, (float)(2.0 / npix), dfield, cpart, ppart, counters,
+                     cost_out, perr_out};
+  const cudaError_t e = launch_synth_objective(static_cast<const float2*>(image_box), g0, n, n_fields, tw, blockmax,
+                                               cbuf, obj, s);
   return e == cudaSuccess ? LITHO_OK : (int)e;
 }
 

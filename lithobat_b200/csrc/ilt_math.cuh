@@ -1,0 +1,45 @@
+// Per-pixel arithmetic of the ILT objective, shared by the objective kernel
+// (ilt.cu) and the synthesis that applies it to the image it makes (rows.cu),
+// so both give the same values bit for bit.
+#pragma once
+
+#include "common.cuh"
+
+namespace litho {
+
+// sigmoid(s) with s clipped to [-60, 60] (opc/ilt.py:326, 378).
+__device__ __forceinline__ float sigmoid_clipped(float s) {
+  s = fminf(fmaxf(s, -60.f), 60.f);
+  return 1.0f / (1.0f + expf(-s));
+}
+
+// One pixel of the relaxed resist objective (opc/ilt.py:_Objective, :313-336)
+// for image value img and target t: signed = sign (scale img - level),
+// z = sigmoid(a signed), r = z - t; accumulates r^2 into cost and the pattern
+// error into perr; returns dJ/dfield = sign (2 / npix) r a z (1 - z) (the
+// factor 2 / npix as inv_npix2); *signed_out receives signed.
+__device__ __forceinline__ float ilt_objective_pixel(float img, float t, float scale, float level, float sign,
+                                                     float a, float inv_npix2, float& cost, unsigned int& perr,
+                                                     float* signed_out) {
+  const float s = sign * (img * scale - level);
+  const float z = sigmoid_clipped(a * s);
+  const float r = z - t;
+  cost = fmaf(r, r, cost);
+  perr += ((s > 0.f) != (t > 0.5f)) ? 1u : 0u;
+  *signed_out = s;
+  return sign * (inv_npix2 * r * (a * z * (1.0f - z)));
+}
+
+// Operands of the objective applied inside the image synthesis.
+struct SynthObj {
+  const float* target;
+  float scale, level, sign, a, inv_npix2;
+  float* dfield;
+  double* cost_part;       // [field][block]
+  unsigned int* perr_part;
+  unsigned int* counters;  // [field], zero between calls
+  double* cost_out;        // [field]: sum / npix
+  long long* perr_out;
+};
+
+}  // namespace litho

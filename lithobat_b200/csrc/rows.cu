@@ -18,6 +18,7 @@
 // block maxima (no HBM traffic), pass 1 recomputes and writes
 // raw * scale / peak. Every reduction is in a fixed order.
 #include "common.cuh"
+#include "ilt_math.cuh"
 #include "rows.cuh"
 
 namespace litho {
@@ -25,6 +26,7 @@ namespace litho {
 constexpr int kSyWarps = 8;
 constexpr int kSyRows = 64;      // rows per block
 constexpr int kSyG0Max = 31;     // box half-width limit: G = 2 g0 + 1 <= 63
+constexpr int kSyObjStage = 2048;  // target values staged per warp (2 P rows of n <= 1024)
 
 // Shared-memory plan of one synthesis block.
 struct SynthSmem {
@@ -47,6 +49,11 @@ __host__ __device__ inline SynthSmem synth_smem(int n, int g0) {
   s.total = s.off_b + (size_t)s.G * s.G * 8;
   return s;
 }
+
+// Offset of the objective's target stage: after the synthesis operands,
+// rounded up to 128 bytes (its 16-byte copies need aligned destinations; the
+// operands end with the G x G box, an odd multiple of 8 bytes for odd G).
+__host__ __device__ inline size_t obj_stage_off(const SynthSmem& s) { return (s.total + 127) & ~(size_t)127; }
 
 // Is the pair-FFT synthesis available for this grid and box?
 bool synth_pairs_ok(int n, int g0) {
@@ -102,11 +109,17 @@ k_synth_cols(const float2* __restrict__ Bbox, int g0, int n, const float2* __res
   }
 }
 
-template <int PASS>
+// OBJ (PASS 1 only): the image is not stored; each pixel goes through the ILT
+// objective (ilt_objective_pixel against obj.target, whose rows are copied to
+// shared memory while the row pair's transform runs), dJ/dfield is stored in
+// obj.dfield, and the block's cost and pattern-error sums go to the partial
+// arrays, which the last block of each output totals (as k_ilt_objective).
+template <int PASS, bool OBJ = false>
 __global__ void __launch_bounds__(kSyWarps * 32, 2)
 k_synth_pairs(const float2* __restrict__ Bbox, int g0, int n, const float2* __restrict__ tw_inv,
               const LithoNorm* __restrict__ norm, const float* __restrict__ peak, float* __restrict__ image,
-              float* __restrict__ blockmax, const float2* __restrict__ Cg) {
+              float* __restrict__ blockmax, const float2* __restrict__ Cg, SynthObj obj = SynthObj{}) {
+  static_assert(!OBJ || PASS == 1, "the objective runs in the writing pass");
   extern __shared__ __align__(16) unsigned char sy_raw[];
   const SynthSmem L = synth_smem(n, g0);
   const int o = blockIdx.y, y0 = blockIdx.x * kSyRows;
@@ -158,8 +171,17 @@ k_synth_pairs(const float2* __restrict__ Bbox, int g0, int n, const float2* __re
   const int pg = lane / L.Lp, bl = lane % L.Lp;
   const int iters = kSyRows / (2 * kSyWarps * L.P);
   float mx = 0.f;
+  double ocost = 0.0;
+  unsigned int operr = 0;
+  // OBJ: this warp's 2 P target rows (2048 contiguous values for n <= 1024)
+  float* tg = reinterpret_cast<float*>(sy_raw + obj_stage_off(L)) + warp * kSyObjStage;
   for (int it = 0; it < iters; ++it) {
     const int pair = (it * kSyWarps + warp) * L.P + pg;
+    if (OBJ) {
+      const float* src = obj.target + ((size_t)o * n + y0 + 2 * (it * kSyWarps + warp) * L.P) * n;
+      for (int e = lane * 4; e < kSyObjStage; e += 128) cp_async16(tg + e, src + e);
+      cp_async_commit();
+    }
     const float2* c1 = C + (2 * pair) * gp;
     const float2* c2 = c1 + gp;
     float* row1 = image + ((size_t)o * n + y0 + 2 * pair) * n;
@@ -187,7 +209,24 @@ k_synth_pairs(const float2* __restrict__ Bbox, int g0, int n, const float2* __re
       fft_reg<32, +1>(Q);
 #pragma unroll
       for (int a = 0; a < 32; ++a) mx = fmaxf(mx, fmaxf(Q[a].x, Q[a].y));
-      if (PASS == 1) {
+      if (PASS == 1 && OBJ) {
+        const size_t i1 = ((size_t)o * n + y0 + 2 * pair) * n + b;
+        const float* t1 = tg + 2 * pg * n + b;
+        float* __restrict__ d1 = obj.dfield + i1;
+        float cc = 0.f, sg;
+        cp_async_wait_all();
+        __syncwarp();
+#pragma unroll
+        for (int a = 0; a < 32; ++a) {
+          const float ta = t1[M * a], tb = t1[n + M * a];
+          __stcs(d1 + M * a, ilt_objective_pixel(Q[a].x * sc, ta, obj.scale, obj.level, obj.sign, obj.a,
+                                                 obj.inv_npix2, cc, operr, &sg));
+          __stcs(d1 + n + M * a, ilt_objective_pixel(Q[a].y * sc, tb, obj.scale, obj.level, obj.sign, obj.a,
+                                                     obj.inv_npix2, cc, operr, &sg));
+        }
+        ocost += (double)cc;
+        __syncwarp();  // every lane is done with the stage before the next copy into it
+      } else if (PASS == 1) {
 #pragma unroll
         for (int a = 0; a < 32; ++a) {
           __stcs(row1 + b + M * a, Q[a].x * sc);
@@ -204,6 +243,46 @@ k_synth_pairs(const float2* __restrict__ Bbox, int g0, int n, const float2* __re
     float m = red[0];
     for (int i = 1; i < kSyWarps; ++i) m = fmaxf(m, red[i]);
     blockmax[(size_t)o * gridDim.x + blockIdx.x] = m;
+  }
+  if (OBJ) {
+    __shared__ double rc[kSyWarps];
+    __shared__ unsigned int rp[kSyWarps];
+    __shared__ bool last;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      ocost += __shfl_xor_sync(0xffffffffu, ocost, off);
+      operr += __shfl_xor_sync(0xffffffffu, operr, off);
+    }
+    if (lane == 0) {
+      rc[warp] = ocost;
+      rp[warp] = operr;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double c = 0.0;
+      unsigned int p = 0;
+      for (int i = 0; i < kSyWarps; ++i) {
+        c += rc[i];
+        p += rp[i];
+      }
+      obj.cost_part[(size_t)o * gridDim.x + blockIdx.x] = c;
+      obj.perr_part[(size_t)o * gridDim.x + blockIdx.x] = p;
+      __threadfence();  // the partials are visible before this block is counted
+      last = atomicAdd(&obj.counters[o], 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+      __threadfence();
+      double c = 0.0;
+      long long p = 0;
+      for (unsigned int i = 0; i < gridDim.x; ++i) {
+        c += __ldcg(obj.cost_part + (size_t)o * gridDim.x + i);
+        p += __ldcg(obj.perr_part + (size_t)o * gridDim.x + i);
+      }
+      obj.cost_out[o] = c / ((double)n * (double)n);
+      obj.perr_out[o] = p;
+      obj.counters[o] = 0u;
+    }
   }
 }
 
@@ -260,5 +339,30 @@ cudaError_t launch_synth_pairs(const float2* box, int g0, int n, int n_out, cons
 }
 
 int64_t synth_cols_bytes(int n_out, int n, int g0) { return (int64_t)n_out * (g0 + 1) * n * 8; }
+
+// The objective synthesis stages each warp's 2 P target rows (2 P n = 2048
+// values) in shared memory next to the synthesis operands.
+bool synth_objective_ok(int n, int g0) {
+  return synth_pairs_ok(n, g0) && n <= 1024 &&
+         obj_stage_off(synth_smem(n, g0)) + (size_t)kSyWarps * kSyObjStage * 4 <= 110 * 1024;
+}
+
+// The image synthesis of launch_synth_pairs (no normalisation) with the ILT
+// objective applied to every pixel instead of storing the image; the column
+// stage runs ahead into cbuf. Partials: [n_out][n / kSyRows] in obj.
+cudaError_t launch_synth_objective(const float2* box, int g0, int n, int n_out, const float2* tw, float* blockmax,
+                                   float2* cbuf, const SynthObj& obj, cudaStream_t s) {
+  const SynthSmem L = synth_smem(n, g0);
+  const dim3 grid(n / kSyRows, n_out);
+  const size_t smc = (size_t)(g0 + 1) * (n >> 5) * 8;
+  k_synth_cols<<<dim3((g0 + 1 + kColWarps - 1) / kColWarps, n_out), kColWarps * 32, smc, s>>>(box, g0, n, tw, cbuf);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const size_t sm = obj_stage_off(L) + (size_t)kSyWarps * kSyObjStage * 4;
+  cudaFuncSetAttribute(k_synth_pairs<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_synth_pairs<1, true><<<grid, kSyWarps * 32, sm, s>>>(box, g0, n, tw, nullptr, nullptr, nullptr, blockmax, cbuf,
+                                                         obj);
+  return cudaGetLastError();
+}
 
 }  // namespace litho
