@@ -69,6 +69,7 @@ class _Stages:
         self._ws = {}
         self._blur = {}
         self._obj_counters = None     # litho_ilt_objective_totals' per-field block counters
+        self._imgobj_ok = None
 
     def stream(self):
         return nat.stream_ptr(self.torch, self.dev)
@@ -167,16 +168,31 @@ class _Stages:
         None, perr (C,)). Synthesis of the image, the per-pixel resist, the
         band of dJ/dI, the adjoint to the gradient's band box."""
         torch, L = self.torch, self.L
-        raw = self.image(mbox)
         a = steepness / max(abs(level), 1e-12)
-        dfield = torch.empty_like(raw)
-        signed = torch.empty_like(raw) if want_signed else None
-        cpart = torch.empty((self.C, N_PART), dtype=torch.float64, device=self.dev)
-        ppart = torch.empty((self.C, N_PART), dtype=torch.int32, device=self.dev)
         if self._obj_counters is None:
             self._obj_counters = torch.zeros((self.C,), dtype=torch.int32, device=self.dev)
         cost = torch.empty((self.C,), dtype=torch.float64, device=self.dev)
         perr = torch.empty((self.C,), dtype=torch.int64, device=self.dev)
+        if not want_signed and self.image_objective_ok() and target.data_ptr() % 16 == 0:
+            # the image is synthesised straight into the objective (never stored)
+            ibox = self.image_box(mbox)
+            nb = C.c_size_t(0)
+            nat.check("litho_ilt_image_objective_workspace", L.litho_ilt_image_objective_workspace(
+                self.C, self.n, 2 * self.h, C.byref(nb)))
+            ws = self.ws("imgobj", nb.value)
+            dfield = torch.empty((self.C, self.n, self.n), dtype=torch.float32, device=self.dev)
+            nat.check("litho_ilt_image_objective", L.litho_ilt_image_objective(
+                ibox.data_ptr(), self.C, self.n, 2 * self.h, target.data_ptr(), float(scale), float(level),
+                float(sign), float(a), dfield.data_ptr(), self._obj_counters.data_ptr(), cost.data_ptr(),
+                perr.data_ptr(), ws.data_ptr(), ws.numel(), self.stream()))
+            gbox = self.band(dfield, 2 * self.h, float(scale) / (self.n * self.n))
+            hbox = self.adjoint_box(gbox, mbox, out=out_hbox)
+            return cost, hbox, None, perr
+        raw = self.image(mbox)
+        dfield = torch.empty_like(raw)
+        signed = torch.empty_like(raw) if want_signed else None
+        cpart = torch.empty((self.C, N_PART), dtype=torch.float64, device=self.dev)
+        ppart = torch.empty((self.C, N_PART), dtype=torch.int32, device=self.dev)
         nat.check("litho_ilt_objective_totals", L.litho_ilt_objective_totals(
             raw.data_ptr(), target.data_ptr(), self.C, self.n, float(scale), float(level), float(sign), float(a),
             dfield.data_ptr(), None if signed is None else signed.data_ptr(), cpart.data_ptr(), ppart.data_ptr(),
@@ -184,6 +200,16 @@ class _Stages:
         gbox = self.band(dfield, 2 * self.h, float(scale) / (self.n * self.n))
         hbox = self.adjoint_box(gbox, mbox, out=out_hbox)
         return cost, hbox, signed, perr
+
+    def image_objective_ok(self) -> bool:
+        """Whether litho_ilt_image_objective serves this grid and band."""
+        if self._imgobj_ok is None:
+            nb = C.c_size_t(0)
+            st = self.L.litho_ilt_image_objective_workspace(self.C, self.n, 2 * self.h, C.byref(nb))
+            if st not in (0, nat.LITHO_E_UNSUPPORTED):
+                nat.check("litho_ilt_image_objective_workspace", st)
+            self._imgobj_ok = st == 0
+        return self._imgobj_ok
 
     def update_split(self, hbox, theta, m1, m2, beta, beta_next, step, b1, b2, eps, it):
         """dJ/dm from its band box -> dJ/dtheta -> Adam (theta, m1, m2 in

@@ -203,3 +203,52 @@ def test_graph_replayed_steps_match_eager_steps(lb):
     np.testing.assert_allclose(b.cost.cpu().numpy(), a.cost.cpu().numpy(), rtol=1e-6)
     with pytest.raises(RuntimeError):
         b.step()
+
+
+def test_image_objective_matches_synthesis_then_objective(lb):
+    """litho_ilt_image_objective (the objective applied inside the image
+    synthesis) against litho_band_synthesis + litho_ilt_objective_totals on the
+    same band boxes: dJ/dfield identical, pattern errors identical, cost to
+    summation order (FP32 runs of 64 pixels before FP64 against 4)."""
+    import ctypes as C
+    import torch
+    from lithobat_b200 import _native as nat
+    from lithobat_b200 import ilt
+    from lithobat_b200.patterns import manhattan_clip
+    o = lb.OpticsConfig(wavelength=193e-9, NA=1.35, n_immersion=1.44, source_type="annular", sigma_inner=0.5,
+                        sigma_outer=0.8, source_grid=11, normalisation="clear")
+    for n, F in ((256, 3), (512, 2), (1024, 2)):
+        g = lb.GridConfig(n_pixels=n, pixel_size=2e-9 * 256 / n)
+        k = lb.SOCSKernels.build(o, g, tol=0.0, max_kernels=8)
+        st = ilt.stages(k, F, "fused")
+        assert st.image_objective_ok()
+        rng = np.random.default_rng(n)
+        tg = np.stack([manhattan_clip(rng, n, g.pixel_size, n_rect=(4, 8), width_nm=(40, 120)) for _ in range(F)])
+        target = torch.from_numpy(tg.astype(np.float32)).to(st.dev)
+        mask = torch.from_numpy(rng.random((F, n, n)).astype(np.float32)).to(st.dev)
+        ibox = st.image_box(st.mask_box(mask))
+        scale, level, sign, a = 1.0 / k.clear, 0.3, 1.0, 50.0
+        raw = st.synth(ibox, 2 * st.h, False)
+        d0 = torch.empty_like(raw)
+        cp = torch.empty((F, 64), dtype=torch.float64, device=st.dev)
+        pp = torch.empty((F, 64), dtype=torch.int32, device=st.dev)
+        ctr = torch.zeros((F,), dtype=torch.int32, device=st.dev)
+        c0 = torch.empty((F,), dtype=torch.float64, device=st.dev)
+        p0 = torch.empty((F,), dtype=torch.int64, device=st.dev)
+        nat.check("totals", st.L.litho_ilt_objective_totals(
+            raw.data_ptr(), target.data_ptr(), F, n, scale, level, sign, a, d0.data_ptr(), None, cp.data_ptr(),
+            pp.data_ptr(), 64, ctr.data_ptr(), c0.data_ptr(), p0.data_ptr(), st.stream()))
+        nb = C.c_size_t(0)
+        nat.check("ws", st.L.litho_ilt_image_objective_workspace(F, n, 2 * st.h, C.byref(nb)))
+        ws = torch.empty(nb.value, dtype=torch.uint8, device=st.dev)
+        d1 = torch.empty_like(raw)
+        c1 = torch.empty_like(c0)
+        p1 = torch.empty_like(p0)
+        for _ in range(2):   # the counters are left at zero for the next call
+            nat.check("imgobj", st.L.litho_ilt_image_objective(
+                ibox.data_ptr(), F, n, 2 * st.h, target.data_ptr(), scale, level, sign, a, d1.data_ptr(),
+                ctr.data_ptr(), c1.data_ptr(), p1.data_ptr(), ws.data_ptr(), ws.numel(), st.stream()))
+        torch.cuda.synchronize()
+        assert torch.equal(d0, d1)
+        assert torch.equal(p0, p1) and int(ctr.abs().sum()) == 0
+        np.testing.assert_allclose(c1.cpu().numpy(), c0.cpu().numpy(), rtol=1e-7)
