@@ -505,7 +505,12 @@ def run_ours(args) -> None:
     pd = aerial.plan_abbe([view] * B, N, PX, [[(view.defocus, view.image_index)]] * B, 1.0, False, True)
     out = torch.empty((B, N, N), dtype=torch.float32, device=dev)
     peak = torch.empty((B,), dtype=torch.float32, device=dev)
-    launches_per_step = 7   # twiddles, band rows, band columns, coarse, reduce, synthesis, normalise
+    # twiddles, band rows, band columns, coarse, reduce, then the synthesis: on the tensor cores
+    # (enough 128 x 256 output tiles for about 16 per SM) P planes, Q planes, peak pass, peak,
+    # writing pass, peak; otherwise column stage, peak pass, peak, writing pass, peak
+    g0 = 2 * int(pd.plan.h)
+    tensor_synth = g0 <= 31 and B * (N // 256) * (N // 128) >= 16 * 148
+    launches_per_step = 5 + (6 if tensor_synth else 5)
 
     def step(i):
         aerial.run_abbe(pd, dmasks[i % ROTATE], out, peak)
