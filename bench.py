@@ -12,11 +12,16 @@ coherent transforms per image), peak normalisation. Each rank images its own
 clips (weak scaling, no collective on the data path).
 
 Prints one JSON line (rank 0). ``value`` is whole-job images/s with inputs
-resident in HBM; ``e2e`` is the same metric through the public API
-(``compute_aerial_batch``) from pinned host buffers, copies included.
-``--impl reference`` times the reference's algorithm on the host CPU (the
-FP64 numpy restatement in ``oracle/``, the same numpy/scipy calls), on a
-bounded sample of source points, and prints the same line for it.
+resident in HBM; ``e2e`` is the same metric through the public host-to-host
+API (``lithobat_b200.pipeline.AbbePipeline``) from pinned host buffers, the
+H2D and D2H copies inside the timed region. Extra keys time the other
+workloads (``c1``, ``c2``, ``ilt``, ``uneven``). ``cpu_baseline`` is one whole
+workload image through the FP64 numpy restatement of the reference's
+algorithm (``oracle/``) on the host cores; its output is also the FP64
+reference of ``max_rel_err_vs_fp64`` (one image of the timed batch).
+``--impl reference`` times that CPU algorithm for the reference arm: every
+step a bounded sample (a fixed set of the image's source points), reported
+as images/s of the work the step really did.
 """
 
 from __future__ import annotations
@@ -127,6 +132,7 @@ def bench_ilt(args, torch, dev, world, max_over_ranks, barrier) -> dict:
     e1.record()
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1))
+    b.check_status()
     value = world * nclip * args.steps / (ms / 1000.0)
     # stage times of one step (events on the launching stream)
     st = b.st
@@ -227,7 +233,30 @@ def bench_ilt(args, torch, dev, world, max_over_ranks, barrier) -> dict:
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1000.0))
     NN = N * N
+    # the FP64 check of one clip at the batch's initial state (same 16-clip stages)
+    chk = ilt.IltBatch(k, torch.from_numpy(targets).to(dev), torch.from_numpy(theta).to(dev), params)
+    chk.check_status()
+    fp64_case = {"target": targets[0], "theta": theta[0], "beta": float(params.beta),
+                 "cost": float(chk.cost[0]), "grad": chk.grad_m[0].double().cpu().numpy()}
+    del chk
+    # algorithmic bytes of one fast step per clip pixel: gradient synthesis
+    # writes g (4); the update reads g and theta, m1, m2 (16) and writes
+    # theta, m1, m2 and the mask (16); the mask's band rows read it (4); the
+    # image objective reads the target and writes dJ/dI (8); dJ/dI's band rows
+    # read it (4). Band boxes and kernel tables are below 0.1 %.
+    ilt_bytes = {"gradient_write": 4, "update_read": 16, "update_write": 16, "mask_band_read": 4,
+                 "objective_target_read": 4, "objective_dJdI_write": 4, "sensitivity_band_read": 4}
+    per_px = sum(ilt_bytes.values())
+    hbm = float(measured_peaks()["hbm_gbs"])
+    ach = per_px * NN * nclip / (ms / args.steps / 1000.0) / 1e9
+    upd_ms = stages.get("theta_grad+adam+mask")
+    roof = {"bound": "hbm", "kernel": "whole step (graph replay)", "achieved": ach, "peak": hbm, "unit": "GB/s",
+            "frac": ach / hbm, "bytes_per_clip_pixel": ilt_bytes, "bytes_per_step": per_px * NN * nclip}
+    if upd_ms:
+        roof["update_kernel"] = {"bytes_per_launch": 32 * NN * nclip, "ms": upd_ms,
+                                 "frac": 32 * NN * nclip / (upd_ms / 1000.0) / 1e9 / hbm}
     return {
+        "_fp64_case": fp64_case, "roofline": roof,
         "metric": "ILT gradient steps/s @1024^2 (clip-steps)", "value": value, "unit": "clip-steps/s",
         "ms_per_step": ms / args.steps, "clips_per_step": nclip, "workload": ILT_WORKLOAD,
         "kernels": len(k), "socs_build_ms": build_ms, "fast_step": bool(b.fast),
@@ -328,19 +357,128 @@ def bench_uneven(args, torch, dev, world, max_over_ranks, barrier) -> dict:
             "setup_and_tuning_s": setup_s, "max_rel_diff_vs_single_clip": worst}
 
 
-def cpu_ilt_seconds() -> tuple[float, int]:
-    """FP64 numpy objective (forward + adjoint) of one clip of the ILT workload, K = 24."""
+def cpu_ilt_check(case: dict) -> tuple[float, float, float]:
+    """FP64 numpy objective (forward + adjoint, K = 24) of one clip of the ILT
+    batch at the GPU's state: (seconds, cost error, gradient error)."""
     from oracle import litho_oracle as O
     o = ilt_optics()
 
     class G:
         n_pixels, pixel_size = N, PX
     k = O.socs_build(o, G, tol=0.0, max_kernels=24)
-    targets, theta = ilt_inputs(500, 1)
-    m = O.mask_of(theta[0].astype(np.float64), 4.0, 0.0)
+    m = O.mask_of(case["theta"].astype(np.float64), case["beta"], 0.0)
     t0 = time.perf_counter()
-    O.objective(k, targets[0].astype(np.float64), m, 1.0 / k.clear, 0.3, 0.0, 1.0, 15.0)
-    return time.perf_counter() - t0, 1
+    cost, grad, _, _ = O.objective(k, case["target"].astype(np.float64), m, 1.0 / k.clear, 0.3, 0.0, 1.0, 15.0)
+    t = time.perf_counter() - t0
+    e_cost = abs(case["cost"] - cost) / abs(cost)
+    e_grad = float(np.abs(case["grad"] - grad).max() / np.abs(grad).max())
+    return t, e_cost, e_grad
+
+
+def cpu_config_check(case: dict) -> dict:
+    """One image of a config through the FP64 reference algorithm on the host:
+    its time (the config's CPU baseline) and the GPU image's error against it."""
+    from oracle import litho_oracle as O
+
+    class G:
+        n_pixels, pixel_size = case["n"], case["px"]
+    t0 = time.perf_counter()
+    raw, pk, _ = O.compute_aerial_image(case["mask"], case["optics"], G, return_raw=True)
+    t = time.perf_counter() - t0
+    ref = raw / pk if case["peak_normalised"] else raw
+    return {"cpu_baseline": {"value": 1.0 / t, "unit": "images/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": "one whole image of the timed batch, FP64 numpy/scipy (FFT workers=-1)"},
+            "max_rel_err_vs_fp64": float(np.abs(case["gpu"] - ref).max() / np.abs(ref).max())}
+
+
+C1_WORKLOAD = ("scalar Abbe 256^2 @4 nm, ArF dry NA 0.93, annular 0.5-0.8 (source_grid 31, 264 pts), "
+               "L/S 200/100 nm binary mask, peak normalisation")
+C2_WORKLOAD = ("scalar Abbe 512^2 @2 nm x64 Manhattan clips (complex64), NA 1.35/1.44 quadrupole 0.7-0.9 30 deg, "
+               "per-clip defocus U(-60,60) nm and Z4-Z21 U(-0.02,0.02) waves, peak normalisation")
+
+
+def bench_config(tag: str, args, torch, dev, world, max_over_ranks, barrier) -> dict:
+    """Images/s of the first two workloads (c1: 1024 images of 256^2 per step;
+    c2: the 64-clip 512^2 batch per step), two rotating input batches larger
+    than L2, with stage times, the HBM roofline of the streaming stages and
+    (C1) the latency of one single-image call."""
+    import lithobat_b200 as lb
+    from lithobat_b200 import aerial, patterns
+    rank = int(os.environ.get("RANK", "0"))
+    if tag == "c1":
+        n, px, B = 256, 4e-9, 1024
+        o = lb.OpticsConfig(wavelength=193e-9, NA=0.93, source_type="annular", sigma_inner=0.5, sigma_outer=0.8,
+                            source_grid=31)
+        one = patterns.lines_and_spaces(n, px, 200e-9, 100e-9).astype(np.float32)
+        host = [np.broadcast_to(one, (B, n, n)) for _ in range(ROTATE)]
+        optics = [o] * B
+        workload = C1_WORKLOAD
+    else:
+        n, px, B = 512, 2e-9, 64
+        src = lb.Source.quadrupole(0.9, 0.7, 30, 0).to_dict()
+        host, optics = [], None
+        for r in range(ROTATE):
+            rng = np.random.default_rng(40 + 10 * rank + r)
+            host.append(np.stack([patterns.manhattan_clip(rng, n, px) for _ in range(B)]).astype(np.complex64))
+            if optics is None:
+                optics = [lb.OpticsConfig(NA=1.35, n_immersion=1.44, source_spec=src,
+                                          defocus=float(rng.uniform(-60e-9, 60e-9)),
+                                          zernike_coeffs={j: float(rng.uniform(-0.02, 0.02)) for j in range(4, 22)})
+                          for _ in range(B)]
+        workload = C2_WORKLOAD
+    views = [lb.config.optics_view(x) for x in optics]
+    dmasks = [torch.from_numpy(np.ascontiguousarray(h)).to(dev) for h in host]
+    pd = aerial.plan_abbe(views, n, px, [[(v.defocus, v.image_index)] for v in views], 1.0, False,
+                          bool(dmasks[0].is_complex()))
+    out = torch.empty((B, n, n), dtype=torch.float32, device=dev)
+    peak = torch.empty((B,), dtype=torch.float32, device=dev)
+    for i in range(max(3, args.warmup)):
+        aerial.run_abbe(pd, dmasks[i % ROTATE], out, peak)
+    torch.cuda.synchronize()
+    barrier()
+    steps = args.steps
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(steps):
+        aerial.run_abbe(pd, dmasks[i % ROTATE], out, peak)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / steps)
+    aerial.check_status(pd, dev)
+    stages = aerial.profile_abbe(pd, dmasks[0], reps=max(3, min(steps, 10)))
+    NN = n * n
+    Bm = 2 * pd.plan.bm + 1
+    esz = 8 if dmasks[0].is_complex() else 4
+    stage_bytes = {"band_rows": B * (NN * esz + n * Bm * 8), "synthesis": B * NN * 4}
+    dom = max(stage_bytes, key=stages.get)
+    hbm = float(measured_peaks()["hbm_gbs"])
+    achieved = stage_bytes[dom] / (stages[dom] / 1000.0) / 1e9
+    res = {"workload": workload, "value": world * B / (ms / 1000.0), "unit": "images/s", "ms_per_step": ms,
+           "images_per_step": B, "source_points": pd.jobs // B, "transforms_per_image": pd.transforms // B,
+           "engine": aerial.engine_info(pd), "stages_ms": stages,
+           "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                        "frac": achieved / hbm, "bytes_per_launch": stage_bytes[dom]},
+           "l2": f"{ROTATE} rotating input batches of {B * NN * esz >> 20} MiB"}
+    if tag == "c1":
+        # one image per call: the latency a single-image caller sees
+        pd1 = aerial.plan_abbe(views[:1], n, px, [[(views[0].defocus, views[0].image_index)]], 1.0, False, False)
+        m1 = dmasks[0][:1].contiguous()
+        o1 = torch.empty((1, n, n), dtype=torch.float32, device=dev)
+        p1 = torch.empty((1,), dtype=torch.float32, device=dev)
+        for _ in range(3):
+            aerial.run_abbe(pd1, m1, o1, p1)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(20):
+            aerial.run_abbe(pd1, m1, o1, p1)
+        e1.record()
+        torch.cuda.synchronize()
+        res["single_image_ms"] = e0.elapsed_time(e1) / 20
+    aerial.run_abbe(pd, dmasks[0], out, peak)
+    res["_fp64_case"] = {"n": n, "px": px, "optics": optics[0], "mask": host[0][0].astype(np.complex128),
+                         "gpu": out[0].double().cpu().numpy(), "peak_normalised": True}
+    del dmasks, out
+    return res
 
 
 def measured_peaks() -> dict:
@@ -410,16 +548,29 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU (reference algorithm) timing
 # ---------------------------------------------------------------------------
+def cpu_info() -> dict:
+    """The host CPU the CPU numbers ran on: model name and logical cores."""
+    model = "unknown"
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"model": model, "logical_cores": os.cpu_count()}
+
+
 class CpuAbbeSample:
     """The FP64 numpy Abbe sum (the reference algorithm, restated in the
-    oracle) over the first k source points of one workload image."""
+    oracle) of one workload image, whole or over its first k source points."""
 
-    def __init__(self):
+    def __init__(self, mask=None):
         from oracle import litho_oracle as O
         self.O = O
         self.o = optics_c3()
         self.S = len(O.source_points(self.o))
-        self.mask = masks_c3(1, 1)[0].astype(np.complex128)
+        self.mask = (masks_c3(1, 1)[0] if mask is None else np.asarray(mask)).astype(np.complex128)
 
         class G:
             n_pixels, pixel_size = N, PX
@@ -427,41 +578,46 @@ class CpuAbbeSample:
         self.planes = [(self.o.defocus, self.o.image_index)]
         self(2)  # warm the FFT plans
 
-    def __call__(self, k: int) -> float:
+    def __call__(self, k: int | None = None) -> float:
         t0 = time.perf_counter()
-        self.O.abbe_sum(self.mask, self.o, self.G, self.planes, source_subset=range(k))
+        self.last = self.O.abbe_sum(self.mask, self.o, self.G, self.planes,
+                                    source_subset=None if k is None else range(k))
         return time.perf_counter() - t0
 
 
-def cpu_sample_seconds(n_src: int = 12, repeats: int = 2) -> tuple[float, int, int]:
-    """Median seconds of the CPU Abbe sum over the first n_src source points
-    of one workload image; returns (t, n_src, S_total)."""
-    smp = CpuAbbeSample()
-    return statistics.median(smp(n_src) for _ in range(repeats)), n_src, smp.S
-
-
 def run_reference(args) -> None:
+    """The reference arm: the reference's CPU algorithm on the host cores.
+
+    Each step is a bounded sample of the workload, the same first k source
+    points of one workload image (3k of its 1200 coherent transforms, FP64,
+    scipy FFTs on all cores), with k sized so the whole warm-up + timed run
+    takes about 150 s. ``value`` is the images/s that work amounts to
+    (k / 400 of an image per step) and ``ms_per_step`` its measured time."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     smp = CpuAbbeSample()
-    # source points per step: the whole run stays near 150 s of CPU work
-    t1 = smp(2) / 2.0
-    k = int(max(1, min(12, 150.0 / max(1, args.warmup + args.steps) / max(t1, 1e-3))))
     S = smp.S
-    vals = []
-    for i in range(args.warmup + args.steps):
-        t = smp(k)
-        if i >= args.warmup:
-            vals.append(1.0 / (t * S / k))
-    v = statistics.median(vals)
+    t1 = smp(2) / 2.0
+    k = int(max(1, min(S, 150.0 / max(1, args.warmup + args.steps) / max(t1, 1e-3))))
+    for _ in range(args.warmup):
+        smp(k)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        smp(k)
+    total = time.perf_counter() - t0
+    v = (k / S) * args.steps / total
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "images/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "c128/f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "images_per_step": 1},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128/f64",
+        "data": "synthetic (seeded att-PSM contact-hole clips)",
+        "config": {"workload": WORKLOAD, "images_per_step": k / S, "source_points_per_step": k,
+                   "source_points_per_image": S},
+        "cpu": cpu_info(),
         "cpu_baseline": {"value": v, "unit": "images/s", "cores": os.cpu_count(), "kind": "port",
-                         "sample": f"{k} of {S} source points of one image per step, scaled by {S}/{k}"},
+                         "sample": f"each step: the first {k} of one image's {S} source points ({3 * k} of its "
+                                   f"{3 * S} coherent transforms), FP64 numpy/scipy (FFT workers=-1)"},
         "e2e": {"value": v, "unit": "images/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -508,8 +664,7 @@ def run_ours(args) -> None:
     # twiddles, band rows, band columns, coarse, reduce, then the synthesis: on the tensor cores
     # (enough 128 x 256 output tiles for about 16 per SM) P planes, Q planes, peak pass, peak,
     # writing pass, peak; otherwise column stage, peak pass, peak, writing pass, peak
-    g0 = 2 * int(pd.plan.h)
-    tensor_synth = g0 <= 31 and B * (N // 256) * (N // 128) >= 16 * 148
+    tensor_synth = aerial.engine_info(pd)["synthesis"] == "tensor_cores"
     launches_per_step = 5 + (6 if tensor_synth else 5)
 
     def step(i):
@@ -530,6 +685,7 @@ def run_ours(args) -> None:
         torch.cuda.synchronize()
     barrier()
     ms = max_over_ranks(e0.elapsed_time(e1))
+    aerial.check_status(pd, dev)      # no bounded wait gave up in the timed steps
     clocks = clk.summary()
     value = world * B * args.steps / (ms / 1000.0)
     line = {
@@ -610,8 +766,12 @@ def run_ours(args) -> None:
         agree = float(((fused_img.double() - plain_img.double()).abs().amax(dim=(1, 2))
                        / plain_img.double().abs().amax(dim=(1, 2))).max())
         del plain_img
+        # a perfect dense-FFT plain loop moves N^2 (16 T + 24) bytes per image
+        dense_ceiling = measured_peaks()["hbm_gbs"] * 1e9 / (NN * (16 * transforms + 24))
         line["plain"] = {"value": plain_value, "unit": "images/s", "fused_over_plain": value / plain_value,
-                         "images_per_call": PLAIN_IMAGES, "max_rel_diff_fused_vs_plain": agree}
+                         "images_per_call": PLAIN_IMAGES, "max_rel_diff_fused_vs_plain": agree,
+                         "dense_fft_roofline_images_per_s": dense_ceiling,
+                         "fused_over_dense_roofline": value / dense_ceiling}
 
     # ---- end to end from pinned host memory: masks in, images out ----
     if "e2e" not in args.skip:
@@ -640,19 +800,39 @@ def run_ours(args) -> None:
                        "images_per_step": E2E_IMAGES, "api": "lithobat_b200.pipeline.AbbePipeline (copies of "
                        "consecutive batches overlapped with compute)",
                        "serial_one_call_value": world * E2E_IMAGES * ser / (ser_ms / 1000.0)}
+    for key in ("c1", "c2"):
+        if key not in args.skip:
+            line[key] = bench_config(key, args, torch, dev, world, max_over_ranks, barrier)
     if "ilt" not in args.skip:
         line["ilt"] = bench_ilt(args, torch, dev, world, max_over_ranks, barrier)
     if "uneven" not in args.skip:
         line["uneven"] = bench_uneven(args, torch, dev, world, max_over_ranks, barrier)
     if rank == 0 and world == 1 and not args.no_cpu:
-        t, k, S = cpu_sample_seconds()
-        cv = 1.0 / (t * S / k)
-        line["cpu_baseline"] = {"value": cv, "unit": "images/s", "cores": os.cpu_count(), "kind": "port",
-                                "sample": f"{k} of {S} source points of one image, scaled by {S}/{k}"}
-        if "ilt" in line:
-            ti, _ = cpu_ilt_seconds()
+        # one whole image of the timed batch through the FP64 reference
+        # algorithm: the CPU baseline, and the FP64 reference of that image
+        aerial.run_abbe(pd, dmasks[0], out, peak)
+        gpu0 = out[0].double().cpu().numpy()
+        smp = CpuAbbeSample(dmasks[0][0].cpu().numpy())
+        t = smp()
+        raw, rpk, _ = smp.last
+        line["cpu_baseline"] = {"value": 1.0 / t, "unit": "images/s", "cores": os.cpu_count(), "kind": "port",
+                                "sample": f"one whole image of the timed batch ({smp.S} source points, "
+                                          f"{3 * smp.S} coherent transforms), FP64 numpy/scipy (FFT workers=-1)"}
+        line["cpu"] = cpu_info()
+        line["max_rel_err_vs_fp64"] = float(np.abs(gpu0 - raw[0] / rpk[0]).max())
+        if line.get("ilt") and line["ilt"].get("_fp64_case"):
+            case = line["ilt"].pop("_fp64_case")
+            ti, e_cost, e_grad = cpu_ilt_check(case)
             line["ilt"]["cpu_baseline"] = {"value": 1.0 / ti, "unit": "clip-steps/s", "cores": os.cpu_count(),
-                                           "kind": "port", "sample": "one 1024^2 clip objective + adjoint (K=24)"}
+                                           "kind": "port",
+                                           "sample": "one 1024^2 clip of the batch: FP64 objective + adjoint, K=24"}
+            line["ilt"]["max_rel_err_vs_fp64"] = {"cost": e_cost, "gradient": e_grad}
+        for key in ("c1", "c2"):
+            if line.get(key) and line[key].get("_fp64_case"):
+                line[key].update(cpu_config_check(line[key].pop("_fp64_case")))
+    for key in ("ilt", "c1", "c2"):
+        if line.get(key):
+            line[key].pop("_fp64_case", None)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -668,7 +848,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--images", type=int, default=IMAGES_PER_STEP,
                     help="images per step (a small value makes a profiling case)")
-    ap.add_argument("--skip", default="", help="comma list of phases to skip: plain,e2e,profile,cpu,ilt,iltplain,uneven,unevenilt")
+    ap.add_argument("--skip", default="", help="comma list of phases to skip: plain,e2e,profile,cpu,c1,c2,ilt,iltplain,uneven,"
+                                        "unevenilt")
     ap.add_argument("--ilt-clips", type=int, default=ILT_CLIPS, help="clips per ILT step")
     ap.add_argument("--uneven-clips", type=int, default=256, help="clips in the uneven-size batch")
     args = ap.parse_args()

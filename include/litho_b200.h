@@ -174,10 +174,52 @@ int litho_abbe_noalloc(const LithoAbbePlan* plan, const void* plan_blob_dev,
                        const void* mask_dev, float* image_dev, float* peak_dev,
                        cudaStream_t stream);
 
+/* litho_abbe_status() for the fixed scratch of litho_abbe_noalloc() on the
+ * current device: synchronise `stream` and return 0, or LITHO_E_TIMEOUT if a
+ * bounded wait inside the last litho_abbe_noalloc() call on this device gave
+ * up (its images and peaks are then invalid). No counterpart in the
+ * reference; allocates nothing. */
+int litho_abbe_noalloc_status(const LithoAbbePlan* plan, cudaStream_t stream);
+
 /* Synchronise `stream` and return the device status word of the last
  * litho_abbe*() call that used this workspace: 0, or LITHO_E_TIMEOUT if a
  * bounded wait inside a kernel gave up (its outputs are then invalid). */
 int litho_abbe_status(const LithoAbbePlan* plan, const void* workspace_dev, cudaStream_t stream);
+
+/* Test hooks of the failure reporting (no counterpart in the reference, which
+ * reports failures on the host only: app/worker.py:84-88). Every wait inside
+ * a kernel is bounded; one that gives up drains its block's copies and MMAs
+ * in flight, sets LITHO_E_TIMEOUT in the call's status word (the first word
+ * of its workspace) and lets the block exit, so nothing hangs or faults.
+ *
+ * litho_set_wait_limit: the clock budget (cycles) of the waits that make
+ * progress, on the current device; 0 restores the default (~2 s). Drain waits
+ * keep the full budget. A short limit makes a pipeline report LITHO_E_TIMEOUT
+ * with invalid outputs: for tests only. Synchronous.
+ *
+ * litho_wait_probe: one thread waits `cycles` (1 .. 4e9) on an mbarrier that
+ * nothing arrives at and sets *status_dev = LITHO_E_TIMEOUT, exactly as a
+ * pipeline wait that gives up. Pass a workspace's first word to check that a
+ * status reader (litho_abbe_status and the like) sees it. */
+int litho_set_wait_limit(long long cycles);
+int litho_wait_probe(int* status_dev, long long cycles, cudaStream_t stream);
+
+/* The clear throughput of every output in FP64, on the device: what an
+ * unpatterned mask images to (expose/aerial_image.py:_abbe_sum, :464 for the
+ * scalar model, :482-486 for the vector model, times the blank's specular
+ * |r|^2 for a mirrored mask, :431-438): clear_out_dev[o] = sum over the
+ * output's jobs of weight x [rho(DC) <= 1] x sum_c |V_c(DC)|^2 x |r|^2.
+ * The `clear` normalisation divides the raw image by it. */
+int litho_abbe_clear(const LithoAbbePlan* plan, const void* plan_blob_dev, double* clear_out_dev,
+                     cudaStream_t stream);
+
+/* Which engine litho_abbe() runs for this plan (no counterpart in the
+ * reference, which has one dense path): info[0] = 1 for the on-chip coarse
+ * grid (L = 32 or 64), 2 for the wide-pupil engine (L = 128..1024); info[1]
+ * = the image synthesis: 0 direct with a normalising pass, 1 row-pair FFT,
+ * 2 tcgen05 tensor cores (FP16 hi/lo planes), 3 the wide engine's own.
+ * Writes min(n, 2) values. For tests and launch accounting. */
+int litho_abbe_engine(const LithoAbbePlan* plan, int32_t* info, int n);
 
 /* Bytes of the pupil table of a plan: n_tab x ncomp_max x (2h+1)^2 complex
  * float. The table depends on the optics and source only, not on the masks,
@@ -251,6 +293,41 @@ int litho_plain_socs_adjoint(const float2* fields_dev, const float* sens_dev, in
                              const float2* phi_dev, const float* lam_host, const int32_t* bkx_dev,
                              const int32_t* bky_dev, int nb, float* grad_out_dev, void* workspace_dev,
                              size_t workspace_bytes, cudaStream_t stream);
+
+/* ---- SOCS imaging and its gradient over a kernel table ------------------ */
+
+/* Workspace bytes of litho_socs_forward(). */
+int litho_socs_forward_workspace(int n_clips, int n, int K, int h, int mask_complex, size_t* bytes);
+
+/* The SOCS image of a batch of masks: expose/hopkins.py:SOCSKernels.raw /
+ * .image (:205-223), the intensity of opc/ilt.py:socs_fields (:227-231):
+ *   raw_c = sum_k lambda_k |ifft2(phi_k fft2(mask_c))|^2,
+ *   image_out[c] = raw_c x s_c, peak_out[c] = max raw_c,
+ * s_c = norm_scale (norm_mode 0; 1 gives the raw sum) or norm_scale / peak
+ * (norm_mode 1, peak normalisation with dose norm_scale).
+ * table_dev: K x (2h+1)^2 complex64, kernel k's band value at signed bins
+ * (kx, ky), |kx|, |ky| <= h, stored at [k][(ky + h)(2h + 1) + kx + h];
+ * weights_dev: K doubles lambda_k on the device; mask_dev: [n_clips][n][n]
+ * float32 (mask_complex 0) or complex64. Workspace 256-byte aligned; the job
+ * list is built inside it on the device. */
+int litho_socs_forward(const void* table_dev, const double* weights_dev, int K, int h, const void* mask_dev,
+                       int mask_complex, int n_clips, int n, int norm_mode, float norm_scale, float* image_out_dev,
+                       float* peak_out_dev, void* workspace_dev, size_t workspace_bytes, cudaStream_t stream);
+
+/* Workspace bytes of litho_socs_backward(). */
+int litho_socs_backward_workspace(int n_clips, int n, int K, int h, size_t* bytes);
+
+/* The gradient of sum_x sens_scale sens_c(x) raw_c(x) with respect to the
+ * real mask m_c, raw_c the SOCS image of litho_socs_forward():
+ * opc/ilt.py:socs_gradient (:235-266) applied to the fields of socs_fields
+ * (:227-231), 2 Re sum_k lambda_k ifft2(conj(phi_k) fft2(g E_k)) with
+ * g = sens_scale sens. Band-limited: the mask's band (|k| <= h), the
+ * sensitivity's band (|g| <= 2h), the coarse-grid adjoint, one synthesis.
+ * grad_out_dev: [n_clips][n][n] float32. The backward of litho_socs_forward
+ * for autograd. */
+int litho_socs_backward(const void* table_dev, const double* weights_dev, int K, int h, const float* mask_dev,
+                        int n_clips, int n, const float* sens_dev, float sens_scale, float* grad_out_dev,
+                        void* workspace_dev, size_t workspace_bytes, cudaStream_t stream);
 
 /* ---- SOCS (Hopkins) decomposition ---------------------------------------- */
 

@@ -119,6 +119,15 @@ def lib():
     vp, i32, f32, sz = C.c_void_p, C.c_int, C.c_float, C.c_size_t
     sigs = {
         "litho_coarse_image": [C.POINTER(AbbePlan), vp, vp, vp, vp, vp, sz, vp],
+        "litho_abbe_engine": [C.POINTER(AbbePlan), vp, i32],
+        "litho_abbe_noalloc_status": [C.POINTER(AbbePlan), vp],
+        "litho_abbe_clear": [C.POINTER(AbbePlan), vp, vp, vp],
+        "litho_socs_forward_workspace": [i32, i32, i32, i32, i32, C.POINTER(sz)],
+        "litho_socs_forward": [vp, vp, i32, i32, vp, i32, i32, i32, i32, f32, vp, vp, vp, sz, vp],
+        "litho_socs_backward_workspace": [i32, i32, i32, i32, C.POINTER(sz)],
+        "litho_socs_backward": [vp, vp, i32, i32, vp, i32, i32, vp, f32, vp, vp, sz, vp],
+        "litho_set_wait_limit": [C.c_longlong],
+        "litho_wait_probe": [vp, C.c_longlong, vp],
         "litho_band_spectrum_workspace": [i32, i32, i32, C.POINTER(sz)],
         "litho_band_spectrum": [vp, i32, i32, i32, i32, f32, vp, vp, sz, vp],
         "litho_band_synthesis_workspace": [i32, i32, C.POINTER(sz)],

@@ -18,6 +18,7 @@ runs in ``liblitho_b200.so``; there is no CPU path.
 
 from __future__ import annotations
 
+import ctypes
 import math
 from dataclasses import dataclass
 from typing import Sequence
@@ -96,23 +97,37 @@ _PLANS: dict = {}
 
 
 def plan_abbe(views: Sequence, n: int, pixel_size: float, planes: Sequence[Sequence[tuple]],
-              dose: float, return_raw: bool, mask_complex: bool, items_per_job_group: int = 0) -> AbbePlanData:
+              dose: float, return_raw: bool, mask_complex: bool, items_per_job_group: int = 0,
+              sources: tuple[int, int] | None = None) -> AbbePlanData:
     """Build (or fetch from a small cache) the device descriptors of one
     batched Abbe sum. views[c] is the optics of clip c, planes[c] its list of
-    (defocus, n_image); every clip has the same number of planes."""
+    (defocus, n_image); every clip has the same number of planes. ``sources``
+    (start, stop) keeps only those source points of every clip (in the
+    reference's order): the plan then sums part of the Abbe sum, and its
+    ``clears`` are that part's share of the clear throughput."""
     key = (tuple(repr(v) for v in views), n, pixel_size, tuple(tuple(map(tuple, p)) for p in planes),
-           float(dose), bool(return_raw), bool(mask_complex), items_per_job_group)
+           float(dose), bool(return_raw), bool(mask_complex), items_per_job_group,
+           None if sources is None else (int(sources[0]), int(sources[1])))
     hit = _PLANS.get(key)
     if hit is not None:
         return hit
-    pd = _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, items_per_job_group)
+    pd = _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, items_per_job_group, sources)
     if len(_PLANS) > 32:
         _PLANS.clear()
     _PLANS[key] = pd
     return pd
 
 
-def _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, items_per_job_group):
+def _source_slice(src, sources):
+    if sources is None:
+        return src
+    a, b = int(sources[0]), int(sources[1])
+    if not 0 <= a < b <= len(src):
+        raise ValueError(f"source range {sources} outside the {len(src)} source points")
+    return type(src)(weight=src.weight[a:b], fx=src.fx[a:b], fy=src.fy[a:b], phi=src.phi[a:b], grid=src.grid)
+
+
+def _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, items_per_job_group, sources=None):
     C = len(views)
     P = len(planes[0])
     if any(len(p) != P for p in planes):
@@ -139,7 +154,7 @@ def _plan_abbe(views, n, pixel_size, planes, dose, return_raw, mask_complex, ite
         vector = v.imaging_model.lower() == "vector"
         vec_any |= vector
         exact = v.exact_defocus or vector
-        src = source_points(v)
+        src = _source_slice(source_points(v), sources)
         S = len(src)
         if S == 0:
             raise ValueError("the source has no points")
@@ -409,6 +424,28 @@ def run_abbe(pd: AbbePlanData, masks_dev, out=None, peak=None, stream=None, engi
     return out, peak
 
 
+SYNTHESIS = ("direct", "row_pairs", "tensor_cores", "wide")
+
+
+def engine_info(pd: AbbePlanData) -> dict:
+    """Which engine and image synthesis ``run_abbe`` uses for this plan
+    (``litho_abbe_engine``)."""
+    info = (ctypes.c_int32 * 2)()
+    nat.check("litho_abbe_engine", nat.lib().litho_abbe_engine(ctypes.byref(pd.plan), info, 2))
+    return {"engine": "coarse" if info[0] == 1 else "wide", "synthesis": SYNTHESIS[info[1]]}
+
+
+def check_status(pd: AbbePlanData, dev, engine: str = "fused", stream=None) -> None:
+    """Synchronise and raise if a bounded wait inside the last fused Abbe
+    call on this device's workspace gave up (its images are then invalid)."""
+    if engine != "fused" or not fused_supported(pd.plan.n, int(pd.plan.L)):
+        return
+    torch = nat.require_cuda()
+    ws = nat.Workspace.get(torch, dev, 0, tag="fused")
+    s = stream if stream is not None else nat.stream_ptr(torch, dev)
+    nat.check("litho_abbe_status", nat.lib().litho_abbe_status(ctypes.byref(pd.plan), ws.data_ptr(), s))
+
+
 # Stage names of litho_abbe_profile. "peak_pass" is the compute-only synthesis
 # pass of peak-normalised outputs (on grids without the pair-FFT synthesis it
 # is the direct synthesis and "synthesis" the separate normalising pass).
@@ -439,13 +476,17 @@ def _grid(grid):
 
 
 def compute_aerial_batch(masks, optics, grid, planes=None, dose: float = 1.0, return_raw: bool = False,
-                         engine: str = "fused"):
+                         engine: str = "fused", check: bool | None = None):
     """Abbe images of a batch of clips on the GPU.
 
     masks: (C, N, N) numpy array or torch tensor (real or complex).
     optics: one optics object for all clips, or a sequence of C of them.
     planes: None (each clip's own defocus / image index), a list of
         (defocus, n_image) shared by all clips, or a list of C such lists.
+    check: synchronise and raise ``LithoError`` (status ``LITHO_E_TIMEOUT``)
+        if a bounded wait inside a kernel gave up; default: for host (numpy)
+        masks, whose results are read on the host anyway; device masks keep
+        the call asynchronous (call :func:`check_status` when needed).
     Returns (images, peaks, clears): images (C, P, N, N) float32 CUDA tensor,
     peaks (C, P) raw maxima, clears (C, P) float64 numpy.
     """
@@ -466,6 +507,8 @@ def compute_aerial_batch(masks, optics, grid, planes=None, dose: float = 1.0, re
         pl = [list(planes)] * Cn
     pd = plan_abbe(views, n, px, pl, dose, return_raw, md.is_complex())
     img, pk = run_abbe(pd, md, engine=engine)
+    if check if check is not None else not _is_torch(masks):
+        check_status(pd, md.device, engine)
     P = len(pl[0])
     return img.view(Cn, P, n, n), pk.view(Cn, P), pd.clears.reshape(Cn, P)
 

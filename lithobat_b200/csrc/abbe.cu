@@ -84,6 +84,59 @@ __global__ void k_pupil_table(const LithoJob* __restrict__ jobs, const int32_t* 
   }
 }
 
+// What an unpatterned mask images to, per output: the clear throughput of
+// expose/aerial_image.py:_abbe_sum (:464 scalar, :482-486 vector, times the
+// blank's specular reflectance |r|^2 for a mirrored mask, :431-438), in FP64.
+// At the DC order |exp(iW)| = 1, so a job adds weight x [rho(DC) <= 1] x
+// (vector: sum_c |V_c(DC)|^2) x |r|^2. One block per output; each thread sums
+// a fixed stride of the output's jobs, then a fixed-order tree: deterministic.
+__global__ void k_abbe_clear(const LithoJob* __restrict__ jobs, const LithoItem* __restrict__ items,
+                             const int32_t* __restrict__ out_items, const LithoPupil* __restrict__ pupils,
+                             const LithoMirror* __restrict__ mirrors, int n, double pixel_size,
+                             double* __restrict__ clear_out) {
+  __shared__ double red[128];
+  const int o = blockIdx.x;
+  const double val = ddiv(1.0, dmul((double)n, pixel_size));
+  double acc = 0.0;
+  for (int it = out_items[o]; it < out_items[o + 1]; ++it) {
+    const LithoItem item = items[it];
+    for (int j = item.job_begin + (int)threadIdx.x; j < item.job_end; j += blockDim.x) {
+      const LithoJob job = jobs[j];
+      const LithoPupil P = pupils[job.pupil];
+      double fx, fy;
+      const double rho = aperture_rho(0, 0, val, job.fsx, job.fsy, ddiv(P.NA, P.wavelength), fx, fy);
+      if (!(rho <= 1.0)) continue;
+      double t = 1.0;
+      if (P.vector) {
+        double cp, sp;
+        pupil_direction(fx, fy, cp, sp);
+        const double s = rho * (P.NA / P.n_image);
+        const double s2 = fmin(fmax(s * s, 0.0), 1.0);
+        const double ct = sqrt(1.0 - s2), st = sqrt(s2);
+        const double es = -job.jx * sp + job.jy * cp, ep = job.jx * cp + job.jy * sp;
+        const double vx = -es * sp + ep * ct * cp, vy = es * cp + ep * ct * sp, vz = -ep * st;
+        t = vx * vx + vy * vy + vz * vz;
+        if (P.obliquity) t *= ct;
+      }
+      if (mirrors && mirrors[job.pupil].n_theta >= 2) {
+        const LithoMirror M = mirrors[job.pupil];
+        const double* mtab = reinterpret_cast<const double*>(reinterpret_cast<const char*>(mirrors) + M.off_table);
+        double rr, ri;
+        mirror_reflection(M, mtab, 0.0, 0.0, job.fsx, job.fsy, rr, ri);
+        t *= rr * rr + ri * ri;
+      }
+      acc += job.weight * t;
+    }
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) clear_out[o] = red[0];
+}
+
 // The pupil table of a plan (every engine builds it the same way).
 cudaError_t launch_pupil_table(const LithoAbbePlan& p, const void* blob, float2* table, cudaStream_t s) {
   const char* b = static_cast<const char*>(blob);
@@ -860,6 +913,40 @@ extern "C" int litho_abbe_status(const LithoAbbePlan* plan, const void* ws, cuda
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return (int)e;
   return h;
+}
+
+extern "C" int litho_abbe_clear(const LithoAbbePlan* plan, const void* blob, double* clear_out, cudaStream_t s) {
+  const int st = check_plan(plan);
+  if (st) return st;
+  if (!blob || !clear_out) return LITHO_E_NULL;
+  if (((uintptr_t)blob & 15) || ((uintptr_t)clear_out & 7)) return LITHO_E_ALIGN;
+  const LithoAbbePlan& p = *plan;
+  const char* b = static_cast<const char*>(blob);
+  const LithoMirror* mirrors = p.mirrored ? reinterpret_cast<const LithoMirror*>(b + p.off_mirrors) : nullptr;
+  k_abbe_clear<<<p.n_out, 128, 0, s>>>(reinterpret_cast<const LithoJob*>(b + p.off_jobs),
+                                       reinterpret_cast<const LithoItem*>(b + p.off_items),
+                                       reinterpret_cast<const int32_t*>(b + p.off_out_items),
+                                       reinterpret_cast<const LithoPupil*>(b + p.off_pupils), mirrors, p.n,
+                                       p.pixel_size, clear_out);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+extern "C" int litho_abbe_engine(const LithoAbbePlan* plan, int32_t* info, int n) {
+  const int st = check_plan(plan);
+  if (st) return st;
+  if (!info || n < 1) return LITHO_E_NULL;
+  const LithoAbbePlan& p = *plan;
+  int32_t v[2];
+  if (p.L > 64) {
+    v[0] = 2;
+    v[1] = 3;
+  } else {
+    v[0] = 1;
+    v[1] = synth_mma_pick(p.n_out, p.n, 2 * p.h) ? 2 : synth_pairs_ok(p.n, 2 * p.h) ? 1 : 0;
+  }
+  for (int i = 0; i < n && i < 2; ++i) info[i] = v[i];
+  return LITHO_OK;
 }
 
 extern "C" int litho_abbe_table_bytes(const LithoAbbePlan* plan, size_t* bytes) {

@@ -69,7 +69,9 @@ k_row_band_tma(const void* __restrict__ in, int n_rows, int rows_per_clip, int n
   __shared__ int s_fail;
 
   const int n_tiles = (n_rows + L.tile_rows - 1) / L.tile_rows;
+  int n_issued[2] = {0, 0};   // copies thread 0 has issued into each stage
   auto issue = [&](int t, int st) {
+    ++n_issued[st];
     const int r0 = t * L.tile_rows;
     const int rows = (n_rows - r0) < L.tile_rows ? (n_rows - r0) : L.tile_rows;
     const uint32_t bytes = (uint32_t)((size_t)rows * n * esz);
@@ -157,9 +159,12 @@ k_row_band_tma(const void* __restrict__ in, int n_rows, int rows_per_clip, int n
     }
   }
   if (s_fail) {
-    // drain: give any copy still in flight a bounded chance to land, then report
+    // drain: the latest copy into each stage (parity of its last phase; a
+    // stage is refilled only after its previous copy was consumed) lands
+    // before the block exits, then report
     if (threadIdx.x == 0) {
-      mbar_wait(&mbar[0], (it >> 1) & 1);
+      for (int sg = 0; sg < 2; ++sg)
+        if (n_issued[sg] > 0) mbar_wait_drain(&mbar[sg], (uint32_t)((n_issued[sg] - 1) & 1));
       atomicExch(status, LITHO_E_TIMEOUT);
     }
   }
@@ -540,4 +545,9 @@ cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_
   return cudaGetLastError();
 }
 
+}  // namespace litho
+
+namespace litho {
+// This module's progress-wait budget on the current device (litho_set_wait_limit).
+cudaError_t set_wait_limit_band(long long cycles) { return set_wait_limit_here(cycles); }
 }  // namespace litho

@@ -219,6 +219,18 @@ __host__ __device__ __forceinline__ int64_t align16(int64_t x) { return (x + 15)
 // ---------------------------------------------------------------------------
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 
+// Clock budget of the waits that make progress (a stage's operands, an MMA's
+// accumulator). One copy per translation unit (each .cu is its own device
+// module); litho_set_wait_limit() lowers it on the current device so tests
+// can make those waits give up. Waits that drain copies or MMAs already in
+// flight before a block exits (mbar_wait_drain) always get kWaitCycles.
+static __device__ long long g_wait_limit = kWaitCycles;
+
+// Host: set this translation unit's g_wait_limit on the current device.
+[[maybe_unused]] static inline cudaError_t set_wait_limit_here(long long cycles) {
+  return cudaMemcpyToSymbol(g_wait_limit, &cycles, sizeof(cycles));
+}
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -265,13 +277,23 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// true when the phase with this parity completed within the clock budget.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// true when the phase with this parity completed within `limit` clock cycles.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t* bar, uint32_t parity, long long limit) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
-  while (clock64() - t0 < kWaitCycles)
+  while (clock64() - t0 < limit)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
+}
+// A progress wait: within this translation unit's g_wait_limit.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  return mbar_wait_for(bar, parity, *(volatile long long*)&g_wait_limit);
+}
+// A drain wait (copies or MMAs this block already issued, before it exits or
+// releases TMEM): the full budget, whatever g_wait_limit says.
+__device__ __forceinline__ bool mbar_wait_drain(uint64_t* bar, uint32_t parity) {
+  return mbar_wait_for(bar, parity, kWaitCycles);
 }
 // Order this thread's earlier generic-proxy shared accesses before later
 // async-proxy (TMA) accesses to the same buffer.

@@ -60,3 +60,10 @@ extern "C" int litho_abbe_noalloc(const LithoAbbePlan* plan, const void* plan_bl
   return litho_abbe(plan, plan_blob_dev, mask_dev, image_dev, peak_dev, scratch,
                     (size_t)LITHO_NOALLOC_SCRATCH_BYTES, stream);
 }
+
+extern "C" int litho_abbe_noalloc_status(const LithoAbbePlan* plan, cudaStream_t stream) {
+  void* scratch = nullptr;
+  const int st = scratch_for_current_device(&scratch);
+  if (st) return st;
+  return litho_abbe_status(plan, scratch, stream);
+}

@@ -198,7 +198,10 @@ k_gram_umma(const double* __restrict__ Are, const double* __restrict__ Aim, int 
     }
   }
   if (s_fail && threadIdx.x == 0) {
-    mbar_wait(&s_mbar, phase);  // bounded: let an MMA still in flight land before TMEM is released
+    // let the MMAs of the last commit (parity phase ^ 1: the loop flipped
+    // phase after waiting on it) land before TMEM is released; returns at
+    // once if that phase already completed
+    if (issued) mbar_wait_drain(&s_mbar, phase ^ 1u);
     atomicExch(status, LITHO_E_TIMEOUT);
   }
   tc_fence_before();
@@ -550,3 +553,8 @@ extern "C" int litho_socs_debug(int n_source, int n_band, const void* ws, double
     e = cudaMemcpyAsync(evals_out, w + l.evals, (size_t)l.ldg * 8, cudaMemcpyDeviceToDevice, s);
   return e == cudaSuccess ? LITHO_OK : (int)e;
 }
+
+namespace litho {
+// This module's progress-wait budget on the current device (litho_set_wait_limit).
+cudaError_t set_wait_limit_gram(long long cycles) { return set_wait_limit_here(cycles); }
+}  // namespace litho

@@ -370,9 +370,11 @@ k_synth_mma(const __half* __restrict__ pplanes, const __half* __restrict__ qplan
       }
       if (!ok) s_fail = 1;
       // let the last copy into each buffer land before the block can exit
+      // (the latest phase of a buffer's barrier; earlier phases completed
+      // before it was refilled)
       for (int k = 1; k <= 2; ++k) {
-        if (i - k >= 0) mbar_wait(&bar_bfull[(i - k) & 1], ((i - k) >> 1) & 1);
-        if (a - k >= 0) mbar_wait(&bar_afull[(a - k) & 1], ((a - k) >> 1) & 1);
+        if (i - k >= 0 && !mbar_wait_drain(&bar_bfull[(i - k) & 1], ((i - k) >> 1) & 1)) s_fail = 1;
+        if (a - k >= 0 && !mbar_wait_drain(&bar_afull[(a - k) & 1], ((a - k) >> 1) & 1)) s_fail = 1;
       }
     }
   } else if (warp == kSmDrainWarps + 1) {
@@ -416,7 +418,7 @@ k_synth_mma(const __half* __restrict__ pplanes, const __half* __restrict__ qplan
       if (!ok) s_fail = 1;
       if (c > 0) {  // every MMA this thread issued has completed before TMEM is released
         umma_commit(&bar_drain);
-        mbar_wait(&bar_drain, 0);
+        if (!mbar_wait_drain(&bar_drain, 0)) s_fail = 1;
       }
     }
   } else {
@@ -593,4 +595,9 @@ cudaError_t launch_synth_mma(const float2* box, int g0, int n, int n_out, const 
   return cudaGetLastError();
 }
 
+}  // namespace litho
+
+namespace litho {
+// This module's progress-wait budget on the current device (litho_set_wait_limit).
+cudaError_t set_wait_limit_synth(long long cycles) { return set_wait_limit_here(cycles); }
 }  // namespace litho

@@ -77,6 +77,20 @@ class SOCSKernels:
     def __len__(self) -> int:
         return int(self.weights.size)
 
+    def subset(self, index) -> "SOCSKernels":
+        """The kernels at ``index`` (a slice or index array) as kernels of their
+        own: same optics, grid, band and clear (the full set's open-frame
+        intensity, so normalisation is unchanged). Images and gradients are
+        linear in the kernel set, so the parts of a partition sum to the
+        whole (the SOCS split of one clip over several GPUs)."""
+        import torch
+        idx = np.arange(len(self))[index]
+        sel = torch.from_numpy(idx.astype(np.int64)).to(self._phi.device)
+        return SOCSKernels(weights=self.weights[idx], clear=self.clear, energy_kept=self.energy_kept,
+                           n_band=self.n_band, n_source=self.n_source, optics=self.optics, grid=self.grid,
+                           band_kx=self.band_kx, band_ky=self.band_ky, phi_dev=self._phi.index_select(0, sel),
+                           gram_sweeps=self.gram_sweeps)
+
     @staticmethod
     def supports(optics) -> bool:
         v = optics_view(optics)
@@ -211,6 +225,9 @@ class SOCSKernels:
         from .aerial import _as_device_masks, _is_torch
         md = _as_device_masks(torch, mask, n)
         img, pk = self.raw_batch(md)
+        if not _is_torch(mask):
+            from .aerial import check_status
+            check_status(self._plan(1, bool(md.is_complex()), (0, 1.0)), md.device)
         a = img[0] if _is_torch(mask) else img[0].cpu().numpy().astype(np.float64)
         return a, float(pk[0]), self.clear
 

@@ -82,13 +82,13 @@ class _Stages:
         return t
 
     # -- transforms ---------------------------------------------------------
-    def band(self, fields, bm: int, scale: float):
+    def band(self, fields, bm: int, scale: float, tag: str = "band"):
         """(F, (2bm+1)^2) complex64 band boxes of F dense fields."""
         torch, L = self.torch, self.L
         F = int(fields.shape[0])
         nb = C.c_size_t(0)
         nat.check("litho_band_spectrum_workspace", L.litho_band_spectrum_workspace(F, self.n, bm, C.byref(nb)))
-        ws = self.ws("band", nb.value)
+        ws = self.ws(tag, nb.value)
         out = torch.empty((F, (2 * bm + 1) ** 2), dtype=torch.complex64, device=self.dev)
         nat.check("litho_band_spectrum", L.litho_band_spectrum(
             fields.data_ptr(), int(fields.is_complex()), F, self.n, bm, scale, out.data_ptr(), ws.data_ptr(),
@@ -109,7 +109,23 @@ class _Stages:
         return out
 
     def mask_box(self, masks):
-        return self.band(masks, self.h, 1.0 / (self.n * self.n))
+        return self.band(masks, self.h, 1.0 / (self.n * self.n), tag="band_mask")
+
+    # workspaces whose first word is a device status (litho_band_spectrum,
+    # litho_band_synthesis: LITHO_E_TIMEOUT when a bounded wait gave up); one
+    # per call site of a step, so a step's every call keeps its own word
+    STATUS_TAGS = ("band_mask", "band", "synth")
+
+    def check_status(self) -> None:
+        """Synchronise and raise ``LithoError`` if a bounded wait inside the
+        latest band spectrum or synthesis call of any kind gave up."""
+        self.torch.cuda.synchronize(self.dev)
+        for tag in self.STATUS_TAGS:
+            t = self._ws.get(tag)
+            if t is not None:
+                st = int(t[:4].view(self.torch.int32).item())
+                if st:
+                    nat.check(f"litho_band_{'synthesis' if tag == 'synth' else 'spectrum'}", st)
 
     def image_box(self, mbox):
         """Band box (C, (4h+1)^2) of the raw SOCS intensity from the mask band boxes."""
@@ -167,6 +183,15 @@ class _Stages:
         between steps: (cost (C,), gradient band box (C, (2h+1)^2), signed or
         None, perr (C,)). Synthesis of the image, the per-pixel resist, the
         band of dJ/dI, the adjoint to the gradient's band box."""
+        ibox = self.image_box(mbox)
+        cost, gbox, signed, perr = self.objective_from_box(ibox, target, scale, level, sign, steepness, want_signed)
+        hbox = self.adjoint_box(gbox, mbox, out=out_hbox)
+        return cost, hbox, signed, perr
+
+    def objective_from_box(self, ibox, target, scale, level, sign, steepness, want_signed=True):
+        """The resist objective of the image whose band box (C, (4h+1)^2) is
+        ``ibox``: (cost (C,), band box of scale * dJ/dI / N^2 on |g| <= 2h,
+        signed or None, perr (C,))."""
         torch, L = self.torch, self.L
         a = steepness / max(abs(level), 1e-12)
         if self._obj_counters is None:
@@ -175,7 +200,6 @@ class _Stages:
         perr = torch.empty((self.C,), dtype=torch.int64, device=self.dev)
         if not want_signed and self.image_objective_ok() and target.data_ptr() % 16 == 0:
             # the image is synthesised straight into the objective (never stored)
-            ibox = self.image_box(mbox)
             nb = C.c_size_t(0)
             nat.check("litho_ilt_image_objective_workspace", L.litho_ilt_image_objective_workspace(
                 self.C, self.n, 2 * self.h, C.byref(nb)))
@@ -186,9 +210,8 @@ class _Stages:
                 float(sign), float(a), dfield.data_ptr(), self._obj_counters.data_ptr(), cost.data_ptr(),
                 perr.data_ptr(), ws.data_ptr(), ws.numel(), self.stream()))
             gbox = self.band(dfield, 2 * self.h, float(scale) / (self.n * self.n))
-            hbox = self.adjoint_box(gbox, mbox, out=out_hbox)
-            return cost, hbox, None, perr
-        raw = self.image(mbox)
+            return cost, gbox, None, perr
+        raw = self.synth(ibox, 2 * self.h, False)
         dfield = torch.empty_like(raw)
         signed = torch.empty_like(raw) if want_signed else None
         cpart = torch.empty((self.C, N_PART), dtype=torch.float64, device=self.dev)
@@ -198,8 +221,7 @@ class _Stages:
             dfield.data_ptr(), None if signed is None else signed.data_ptr(), cpart.data_ptr(), ppart.data_ptr(),
             N_PART, self._obj_counters.data_ptr(), cost.data_ptr(), perr.data_ptr(), self.stream()))
         gbox = self.band(dfield, 2 * self.h, float(scale) / (self.n * self.n))
-        hbox = self.adjoint_box(gbox, mbox, out=out_hbox)
-        return cost, hbox, signed, perr
+        return cost, gbox, signed, perr
 
     def image_objective_ok(self) -> bool:
         """Whether litho_ilt_image_objective serves this grid and band."""
@@ -386,6 +408,7 @@ def socs_fields(kernels: SOCSKernels, mask):
     f = st.fields(mbox)[0]
     if _is_torch(mask):
         return f, inten
+    st.check_status()
     out = f.cpu().numpy().astype(np.complex128).view(SocsFields)
     out._mbox = mbox
     out._kernels = kernels
@@ -410,7 +433,10 @@ def socs_gradient(kernels: SOCSKernels, fields, sensitivity):
             return grad if _is_torch(sensitivity) else grad.cpu().numpy().astype(np.float64)
         fb = st.band(fl.reshape(-1, st.n, st.n).contiguous(), st.h, 1.0 / (st.n * st.n))
         grad = st.adjoint(g, field_boxes=fb)[0]
-    return grad if _is_torch(sensitivity) else grad.cpu().numpy().astype(np.float64)
+    if _is_torch(sensitivity):
+        return grad
+    st.check_status()
+    return grad.cpu().numpy().astype(np.float64)
 
 
 def _plain_adjoint(pst, fields, sens):
@@ -446,6 +472,7 @@ class Objective:
         tg = _as_device_masks(torch, self.target, st.n)
         cost, grad, signed, perr = st.objective(md, tg, self.scale, self.level, self.sigma_px, self.sign,
                                                 self.steepness, self.weight_tv, self.weight_discrete)
+        st.check_status()
         if _is_torch(mask):
             return float(cost[0]), grad[0], signed[0], int(perr[0])
         return (float(cost[0]), grad[0].cpu().numpy().astype(np.float64),
@@ -605,6 +632,11 @@ class IltBatch:
         p = self.p
         return self.st.objective_split(self.mbox, self.target, p.scale, p.level, p.sign, p.steepness, want_signed)
 
+    def check_status(self) -> None:
+        """Synchronise and raise ``LithoError`` if a bounded device wait gave
+        up in the latest step (its results are then invalid)."""
+        self.st.check_status()
+
     @property
     def mask(self):
         if self._mask is None:
@@ -736,6 +768,7 @@ def run_ilt(target, kernels: SOCSKernels, *, level: float, dose: float = 1.0, si
                        steepness=steepness, weight_tv=weight_tv, weight_discrete=weight_discrete,
                        smooth_px=smooth_px, step=step, beta=beta, growth=growth)
     b = IltBatch(kernels, tgt[None], theta0[None], params)
+    b.check_status()
     lit = int((b.signed > 0).sum())
     if lit == 0 or lit == n * n:
         raise ValueError(f"the initial mask prints {'nothing' if lit == 0 else 'everywhere'} — no contour "
@@ -748,6 +781,7 @@ def run_ilt(target, kernels: SOCSKernels, *, level: float, dose: float = 1.0, si
     for it in range(1, max_iter + 1):
         b.step()
         taken = it
+        b.check_status()
         cost = float(b.cost[0])
         hist.append({"iteration": it, "cost": cost, "pattern_error": int(b.perr[0]), "beta": b.beta,
                      "grad_norm": float(b.grad_m.double().norm())})

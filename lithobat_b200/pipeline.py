@@ -25,7 +25,8 @@ class AbbePipeline:
     ``run(inputs, outputs)``: inputs[i] (batch, N, N) float32 or complex64
     pinned CPU tensors, outputs[i] (batch, N, N) float32 pinned CPU tensors
     (the same tensor may appear several times in either list; an output is
-    complete once ``run`` returns)."""
+    complete once ``run`` returns). ``run`` raises ``LithoError`` if a bounded
+    wait inside any batch's kernels gave up (``LITHO_E_TIMEOUT``)."""
 
     def __init__(self, optics, grid, batch: int, mask_complex: bool, dose: float = 1.0, return_raw: bool = False,
                  depth: int = 2, device=None):
@@ -53,6 +54,10 @@ class AbbePipeline:
         self.s_in = torch.cuda.Stream(device=self.dev)
         self.s_run = torch.cuda.Stream(device=self.dev)
         self.s_out = torch.cuda.Stream(device=self.dev)
+        # the workspace's status word (offset 0) is cleared by every call; the
+        # worst status of a run is kept here, read once the run has synchronised
+        self._status = self.ws[:4].view(torch.int32)
+        self._worst = torch.zeros((1,), dtype=torch.int32, device=self.dev)
 
     def run(self, inputs, outputs) -> None:
         torch, L = self.torch, self.L
@@ -77,6 +82,7 @@ class AbbePipeline:
                     C.byref(self.pd.plan), self.pd._blob_dev.data_ptr(), self.table.data_ptr(),
                     self.d_in[k].data_ptr(), self.d_out[k].data_ptr(), self.d_peak[k].data_ptr(),
                     self.ws.data_ptr(), self.ws.numel(), int(self.s_run.cuda_stream)))
+                torch.maximum(self._worst, self._status, out=self._worst)
                 done = ev()
                 done.record(self.s_run)
                 read_done[k] = done
@@ -87,6 +93,11 @@ class AbbePipeline:
                 fin.record(self.s_out)
                 sent[k] = fin
         self.s_out.synchronize()
+        self.s_run.synchronize()
+        worst = int(self._worst.item())
+        if worst:
+            self._worst.zero_()
+            nat.check("litho_abbe_tabled", worst)
 
 
 __all__ = ["AbbePipeline"]

@@ -177,6 +177,15 @@ class UnevenAbbe:
                 out[i] = g.image[j]
         return out
 
+    def check_status(self) -> None:
+        """Synchronise and raise ``LithoError`` if a bounded device wait gave
+        up in the latest run of any size group (its images are then invalid)."""
+        self.torch.cuda.synchronize(self.dev)
+        for g in self.groups:
+            st = int(g.ws[:4].view(self.torch.int32).item())
+            if st:
+                nat.check("litho_abbe_tabled", st)
+
     def peaks(self):
         out = [None] * len(self.sizes)
         for g in self.groups:

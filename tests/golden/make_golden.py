@@ -1,9 +1,9 @@
 """Generate the golden fixtures in this folder from the reference itself.
 
-Run in a container that has the reference checked out (default
-``/root/reference``; override with ``LITHO_REFERENCE``)::
+Run in a container that has the reference checked out, with
+``LITHO_REFERENCE`` naming its root (the folder that holds ``src/litho_sim``)::
 
-    python tests/golden/make_golden.py
+    LITHO_REFERENCE=<path to the reference checkout> python tests/golden/make_golden.py
 
 It imports the reference package ``litho_sim`` from ``<ref>/src`` unmodified.
 ``litho_sim.opc`` imports matplotlib for layout rasterisation (mask/geometry.py),
@@ -28,10 +28,20 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("LITHO_REFERENCE", "/root/reference"))
+
+
+def _reference_root() -> Path:
+    root = os.environ.get("LITHO_REFERENCE")
+    if not root:
+        raise SystemExit("set LITHO_REFERENCE to the reference checkout (the folder holding src/litho_sim)")
+    path = Path(root)
+    if not (path / "src" / "litho_sim").is_dir():
+        raise SystemExit(f"LITHO_REFERENCE={root!r} does not hold src/litho_sim")
+    return path
 
 
 def _import_reference():
+    REF = _reference_root()
     stub = Path(tempfile.mkdtemp()) / "matplotlib"
     stub.mkdir()
     (stub / "__init__.py").write_text("")

@@ -76,6 +76,9 @@ def test_noalloc_matches_workspace_entry_point_on_two_calls_in_a_row(env):
         err = float(((img_b.double() - img_a.double()).abs().amax() / img_a.double().abs().amax()))
         assert err <= TOL, f"call {call}: {err:.3e}"
         assert float(((pk_b - pk_a).abs() / pk_a.abs()).max()) <= TOL
+        # the status reader of the fixed scratch: no bounded wait gave up
+        L = env[2].lib()
+        assert L.litho_abbe_noalloc_status(C.byref(pd.plan), torch.cuda.current_stream().cuda_stream) == 0
 
 
 def test_noalloc_rejects_plans_beyond_its_scratch(env):
