@@ -329,6 +329,40 @@ int litho_socs_backward(const void* table_dev, const double* weights_dev, int K,
                         int n_clips, int n, const float* sens_dev, float sens_scale, float* grad_out_dev,
                         void* workspace_dev, size_t workspace_bytes, cudaStream_t stream);
 
+/* ---- the band TCC: SOCS image and adjoint boxes without per-kernel FFTs -- */
+
+/* Bytes of the band TCC of a kernel set with n_band band points inside the
+ * box |kx|, |ky| <= h; LITHO_E_UNSUPPORTED when it would not stay resident in
+ * L2 (more than 96 MiB) or h > 31 (then use litho_coarse_image and
+ * litho_socs_adjoint). */
+int litho_socs_tcc_bytes(int n_band, int h, size_t* bytes);
+
+/* Build the band TCC T(f, f') = sum_k lambda_k conj phi_k(f) phi_k(f') of the
+ * K kept kernels (expose/hopkins.py:SOCSKernels, :144-198, truncated at K)
+ * in FP64 and store it as complex64 in two layouts, with the band's index
+ * maps. phi_dev: K x n_band complex128 (unit eigenvectors on the band, in
+ * band order), lam_dev: K doubles, band_kx/ky_dev: signed bins of the band
+ * points. *status_dev is set non-zero if a band point lies outside the box. */
+int litho_socs_tcc_build(const void* phi_dev, const double* lam_dev, int K, const int32_t* band_kx_dev,
+                         const int32_t* band_ky_dev, int n_band, int h, void* tcc_dev, size_t tcc_bytes,
+                         int* status_dev, cudaStream_t stream);
+
+/* The SOCS image band box of each clip from its mask band box (the
+ * forward of opc/ilt.py:socs_fields, :227-231, and expose/hopkins.py:
+ * SOCSKernels.raw, :215-217, on the band): B(g) = sum_f Tc(f + g, f) M(f + g)
+ * conj M(f), Tc = conj T, |g| <= 2h. mask_box_dev: n_clips x (2h+1)^2
+ * (F(m) / N^2); image_box_out_dev: n_clips x (4h+1)^2, the box of
+ * litho_coarse_image() (synthesise with litho_band_synthesis, h' = 2h). */
+int litho_socs_tcc_image(const void* tcc_dev, int n_band, int h, const void* mask_box_dev, int n_clips,
+                         void* image_box_out_dev, cudaStream_t stream);
+
+/* The gradient band box of sum_x G(x) I(x) (opc/ilt.py:socs_gradient,
+ * :235-266): H(f) = A(f) + conj A(-f), A(f) = sum_f' T(f, f') M(f')
+ * Gs(f - f'), |f| <= h. sens_box_dev: n_clips x (4h+1)^2, F(G) / N^2 (the
+ * sens box of litho_socs_adjoint); grad_box_out_dev: n_clips x (2h+1)^2. */
+int litho_socs_tcc_adjoint(const void* tcc_dev, int n_band, int h, const void* mask_box_dev,
+                           const void* sens_box_dev, int n_clips, void* grad_box_out_dev, cudaStream_t stream);
+
 /* ---- SOCS (Hopkins) decomposition ---------------------------------------- */
 
 /* Workspace bytes of litho_socs_build() for n_source points and n_band band
@@ -481,7 +515,8 @@ typedef struct LithoIltSched {
     double beta, beta_next, growth;
     int32_t it;
     float c1, c2;         /* Adam bias corrections 1 - b1^it, 1 - b2^it     */
-    int32_t pad;
+    int32_t pad;          /* the update's block counter: 0 before the first */
+                          /* call, left 0 by every call                     */
 } LithoIltSched;          /* 40 bytes */
 
 int litho_ilt_update_sched(const float* g_dev, long long count, LithoIltSched* sched_dev, float step, float b1,

@@ -11,6 +11,7 @@ from .config import GridConfig, OpticsConfig
 from .hopkins import SOCSKernels
 from .source import Pole, Source, SourcePoints, build_source, source_points
 from . import patterns
+from . import torch_ops  # registers torch.ops.litho.*
 
 __all__ = [
     "GridConfig", "OpticsConfig", "Pole", "SOCSKernels", "Source", "SourcePoints", "SOURCE_TILT_SIGN",

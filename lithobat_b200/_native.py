@@ -18,6 +18,7 @@ LIB_PATH = Path(__file__).resolve().parent / "liblitho_b200.so"
 
 NOALLOC_SCRATCH_BYTES = 32 << 20   # LITHO_NOALLOC_SCRATCH_BYTES
 LITHO_E_UNSUPPORTED = -5           # a valid request this build does not serve
+LITHO_E_BAND = -4                  # band / coarse-grid geometry inconsistent
 
 
 class NativeUnavailable(RuntimeError):
@@ -126,6 +127,10 @@ def lib():
         "litho_socs_forward": [vp, vp, i32, i32, vp, i32, i32, i32, i32, f32, vp, vp, vp, sz, vp],
         "litho_socs_backward_workspace": [i32, i32, i32, i32, C.POINTER(sz)],
         "litho_socs_backward": [vp, vp, i32, i32, vp, i32, i32, vp, f32, vp, vp, sz, vp],
+        "litho_socs_tcc_bytes": [i32, i32, C.POINTER(sz)],
+        "litho_socs_tcc_build": [vp, vp, i32, vp, vp, i32, i32, vp, sz, vp, vp],
+        "litho_socs_tcc_image": [vp, i32, i32, vp, i32, vp, vp],
+        "litho_socs_tcc_adjoint": [vp, i32, i32, vp, vp, i32, vp, vp],
         "litho_set_wait_limit": [C.c_longlong],
         "litho_wait_probe": [vp, C.c_longlong, vp],
         "litho_band_spectrum_workspace": [i32, i32, i32, C.POINTER(sz)],

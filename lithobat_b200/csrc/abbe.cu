@@ -779,7 +779,7 @@ static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* tab
 
   char* w = static_cast<char*>(ws);
   int* status = reinterpret_cast<int*>(w + l.status);
-  float2* tw = reinterpret_cast<float2*>(w + l.tw);
+  float2* tw_own = reinterpret_cast<float2*>(w + l.tw);
   float2* u1 = reinterpret_cast<float2*>(w + l.u1);
   float2* mb = reinterpret_cast<float2*>(w + l.mb);
   float2* table = table_in ? (float2*)table_in : reinterpret_cast<float2*>(w + l.table);
@@ -794,7 +794,7 @@ static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* tab
 
   mark(0);
   if ((e = cudaMemsetAsync(status, 0, sizeof(int), s)) != cudaSuccess) return (int)e;
-  k_twiddle_table<<<(p.n + 255) / 256, 256, 0, s>>>(tw, p.n, +1);
+  const float2* tw = twiddles_for(p.n, tw_own, s);
   if (!table_in)
     if ((e = launch_pupil_table(p, blob, table, s)) != cudaSuccess) return (int)e;
   mark(1);

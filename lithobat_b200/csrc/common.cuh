@@ -316,4 +316,17 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Device twiddle table w[j] = exp(sign * 2 pi i j / n), FP64 evaluated, FP32 stored.
 __global__ void k_twiddle_table(float2* w, int n, int sign);
 
+// The shared exp(+2 pi i j / n) table of a power-of-two n <= 8192 on the
+// current device (twiddle_cache.cu), or nullptr: then the caller builds its
+// own with k_twiddle_table (other sizes, or a stream that is capturing before
+// the device's tables exist).
+const float2* shared_twiddles(int n, cudaStream_t s);
+
+// `own` filled with exp(+2 pi i j / n) on `s` unless the shared table serves n.
+inline const float2* twiddles_for(int n, float2* own, cudaStream_t s) {
+  if (const float2* t = shared_twiddles(n, s)) return t;
+  k_twiddle_table<<<(n + 255) / 256, 256, 0, s>>>(own, n, +1);
+  return own;
+}
+
 }  // namespace litho

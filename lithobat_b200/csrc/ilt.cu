@@ -415,24 +415,40 @@ __global__ void k_ilt_update(const float* __restrict__ g, long long total, float
   ilt_update_body(g, total, beta, beta_next, step, b1, b2, eps, c1, c2, theta, m1, m2, mask);
 }
 
-// The same step with beta, beta_next and the bias corrections read from a
-// device schedule (advanced by k_ilt_sched_advance just before).
-__global__ void k_ilt_update_s(const float* __restrict__ g, long long total, const LithoIltSched* __restrict__ sc,
-                               float step, float b1, float b2, float eps, float* __restrict__ theta,
-                               float* __restrict__ m1, float* __restrict__ m2, float* __restrict__ mask) {
-  ilt_update_body(g, total, (float)sc->beta, (float)sc->beta_next, step, b1, b2, eps, sc->c1, sc->c2, theta, m1, m2,
-                  mask);
-}
-
-__global__ void k_ilt_sched_advance(LithoIltSched* sc, double b1, double b2) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  LithoIltSched v = *sc;
+// The schedule one step on: beta = beta_next, it + 1, beta_next = beta x
+// growth, Adam's bias corrections 1 - b^it (FP64, rounded to FP32).
+__device__ __forceinline__ LithoIltSched sched_next(LithoIltSched v, double b1, double b2) {
   v.beta = v.beta_next;
   v.it += 1;
   v.beta_next = v.beta * v.growth;
   v.c1 = (float)(1.0 - pow(b1, (double)v.it));
   v.c2 = (float)(1.0 - pow(b2, (double)v.it));
-  *sc = v;
+  return v;
+}
+
+// litho_ilt_update_sched in one launch: every block takes the advanced
+// schedule from the previous one, runs the update, and the last block to
+// finish (counted in sc->pad, which it resets) stores the advanced schedule
+// for the next step. Every block read the schedule before it was counted,
+// so the store cannot overtake a read.
+__global__ void k_ilt_update_sf(const float* __restrict__ g, long long total, LithoIltSched* __restrict__ sc,
+                                float step, float b1, float b2, float eps, float* __restrict__ theta,
+                                float* __restrict__ m1, float* __restrict__ m2, float* __restrict__ mask) {
+  __shared__ LithoIltSched s_v;
+  if (threadIdx.x == 0) s_v = sched_next(*sc, (double)b1, (double)b2);
+  __syncthreads();
+  ilt_update_body(g, total, (float)s_v.beta, (float)s_v.beta_next, step, b1, b2, eps, s_v.c1, s_v.c2, theta, m1, m2,
+                  mask);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int done = atomicAdd(reinterpret_cast<unsigned int*>(&sc->pad), 1u);
+    if (done == gridDim.x - 1) {
+      LithoIltSched v = s_v;
+      v.pad = 0;
+      *sc = v;
+    }
+  }
 }
 
 __device__ __forceinline__ void ilt_update_body(const float* __restrict__ g, long long total, float beta,
@@ -606,12 +622,12 @@ extern "C" int litho_band_spectrum(const void* in, int is_complex, int n_fields,
   if (((uintptr_t)ws & 15) || ((uintptr_t)in & 7)) return LITHO_E_ALIGN;
   char* w = static_cast<char*>(ws);
   int* status = reinterpret_cast<int*>(w);
-  float2* tw = reinterpret_cast<float2*>(w + align16(16));
+  float2* tw_own = reinterpret_cast<float2*>(w + align16(16));
   float2* u1 = reinterpret_cast<float2*>(w + align16(16) + align16((int64_t)n * 8));
   const int Bm = 2 * bm + 1;
   cudaError_t e = cudaMemsetAsync(status, 0, sizeof(int), s);
   if (e != cudaSuccess) return (int)e;
-  k_twiddle_table<<<(n + 255) / 256, 256, 0, s>>>(tw, n, +1);
+  const float2* tw = twiddles_for(n, tw_own, s);
   e = launch_row_band_dft(in, is_complex != 0, n_fields * n, n, n, bm, u1, 1.0f, tw, sms_here(), s, status);
   if (e != cudaSuccess) return (int)e;
   e = launch_row_band_dft(u1, true, n_fields * Bm, Bm, n, bm, static_cast<float2*>(box_out), scale, tw, sms_here(), s,
@@ -623,6 +639,8 @@ extern "C" int litho_band_spectrum(const void* in, int is_complex, int n_fields,
 // engine in use: the operand planes of the tensor-core synthesis or the column
 // buffer of the pair synthesis (boxes up to half-width 31), or the spectrum of
 // the synthesis of wider boxes
+constexpr int64_t kColsAheadMin = 148 * 8;   // columns (fields x (h + 1)) for a separate column stage
+
 static int64_t band_synth_region(int n_fields, int n) {
   int64_t r = align16(synth_cols_bytes(n_fields, n, 31));
   if (synth_mma_ok(n, 31)) r = std::max(r, align16(synth_mma_bytes(n_fields, n, 31)));
@@ -651,11 +669,11 @@ extern "C" int litho_band_synthesis(const void* box, int n_fields, int n, int h,
   if ((uintptr_t)ws & 15) return LITHO_E_ALIGN;
   char* w0 = static_cast<char*>(ws);
   int* status = reinterpret_cast<int*>(w0);
-  float2* tw = reinterpret_cast<float2*>(w0 + align16(16));
+  float2* tw_own = reinterpret_cast<float2*>(w0 + align16(16));
   float* blockmax = reinterpret_cast<float*>(w0 + align16(16) + align16((int64_t)n * 8));
   cudaError_t e = cudaMemsetAsync(status, 0, sizeof(int), s);
   if (e != cudaSuccess) return (int)e;
-  k_twiddle_table<<<(n + 255) / 256, 256, 0, s>>>(tw, n, +1);
+  const float2* tw = twiddles_for(n, tw_own, s);
   if (complex_out) {
     const int side = 2 * h + 1;
     const size_t sm = (size_t)n * 8 + (size_t)kCsRows * side * 8;
@@ -671,7 +689,10 @@ extern "C" int litho_band_synthesis(const void* box, int n_fields, int n, int h,
       e = wide_synth_real(static_cast<const float2*>(box), h, n, n_fields, static_cast<float*>(out),
                           reinterpret_cast<float2*>(wb), tw, s);
     } else {
-      float2* cbuf = h <= 31 ? reinterpret_cast<float2*>(wb) : nullptr;
+      // column stage ahead (k_synth_cols) for batches with enough columns to
+      // fill the GPU; smaller batches form it inside each synthesis block
+      const bool cols_ahead = (int64_t)n_fields * (h + 1) >= kColsAheadMin;
+      float2* cbuf = h <= 31 && cols_ahead ? reinterpret_cast<float2*>(wb) : nullptr;
       e = launch_synth_real(static_cast<const float2*>(box), 2 * h + 1, n, n_fields, tw, nullptr,
                             static_cast<float*>(out), blockmax, s, cbuf, status);
     }
@@ -792,7 +813,7 @@ extern "C" int litho_ilt_image_objective(const void* image_box, int n_fields, in
   if (((uintptr_t)ws | (uintptr_t)target) & 15) return LITHO_E_ALIGN;  // target rows are copied in 16-byte pieces
   const int64_t nb = (int64_t)n_fields * synth_pairs_blocks(n);
   char* w = static_cast<char*>(ws);
-  float2* tw = reinterpret_cast<float2*>(w);
+  float2* tw_own = reinterpret_cast<float2*>(w);
   w += align16((int64_t)n * 8);
   float* blockmax = reinterpret_cast<float*>(w);
   w += align16(nb * 4);
@@ -801,7 +822,7 @@ extern "C" int litho_ilt_image_objective(const void* image_box, int n_fields, in
   unsigned int* ppart = reinterpret_cast<unsigned int*>(w);
   w += align16(nb * 4);
   float2* cbuf = reinterpret_cast<float2*>(w);
-  k_twiddle_table<<<(n + 255) / 256, 256, 0, s>>>(tw, n, +1);
+  const float2* tw = twiddles_for(n, tw_own, s);
   const double npix = (double)n * n;
   const SynthObj obj{target, scale, level, sign, steepness_a, (float)(2.0 / npix), dfield, cpart, ppart, counters,
                      cost_out, perr_out};
@@ -869,9 +890,8 @@ extern "C" int litho_ilt_update_sched(const float* g, long long count, LithoIltS
   if (count < 0 || (count & 3)) return LITHO_E_SIZE;
   if (((uintptr_t)g | (uintptr_t)theta | (uintptr_t)m1 | (uintptr_t)m2 | (uintptr_t)mask) & 15) return LITHO_E_ALIGN;
   if ((uintptr_t)sched & 7) return LITHO_E_ALIGN;
-  k_ilt_sched_advance<<<1, 32, 0, s>>>(sched, (double)b1, (double)b2);
-  k_ilt_update_s<<<grid_for(count / 4, 256, sms_here() * 16), 256, 0, s>>>(g, count, sched, step, b1, b2, eps, theta,
-                                                                          m1, m2, mask);
+  k_ilt_update_sf<<<grid_for(count / 4, 256, sms_here() * 16), 256, 0, s>>>(g, count, sched, step, b1, b2, eps,
+                                                                           theta, m1, m2, mask);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? LITHO_OK : (int)e;
 }

@@ -34,7 +34,10 @@ struct SynthSmem {
   size_t off_tw, off_tb, off_c, off_b, total;
 };
 
-__host__ __device__ inline SynthSmem synth_smem(int n, int g0) {
+// cols_ahead: the column stage was done ahead (k_synth_cols), so the block
+// needs only the row-stage twiddles TB and its rows' C; the full table tw and
+// the box B (the direct column stage's operands) are left out.
+__host__ __device__ inline SynthSmem synth_smem(int n, int g0, bool cols_ahead = false) {
   SynthSmem s{};
   s.M = n >> 5;
   s.Lp = s.M < 32 ? s.M : 32;
@@ -43,10 +46,10 @@ __host__ __device__ inline SynthSmem synth_smem(int n, int g0) {
   s.G = 2 * g0 + 1;
   s.gp = g0 + 1;
   s.off_tw = 0;
-  s.off_tb = s.off_tw + (size_t)n * 8;
+  s.off_tb = cols_ahead ? 0 : s.off_tw + (size_t)n * 8;
   s.off_c = s.off_tb + (size_t)s.gp * s.M * 8;
   s.off_b = s.off_c + (size_t)kSyRows * s.gp * 8;
-  s.total = s.off_b + (size_t)s.G * s.G * 8;
+  s.total = cols_ahead ? s.off_b : s.off_b + (size_t)s.G * s.G * 8;
   return s;
 }
 
@@ -121,7 +124,7 @@ k_synth_pairs(const float2* __restrict__ Bbox, int g0, int n, const float2* __re
               float* __restrict__ blockmax, const float2* __restrict__ Cg, SynthObj obj = SynthObj{}) {
   static_assert(!OBJ || PASS == 1, "the objective runs in the writing pass");
   extern __shared__ __align__(16) unsigned char sy_raw[];
-  const SynthSmem L = synth_smem(n, g0);
+  const SynthSmem L = synth_smem(n, g0, Cg != nullptr);
   const int o = blockIdx.y, y0 = blockIdx.x * kSyRows;
   const LithoNorm nm = norm ? norm[o] : LithoNorm{0, 1.0f};
   if (PASS == 0 && nm.mode != 1) return;
@@ -314,7 +317,7 @@ int synth_pairs_blocks(int n) { return n / kSyRows; }
 cudaError_t launch_synth_pairs(const float2* box, int g0, int n, int n_out, const float2* tw, const LithoNorm* norm,
                                float* image, float* peak, float* blockmax, cudaStream_t s, cudaEvent_t mid,
                                float2* cbuf) {
-  const SynthSmem L = synth_smem(n, g0);
+  const SynthSmem L = synth_smem(n, g0, cbuf != nullptr);
   const dim3 grid(n / kSyRows, n_out);
   const int pk_blocks = (n_out + 7) / 8;
   cudaError_t e;
@@ -344,7 +347,7 @@ int64_t synth_cols_bytes(int n_out, int n, int g0) { return (int64_t)n_out * (g0
 // values) in shared memory next to the synthesis operands.
 bool synth_objective_ok(int n, int g0) {
   return synth_pairs_ok(n, g0) && n <= 1024 &&
-         obj_stage_off(synth_smem(n, g0)) + (size_t)kSyWarps * kSyObjStage * 4 <= 110 * 1024;
+         obj_stage_off(synth_smem(n, g0, true)) + (size_t)kSyWarps * kSyObjStage * 4 <= 110 * 1024;
 }
 
 // The image synthesis of launch_synth_pairs (no normalisation) with the ILT
@@ -352,7 +355,7 @@ bool synth_objective_ok(int n, int g0) {
 // stage runs ahead into cbuf. Partials: [n_out][n / kSyRows] in obj.
 cudaError_t launch_synth_objective(const float2* box, int g0, int n, int n_out, const float2* tw, float* blockmax,
                                    float2* cbuf, const SynthObj& obj, cudaStream_t s) {
-  const SynthSmem L = synth_smem(n, g0);
+  const SynthSmem L = synth_smem(n, g0, true);
   const dim3 grid(n / kSyRows, n_out);
   const size_t smc = (size_t)(g0 + 1) * (n >> 5) * 8;
   k_synth_cols<<<dim3((g0 + 1 + kColWarps - 1) / kColWarps, n_out), kColWarps * 32, smc, s>>>(box, g0, n, tw, cbuf);

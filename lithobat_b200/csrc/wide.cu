@@ -584,8 +584,8 @@ int abbe_wide_run(const LithoAbbePlan& p, const void* blob, const void* table_in
   const LithoNorm* norm = reinterpret_cast<const LithoNorm*>(b + p.off_norm);
   char* w = static_cast<char*>(ws);
   int* status = reinterpret_cast<int*>(w + l.status);
-  float2* twN = reinterpret_cast<float2*>(w + l.twN);
-  float2* twL = reinterpret_cast<float2*>(w + l.twL);
+  float2* twN_own = reinterpret_cast<float2*>(w + l.twN);
+  float2* twL_own = reinterpret_cast<float2*>(w + l.twL);
   float2* u1 = reinterpret_cast<float2*>(w + l.u1);
   float2* mb = reinterpret_cast<float2*>(w + l.mb);
   float2* table = table_in ? (float2*)table_in : reinterpret_cast<float2*>(w + l.table);
@@ -603,8 +603,8 @@ int abbe_wide_run(const LithoAbbePlan& p, const void* blob, const void* table_in
 
   mark(0);
   if ((e = cudaMemsetAsync(status, 0, sizeof(int), s)) != cudaSuccess) return (int)e;
-  k_twiddle_table<<<(n + 255) / 256, 256, 0, s>>>(twN, n, +1);
-  k_twiddle_table<<<(L + 255) / 256, 256, 0, s>>>(twL, L, +1);
+  const float2* twN = twiddles_for(n, twN_own, s);
+  const float2* twL = twiddles_for(L, twL_own, s);
   if (!table_in && (e = launch_pupil_table(p, blob, table, s)) != cudaSuccess) return (int)e;
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
   mark(1);
@@ -694,14 +694,14 @@ int wide_socs_adjoint(const LithoAbbePlan& p, const void* blob, const float2* ta
   const WideAdjLayout l = wide_adj_layout(p.n_clips, h);
   const LithoJob* jobs = reinterpret_cast<const LithoJob*>(static_cast<const char*>(blob) + p.off_jobs);
   char* w = static_cast<char*>(ws);
-  float2* twL = reinterpret_cast<float2*>(w + l.twL);
+  float2* twL_own = reinterpret_cast<float2*>(w + l.twL);
   float2* gL = reinterpret_cast<float2*>(w + l.gL);
   float2* T = reinterpret_cast<float2*>(w + l.T);
   float2* T2 = reinterpret_cast<float2*>(w + l.T2);
   float2* Yt = reinterpret_cast<float2*>(w + l.Yt);
   float2* A = reinterpret_cast<float2*>(w + l.A);
   cudaError_t e;
-  k_twiddle_table<<<(L + 255) / 256, 256, 0, s>>>(twL, L, +1);
+  const float2* twL = twiddles_for(L, twL_own, s);
   if ((e = cudaMemsetAsync(gL, 0, (size_t)p.n_clips * L * L * 8, s)) != cudaSuccess) return (int)e;
   if ((e = cudaMemsetAsync(A, 0, (size_t)p.n_clips * npts * 8, s)) != cudaSuccess) return (int)e;
   const int G = 4 * h + 1;
@@ -729,14 +729,14 @@ int wide_coarse_box(const LithoAbbePlan& p, const void* blob, const float2* tabl
   const LithoItem* items = reinterpret_cast<const LithoItem*>(b + p.off_items);
   const int32_t* out_items = reinterpret_cast<const int32_t*>(b + p.off_out_items);
   char* w = static_cast<char*>(ws);
-  float2* twL = reinterpret_cast<float2*>(w + l.twL);
+  float2* twL_own = reinterpret_cast<float2*>(w + l.twL);
   float2* T = reinterpret_cast<float2*>(w + l.T);
   float* partial = reinterpret_cast<float*>(w + l.partial);
   float* J = reinterpret_cast<float*>(w + l.J);
   float2* F = reinterpret_cast<float2*>(w + l.F);
   const int L = p.L, G = 4 * p.h + 1;
   cudaError_t e;
-  k_twiddle_table<<<(L + 255) / 256, 256, 0, s>>>(twL, L, +1);
+  const float2* twL = twiddles_for(L, twL_own, s);
   if ((e = cudaMemsetAsync(partial, 0, (size_t)p.n_items * L * L * 4, s)) != cudaSuccess) return (int)e;
   for (int j0 = 0; j0 < p.n_jobs; j0 += l.jobs_per_chunk) {
     const int nj = (p.n_jobs - j0) < l.jobs_per_chunk ? (p.n_jobs - j0) : l.jobs_per_chunk;

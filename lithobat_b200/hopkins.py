@@ -73,6 +73,7 @@ class SOCSKernels:
         self.gram_sweeps = gram_sweeps
         self._plans: dict = {}
         self._table = None
+        self._tcc = None             # band TCC blob (device), False where it does not fit
 
     def __len__(self) -> int:
         return int(self.weights.size)
@@ -199,6 +200,39 @@ class SOCSKernels:
             tab[:, pos] = self._phi.to(torch.complex64)
             self._table = tab.contiguous()
         return self._table
+
+    def tcc(self):
+        """The band TCC of these kernels on the device (``litho_socs_tcc_build``:
+        T(f, f') = sum_k lambda_k conj phi_k(f) phi_k(f') in FP64, stored as
+        complex64 with its index maps), built once; None where it would not
+        stay resident in L2 (wide bands), and the per-kernel engines serve."""
+        if self._tcc is False:
+            return None
+        if self._tcc is None:
+            torch = nat.require_cuda()
+            L = nat.lib()
+            nb, h = int(self.band_kx.size), self.halfwidth
+            nbytes = C.c_size_t(0)
+            st = L.litho_socs_tcc_bytes(nb, h, C.byref(nbytes))
+            if st == nat.LITHO_E_UNSUPPORTED:
+                self._tcc = False
+                return None
+            nat.check("litho_socs_tcc_bytes", st)
+            dev = self._phi.device
+            buf = torch.empty(nbytes.value, dtype=torch.uint8, device=dev)
+            kx = torch.from_numpy(self.band_kx.astype(np.int32)).to(dev)
+            ky = torch.from_numpy(self.band_ky.astype(np.int32)).to(dev)
+            lam = torch.from_numpy(self.weights.copy()).to(dev)
+            bad = torch.zeros((1,), dtype=torch.int32, device=dev)
+            phi = self._phi.contiguous()
+            nat.check("litho_socs_tcc_build", L.litho_socs_tcc_build(
+                phi.data_ptr(), lam.data_ptr(), len(self), kx.data_ptr(), ky.data_ptr(), nb, h, buf.data_ptr(),
+                buf.numel(), bad.data_ptr(), nat.stream_ptr(torch, dev)))
+            if int(bad.item()):
+                raise nat.LithoError("litho_socs_tcc_build", nat.LITHO_E_BAND,
+                                     "a band point lies outside the kernel box")
+            self._tcc = buf
+        return self._tcc
 
     def _plan(self, n_clips: int, mask_complex: bool, norm_mode: tuple):
         key = (n_clips, mask_complex, norm_mode)

@@ -52,9 +52,15 @@ def gaussian_weights(sigma: float, truncate: float = 4.0) -> np.ndarray:
 
 
 class _Stages:
-    """Device stages bound to one set of SOCS kernels and one batch size."""
+    """Device stages bound to one set of SOCS kernels and one batch size.
 
-    def __init__(self, kernels: SOCSKernels, n_clips: int):
+    The image and adjoint band boxes come from the band TCC
+    (``litho_socs_tcc_image`` / ``litho_socs_tcc_adjoint``) when the kernels'
+    TCC stays resident in L2 and ``use_tcc`` allows it, else from the
+    per-kernel coarse-grid engines (``litho_coarse_image``,
+    ``litho_socs_adjoint``)."""
+
+    def __init__(self, kernels: SOCSKernels, n_clips: int, use_tcc: bool = True):
         self.torch = nat.require_cuda()
         self.L = nat.lib()
         self.k = kernels
@@ -66,6 +72,8 @@ class _Stages:
         self.pd = plan_from_table(self.n, float(kernels.grid.pixel_size), self.C, kernels.weights, self.h, False)
         self.blob = self.torch.from_numpy(self.pd.blob).to(self.dev)
         self.table = kernels.table()
+        self.tcc = kernels.tcc() if use_tcc else None
+        self.nb = int(kernels.band_kx.size)
         self._ws = {}
         self._blur = {}
         self._obj_counters = None     # litho_ilt_objective_totals' per-field block counters
@@ -82,14 +90,16 @@ class _Stages:
         return t
 
     # -- transforms ---------------------------------------------------------
-    def band(self, fields, bm: int, scale: float, tag: str = "band"):
-        """(F, (2bm+1)^2) complex64 band boxes of F dense fields."""
+    def band(self, fields, bm: int, scale: float, tag: str = "band", out=None):
+        """(F, (2bm+1)^2) complex64 band boxes of F dense fields (into ``out``
+        when given)."""
         torch, L = self.torch, self.L
         F = int(fields.shape[0])
         nb = C.c_size_t(0)
         nat.check("litho_band_spectrum_workspace", L.litho_band_spectrum_workspace(F, self.n, bm, C.byref(nb)))
         ws = self.ws(tag, nb.value)
-        out = torch.empty((F, (2 * bm + 1) ** 2), dtype=torch.complex64, device=self.dev)
+        if out is None:
+            out = torch.empty((F, (2 * bm + 1) ** 2), dtype=torch.complex64, device=self.dev)
         nat.check("litho_band_spectrum", L.litho_band_spectrum(
             fields.data_ptr(), int(fields.is_complex()), F, self.n, bm, scale, out.data_ptr(), ws.data_ptr(),
             ws.numel(), self.stream()))
@@ -108,8 +118,8 @@ class _Stages:
             self.stream()))
         return out
 
-    def mask_box(self, masks):
-        return self.band(masks, self.h, 1.0 / (self.n * self.n), tag="band_mask")
+    def mask_box(self, masks, out=None):
+        return self.band(masks, self.h, 1.0 / (self.n * self.n), tag="band_mask", out=out)
 
     # workspaces whose first word is a device status (litho_band_spectrum,
     # litho_band_synthesis: LITHO_E_TIMEOUT when a bounded wait gave up); one
@@ -130,6 +140,12 @@ class _Stages:
     def image_box(self, mbox):
         """Band box (C, (4h+1)^2) of the raw SOCS intensity from the mask band boxes."""
         torch, L = self.torch, self.L
+        if self.tcc is not None:
+            G = 4 * self.h + 1
+            bbox = torch.empty((self.C, G * G), dtype=torch.complex64, device=self.dev)
+            nat.check("litho_socs_tcc_image", L.litho_socs_tcc_image(
+                self.tcc.data_ptr(), self.nb, self.h, mbox.data_ptr(), self.C, bbox.data_ptr(), self.stream()))
+            return bbox
         nb = C.c_size_t(0)
         nat.check("litho_abbe_workspace", L.litho_abbe_workspace(C.byref(self.pd.plan), C.byref(nb)))
         ws = self.ws("coarse", nb.value)
@@ -160,12 +176,17 @@ class _Stages:
         scale * dJ/dI on |g| <= 2h (already divided by N^2); into ``out``
         when given."""
         torch, L = self.torch, self.L
+        hbox = out if out is not None else torch.empty((self.C, self.side * self.side), dtype=torch.complex64,
+                                                       device=self.dev)
+        if self.tcc is not None and field_boxes is None and mbox is not None:
+            nat.check("litho_socs_tcc_adjoint", L.litho_socs_tcc_adjoint(
+                self.tcc.data_ptr(), self.nb, self.h, mbox.data_ptr(), gbox.data_ptr(), self.C, hbox.data_ptr(),
+                self.stream()))
+            return hbox
         nb = C.c_size_t(0)
         nat.check("litho_socs_adjoint_workspace", L.litho_socs_adjoint_workspace(
             self.C, self.pd.plan.n_items, self.h, C.byref(nb)))
         ws = self.ws("adjoint", nb.value)
-        hbox = out if out is not None else torch.empty((self.C, self.side * self.side), dtype=torch.complex64,
-                                                       device=self.dev)
         nat.check("litho_socs_adjoint", L.litho_socs_adjoint(
             C.byref(self.pd.plan), self.blob.data_ptr(), self.table.data_ptr(),
             None if mbox is None else mbox.data_ptr(),
@@ -178,17 +199,21 @@ class _Stages:
         return (p.sigma_px < 1e-3 and p.smooth_px < 1e-3 and p.weight_tv == 0.0 and p.weight_discrete == 0.0
                 and self.n % 4 == 0)
 
-    def objective_split(self, mbox, target, scale, level, sign, steepness, want_signed=True, out_hbox=None):
+    def objective_split(self, mbox, target, scale, level, sign, steepness, want_signed=True, out_hbox=None,
+                        out_cost=None, out_perr=None):
         """The objective from the mask band boxes, keeping only band boxes
         between steps: (cost (C,), gradient band box (C, (2h+1)^2), signed or
         None, perr (C,)). Synthesis of the image, the per-pixel resist, the
-        band of dJ/dI, the adjoint to the gradient's band box."""
+        band of dJ/dI, the adjoint to the gradient's band box. ``out_*``:
+        write into these tensors (views of a larger batch's state)."""
         ibox = self.image_box(mbox)
-        cost, gbox, signed, perr = self.objective_from_box(ibox, target, scale, level, sign, steepness, want_signed)
+        cost, gbox, signed, perr = self.objective_from_box(ibox, target, scale, level, sign, steepness, want_signed,
+                                                           out_cost, out_perr)
         hbox = self.adjoint_box(gbox, mbox, out=out_hbox)
         return cost, hbox, signed, perr
 
-    def objective_from_box(self, ibox, target, scale, level, sign, steepness, want_signed=True):
+    def objective_from_box(self, ibox, target, scale, level, sign, steepness, want_signed=True, out_cost=None,
+                           out_perr=None):
         """The resist objective of the image whose band box (C, (4h+1)^2) is
         ``ibox``: (cost (C,), band box of scale * dJ/dI / N^2 on |g| <= 2h,
         signed or None, perr (C,))."""
@@ -196,8 +221,8 @@ class _Stages:
         a = steepness / max(abs(level), 1e-12)
         if self._obj_counters is None:
             self._obj_counters = torch.zeros((self.C,), dtype=torch.int32, device=self.dev)
-        cost = torch.empty((self.C,), dtype=torch.float64, device=self.dev)
-        perr = torch.empty((self.C,), dtype=torch.int64, device=self.dev)
+        cost = out_cost if out_cost is not None else torch.empty((self.C,), dtype=torch.float64, device=self.dev)
+        perr = out_perr if out_perr is not None else torch.empty((self.C,), dtype=torch.int64, device=self.dev)
         if not want_signed and self.image_objective_ok() and target.data_ptr() % 16 == 0:
             # the image is synthesised straight into the objective (never stored)
             nb = C.c_size_t(0)
@@ -308,7 +333,7 @@ class _PlainStages(_Stages):
     adjoint (one 2-D FFT per kernel and direction), for comparison."""
 
     def __init__(self, kernels: SOCSKernels, n_clips: int):
-        super().__init__(kernels, n_clips)
+        super().__init__(kernels, n_clips, use_tcc=False)
         torch = self.torch
         self.phi = kernels._phi.to(torch.complex64).contiguous()
         self.lam = (C.c_float * len(kernels))(*[float(x) for x in kernels.weights])
@@ -371,8 +396,10 @@ def stages(kernels: SOCSKernels, n_clips: int, engine: str = "fused") -> _Stages
         # the band-limited stages cover kernel bands up to 15 bins on chip (a
         # 64-point coarse grid) and wider ones on coarse grids of 128..1024
         # points; bands wider than that run both directions on the full grid
-        fused = engine == "fused" and band_limited_ok(int(kernels.grid.n_pixels), kernels.halfwidth)
-        st = (_Stages if fused else _PlainStages)(kernels, n_clips)
+        if engine not in ("fused", "coarse", "plain"):
+            raise ValueError(f"engine must be 'fused', 'coarse' or 'plain', got {engine!r}")
+        fused = engine != "plain" and band_limited_ok(int(kernels.grid.n_pixels), kernels.halfwidth)
+        st = _Stages(kernels, n_clips, use_tcc=engine == "fused") if fused else _PlainStages(kernels, n_clips)
         _STAGES[key] = st
     return st
 
@@ -588,6 +615,22 @@ class IltParams:
     eps: float = 1e-8
 
 
+def default_lanes(n_clips: int) -> int:
+    """Parallel clip groups of a graph-replayed fast step: two once a group
+    still has 4 clips to keep its pixel passes wide."""
+    return 2 if n_clips >= 8 else 1
+
+
+def _lane_ranges(n_clips: int, lanes: int):
+    base, extra = divmod(n_clips, lanes)
+    out, a = [], 0
+    for r in range(lanes):
+        b = a + base + (1 if r < extra else 0)
+        out.append((a, b))
+        a = b
+    return out
+
+
 class IltBatch:
     """A batch of ILT solves advanced together on the device.
 
@@ -601,8 +644,11 @@ class IltBatch:
     synthesised on demand. ``fast=False`` forces the stage-by-stage path."""
 
     def __init__(self, kernels: SOCSKernels, targets, theta0, params: IltParams, engine: str = "fused",
-                 fast: bool | None = None):
+                 fast: bool | None = None, lanes: int | None = None):
         self.st = stages(kernels, int(theta0.shape[0]), engine)
+        C = int(theta0.shape[0])
+        #: clip groups the graph-replayed fast step runs on parallel branches
+        self.lanes = max(1, min(C, int(lanes) if lanes is not None else default_lanes(C)))
         torch = self.st.torch
         n = self.st.n
         self.p = params
@@ -635,7 +681,8 @@ class IltBatch:
     def check_status(self) -> None:
         """Synchronise and raise ``LithoError`` if a bounded device wait gave
         up in the latest step (its results are then invalid)."""
-        self.st.check_status()
+        for st in getattr(self, "_lane_st", None) or [self.st]:
+            st.check_status()
 
     @property
     def mask(self):
@@ -676,30 +723,58 @@ class IltBatch:
         return self.cost
 
     def _capture(self):
+        """Record one fast step as a CUDA graph. The clips are split into
+        ``self.lanes`` groups, each with its own stages (workspaces) and step
+        schedule, recorded on parallel branches of the graph: a lane's
+        latency-bound coarse-grid kernels then overlap another lane's
+        pixel passes. Clips are independent, so the results are those of one
+        lane; every kernel's arithmetic is per clip."""
         torch = self.st.torch
         p = self.p
+        C = int(self.theta.shape[0])
+        ranges = [(a, b) for a, b in _lane_ranges(C, self.lanes) if b > a]
         sched = np.zeros(1, dtype=nat.ILT_SCHED_DTYPE)
         sched["beta"] = sched["beta_next"] = self.beta
         sched["growth"] = p.growth
         sched["it"] = self.it
-        self._sched = torch.from_numpy(sched.view(np.uint8)).to(self.st.dev)
+        self._sched = [torch.from_numpy(sched.view(np.uint8).copy()).to(self.st.dev) for _ in ranges]
         hbox = torch.empty_like(self.hbox)
         hbox.copy_(self.hbox)
         self.hbox = hbox
+        lane_st = [self.st] if len(ranges) == 1 else [_Stages(self.st.k, b - a, use_tcc=self.st.tcc is not None)
+                                                      for a, b in ranges]
+        mask = torch.empty_like(self.theta)
+        mbox = torch.empty((C, self.st.side * self.st.side), dtype=torch.complex64, device=self.st.dev)
+        cost = torch.empty((C,), dtype=torch.float64, device=self.st.dev)
+        perr = torch.empty((C,), dtype=torch.int64, device=self.st.dev)
+        if len(ranges) > 1:
+            # the lanes' first calls size their workspaces outside the capture
+            for st, (a, b) in zip(lane_st, ranges):
+                mb = st.mask_box(self._mask[a:b])
+                st.objective_split(mb, self.target[a:b], p.scale, p.level, p.sign, p.steepness, want_signed=False)
+                st.synth(self.hbox[a:b], st.h, False)
         torch.cuda.synchronize(self.st.dev)
+        streams = [torch.cuda.Stream(device=self.st.dev) for _ in ranges]
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
-            st = self.st
-            grad = st.synth(self.hbox, st.h, False)
-            mask = torch.empty_like(self.theta)
-            nat.check("litho_ilt_update_sched", st.L.litho_ilt_update_sched(
-                grad.data_ptr(), grad.numel(), self._sched.data_ptr(), float(p.step), float(p.b1), float(p.b2),
-                float(p.eps), self.theta.data_ptr(), self.m1.data_ptr(), self.m2.data_ptr(), mask.data_ptr(),
-                st.stream()))
-            mbox = st.mask_box(mask)
-            cost, _, _, perr = st.objective_split(mbox, self.target, p.scale, p.level, p.sign, p.steepness,
-                                                  want_signed=False, out_hbox=self.hbox)
+            main = torch.cuda.current_stream(self.st.dev)
+            for s in streams:
+                s.wait_stream(main)
+            for st, s, sch, (a, b) in zip(lane_st, streams, self._sched, ranges):
+                with torch.cuda.stream(s):
+                    grad = st.synth(self.hbox[a:b], st.h, False)
+                    nat.check("litho_ilt_update_sched", st.L.litho_ilt_update_sched(
+                        grad.data_ptr(), grad.numel(), sch.data_ptr(), float(p.step), float(p.b1), float(p.b2),
+                        float(p.eps), self.theta[a:b].data_ptr(), self.m1[a:b].data_ptr(), self.m2[a:b].data_ptr(),
+                        mask[a:b].data_ptr(), st.stream()))
+                    st.mask_box(mask[a:b], out=mbox[a:b])
+                    st.objective_split(mbox[a:b], self.target[a:b], p.scale, p.level, p.sign, p.steepness,
+                                       want_signed=False, out_hbox=self.hbox[a:b], out_cost=cost[a:b],
+                                       out_perr=perr[a:b])
+            for s in streams:
+                main.wait_stream(s)
         self._graph = g
+        self._lane_st = lane_st
         self._mask, self.mbox, self.cost, self.perr = mask, mbox, cost, perr
         self._grad_m = None
 

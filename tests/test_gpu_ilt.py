@@ -10,7 +10,7 @@ from oracle import litho_oracle as O
 
 pytestmark = pytest.mark.gpu
 TOL_I = 1e-5      # intensities
-TOL_G = 1e-4      # gradients: FP32 engine vs FP64 reference, relative to max |grad|
+TOL_G = 1e-5      # gradients: FP32 engine vs FP64 reference, max |dg| / max |g|
 
 
 @pytest.fixture(scope="module")
@@ -29,8 +29,11 @@ def _optics(lb, od):
     return lb.OpticsConfig(**keep)
 
 
-def rel(a, b):
-    return float(np.abs(np.asarray(a, np.float64) - b).max() / np.abs(b).max())
+def rel(a, b, case=None):
+    e = float(np.abs(np.asarray(a, np.float64) - b).max() / np.abs(b).max())
+    if case:
+        print(f"PARITY {case} {e:.3e}")
+    return e
 
 
 @pytest.fixture(scope="module")
@@ -57,10 +60,10 @@ def test_socs_adjoint_matches_reference(lb, small):
     a, k = small
     fields, _ = ilt.socs_fields(k, a["mask"])
     g = ilt.socs_gradient(k, fields, a["sens"])
-    assert rel(g, a["grad"]) <= TOL_G
+    assert rel(g, a["grad"], "ilt_small_socs_gradient") <= TOL_G
     # a plain array of fields takes the general route
     g2 = ilt.socs_gradient(k, np.asarray(fields).copy(), a["sens"])
-    assert rel(g2, a["grad"]) <= TOL_G
+    assert rel(g2, a["grad"], "ilt_small_socs_gradient_from_fields") <= TOL_G
 
 
 def test_full_objective_with_blur_and_penalties(lb, small):
@@ -71,7 +74,7 @@ def test_full_objective_with_blur_and_penalties(lb, small):
     assert cost == pytest.approx(float(a["cost"]), rel=1e-5)
     assert rel(signed, a["signed"]) <= TOL_I
     assert abs(perr - int(a["perr"])) <= 2
-    assert rel(grad, a["grad_obj"]) <= TOL_G
+    assert rel(grad, a["grad_obj"], "ilt_small_objective_blur_tv_discrete_gradient") <= TOL_G
 
 
 def test_dark_tone_objective(lb, small):
@@ -80,7 +83,7 @@ def test_dark_tone_objective(lb, small):
     obj = ilt.Objective(k, a["target3"], 2.0, 0.3, 0.0, -1.0, 20.0)
     cost, grad, signed, perr = obj(a["mask3"])
     assert cost == pytest.approx(float(a["cost0"]), rel=1e-5)
-    assert rel(grad, a["grad_obj0"]) <= TOL_G
+    assert rel(grad, a["grad_obj0"], "ilt_small_dark_tone_gradient") <= TOL_G
     assert abs(perr - int(a["perr0"])) <= 2
 
 
@@ -102,7 +105,7 @@ def test_mid_size_k24_objective(lb):
     obj = ilt.Objective(k, a["target"].astype(np.float64), 1.0 / k.clear, 0.3, 0.0, 1.0, 15.0)
     cost, grad, signed, perr = obj(m)
     assert cost == pytest.approx(float(a["cost"]), rel=1e-5)
-    assert rel(grad, a["grad"]) <= TOL_G
+    assert rel(grad, a["grad"], "ilt_imm_128_k24_gradient") <= TOL_G
     assert abs(perr - int(a["perr"])) <= 4
 
 
@@ -133,7 +136,7 @@ def test_autograd_function(lb, small):
     img = ilt.socs_image(m, k)
     assert rel(img[0].detach().cpu().numpy(), a["intensity"]) <= TOL_I
     (img * sens).sum().backward()
-    assert rel(m.grad[0].cpu().numpy(), a["grad"]) <= TOL_G
+    assert rel(m.grad[0].cpu().numpy(), a["grad"], "ilt_small_autograd_gradient") <= TOL_G
 
 
 def test_fused_steps_follow_the_reference_loop(lb):
@@ -157,8 +160,18 @@ def test_fused_steps_follow_the_reference_loop(lb):
         mk = O.mask_of(th, beta, 0.0)
         cost, gm, _, _ = O.objective(ref, tgt, mk, 1.0 / ref.clear, 0.3, 0.0, 1.0, 15.0)
         b.step()
-        assert float(b.cost[0]) == pytest.approx(cost, rel=1e-4)
-    assert np.abs(b.theta[0].cpu().numpy() - th).max() <= 1e-3 * np.abs(th).max()
+        e_c = abs(float(b.cost[0]) - cost) / abs(cost)
+        print(f"PARITY ilt_imm_128_k24_fused_step{it}_cost {e_c:.3e}")
+        assert e_c <= 1e-5
+    # Adam divides by sqrt(v) + eps: where |g| is near eps the step's size
+    # follows FP32 rounding of g, so theta is held to 1 % of the step size
+    # (the rest of theta, and the costs above, to the 1e-5 bar)
+    d = np.abs(b.theta[0].cpu().numpy() - th)
+    e_t = float(d.max() / 0.05)
+    q = float(np.quantile(d, 0.99) / np.abs(th).max())
+    print(f"PARITY ilt_imm_128_k24_fused_3steps_theta {e_t:.3e} of the step; 99th percentile {q:.3e} of max|theta|")
+    assert e_t <= 0.01
+    assert q <= 1e-5
 
 
 def test_plain_engine_gives_the_same_objective(lb):
@@ -170,8 +183,9 @@ def test_plain_engine_gives_the_same_objective(lb):
     fused = ilt.IltBatch(k, tgt[None], a["theta"][None], p)
     plain = ilt.IltBatch(k, tgt[None], a["theta"][None], p, engine="plain")
     assert float(plain.cost[0]) == pytest.approx(float(a["cost"]), rel=1e-5)
-    assert rel(plain.grad_m[0].cpu().numpy(), a["grad"]) <= TOL_G
-    assert rel(fused.grad_m[0].cpu().numpy(), plain.grad_m[0].cpu().numpy().astype(np.float64)) <= TOL_G
+    assert rel(plain.grad_m[0].cpu().numpy(), a["grad"], "ilt_imm_128_k24_plain_gradient") <= TOL_G
+    assert rel(fused.grad_m[0].cpu().numpy(), plain.grad_m[0].cpu().numpy().astype(np.float64),
+               "ilt_imm_128_k24_fused_vs_plain_gradient") <= TOL_G
 
 
 def test_graph_replayed_steps_match_eager_steps(lb):
@@ -217,8 +231,10 @@ def test_image_objective_matches_synthesis_then_objective(lb):
     from lithobat_b200.patterns import manhattan_clip
     o = lb.OpticsConfig(wavelength=193e-9, NA=1.35, n_immersion=1.44, source_type="annular", sigma_inner=0.5,
                         sigma_outer=0.8, source_grid=11, normalisation="clear")
-    for n, F in ((256, 3), (512, 2), (1024, 2)):
-        g = lb.GridConfig(n_pixels=n, pixel_size=2e-9 * 256 / n)
+    # the last case is the benchmark's grid and band: 1024^2 at 1 nm, box
+    # half-width 2h = 30
+    for n, F, px in ((256, 3, 2e-9), (512, 2, 1e-9), (1024, 2, 5e-10), (1024, 3, 1e-9)):
+        g = lb.GridConfig(n_pixels=n, pixel_size=px)
         k = lb.SOCSKernels.build(o, g, tol=0.0, max_kernels=8)
         st = ilt.stages(k, F, "fused")
         assert st.image_objective_ok()
@@ -252,3 +268,96 @@ def test_image_objective_matches_synthesis_then_objective(lb):
         assert torch.equal(d0, d1)
         assert torch.equal(p0, p1) and int(ctr.abs().sum()) == 0
         np.testing.assert_allclose(c1.cpu().numpy(), c0.cpu().numpy(), rtol=1e-7)
+
+
+@pytest.mark.parametrize("lanes", [2, 3])
+def test_graph_lanes_give_the_iterates_of_eager_steps(lb, lanes):
+    """The graph-replayed step split into clip lanes on parallel graph
+    branches (own workspaces and schedules per lane) reproduces eager steps
+    of the whole batch, beta annealing included."""
+    import torch
+    from lithobat_b200 import ilt
+    from lithobat_b200.patterns import manhattan_clip
+    o = lb.OpticsConfig(wavelength=193e-9, NA=1.35, n_immersion=1.44, source_type="annular", sigma_inner=0.5,
+                        sigma_outer=0.8, source_grid=11, normalisation="clear")
+    g = lb.GridConfig(n_pixels=256, pixel_size=2e-9)
+    k = lb.SOCSKernels.build(o, g, tol=0.0, max_kernels=12)
+    rng = np.random.default_rng(33)
+    tg = np.stack([manhattan_clip(rng, 256, 2e-9, n_rect=(4, 8), width_nm=(40, 120)) for _ in range(8)])
+    th = 0.5 * rng.standard_normal((8, 256, 256))
+    p = ilt.IltParams(scale=1.0 / k.clear, level=0.3, steepness=15.0, step=0.2, beta=4.0, growth=1.05)
+    a = ilt.IltBatch(k, tg, th, p, lanes=1)
+    b = ilt.IltBatch(k, tg, th, p, lanes=lanes)
+    for _ in range(4):
+        a.step(want_signed=False)
+    b.run(4)
+    b.check_status()
+    torch.cuda.synchronize()
+    assert b.lanes == lanes and len(b._lane_st) == lanes
+    assert float((a.theta - b.theta).abs().max()) < 1e-6
+    assert float((a.mask - b.mask).abs().max()) < 1e-6
+    np.testing.assert_allclose(b.cost.cpu().numpy(), a.cost.cpu().numpy(), rtol=1e-6)
+    np.testing.assert_array_equal(b.perr.cpu().numpy(), a.perr.cpu().numpy())
+
+
+def test_band_tcc_serves_only_bands_of_half_width_15(lb):
+    """Wider kernel bands keep the per-kernel wide engine: EUV at 128^2 and
+    5 nm (3077 band points, h = 31; its TCC would take 255 MB) and ArF
+    immersion at 512^2 and 2.8 nm (h = 20)."""
+    from lithobat_b200 import ilt
+    a, od, gd = load_golden("socs_euv_wide_128_k24")
+    k = lb.SOCSKernels.build(_optics(lb, od), lb.GridConfig(**gd), tol=0.0, max_kernels=24)
+    assert k.tcc() is None and ilt.stages(k, 1, "fused").tcc is None
+    o = lb.OpticsConfig(wavelength=193e-9, NA=1.35, n_immersion=1.44, source_type="annular", sigma_inner=0.5,
+                        sigma_outer=0.8, normalisation="clear")
+    k2 = lb.SOCSKernels.build(o, lb.GridConfig(n_pixels=512, pixel_size=2.8e-9), tol=0.0, max_kernels=24)
+    assert k2.halfwidth > 15 and k2.tcc() is None
+
+
+@pytest.mark.parametrize("case", ["imm_1024_k24", "imm_256_k12", "dry_512_k40"])
+def test_band_tcc_boxes_equal_the_per_kernel_engines(lb, case):
+    """The image and gradient band boxes from the band TCC (one contraction
+    with sum_k lambda_k conj phi_k phi_k^T) against the per-kernel coarse-grid
+    engines on the same mask and sensitivity boxes, and one whole objective
+    through each (ArF immersion K = 24 at 1024^2, K = 12 at 256^2; ArF dry
+    NA 0.93 with 40 kernels at 512^2)."""
+    import torch
+    from lithobat_b200 import ilt
+    from lithobat_b200.patterns import manhattan_clip
+    n, px, K = {"imm_1024_k24": (1024, 1e-9, 24), "imm_256_k12": (256, 2e-9, 12),
+                "dry_512_k40": (512, 2e-9, 40)}[case]
+    if case == "dry_512_k40":
+        o = lb.OpticsConfig(wavelength=193e-9, NA=0.93, source_type="annular", sigma_inner=0.5, sigma_outer=0.8,
+                            normalisation="clear", source_grid=21)
+    else:
+        o = lb.OpticsConfig(wavelength=193e-9, NA=1.35, n_immersion=1.44, source_type="annular", sigma_inner=0.5,
+                            sigma_outer=0.8, normalisation="clear")
+    k = lb.SOCSKernels.build(o, lb.GridConfig(n_pixels=n, pixel_size=px), tol=0.0, max_kernels=K)
+    assert k.tcc() is not None
+    n, px = int(k.grid.n_pixels), float(k.grid.pixel_size)
+    rng = np.random.default_rng(41)
+    F = 3
+    tg = np.stack([manhattan_clip(rng, n, px, n_rect=(6, 12), width_nm=(4 * px * 1e9, 30 * px * 1e9))
+                   for _ in range(F)]).astype(np.float32)
+    masks = torch.from_numpy(rng.random((F, n, n)).astype(np.float32)).cuda()
+    sens = torch.from_numpy(rng.standard_normal((F, n, n)).astype(np.float32)).cuda()
+    theta = (0.5 * rng.standard_normal((F, n, n))).astype(np.float32)
+    a_st, b_st = ilt.stages(k, F, "fused"), ilt.stages(k, F, "coarse")
+    assert a_st.tcc is not None and b_st.tcc is None
+    mbox = a_st.mask_box(masks)
+    ia, ib = a_st.image_box(mbox), b_st.image_box(mbox)
+    e_i = float((ia - ib).abs().max() / ib.abs().max())
+    gbox = a_st.band(sens, 2 * a_st.h, 1.0 / (n * n))
+    ha, hb = a_st.adjoint_box(gbox, mbox), b_st.adjoint_box(gbox, mbox)
+    e_h = float((ha - hb).abs().max() / hb.abs().max())
+    p = ilt.IltParams(scale=1.0 / k.clear, level=0.3, steepness=15.0)
+    fa = ilt.IltBatch(k, tg, theta, p, engine="fused")
+    fb = ilt.IltBatch(k, tg, theta, p, engine="coarse")
+    assert float(fb.grad_m.abs().max()) > 0
+    e_g = float((fa.grad_m - fb.grad_m).abs().max() / fb.grad_m.abs().max())
+    print(f"PARITY tcc_vs_coarse_{case} image_box {e_i:.3e} grad_box {e_h:.3e} grad {e_g:.3e}")
+    # boxes: FP32 rounding of two summation orders. The objective's gradient
+    # passes dJ/dI = a z (1 - z) ... with a = 50, which amplifies them; each
+    # engine is held to 1e-5 of the FP64 reference, so each other to 2e-5
+    assert e_i <= 2e-6 and e_h <= 2e-6 and e_g <= 2e-5
+    np.testing.assert_allclose(fa.cost.cpu().numpy(), fb.cost.cpu().numpy(), rtol=1e-5)
