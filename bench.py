@@ -353,7 +353,9 @@ def bench_uneven(args, torch, dev, world, max_over_ranks, barrier) -> dict:
             "ms_per_batch": ms, "steps": steps, "workload": UNEVEN_WORKLOAD, "clips": count,
             "clips_per_size": {int(n): int(sum(1 for x in sizes if x == n)) for n in sorted(set(sizes))},
             "source_points": len(lb.source_points(o)), "graph_replay": run.graph is not None,
+            "engine": run.engine, "queue_tasks": run.queue.n_tasks if run.queue is not None else 0,
             "tuned_items_per_block": {int(k): v["items_per_block"] for k, v in run.tuned.items()},
+            "tuned": {int(k): {kk: vv for kk, vv in v.items() if kk != "ms"} for k, v in run.tuned.items()},
             "setup_and_tuning_s": setup_s, "max_rel_diff_vs_single_clip": worst}
 
 

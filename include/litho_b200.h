@@ -140,6 +140,45 @@ typedef struct LithoAbbePlan {
     int64_t off_mirrors;
 } LithoAbbePlan;
 
+/* One size group of an uneven batch (litho_uneven_run): a plan whose clips
+ * share one grid side, its device buffers, and the work-queue sizes the
+ * tuner picks (0 selects the default of each). Groups of the wide-pupil
+ * engine (plan.L >= 128) run their coherent passes in the shared queue;
+ * groups on the coarse grids of 32 / 64 points run litho_abbe_tabled(). */
+typedef struct LithoUnevenGroup {
+    LithoAbbePlan plan;
+    const void* blob_host;    /* the plan blob in host memory (the schedule  */
+                              /* reads its work items)                        */
+    const void* blob_dev;     /* the same blob on the device                  */
+    const void* table_dev;    /* litho_abbe_pupil_table() of the plan         */
+    const void* masks_dev;    /* [n_clips][N][N]                              */
+    float* image_dev;         /* [n_out][N][N]                                */
+    float* peak_dev;          /* [n_out]                                      */
+    void* workspace_dev;      /* litho_uneven_group_workspace() bytes         */
+    size_t ws_bytes;
+    int32_t slot_kib;         /* pass-A buffer slot target, KiB (0: 16        */
+                              /* transforms per resident block, 16 MiB..1 GiB)*/
+    int32_t n_slots;          /* slots in flight, >= 2 (2)                    */
+    int32_t a_units;          /* warp transforms of 1024/L rows per pass-A    */
+                              /* task (96)                                    */
+    int32_t b_rows;           /* row blocks per pass-B task (2 at L = 128,    */
+                              /* else 1)                                      */
+} LithoUnevenGroup;           /* 200 bytes */
+
+/* One task of the uneven work queue (written by litho_uneven_schedule). */
+typedef struct LithoQueueTask {
+    int32_t kind;             /* 0: pass A (row transforms), 1: pass B        */
+    int32_t group;            /* wide group, in the schedule's order          */
+    int32_t slot;             /* pass-A buffer slot                           */
+    int32_t base;             /* first job of the slot's chunk                */
+    int32_t first;            /* A: first job; B: work item                   */
+    int32_t count;            /* A: jobs; B: first row block                  */
+    int32_t rows;             /* B: row blocks                                */
+    int32_t wait_ctr;         /* counter to wait for (-1: none)               */
+    int32_t wait_value;       /* ... until it reaches this value              */
+    int32_t done_ctr;         /* counter incremented when the task is done    */
+} LithoQueueTask;             /* 40 bytes */
+
 /* ---- library ----------------------------------------------------------- */
 
 /* Human-readable text for a status code returned by any entry point. */
@@ -149,8 +188,9 @@ const char* litho_status_string(int status);
 int litho_version(void);
 
 /* sizeof() of the public structs, in declaration order: LithoPupil,
- * LithoJob, LithoItem, LithoNorm, LithoAbbePlan, LithoMirror. Writes min(n, 6) values;
- * returns how many structs the ABI has. For binding generators. */
+ * LithoJob, LithoItem, LithoNorm, LithoAbbePlan, LithoMirror,
+ * LithoUnevenGroup, LithoQueueTask. Writes min(n, 8) values; returns how many
+ * structs the ABI has. For binding generators. */
 int litho_abi_sizes(int32_t* out, int n);
 
 /* ---- Abbe imaging ------------------------------------------------------ */
@@ -259,6 +299,43 @@ int litho_abbe_profile(const LithoAbbePlan* plan, const void* plan_blob_dev,
                        const void* table_dev /* NULL: built each run */, const void* mask_dev, float* image_dev, float* peak_dev,
                        void* workspace_dev, size_t workspace_bytes, cudaStream_t stream,
                        int reps, float* stage_ms);
+
+/* ---- uneven batches ------------------------------------------------------
+ * Clips of several grid sides imaged in one call: the reference images one
+ * clip per compute_aerial_image() call whatever its size
+ * (expose/aerial_image.py:502-548, batching transforms only within a clip in
+ * _Batch, :312-348). Here every size group's coherent transforms on the
+ * wide-pupil coarse grids run in ONE persistent kernel that drains a device
+ * work queue of (chunk of jobs, pass A) and (work item, row block, pass B)
+ * tasks across all groups; each task waits (bounded) on counters of earlier
+ * tasks only, so the queue cannot deadlock. Usage: size every group's
+ * workspace, build the schedule once on the host, copy the task list to the
+ * device, then call litho_uneven_run() per batch (it is stream-ordered and
+ * holds no host synchronisation, so it can be captured in a CUDA graph once
+ * the device's twiddle tables exist, i.e. after one uncaptured call). */
+int litho_uneven_group_workspace(const LithoUnevenGroup* group, size_t* bytes);
+
+/* The task list of a batch: call with tasks == NULL for *n_tasks and
+ * *n_counters, then with a buffer of max_tasks >= *n_tasks. Host only. */
+int litho_uneven_schedule(const LithoUnevenGroup* groups, int n_groups, LithoQueueTask* tasks,
+                          int max_tasks, int* n_tasks, int* n_counters);
+
+/* Bytes of the queue's own workspace (status word, head, counters). */
+int litho_uneven_queue_workspace(int n_counters, size_t* bytes);
+
+/* Image every group: coarse-grid groups through litho_abbe_tabled(), then the
+ * wide groups' band DFTs, the queue launch and their reductions, syntheses
+ * and normalisations. Outputs as litho_abbe() per group. */
+int litho_uneven_run(const LithoUnevenGroup* groups, int n_groups, const LithoQueueTask* tasks_dev,
+                     int n_tasks, int n_counters, void* queue_workspace_dev, size_t queue_ws_bytes,
+                     cudaStream_t stream);
+
+/* Synchronise `stream` and return the queue's status word: 0, or
+ * LITHO_E_TIMEOUT if a task's bounded wait gave up in the last run, or
+ * LITHO_E_BAND if the task list held a task outside its group's buffers
+ * (skipped); either way the images are invalid. Each group's own word:
+ * litho_abbe_status(). */
+int litho_uneven_status(const void* queue_workspace_dev, cudaStream_t stream);
 
 /* Workspace bytes litho_abbe_plain() needs when it transforms `batch`
  * coherent systems (times their field components) at a time. */

@@ -65,6 +65,18 @@ class AbbePlan(C.Structure):
     ]
 
 
+class UnevenGroup(C.Structure):
+    _fields_ = [
+        ("plan", AbbePlan), ("blob_host", C.c_void_p), ("blob_dev", C.c_void_p), ("table_dev", C.c_void_p),
+        ("masks_dev", C.c_void_p), ("image_dev", C.c_void_p), ("peak_dev", C.c_void_p),
+        ("workspace_dev", C.c_void_p), ("ws_bytes", C.c_size_t), ("slot_kib", C.c_int32), ("n_slots", C.c_int32),
+        ("a_units", C.c_int32), ("b_rows", C.c_int32),
+    ]
+
+
+QUEUE_TASK_DTYPE = np.dtype([(k, "<i4") for k in (
+    "kind", "group", "slot", "base", "first", "count", "rows", "wait_ctr", "wait_value", "done_ctr")])
+
 MIRROR_DTYPE = np.dtype([
     ("wavelength", "<f8"), ("reduction", "<f8"), ("tilt_sign", "<f8"), ("sin_cx", "<f8"), ("sin_cy", "<f8"),
     ("n_theta", "<i4"), ("pad", "<i4"), ("off_table", "<i8"),
@@ -76,6 +88,7 @@ ILT_SCHED_DTYPE = np.dtype([
 ], align=True)
 
 assert C.sizeof(AbbePlan) == 120 and MIRROR_DTYPE.itemsize == 56 and ILT_SCHED_DTYPE.itemsize == 40
+assert C.sizeof(UnevenGroup) == 200 and QUEUE_TASK_DTYPE.itemsize == 40
 
 _lib = None
 
@@ -153,6 +166,11 @@ def lib():
         "litho_ilt_update_sched": [vp, C.c_longlong, vp, f32, f32, f32, f32, vp, vp, vp, vp, vp],
         "litho_dose_stack": [vp, vp, vp, i32, i32, C.c_longlong, vp, i32, vp, vp],
         "litho_clamp": [vp, C.c_longlong, f32, f32, vp],
+        "litho_uneven_group_workspace": [C.POINTER(UnevenGroup), C.POINTER(sz)],
+        "litho_uneven_schedule": [C.POINTER(UnevenGroup), i32, vp, i32, C.POINTER(i32), C.POINTER(i32)],
+        "litho_uneven_queue_workspace": [i32, C.POINTER(sz)],
+        "litho_uneven_run": [C.POINTER(UnevenGroup), i32, vp, i32, i32, vp, sz, vp],
+        "litho_uneven_status": [vp, vp],
         "litho_plain_socs_workspace": [i32, i32, C.POINTER(sz)],
         "litho_plain_socs_forward": [vp, i32, i32, i32, vp, vp, vp, vp, i32, vp, vp, vp, sz, vp],
         "litho_plain_socs_adjoint": [vp, vp, i32, i32, i32, vp, vp, vp, vp, i32, vp, vp, sz, vp],

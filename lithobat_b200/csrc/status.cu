@@ -27,7 +27,8 @@ extern "C" int litho_version(void) { return 200; }
 extern "C" int litho_abi_sizes(int32_t* out, int n) {
   const int32_t sz[] = {(int32_t)sizeof(LithoPupil), (int32_t)sizeof(LithoJob), (int32_t)sizeof(LithoItem),
                         (int32_t)sizeof(LithoNorm), (int32_t)sizeof(LithoAbbePlan),
-                        (int32_t)sizeof(LithoMirror)};
+                        (int32_t)sizeof(LithoMirror), (int32_t)sizeof(LithoUnevenGroup),
+                        (int32_t)sizeof(LithoQueueTask)};
   const int k = (int)(sizeof(sz) / sizeof(sz[0]));
   for (int i = 0; i < n && i < k && out; ++i) out[i] = sz[i];
   return k;

@@ -11,6 +11,7 @@ namespace litho {
 cudaError_t set_wait_limit_band(long long cycles);
 cudaError_t set_wait_limit_synth(long long cycles);
 cudaError_t set_wait_limit_gram(long long cycles);
+cudaError_t set_wait_limit_queue(long long cycles);
 
 // One thread waits, within `cycles`, on an mbarrier that nothing arrives at,
 // and records the outcome the way the pipeline kernels do.
@@ -32,6 +33,7 @@ extern "C" int litho_set_wait_limit(long long cycles) {
   if ((e = set_wait_limit_band(c)) != cudaSuccess) return (int)e;
   if ((e = set_wait_limit_synth(c)) != cudaSuccess) return (int)e;
   if ((e = set_wait_limit_gram(c)) != cudaSuccess) return (int)e;
+  if ((e = set_wait_limit_queue(c)) != cudaSuccess) return (int)e;
   return LITHO_OK;
 }
 

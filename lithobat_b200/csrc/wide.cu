@@ -25,6 +25,7 @@
 #include "common.cuh"
 #include "fftsmem.cuh"
 #include "fftwarp.cuh"
+#include "wide.cuh"
 
 namespace litho {
 
@@ -187,11 +188,19 @@ __global__ void k_wide_reduce(const int32_t* __restrict__ out_items, const float
 }
 
 // Image band box B(g) = F(g mod L), |g| <= 2h (F already scaled by 1/L^2).
-__global__ void k_wide_box(const float2* __restrict__ F, int L, int h, float2* __restrict__ bbox) {
+// transposed: F is the transform of J^T (the work queue's pass B stores the
+// partials column by column), so B(gx, gy) = F(gy, gx).
+__global__ void k_wide_box(const float2* __restrict__ F, int L, int h, float2* __restrict__ bbox,
+                           int transposed) {
   const int o = blockIdx.y, G = 4 * h + 1, g0 = 2 * h;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G * G; i += gridDim.x * blockDim.x) {
-    const int gy = i / G - g0, gx = i % G - g0;
-    bbox[(size_t)o * G * G + i] = F[((size_t)o * L + (gy & (L - 1))) * L + (gx & (L - 1))];
+    int gy = (i / G - g0) & (L - 1), gx = (i % G - g0) & (L - 1);
+    if (transposed) {
+      const int t = gx;
+      gx = gy;
+      gy = t;
+    }
+    bbox[(size_t)o * G * G + i] = F[((size_t)o * L + gy) * L + gx];
   }
 }
 
@@ -534,16 +543,13 @@ __global__ void k_wide_adj_final(const float2* __restrict__ A, int h, float2* __
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-struct WideLayout {
-  int64_t status, twN, twL, u1, mb, table, T, partial, J, F, bbox, spec, blockmax, total;
-  int jobs_per_chunk;
-};
-
-WideLayout wide_layout(const LithoAbbePlan& p) {
+// t_bytes >= 0: the pass-A buffer T is that many bytes (the work queue's
+// ring of slots); < 0: chunks of jobs within kWideTBudget.
+WideLayout wide_layout(const LithoAbbePlan& p, int64_t t_bytes) {
   WideLayout l{};
   const int64_t Bm = 2 * p.bm + 1, side = 2 * p.h + 1, G = 4 * p.h + 1, L = p.L, NN = (int64_t)p.n * p.n;
   const int64_t per_job = (int64_t)p.ncomp_max * side * L * 8;
-  int64_t jc = kWideTBudget / per_job;
+  int64_t jc = (t_bytes >= 0 ? t_bytes : kWideTBudget) / per_job;
   if (jc < 1) jc = 1;
   if (jc > p.n_jobs) jc = p.n_jobs;
   l.jobs_per_chunk = (int)jc;
@@ -555,7 +561,7 @@ WideLayout wide_layout(const LithoAbbePlan& p) {
   l.u1 = off;       off = align16(off + (int64_t)p.n_clips * Bm * p.n * 8);
   l.mb = off;       off = align16(off + (int64_t)p.n_clips * Bm * Bm * 8);
   l.table = off;    off = align16(off + (int64_t)p.n_tab * p.ncomp_max * side * side * 8);
-  l.T = off;        off = align16(off + jc * per_job);
+  l.T = off;        off = align16(off + (t_bytes >= 0 ? t_bytes : jc * per_job));
   l.partial = off;  off = align16(off + (int64_t)p.n_items * L * L * 4);
   l.J = off;        off = align16(off + (int64_t)p.n_out * L * L * 4);
   l.F = off;        off = align16(off + (int64_t)p.n_out * L * L * 8);
@@ -574,75 +580,101 @@ bool wide_plan_ok(const LithoAbbePlan& p) {
 
 int64_t wide_workspace_bytes(const LithoAbbePlan& p) { return wide_layout(p).total; }
 
-int abbe_wide_run(const LithoAbbePlan& p, const void* blob, const void* table_in, const void* mask, float* image,
-                  float* peak, void* ws, cudaStream_t s, int num_sms, cudaEvent_t* ev) {
-  const WideLayout l = wide_layout(p);
+int wide_prepare(const LithoAbbePlan& p, const void* mask, void* ws, const WideLayout& l, cudaStream_t s,
+                 int num_sms) {
+  char* w = static_cast<char*>(ws);
+  int* status = reinterpret_cast<int*>(w + l.status);
+  float2* u1 = reinterpret_cast<float2*>(w + l.u1);
+  float2* mb = reinterpret_cast<float2*>(w + l.mb);
+  const int n = p.n, Bm = 2 * p.bm + 1;
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(status, 0, sizeof(int), s)) != cudaSuccess) return (int)e;
+  const float2* twN = twiddles_for(n, reinterpret_cast<float2*>(w + l.twN), s);
+  e = launch_row_band_dft(mask, p.mask_complex != 0, p.n_clips * n, n, n, p.bm, u1, 1.0f, twN, num_sms, s, status);
+  if (e != cudaSuccess) return (int)e;
+  e = launch_row_band_dft(u1, true, p.n_clips * Bm, Bm, n, p.bm, mb, 1.0f / ((float)n * (float)n), twN, num_sms, s,
+                          status);
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+// ev (optional): events recorded after the band box and after the synthesis
+static int wide_finish_ev(const LithoAbbePlan& p, const void* blob, float* image, float* peak, void* ws,
+                          const WideLayout& l, bool transposed, cudaStream_t s, cudaEvent_t* ev) {
   const char* b = static_cast<const char*>(blob);
-  const LithoJob* jobs = reinterpret_cast<const LithoJob*>(b + p.off_jobs);
-  const LithoItem* items = reinterpret_cast<const LithoItem*>(b + p.off_items);
   const int32_t* out_items = reinterpret_cast<const int32_t*>(b + p.off_out_items);
   const LithoNorm* norm = reinterpret_cast<const LithoNorm*>(b + p.off_norm);
   char* w = static_cast<char*>(ws);
-  int* status = reinterpret_cast<int*>(w + l.status);
-  float2* twN_own = reinterpret_cast<float2*>(w + l.twN);
-  float2* twL_own = reinterpret_cast<float2*>(w + l.twL);
-  float2* u1 = reinterpret_cast<float2*>(w + l.u1);
-  float2* mb = reinterpret_cast<float2*>(w + l.mb);
-  float2* table = table_in ? (float2*)table_in : reinterpret_cast<float2*>(w + l.table);
-  float2* T = reinterpret_cast<float2*>(w + l.T);
   float* partial = reinterpret_cast<float*>(w + l.partial);
   float* J = reinterpret_cast<float*>(w + l.J);
   float2* F = reinterpret_cast<float2*>(w + l.F);
   float2* bbox = reinterpret_cast<float2*>(w + l.bbox);
   float2* spec = reinterpret_cast<float2*>(w + l.spec);
   float* blockmax = reinterpret_cast<float*>(w + l.blockmax);
-  const int n = p.n, L = p.L, Bm = 2 * p.bm + 1, G = 4 * p.h + 1;
+  const int n = p.n, L = p.L, G = 4 * p.h + 1;
   const size_t NN = (size_t)n * n;
+  const float2* twN = twiddles_for(n, reinterpret_cast<float2*>(w + l.twN), s);
+  const float2* twL = twiddles_for(L, reinterpret_cast<float2*>(w + l.twL), s);
   cudaError_t e;
-  auto mark = [&](int i) { if (ev) cudaEventRecord(ev[i], s); };
-
-  mark(0);
-  if ((e = cudaMemsetAsync(status, 0, sizeof(int), s)) != cudaSuccess) return (int)e;
-  const float2* twN = twiddles_for(n, twN_own, s);
-  const float2* twL = twiddles_for(L, twL_own, s);
-  if (!table_in && (e = launch_pupil_table(p, blob, table, s)) != cudaSuccess) return (int)e;
+  const int LL = L * L;
+  dim3 gr((LL + 255) / 256 < 1024 ? (LL + 255) / 256 : 1024, p.n_out);
+  k_wide_reduce<<<gr, 256, 0, s>>>(out_items, partial, LL, J);
+  e = plain_fft2(J, true, F, p.n_out, L, -1, 1.0f, 1.0f / ((float)L * (float)L), twL, s);
+  if (e != cudaSuccess) return (int)e;
+  dim3 gx((G * G + 255) / 256, p.n_out);
+  k_wide_box<<<gx, 256, 0, s>>>(F, L, p.h, bbox, transposed ? 1 : 0);
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
-  mark(1);
-  e = launch_row_band_dft(mask, p.mask_complex != 0, p.n_clips * n, n, n, p.bm, u1, 1.0f, twN, num_sms, s, status);
-  if (e != cudaSuccess) return (int)e;
-  mark(2);
-  e = launch_row_band_dft(u1, true, p.n_clips * Bm, Bm, n, p.bm, mb, 1.0f / ((float)n * (float)n), twN, num_sms, s,
-                          status);
-  if (e != cudaSuccess) return (int)e;
-  mark(3);
-  // coarse passes, chunk by chunk of jobs
-  if ((e = cudaMemsetAsync(partial, 0, (size_t)p.n_items * L * L * 4, s)) != cudaSuccess) return (int)e;
-  for (int j0 = 0; j0 < p.n_jobs; j0 += l.jobs_per_chunk) {
-    const int nj = (p.n_jobs - j0) < l.jobs_per_chunk ? (p.n_jobs - j0) : l.jobs_per_chunk;
-    if ((e = launch_wide_passes(p, j0, nj, items, jobs, table, mb, twL, T, partial, s)) != cudaSuccess) return (int)e;
-  }
-  mark(4);
-  {
-    const int LL = L * L;
-    dim3 gr((LL + 255) / 256 < 1024 ? (LL + 255) / 256 : 1024, p.n_out);
-    k_wide_reduce<<<gr, 256, 0, s>>>(out_items, partial, LL, J);
-    e = plain_fft2(J, true, F, p.n_out, L, -1, 1.0f, 1.0f / ((float)L * (float)L), twL, s);
-    if (e != cudaSuccess) return (int)e;
-    dim3 gx((G * G + 255) / 256, p.n_out);
-    k_wide_box<<<gx, 256, 0, s>>>(F, L, p.h, bbox);
-    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
-  }
-  mark(5);
+  if (ev) cudaEventRecord(ev[0], s);
   for (int o0 = 0; o0 < p.n_out; o0 += 2 * kWideSpecPairs) {
     const int no = (p.n_out - o0) < 2 * kWideSpecPairs ? (p.n_out - o0) : 2 * kWideSpecPairs;
     const int pairs = (no + 1) / 2;
     e = wide_synth_pairs_w(bbox, o0, p.n_out, 2 * p.h, n, pairs, twN, norm, image, blockmax, spec, s);
     if (e != cudaSuccess) return (int)e;
   }
-  mark(6);
+  if (ev) cudaEventRecord(ev[1], s);
   dim3 gn((unsigned)((NN + 255) / 256 < 512 ? (NN + 255) / 256 : 512), p.n_out);
   k_normalise<<<gn, 256, 0, s>>>(blockmax, kWideMaxBlk, norm, n, image, peak, 0);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+int wide_finish(const LithoAbbePlan& p, const void* blob, float* image, float* peak, void* ws, const WideLayout& l,
+                bool transposed, cudaStream_t s) {
+  return wide_finish_ev(p, blob, image, peak, ws, l, transposed, s, nullptr);
+}
+
+int abbe_wide_run(const LithoAbbePlan& p, const void* blob, const void* table_in, const void* mask, float* image,
+                  float* peak, void* ws, cudaStream_t s, int num_sms, cudaEvent_t* ev) {
+  const WideLayout l = wide_layout(p);
+  const char* b = static_cast<const char*>(blob);
+  const LithoJob* jobs = reinterpret_cast<const LithoJob*>(b + p.off_jobs);
+  const LithoItem* items = reinterpret_cast<const LithoItem*>(b + p.off_items);
+  char* w = static_cast<char*>(ws);
+  float2* mb = reinterpret_cast<float2*>(w + l.mb);
+  float2* table = table_in ? (float2*)table_in : reinterpret_cast<float2*>(w + l.table);
+  float2* T = reinterpret_cast<float2*>(w + l.T);
+  float* partial = reinterpret_cast<float*>(w + l.partial);
+  const int L = p.L;
+  cudaError_t e;
+  auto mark = [&](int i) { if (ev) cudaEventRecord(ev[i], s); };
+
+  mark(0);
+  if (!table_in && (e = launch_pupil_table(p, blob, table, s)) != cudaSuccess) return (int)e;
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  mark(1);
+  int st = wide_prepare(p, mask, ws, l, s, num_sms);
+  if (st) return st;
+  mark(2);
+  mark(3);
+  // coarse passes, chunk by chunk of jobs
+  const float2* twL = twiddles_for(L, reinterpret_cast<float2*>(w + l.twL), s);
+  if ((e = cudaMemsetAsync(partial, 0, (size_t)p.n_items * L * L * 4, s)) != cudaSuccess) return (int)e;
+  for (int j0 = 0; j0 < p.n_jobs; j0 += l.jobs_per_chunk) {
+    const int nj = (p.n_jobs - j0) < l.jobs_per_chunk ? (p.n_jobs - j0) : l.jobs_per_chunk;
+    if ((e = launch_wide_passes(p, j0, nj, items, jobs, table, mb, twL, T, partial, s)) != cudaSuccess) return (int)e;
+  }
+  mark(4);
+  st = wide_finish_ev(p, blob, image, peak, ws, l, false, s, ev ? ev + 5 : nullptr);
+  if (st) return st;
   mark(7);
   return LITHO_OK;
 }
@@ -747,7 +779,7 @@ int wide_coarse_box(const LithoAbbePlan& p, const void* blob, const float2* tabl
                                                                                                  LL, J);
   e = plain_fft2(J, true, F, p.n_out, L, -1, 1.0f, 1.0f / ((float)L * (float)L), twL, s);
   if (e != cudaSuccess) return (int)e;
-  k_wide_box<<<dim3((G * G + 255) / 256, p.n_out), 256, 0, s>>>(F, L, p.h, bbox_out);
+  k_wide_box<<<dim3((G * G + 255) / 256, p.n_out), 256, 0, s>>>(F, L, p.h, bbox_out, 0);
   e = cudaGetLastError();
   return e == cudaSuccess ? LITHO_OK : (int)e;
 }

@@ -41,7 +41,9 @@ class AbbePipeline:
                             float(dose), bool(return_raw), self.complex)
         if not fused_supported(n, int(self.pd.plan.L)):
             raise NotImplementedError("the pipeline runs the band-limited engines only")
-        self.pd._blob_dev = torch.from_numpy(self.pd.blob).to(self.dev)
+        blob = getattr(self.pd, "_blob_dev", None)   # plans are cached and shared: keep an existing copy
+        if blob is None or blob.device != self.dev:
+            self.pd._blob_dev = torch.from_numpy(self.pd.blob).to(self.dev)
         self.table = pupil_table(self.pd, self.dev, nat.stream_ptr(torch, self.dev))
         nb = C.c_size_t(0)
         nat.check("litho_abbe_workspace", self.L.litho_abbe_workspace(C.byref(self.pd.plan), C.byref(nb)))

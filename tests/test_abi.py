@@ -28,8 +28,9 @@ def test_struct_sizes_match_the_python_layouts():
     out = (C.c_int32 * 16)()
     k = L.litho_abi_sizes(out, 16)
     sizes = list(out)[:k]
-    assert sizes[:6] == [nat.PUPIL_DTYPE.itemsize, nat.JOB_DTYPE.itemsize, nat.ITEM_DTYPE.itemsize,
-                         nat.NORM_DTYPE.itemsize, C.sizeof(nat.AbbePlan), nat.MIRROR_DTYPE.itemsize]
+    assert sizes[:8] == [nat.PUPIL_DTYPE.itemsize, nat.JOB_DTYPE.itemsize, nat.ITEM_DTYPE.itemsize,
+                         nat.NORM_DTYPE.itemsize, C.sizeof(nat.AbbePlan), nat.MIRROR_DTYPE.itemsize,
+                         C.sizeof(nat.UnevenGroup), nat.QUEUE_TASK_DTYPE.itemsize]
 
 
 def test_status_strings():

@@ -92,3 +92,94 @@ def test_uneven_ilt_groups_and_steps(lb):
     for _ in range(5):
         b.step(want_signed=False)
     assert float((b.theta[0] - u.theta()[0]).abs().max()) < 1e-5
+
+
+def test_work_queue_matches_the_per_group_launches(lb):
+    """The persistent work queue (one launch for the coherent passes of the
+    512^2, 1024^2 and 2048^2 groups; 256^2 on the on-chip grid) against the
+    per-group launch sequences and against one-clip-at-a-time imaging."""
+    import torch
+    from lithobat_b200.uneven import UnevenAbbe
+    o = _euv(lb)
+    sizes = [512, 256, 2048, 1024, 512, 1024]
+    clips = [torch.from_numpy(c).cuda() for c in _clips(11, sizes)]
+    q = UnevenAbbe(sizes, o, 2e-9, tune=False, graph=True, engine="queue")
+    assert q.queue is not None and q.queue.n_tasks > 0
+    got = [im.clone() for im in q(clips)]
+    q.check_status()
+    g = UnevenAbbe(sizes, o, 2e-9, tune=False, graph=False, engine="groups")
+    ref = g(clips)
+    torch.cuda.synchronize()
+    worst = max(float((a.double() - b.double()).abs().max() / b.double().abs().max()) for a, b in zip(got, ref))
+    print(f"PARITY uneven_queue_vs_groups {worst:.3e}")
+    assert worst <= 2e-6
+    for i in (0, 2):
+        gr = lb.GridConfig(n_pixels=sizes[i], pixel_size=2e-9)
+        r = lb.compute_aerial_image(clips[i].cpu().numpy().astype(np.float64), o, gr)
+        assert float(np.abs(got[i].double().cpu().numpy() - r).max() / np.abs(r).max()) <= TOL
+    # a second batch through the same graph
+    clips2 = [torch.from_numpy(c).cuda() for c in _clips(12, sizes)]
+    got2 = q(clips2)
+    ref2 = g(clips2)
+    torch.cuda.synchronize()
+    assert max(float((a.double() - b.double()).abs().max() / b.double().abs().max())
+               for a, b in zip(got2, ref2)) <= 2e-6
+
+
+def test_work_queue_wait_that_runs_out_is_reported(lb):
+    """A task list whose pass-B task waits for one signal more than its chunk
+    gives: with a short wait limit the wait gives up, the queue's status word
+    reads LITHO_E_TIMEOUT and the launch ends; the next run is clean and
+    matches the first. Nothing faults or hangs (every wait is bounded)."""
+    import ctypes as C
+    import torch
+    from lithobat_b200 import _native as nat
+    from lithobat_b200.uneven import UnevenAbbe
+    L = nat.lib()
+    o = _euv(lb)
+    sizes = [512, 512]
+    run = UnevenAbbe(sizes, o, 2e-9, tune=False, graph=False)
+    clips = [torch.from_numpy(c).cuda() for c in _clips(13, sizes)]
+    first = [im.clone() for im in run(clips)]
+    run.check_status()
+    qu = run.queue
+    bad = qu.tasks_host.copy()
+    kb = int(np.flatnonzero(bad["kind"] == 1)[0])
+    bad["wait_value"][kb] += 1
+    bad_dev = torch.from_numpy(bad.view(np.uint8).copy()).cuda()
+    s = nat.stream_ptr(torch)
+    nat.check("litho_set_wait_limit", L.litho_set_wait_limit(200000))
+    try:
+        nat.check("litho_uneven_run", L.litho_uneven_run(qu.arr, qu.n_groups, bad_dev.data_ptr(), qu.n_tasks,
+                                                         qu.n_counters, qu.ws.data_ptr(), qu.ws.numel(), s))
+        st = L.litho_uneven_status(qu.ws.data_ptr(), s)
+    finally:
+        nat.check("litho_set_wait_limit", L.litho_set_wait_limit(0))
+    assert st == 1000001   # LITHO_E_TIMEOUT
+    with pytest.raises(nat.LithoError):
+        run.check_status()
+    again = run(clips)
+    run.check_status()
+    assert L.litho_uneven_status(qu.ws.data_ptr(), s) == 0
+    for a, b in zip(first, again):
+        assert torch.equal(a, b)
+
+
+def test_tuned_sizes_persist_as_json(lb, tmp_path):
+    """The tuner searches each group once and writes its choice; a second
+    runner of the same batch reads it back instead of searching."""
+    import json
+    from lithobat_b200 import uneven
+    o = _euv(lb)
+    path = tmp_path / "tune.json"
+    sizes = [512, 512, 256]
+    uneven._TUNED.clear()
+    a = uneven.UnevenAbbe(sizes, o, 2e-9, tune=True, graph=False, tune_cache=path)
+    assert a.tuned[512]["source"] == "search" and a.tuned[512]["ms"]["candidates"] >= 5
+    data = json.loads(path.read_text())
+    assert any(k.endswith("|queue") and "n=512" in k for k in data)
+    assert any(k.endswith("|launches") and "n=256" in k for k in data)
+    uneven._TUNED.clear()
+    b = uneven.UnevenAbbe(sizes, o, 2e-9, tune=True, graph=False, tune_cache=path)
+    assert b.tuned[512]["source"] == "cache" and b.tuned[256]["source"] == "cache"
+    assert b.groups[1].tune == a.groups[1].tune
