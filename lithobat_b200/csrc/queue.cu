@@ -95,6 +95,7 @@ __device__ bool wait_counter(const int* ctr, int value) {
 }
 
 __device__ __forceinline__ float2 ldcg2(const float2* p) { return __ldcg(p); }
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
 // Pass A: U[t][ky][u] = sum_kx P(kx, ky) M(cx + kx, cy + ky) e^{+2 pi i kx u / L}
 // for the jobs [first, first + count) of the task's chunk; a warp takes LPW
@@ -115,6 +116,23 @@ __device__ void q_pass_a(const QGroup& G, const LithoQueueTask& t, const float2*
     if (c >= job.ncomp) continue;
     const float2* tp = G.table + ((size_t)job.tab * ncomp + c) * npts;
     const float2* m = G.mb + (size_t)job.clip * Bm * Bm;
+    if (u + kQWarps < units) {   // the next unit's pupil and mask rows towards L2
+      const int tc2 = (u + kQWarps) / groups_per_t, lg2 = u + kQWarps - tc2 * groups_per_t;
+      const int jl2 = div_ncomp(tc2, ncomp), c2 = tc2 - jl2 * ncomp;
+      const LithoJob j2 = G.jobs[t.first + jl2];
+      const float2* tp2 = G.table + ((size_t)j2.tab * ncomp + c2) * npts;
+      const float2* m2 = G.mb + (size_t)j2.clip * Bm * Bm;
+#pragma unroll
+      for (int l = 0; l < LPW; ++l) {
+        const int kyi = lg2 * LPW + l, my = j2.cy + (kyi - h) + G.bm;
+        if (kyi >= side || my < 0 || my >= Bm) continue;
+        for (int kx = lane * 8 - h; kx <= h; kx += 256) {   // one prefetch per 64-byte piece of the rows
+          prefetch_l2(tp2 + kyi * side + kx + h);
+          const int mx = j2.cx + kx + G.bm;
+          if (mx >= 0 && mx < Bm) prefetch_l2(m2 + (size_t)my * Bm + mx);
+        }
+      }
+    }
     float2 x[32];
 #pragma unroll
     for (int l = 0; l < LPW; ++l) {
@@ -153,38 +171,48 @@ __device__ void q_pass_b(const QGroup& G, const LithoQueueTask& t, const float2*
   const LithoItem it = G.items[t.first];
   const float2* Ts = G.T + (size_t)t.slot * G.slot_elems;
   float* J = Jw + lane;  // [s][lane]
+  const int jb = it.job_begin, nt = (it.job_end - jb) * ncomp;
+  // T rows of transform k of row block rb for this lane's registers
+  auto rows_of = [&](int rb, int k) -> const float2* {
+    return Ts + (size_t)((jb - t.base) * ncomp + k) * side * L + (rb * kQWarps + warp) * LPW;
+  };
   for (int rb = t.count; rb < t.count + t.rows; ++rb) {
     const int u0 = (rb * kQWarps + warp) * LPW;
 #pragma unroll
     for (int s = 0; s < 32; ++s) J[s * 32] = 0.f;
-    for (int jj = it.job_begin; jj < it.job_end; ++jj) {
-      const LithoJob job = G.jobs[jj];
+    for (int k = 0; k < nt; ++k) {
+      const int jl = div_ncomp(k, ncomp), c = k - jl * ncomp;
+      const LithoJob job = G.jobs[jb + jl];
+      if (c >= job.ncomp) continue;
       const float w = (float)job.weight;
-      for (int c = 0; c < job.ncomp; ++c) {
-        const float2* Tt = Ts + (size_t)((jj - t.base) * ncomp + c) * side * L + u0;
-        float2 x[32];
+      const float2* Tt = rows_of(rb, k);
+      // the next transform's rows (or the next row block's first) towards L2
+      // while this one is transformed
+      const bool more = k + 1 < nt || rb + 1 < t.count + t.rows;
+      const float2* Tn = k + 1 < nt ? rows_of(rb, k + 1) : rows_of(rb + 1, 0);
+      float2 x[32];
 #pragma unroll
-        for (int q = 0; q < R; ++q) {
-          const int i = lane + 32 * q;
-          const int ky = i <= h ? i : i - L;
-          const bool ok = i <= h || i >= L - h;
-          const float2* src = Tt + (size_t)(ky + h) * L;
-          if constexpr (LPW % 2 == 0) {
+      for (int q = 0; q < R; ++q) {
+        const int i = lane + 32 * q;
+        const int ky = i <= h ? i : i - L;
+        const bool ok = i <= h || i >= L - h;
+        const float2* src = Tt + (size_t)(ky + h) * L;
+        if constexpr (LPW % 2 == 0) {
 #pragma unroll
-            for (int l = 0; l < LPW; l += 2) {
-              float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-              if (ok) v = __ldcg(reinterpret_cast<const float4*>(src + l));
-              x[l * R + q] = make_float2(v.x, v.y);
-              x[(l + 1) * R + q] = make_float2(v.z, v.w);
-            }
-          } else {
-            x[q] = ok ? ldcg2(src) : make_float2(0.f, 0.f);
+          for (int l = 0; l < LPW; l += 2) {
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (ok) v = __ldcg(reinterpret_cast<const float4*>(src + l));
+            x[l * R + q] = make_float2(v.x, v.y);
+            x[(l + 1) * R + q] = make_float2(v.z, v.w);
           }
+        } else {
+          x[q] = ok ? ldcg2(src) : make_float2(0.f, 0.f);
         }
-        warp_fft_lines<L, +1>(x, tb, tw);
-#pragma unroll
-        for (int s = 0; s < 32; ++s) J[s * 32] = fmaf(w, cabs2(x[s]), J[s * 32]);
+        if (ok && more) prefetch_l2(Tn + (size_t)(ky + h) * L);
       }
+      warp_fft_lines<L, +1>(x, tb, tw);
+#pragma unroll
+      for (int s = 0; s < 32; ++s) J[s * 32] = fmaf(w, cabs2(x[s]), J[s * 32]);
     }
     float* pj = G.partial + ((size_t)t.first * L + u0 + lane / R) * L + lane % R;
 #pragma unroll
