@@ -562,6 +562,22 @@ int litho_ilt_image_objective(const void* image_box_dev, int n_fields, int n, in
                               unsigned int* counters_dev, double* cost_out_dev, long long* perr_out_dev,
                               void* workspace, size_t ws_bytes, cudaStream_t stream);
 
+/* litho_ilt_image_objective() without dJ/dfield: the band box of
+ * band_scale x dJ/dfield on |k| <= band_half, (2 band_half + 1)^2 complex
+ * per field (the sensitivity the adjoint needs, opc/ilt.py:_Objective
+ * :313-336 into socs_gradient :262-266), is formed from each row pair as
+ * the synthesis makes it, so dJ/dfield is neither stored nor read back. Same
+ * values as litho_ilt_image_objective() followed by litho_band_spectrum() on
+ * its dJ/dfield (same arithmetic in the same order). The workspace's first
+ * word is a status (LITHO_E_TIMEOUT if a bounded wait of the band transform
+ * gave up). counters: zero on entry, left at zero. */
+int litho_ilt_image_objective_band_workspace(int n_fields, int n, int g0, int band_half, size_t* bytes);
+int litho_ilt_image_objective_band(const void* image_box_dev, int n_fields, int n, int g0, const float* target_dev,
+                                   float scale, float level, float sign, float steepness_a, int band_half,
+                                   float band_scale, void* band_box_out_dev, unsigned int* counters_dev,
+                                   double* cost_out_dev, long long* perr_out_dev, void* workspace_dev,
+                                   size_t workspace_bytes, cudaStream_t stream);
+
 /* TV (periodic neighbours) and discreteness penalties (opc/ilt.py:339-357):
  * adds their gradients to grad_dev and their costs to cost_part_dev. */
 int litho_ilt_penalties(const float* mask_dev, int n_fields, int n, float w_tv, float w_disc,

@@ -155,6 +155,9 @@ def lib():
         "litho_ilt_objective": [vp, vp, i32, i32, f32, f32, f32, f32, vp, vp, vp, vp, i32, vp],
         "litho_ilt_image_objective_workspace": [i32, i32, i32, vp],
         "litho_ilt_image_objective": [vp, i32, i32, i32, vp, f32, f32, f32, f32, vp, vp, vp, vp, vp, sz, vp],
+        "litho_ilt_image_objective_band_workspace": [i32, i32, i32, i32, vp],
+        "litho_ilt_image_objective_band": [vp, i32, i32, i32, vp, f32, f32, f32, f32, i32, f32, vp, vp, vp, vp, vp,
+                                           sz, vp],
         "litho_ilt_objective_totals": [vp, vp, i32, i32, f32, f32, f32, f32, vp, vp, vp, vp, i32, vp, vp, vp,
                                        vp],
         "litho_ilt_penalties": [vp, i32, i32, f32, f32, vp, vp, i32, vp],

@@ -35,6 +35,9 @@ int synth_pairs_blocks(int n);
 bool synth_objective_ok(int n, int g0);
 cudaError_t launch_synth_objective(const float2* box, int g0, int n, int n_out, const float2* tw, float* blockmax,
                                    float2* cbuf, const SynthObj& obj, cudaStream_t s);
+bool synth_objective_band_ok(int n, int g0, int kb);
+cudaError_t launch_synth_objective_band(const float2* box, int g0, int n, int n_out, const float2* tw,
+                                        float* blockmax, float2* cbuf, const SynthObj& obj, cudaStream_t s);
 bool wide_adjoint_ok(int h);
 int64_t wide_adjoint_ws(int n_clips, int h);
 int wide_socs_adjoint(const LithoAbbePlan& p, const void* blob, const float2* table, const float2* mask_box,
@@ -828,6 +831,61 @@ extern "C" int litho_ilt_image_objective(const void* image_box, int n_fields, in
                      cost_out, perr_out};
   const cudaError_t e = launch_synth_objective(static_cast<const float2*>(image_box), g0, n, n_fields, tw, blockmax,
                                                cbuf, obj, s);
+  return e == cudaSuccess ? LITHO_OK : (int)e;
+}
+
+// status word, then image_obj_ws, then the band rows [field][2 kb + 1][n]
+static int64_t image_obj_band_ws(int n_fields, int n, int g0, int kb) {
+  return 16 + image_obj_ws(n_fields, n, g0) + align16((int64_t)n_fields * (2 * kb + 1) * n * 8);
+}
+
+extern "C" int litho_ilt_image_objective_band_workspace(int n_fields, int n, int g0, int band_half, size_t* bytes) {
+  if (!bytes) return LITHO_E_NULL;
+  if (n_fields < 1 || n < 2 || g0 < 0 || band_half < 0) return LITHO_E_SIZE;
+  if (!synth_objective_band_ok(n, g0, band_half)) return LITHO_E_UNSUPPORTED;
+  *bytes = (size_t)image_obj_band_ws(n_fields, n, g0, band_half);
+  return LITHO_OK;
+}
+
+extern "C" int litho_ilt_image_objective_band(const void* image_box, int n_fields, int n, int g0, const float* target,
+                                              float scale, float level, float sign, float steepness_a, int band_half,
+                                              float band_scale, void* band_box_out, unsigned int* counters,
+                                              double* cost_out, long long* perr_out, void* ws, size_t ws_bytes,
+                                              cudaStream_t s) {
+  if (!image_box || !target || !band_box_out || !counters || !cost_out || !perr_out || !ws) return LITHO_E_NULL;
+  size_t need = 0;
+  const int st = litho_ilt_image_objective_band_workspace(n_fields, n, g0, band_half, &need);
+  if (st) return st;
+  if (ws_bytes < need) return LITHO_E_WORKSPACE;
+  if (((uintptr_t)ws | (uintptr_t)target) & 15) return LITHO_E_ALIGN;
+  const int64_t nb = (int64_t)n_fields * synth_pairs_blocks(n);
+  char* w = static_cast<char*>(ws);
+  int* status = reinterpret_cast<int*>(w);
+  w += 16;
+  float2* tw_own = reinterpret_cast<float2*>(w);
+  w += align16((int64_t)n * 8);
+  float* blockmax = reinterpret_cast<float*>(w);
+  w += align16(nb * 4);
+  double* cpart = reinterpret_cast<double*>(w);
+  w += align16(nb * 8);
+  unsigned int* ppart = reinterpret_cast<unsigned int*>(w);
+  w += align16(nb * 4);
+  float2* cbuf = reinterpret_cast<float2*>(w);
+  w += align16(synth_cols_bytes(n_fields, n, g0));
+  float2* u1 = reinterpret_cast<float2*>(w);
+  cudaError_t e = cudaMemsetAsync(status, 0, sizeof(int), s);
+  if (e != cudaSuccess) return (int)e;
+  const float2* tw = twiddles_for(n, tw_own, s);
+  const double npix = (double)n * n;
+  SynthObj obj{target, scale, level, sign, steepness_a, (float)(2.0 / npix), nullptr, cpart, ppart, counters,
+               cost_out, perr_out};
+  obj.band_rows = u1;
+  obj.band_half = band_half;
+  e = launch_synth_objective_band(static_cast<const float2*>(image_box), g0, n, n_fields, tw, blockmax, cbuf, obj, s);
+  if (e != cudaSuccess) return (int)e;
+  const int Bm = 2 * band_half + 1;
+  e = launch_row_band_dft(u1, true, n_fields * Bm, Bm, n, band_half, static_cast<float2*>(band_box_out), band_scale,
+                          tw, sms_here(), s, status);
   return e == cudaSuccess ? LITHO_OK : (int)e;
 }
 

@@ -40,6 +40,10 @@ struct SynthObj {
   unsigned int* counters;  // [field], zero between calls
   double* cost_out;        // [field]: sum / npix
   long long* perr_out;
+  // the band form (no dfield): the band rows of dJ/dfield on |k| <= band_half,
+  // [field][k + band_half][row], are written instead of dJ/dfield itself
+  float2* band_rows = nullptr;
+  int band_half = 0;
 };
 
 }  // namespace litho

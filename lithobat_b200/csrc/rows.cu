@@ -57,6 +57,14 @@ __host__ __device__ inline SynthSmem synth_smem(int n, int g0, bool cols_ahead =
 // rounded up to 128 bytes (its 16-byte copies need aligned destinations; the
 // operands end with the G x G box, an odd multiple of 8 bytes for odd G).
 __host__ __device__ inline size_t obj_stage_off(const SynthSmem& s) { return (s.total + 127) & ~(size_t)127; }
+// Floats of one warp's stage in the band form: the 2 P target rows, or the
+// band DFT's transpose of P row pairs (P x 32 x (M + 1) complex), whichever
+// is larger, in 128-byte units.
+__host__ __device__ inline int band_stage_floats(int M, int P) {
+  const int y = P * 32 * (M + 1) * 2;
+  const int f = y > kSyObjStage ? y : kSyObjStage;
+  return (f + 31) & ~31;
+}
 
 // Is the pair-FFT synthesis available for this grid and box?
 bool synth_pairs_ok(int n, int g0) {
@@ -117,12 +125,18 @@ k_synth_cols(const float2* __restrict__ Bbox, int g0, int n, const float2* __res
 // shared memory while the row pair's transform runs), dJ/dfield is stored in
 // obj.dfield, and the block's cost and pattern-error sums go to the partial
 // arrays, which the last block of each output totals (as k_ilt_objective).
-template <int PASS, bool OBJ = false>
+// BAND (with OBJ): dJ/dfield is not stored either; the row pair's values go
+// through the forward band DFT of its rows (the first pass of
+// litho_band_spectrum, same arithmetic: a 32-point FFT per residue, the
+// per-pass twiddle table and the transpose-sum in the warp's stage buffer)
+// and only the band rows obj.band_rows[o][k + kb][row], |k| <= kb, are written.
+template <int PASS, bool OBJ = false, bool BAND = false>
 __global__ void __launch_bounds__(kSyWarps * 32, 2)
 k_synth_pairs(const float2* __restrict__ Bbox, int g0, int n, const float2* __restrict__ tw_inv,
               const LithoNorm* __restrict__ norm, const float* __restrict__ peak, float* __restrict__ image,
               float* __restrict__ blockmax, const float2* __restrict__ Cg, SynthObj obj = SynthObj{}) {
   static_assert(!OBJ || PASS == 1, "the objective runs in the writing pass");
+  static_assert(!BAND || OBJ, "the band form is a form of the objective pass");
   extern __shared__ __align__(16) unsigned char sy_raw[];
   const SynthSmem L = synth_smem(n, g0, Cg != nullptr);
   const int o = blockIdx.y, y0 = blockIdx.x * kSyRows;
@@ -176,8 +190,21 @@ k_synth_pairs(const float2* __restrict__ Bbox, int g0, int n, const float2* __re
   float mx = 0.f;
   double ocost = 0.0;
   unsigned int operr = 0;
-  // OBJ: this warp's 2 P target rows (2048 contiguous values for n <= 1024)
-  float* tg = reinterpret_cast<float*>(sy_raw + obj_stage_off(L)) + warp * kSyObjStage;
+  // OBJ: this warp's 2 P target rows (2048 contiguous values for n <= 1024);
+  // BAND: the same buffer then holds the band DFT's transpose
+  const int stage_f = BAND ? band_stage_floats(M, L.P) : kSyObjStage;
+  float* tg = reinterpret_cast<float*>(sy_raw + obj_stage_off(L)) + warp * stage_f;
+  const int kb = obj.band_half, Bmb = 2 * kb + 1, npass = (Bmb + 31) >> 5;
+  float2* BTB = reinterpret_cast<float2*>(sy_raw + obj_stage_off(L) + (size_t)kSyWarps * stage_f * 4);
+  float2* Zw = BTB + (size_t)npass * 32 * M + (size_t)warp * L.P * npass * 32;   // [pair group][k + kb]
+  if (BAND) {   // the forward band twiddles w^(-k b) per (pass, register kp, residue b), 0 off the band
+    for (int j = threadIdx.x; j < npass * 32 * M; j += blockDim.x) {
+      const int p = j / (32 * M), kp = (j / M) & 31, b = j % M;
+      const int k = -kb + ((kp + kb) & 31) + 32 * p;
+      BTB[j] = k <= kb ? tw_inv[(-k * b) & nmask] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+  }
   for (int it = 0; it < iters; ++it) {
     const int pair = (it * kSyWarps + warp) * L.P + pg;
     if (OBJ) {
@@ -222,13 +249,56 @@ k_synth_pairs(const float2* __restrict__ Bbox, int g0, int n, const float2* __re
 #pragma unroll
         for (int a = 0; a < 32; ++a) {
           const float ta = t1[M * a], tb = t1[n + M * a];
-          __stcs(d1 + M * a, ilt_objective_pixel(Q[a].x * sc, ta, obj.scale, obj.level, obj.sign, obj.a,
-                                                 obj.inv_npix2, cc, operr, &sg));
-          __stcs(d1 + n + M * a, ilt_objective_pixel(Q[a].y * sc, tb, obj.scale, obj.level, obj.sign, obj.a,
-                                                     obj.inv_npix2, cc, operr, &sg));
+          const float da = ilt_objective_pixel(Q[a].x * sc, ta, obj.scale, obj.level, obj.sign, obj.a,
+                                               obj.inv_npix2, cc, operr, &sg);
+          const float db = ilt_objective_pixel(Q[a].y * sc, tb, obj.scale, obj.level, obj.sign, obj.a,
+                                               obj.inv_npix2, cc, operr, &sg);
+          if (BAND) {
+            Q[a] = make_float2(da, db);
+          } else {
+            __stcs(d1 + M * a, da);
+            __stcs(d1 + n + M * a, db);
+          }
         }
         ocost += (double)cc;
         __syncwarp();  // every lane is done with the stage before the next copy into it
+        if (BAND) {
+          // rows y1 + i y2 of this pair group: X_b(kp) over a, then per pass
+          // the transpose-sum U(k) = sum_b w^(-k b) X_b(k mod 32)
+          fft_reg<32, -1>(Q);
+          float2* Y = reinterpret_cast<float2*>(tg);     // [pair group][kp][b], pitch M + 1
+          const int LD = M + 1;
+          for (int p = 0; p < npass; ++p) {
+            float2* yr = Y + pg * 32 * LD + b;
+            const float2* tb = BTB + p * 32 * M + b;
+#pragma unroll
+            for (int kp = 0; kp < 32; ++kp) yr[kp * LD] = cmul(Q[kp], tb[kp * M]);
+            __syncwarp();
+            const int k = -kb + ((lane + kb) & 31) + 32 * p;
+            for (int r = 0; r < L.P; ++r) {
+              const float2* yq = Y + (r * 32 + lane) * LD;
+              float2 s0 = make_float2(0.f, 0.f), s1 = make_float2(0.f, 0.f);
+              for (int j = 0; j + 1 < M; j += 2) {
+                s0 = cadd(s0, yq[j]);
+                s1 = cadd(s1, yq[j + 1]);
+              }
+              if (M & 1) s0 = cadd(s0, yq[M - 1]);
+              if (k <= kb) Zw[r * npass * 32 + (k + kb)] = cadd(s0, s1);
+            }
+            __syncwarp();
+          }
+          for (int r = 0; r < L.P; ++r) {   // separate the two real rows of each pair: R1 = (Z + Z*(-k)) / 2, ...
+            const int ra = y0 + 2 * ((it * kSyWarps + warp) * L.P + r);
+            const float2* zr = Zw + r * npass * 32;
+            for (int kk = lane; kk < Bmb; kk += 32) {
+              const float2 z = zr[kk], zm = zr[Bmb - 1 - kk];
+              float2* dst = obj.band_rows + ((size_t)o * Bmb + kk) * n + ra;
+              dst[0] = make_float2((z.x + zm.x) * 0.5f, (z.y - zm.y) * 0.5f);
+              dst[1] = make_float2((z.y + zm.y) * 0.5f, (zm.x - z.x) * 0.5f);
+            }
+          }
+          __syncwarp();  // the stage and Z are free before the next copy into them
+        }
       } else if (PASS == 1) {
 #pragma unroll
         for (int a = 0; a < 32; ++a) {
@@ -365,6 +435,35 @@ cudaError_t launch_synth_objective(const float2* box, int g0, int n, int n_out, 
   cudaFuncSetAttribute(k_synth_pairs<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   k_synth_pairs<1, true><<<grid, kSyWarps * 32, sm, s>>>(box, g0, n, tw, nullptr, nullptr, nullptr, blockmax, cbuf,
                                                          obj);
+  return cudaGetLastError();
+}
+
+// Shared memory of the band form: the objective's (with the larger stage),
+// the forward band twiddles and each warp's band values.
+size_t synth_objective_band_smem(int n, int g0, int kb) {
+  const SynthSmem L = synth_smem(n, g0, true);
+  const int npass = (2 * kb + 1 + 31) >> 5;
+  return obj_stage_off(L) + (size_t)kSyWarps * band_stage_floats(L.M, L.P) * 4 + (size_t)npass * 32 * L.M * 8 +
+         (size_t)kSyWarps * L.P * npass * 32 * 8;
+}
+
+bool synth_objective_band_ok(int n, int g0, int kb) {
+  return synth_objective_ok(n, g0) && kb >= 0 && 2 * kb + 1 <= n && synth_objective_band_smem(n, g0, kb) <= 110 * 1024;
+}
+
+// launch_synth_objective with the band rows of dJ/dfield (obj.band_rows,
+// obj.band_half) written instead of dJ/dfield.
+cudaError_t launch_synth_objective_band(const float2* box, int g0, int n, int n_out, const float2* tw,
+                                        float* blockmax, float2* cbuf, const SynthObj& obj, cudaStream_t s) {
+  const dim3 grid(n / kSyRows, n_out);
+  const size_t smc = (size_t)(g0 + 1) * (n >> 5) * 8;
+  k_synth_cols<<<dim3((g0 + 1 + kColWarps - 1) / kColWarps, n_out), kColWarps * 32, smc, s>>>(box, g0, n, tw, cbuf);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const size_t sm = synth_objective_band_smem(n, g0, obj.band_half);
+  cudaFuncSetAttribute(k_synth_pairs<1, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_synth_pairs<1, true, true><<<grid, kSyWarps * 32, sm, s>>>(box, g0, n, tw, nullptr, nullptr, nullptr, blockmax,
+                                                               cbuf, obj);
   return cudaGetLastError();
 }
 

@@ -185,7 +185,9 @@ k_tcc_image(const float2* __restrict__ T2, const int32_t* __restrict__ rows, con
   }
   cp_async_wait_all();
   __syncthreads();
-  for (int q = blockIdx.x * kTccWarps + warp; q < Gh; q += gridDim.x * kTccWarps) {
+  // positions interleaved over the blocks (q = block + grid x warp): the term
+  // count falls off with |g|, so each block gets near and far shifts alike
+  for (int q = blockIdx.x + gridDim.x * warp; q < Gh; q += gridDim.x * kTccWarps) {
     const int p = pc + q, gy = p / G - 2 * h, gx = p % G - 2 * h;
     // rows fy with fy and fy + gy both in [-h, h]; at most side <= 32 of them
     const int fy_lo = gy > 0 ? -h : -h - gy, fy_hi = gy > 0 ? h - gy : h;
@@ -213,13 +215,13 @@ k_tcc_image(const float2* __restrict__ T2, const int32_t* __restrict__ rows, con
 #pragma unroll
     for (int c = 0; c < kImgClips; ++c) acc[c] = make_float2(0.f, 0.f);
     const float2* trow = T2 + (size_t)q * nb;
+    // the run holding term k: the last r with w_start[r] <= k (runs are at
+    // most 2h + 1 <= 31 terms long and k steps by 32, so r moves on by a few
+    // runs per step; the scan starts where the lane's previous term was)
+    int r = 0;
 #pragma unroll 2
     for (int k = lane; k < total; k += 32) {
-      // the run holding term k: the last r with w_start[r] <= k
-      int r = 0;
-#pragma unroll
-      for (int step = 16; step > 0; step >>= 1)
-        if (w_start[r + step] <= k) r += step;
+      while (r < 31 && w_start[r + 1] <= k) ++r;
       const int fy = fy_lo + r, fx = w_fx[r] + (k - w_start[r]);
       const int a = fy + h, b = a + gy;
       const int s = r_lo[a] + fx - r_x0[a];            // sorted index of f
@@ -259,8 +261,12 @@ k_tcc_adjoint(const float2* __restrict__ T, const int32_t* __restrict__ map, con
   const int c0 = blockIdx.y * kAdjClips, nc = min(kAdjClips, n_clips - c0);
   float2* Gs = tcc_sm;                                   // [c][G^2]
   float2* Ms = Gs + (size_t)kAdjClips * GG;              // [c][box position]
-  int* s_kx = reinterpret_cast<int*>(Ms + (size_t)kAdjClips * npts);
-  int* s_ky = s_kx + nb;
+  // per band point f': uy G + ux (the sensitivity offset) and its mask box
+  // position, (ux, uy) clamped to the box so every index stays inside the
+  // staged boxes even for a blob whose index build failed (then the build's
+  // status word reports it)
+  int* s_off = reinterpret_cast<int*>(Ms + (size_t)kAdjClips * npts);
+  int* s_pm = s_off + nb;
   // the clips' sensitivity and mask boxes (contiguous) copied in without
   // waiting per element
   const float2* gsrc = gbox + (size_t)c0 * GG;
@@ -269,8 +275,9 @@ k_tcc_adjoint(const float2* __restrict__ T, const int32_t* __restrict__ map, con
   for (int i = threadIdx.x; i < nc * npts; i += blockDim.x) cp_async8(Ms + i, msrc + i);
   cp_async_commit();
   for (int s = threadIdx.x; s < nb; s += blockDim.x) {
-    s_kx[s] = skx[s];
-    s_ky[s] = sky[s];
+    const int ux = min(max(skx[s], -h), h), uy = min(max(sky[s], -h), h);
+    s_off[s] = uy * G + ux;
+    s_pm[s] = (uy + h) * side + ux + h;
   }
   // positions of the output box off the band are zero
   for (int pp = blockIdx.x * blockDim.x + threadIdx.x; pp < npts; pp += gridDim.x * blockDim.x)
@@ -281,21 +288,19 @@ k_tcc_adjoint(const float2* __restrict__ T, const int32_t* __restrict__ map, con
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int s = blockIdx.x * kTccWarps + warp, sn = nb - 1 - s;   // f and -f
   if (s > sn) return;
-  const int fx = s_kx[s], fy = s_ky[s];
+  const int fx = skx[s], fy = sky[s];
   if (fx < -h || fx > h || fy < -h || fy > h) return;   // only a blob whose index build failed
   const float2* t1 = T + (size_t)s * nb;
   const float2* t2 = T + (size_t)sn * nb;
   float2 a1[kAdjClips], a2[kAdjClips];
 #pragma unroll
   for (int c = 0; c < kAdjClips; ++c) a1[c] = a2[c] = make_float2(0.f, 0.f);
-#pragma unroll 4
+  const int base1 = (fy + 2 * h) * G + (fx + 2 * h), base2 = (-fy + 2 * h) * G + (-fx + 2 * h);
+#pragma unroll 8
   for (int j = lane; j < nb; j += 32) {
-    const int ux = s_kx[j], uy = s_ky[j];
-    if (ux < -h || ux > h || uy < -h || uy > h) continue;
-    const int d1 = (fy - uy + 2 * h) * G + (fx - ux + 2 * h);    // f - f'
-    const int d2 = (-fy - uy + 2 * h) * G + (-fx - ux + 2 * h);  // -f - f'
+    const int off = s_off[j], pm = s_pm[j];                       // pm: box position of f'
+    const int d1 = base1 - off, d2 = base2 - off;                 // f - f', -f - f'
     const float2 w1 = __ldg(t1 + j), w2 = __ldg(t2 + j);
-    const int pm = (uy + h) * side + ux + h;                      // box position of f'
 #pragma unroll
     for (int c = 0; c < kAdjClips; ++c) {
       const float2 m = Ms[c * npts + pm];

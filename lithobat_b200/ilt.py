@@ -124,7 +124,7 @@ class _Stages:
     # workspaces whose first word is a device status (litho_band_spectrum,
     # litho_band_synthesis: LITHO_E_TIMEOUT when a bounded wait gave up); one
     # per call site of a step, so a step's every call keeps its own word
-    STATUS_TAGS = ("band_mask", "band", "synth")
+    STATUS_TAGS = ("band_mask", "band", "synth", "imgobj_band")
 
     def check_status(self) -> None:
         """Synchronise and raise ``LithoError`` if a bounded wait inside the
@@ -223,6 +223,21 @@ class _Stages:
             self._obj_counters = torch.zeros((self.C,), dtype=torch.int32, device=self.dev)
         cost = out_cost if out_cost is not None else torch.empty((self.C,), dtype=torch.float64, device=self.dev)
         perr = out_perr if out_perr is not None else torch.empty((self.C,), dtype=torch.int64, device=self.dev)
+        if not want_signed and self.image_objective_band_ok() and target.data_ptr() % 16 == 0:
+            # the image is synthesised straight into the objective and dJ/dI
+            # straight into its band rows (neither is stored)
+            nb = C.c_size_t(0)
+            nat.check("litho_ilt_image_objective_band_workspace", L.litho_ilt_image_objective_band_workspace(
+                self.C, self.n, 2 * self.h, 2 * self.h, C.byref(nb)))
+            ws = self.ws("imgobj_band", nb.value)
+            G = 4 * self.h + 1
+            gbox = torch.empty((self.C, G * G), dtype=torch.complex64, device=self.dev)
+            nat.check("litho_ilt_image_objective_band", L.litho_ilt_image_objective_band(
+                ibox.data_ptr(), self.C, self.n, 2 * self.h, target.data_ptr(), float(scale), float(level),
+                float(sign), float(a), 2 * self.h, float(scale) / (self.n * self.n), gbox.data_ptr(),
+                self._obj_counters.data_ptr(), cost.data_ptr(), perr.data_ptr(), ws.data_ptr(), ws.numel(),
+                self.stream()))
+            return cost, gbox, None, perr
         if not want_signed and self.image_objective_ok() and target.data_ptr() % 16 == 0:
             # the image is synthesised straight into the objective (never stored)
             nb = C.c_size_t(0)
@@ -247,6 +262,16 @@ class _Stages:
             N_PART, self._obj_counters.data_ptr(), cost.data_ptr(), perr.data_ptr(), self.stream()))
         gbox = self.band(dfield, 2 * self.h, float(scale) / (self.n * self.n))
         return cost, gbox, signed, perr
+
+    def image_objective_band_ok(self) -> bool:
+        """Whether litho_ilt_image_objective_band serves this grid and band."""
+        if getattr(self, "_imgobj_band_ok", None) is None:
+            nb = C.c_size_t(0)
+            st = self.L.litho_ilt_image_objective_band_workspace(self.C, self.n, 2 * self.h, 2 * self.h, C.byref(nb))
+            if st not in (0, nat.LITHO_E_UNSUPPORTED):
+                nat.check("litho_ilt_image_objective_band_workspace", st)
+            self._imgobj_band_ok = st == 0
+        return self._imgobj_band_ok
 
     def image_objective_ok(self) -> bool:
         """Whether litho_ilt_image_objective serves this grid and band."""

@@ -275,6 +275,59 @@ def test_image_objective_matches_synthesis_then_objective(lb):
         np.testing.assert_allclose(c1.cpu().numpy(), c0.cpu().numpy(), rtol=1e-6)
 
 
+def test_image_objective_band_form_matches_objective_then_band_spectrum(lb):
+    """litho_ilt_image_objective_band (dJ/dfield taken to its band rows inside
+    the synthesis, never stored) against litho_ilt_image_objective followed
+    by litho_band_spectrum of its dJ/dfield: the same arithmetic in the same
+    order, so the band boxes, costs and pattern errors are identical (P = 4,
+    2, 1 row pairs per warp at 256^2, 512^2, 1024^2)."""
+    import ctypes as C
+    import torch
+    from lithobat_b200 import _native as nat
+    from lithobat_b200 import ilt
+    from lithobat_b200.patterns import manhattan_clip
+    o = lb.OpticsConfig(wavelength=193e-9, NA=1.35, n_immersion=1.44, source_type="annular", sigma_inner=0.5,
+                        sigma_outer=0.8, source_grid=11, normalisation="clear")
+    for n, F, px in ((256, 3, 2e-9), (512, 2, 1e-9), (1024, 3, 1e-9)):
+        g = lb.GridConfig(n_pixels=n, pixel_size=px)
+        k = lb.SOCSKernels.build(o, g, tol=0.0, max_kernels=8)
+        st = ilt.stages(k, F, "fused")
+        assert st.image_objective_band_ok()
+        rng = np.random.default_rng(n + 1)
+        tg = np.stack([manhattan_clip(rng, n, g.pixel_size, n_rect=(4, 8), width_nm=(40, 120)) for _ in range(F)])
+        target = torch.from_numpy(tg.astype(np.float32)).to(st.dev)
+        mask = torch.from_numpy(rng.random((F, n, n)).astype(np.float32)).to(st.dev)
+        ibox = st.image_box(st.mask_box(mask))
+        scale, level, sign, a = 1.0 / k.clear, 0.3, 1.0, 50.0
+        g0 = kb = 2 * st.h
+        ctr = torch.zeros((F,), dtype=torch.int32, device=st.dev)
+        nb = C.c_size_t(0)
+        nat.check("ws", st.L.litho_ilt_image_objective_workspace(F, n, g0, C.byref(nb)))
+        ws0 = torch.empty(nb.value, dtype=torch.uint8, device=st.dev)
+        d0 = torch.empty((F, n, n), dtype=torch.float32, device=st.dev)
+        c0 = torch.empty((F,), dtype=torch.float64, device=st.dev)
+        p0 = torch.empty((F,), dtype=torch.int64, device=st.dev)
+        nat.check("imgobj", st.L.litho_ilt_image_objective(
+            ibox.data_ptr(), F, n, g0, target.data_ptr(), scale, level, sign, a, d0.data_ptr(), ctr.data_ptr(),
+            c0.data_ptr(), p0.data_ptr(), ws0.data_ptr(), ws0.numel(), st.stream()))
+        box0 = st.band(d0, kb, scale / (n * n))
+        nat.check("ws", st.L.litho_ilt_image_objective_band_workspace(F, n, g0, kb, C.byref(nb)))
+        ws1 = torch.empty(nb.value, dtype=torch.uint8, device=st.dev)
+        G = 2 * kb + 1
+        box1 = torch.empty((F, G * G), dtype=torch.complex64, device=st.dev)
+        c1 = torch.empty_like(c0)
+        p1 = torch.empty_like(p0)
+        for _ in range(2):   # counters are left at zero for the next call
+            nat.check("imgobj_band", st.L.litho_ilt_image_objective_band(
+                ibox.data_ptr(), F, n, g0, target.data_ptr(), scale, level, sign, a, kb, scale / (n * n),
+                box1.data_ptr(), ctr.data_ptr(), c1.data_ptr(), p1.data_ptr(), ws1.data_ptr(), ws1.numel(),
+                st.stream()))
+        torch.cuda.synchronize()
+        assert int(ws1[:4].view(torch.int32).item()) == 0
+        assert torch.equal(box0, box1), float((box0 - box1).abs().max() / box0.abs().max())
+        assert torch.equal(c0, c1) and torch.equal(p0, p1) and int(ctr.abs().sum()) == 0
+
+
 @pytest.mark.parametrize("lanes", [2, 3])
 def test_graph_lanes_give_the_iterates_of_eager_steps(lb, lanes):
     """The graph-replayed step split into clip lanes on parallel graph
