@@ -152,21 +152,20 @@ def bench_ilt(args, torch, dev, world, max_over_ranks, barrier) -> dict:
         ev[2].record()
         mbox = st.mask_box(mk)
         ev[3].record()
-        raw = st.image(mbox)
+        ibox = st.image_box(mbox)
         ev[4].record()
-        dfield = torch.empty_like(raw)
-        nat_.check("obj", st.L.litho_ilt_objective(raw.data_ptr(), b.target.data_ptr(), nclip, N,
-                                                   float(params.scale), 0.3, 1.0, 50.0, dfield.data_ptr(), None,
-                                                   cpart.data_ptr(), ppart.data_ptr(), 64, st.stream()))
+        # the step's own objective call: synthesis + resist objective + the
+        # band of dJ/dI in one pass when the band form serves the grid
+        _c, gbox, _s, _p = st.objective_from_box(ibox, b.target, float(params.scale), 0.3, 1.0,
+                                                 float(params.steepness), want_signed=False)
         ev[5].record()
-        gbox = st.band(dfield, 2 * st.h, float(params.scale) / (N * N))
         ev[6].record()
         st.adjoint_box(gbox, mbox)
         ev[7].record()
         torch.cuda.synchronize()
         names = ["gradient_synthesis", "theta_grad+adam+mask", "mask_band_spectrum",
-                 "coarse_image_and_synthesis", "objective", "sensitivity_band_spectrum",
-                 "adjoint: dJ/dI on the 64 grid, per-kernel adjoint, gradient band box"]
+                 "image_band_box (band TCC)", "image synthesis + objective + dJ/dI band box",
+                 "(in the previous stage)", "adjoint: gradient band box (band TCC)"]
     else:
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(9)]
         ev[0].record()
@@ -242,10 +241,13 @@ def bench_ilt(args, torch, dev, world, max_over_ranks, barrier) -> dict:
     # algorithmic bytes of one fast step per clip pixel: gradient synthesis
     # writes g (4); the update reads g and theta, m1, m2 (16) and writes
     # theta, m1, m2 and the mask (16); the mask's band rows read it (4); the
-    # image objective reads the target and writes dJ/dI (8); dJ/dI's band rows
-    # read it (4). Band boxes and kernel tables are below 0.1 %.
+    # image objective reads the target (4) and, unless it forms dJ/dI's band
+    # rows itself (litho_ilt_image_objective_band), writes dJ/dI (4) for the
+    # band rows to read (4). Band boxes and kernel tables are below 0.1 %.
     ilt_bytes = {"gradient_write": 4, "update_read": 16, "update_write": 16, "mask_band_read": 4,
-                 "objective_target_read": 4, "objective_dJdI_write": 4, "sensitivity_band_read": 4}
+                 "objective_target_read": 4}
+    if not b.st.image_objective_band_ok():
+        ilt_bytes.update({"objective_dJdI_write": 4, "sensitivity_band_read": 4})
     per_px = sum(ilt_bytes.values())
     hbm = float(measured_peaks()["hbm_gbs"])
     ach = per_px * NN * nclip / (ms / args.steps / 1000.0) / 1e9
@@ -295,7 +297,7 @@ def bench_uneven(args, torch, dev, world, max_over_ranks, barrier) -> dict:
                                                       width_nm=(20.0, 80.0)).astype(np.float32)).to(dev)
              for n in sizes]
     t0 = time.perf_counter()
-    run = UnevenAbbe(sizes, o, 2e-9, tune=True, graph=True)
+    run = UnevenAbbe(sizes, o, 2e-9, tune=not args.no_tune, graph=True)
     setup_s = time.perf_counter() - t0
     run.load(masks)
     for _ in range(max(1, args.warmup)):
@@ -854,6 +856,8 @@ def main():
                                         "unevenilt")
     ap.add_argument("--ilt-clips", type=int, default=ILT_CLIPS, help="clips per ILT step")
     ap.add_argument("--uneven-clips", type=int, default=256, help="clips in the uneven-size batch")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="uneven batch with the library's default queue sizes (no search; for profiling)")
     args = ap.parse_args()
     args.skip = set(x for x in args.skip.split(",") if x)
     if "cpu" in args.skip:

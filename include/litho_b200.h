@@ -615,6 +615,30 @@ typedef struct LithoIltSched {
 int litho_ilt_update_sched(const float* g_dev, long long count, LithoIltSched* sched_dev, float step, float b1,
                            float b2, float eps, float* theta_dev, float* m1_dev, float* m2_dev, float* mask_dev,
                            cudaStream_t stream);
+/* One whole ILT iteration of n_clips clips in one call: the loop body of
+ * opc/ilt.py:run_ilt (:576-596 -- dJ/dtheta, Adam, the beta anneal, mask_of)
+ * and the objective with its adjoint (opc/ilt.py:_Objective :292-360 over
+ * socs_fields / socs_gradient :208-266), for kernel bands whose band TCC
+ * fits (litho_socs_tcc_bytes: h <= 15). The gradient is kept as its band
+ * box grad_box_dev ((2h+1)^2 complex per clip, read and replaced); the step
+ * synthesises it, runs litho_ilt_update_sched (sched_dev advanced, theta,
+ * m1, m2 and mask_out_dev written), forms the mask's band box, the image
+ * band box (litho_socs_tcc_image), the objective with the band box of dJ/dI
+ * (litho_ilt_image_objective_band: cost_out_dev, perr_out_dev) and the new
+ * gradient band box (litho_socs_tcc_adjoint). No blur, smoothing or
+ * penalties (the fast form). steepness_a = steepness / |level|. Stream-
+ * ordered, no host synchronisation, nothing allocated; the workspace is the
+ * caller's (litho_ilt_step_workspace). litho_ilt_step_status synchronises
+ * and returns the first non-zero status word of the last step (a bounded
+ * wait that gave up), else 0. */
+int litho_ilt_step_workspace(int n_clips, int n, int h, size_t* bytes);
+int litho_ilt_step(const void* tcc_dev, int n_band, int h, int n_clips, int n, const float* target_dev,
+                   float* theta_dev, float* m1_dev, float* m2_dev, LithoIltSched* sched_dev, void* grad_box_dev,
+                   float* mask_out_dev, float scale, float level, float sign, float steepness_a, float step,
+                   float b1, float b2, float eps, double* cost_out_dev, long long* perr_out_dev,
+                   void* workspace_dev, size_t workspace_bytes, cudaStream_t stream);
+int litho_ilt_step_status(int n_clips, int n, int h, const void* workspace_dev, cudaStream_t stream);
+
 /* One Adam step at iteration it >= 1 (opc/ilt.py:582-591), in place. */
 int litho_ilt_adam(const float* g_dev, long long count, float step, float b1, float b2, float eps,
                    int it, float* theta_dev, float* m1_dev, float* m2_dev, cudaStream_t stream);

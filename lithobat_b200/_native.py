@@ -156,6 +156,10 @@ def lib():
         "litho_ilt_image_objective_workspace": [i32, i32, i32, vp],
         "litho_ilt_image_objective": [vp, i32, i32, i32, vp, f32, f32, f32, f32, vp, vp, vp, vp, vp, sz, vp],
         "litho_ilt_image_objective_band_workspace": [i32, i32, i32, i32, vp],
+        "litho_ilt_step_workspace": [i32, i32, i32, C.POINTER(sz)],
+        "litho_ilt_step": [vp, i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, f32, f32, f32, f32, f32, f32, f32,
+                           f32, vp, vp, vp, sz, vp],
+        "litho_ilt_step_status": [i32, i32, i32, vp, vp],
         "litho_ilt_image_objective_band": [vp, i32, i32, i32, vp, f32, f32, f32, f32, i32, f32, vp, vp, vp, vp, vp,
                                            sz, vp],
         "litho_ilt_objective_totals": [vp, vp, i32, i32, f32, f32, f32, f32, vp, vp, vp, vp, i32, vp, vp, vp,

@@ -419,3 +419,66 @@ def test_band_tcc_boxes_equal_the_per_kernel_engines(lb, case):
     # engine is held to 1e-5 of the FP64 reference, so each other to 2e-5
     assert e_i <= 2e-6 and e_h <= 2e-6 and e_g <= 2e-5
     np.testing.assert_allclose(fa.cost.cpu().numpy(), fb.cost.cpu().numpy(), rtol=1e-5)
+
+
+def test_one_call_ilt_step_matches_the_graph_replayed_step(lb):
+    """litho_ilt_step (the whole fast iteration through the C ABI, one call
+    per step) against IltBatch's graph-replayed step from the same state:
+    theta, Adam moments, mask, gradient band box, cost and pattern error
+    identical after three steps."""
+    import ctypes as C
+    import torch
+    from lithobat_b200 import _native as nat
+    from lithobat_b200 import ilt
+    from lithobat_b200.patterns import manhattan_clip
+    o = lb.OpticsConfig(wavelength=193e-9, NA=1.35, n_immersion=1.44, source_type="annular", sigma_inner=0.5,
+                        sigma_outer=0.8, source_grid=11, normalisation="clear")
+    n, F = 256, 3
+    g = lb.GridConfig(n_pixels=n, pixel_size=2e-9)
+    k = lb.SOCSKernels.build(o, g, tol=0.0, max_kernels=12)
+    rng = np.random.default_rng(41)
+    tg = np.stack([manhattan_clip(rng, n, 2e-9, n_rect=(4, 8), width_nm=(40, 120)) for _ in range(F)])
+    th = (0.5 * rng.standard_normal((F, n, n))).astype(np.float32)
+    p = ilt.IltParams(scale=1.0 / k.clear, level=0.3, steepness=15.0, step=0.2, beta=4.0, growth=1.05)
+    b = ilt.IltBatch(k, torch.from_numpy(tg.astype(np.float32)).cuda(), torch.from_numpy(th).cuda(), p, lanes=1)
+    assert b.fast and b.st.tcc is not None
+    b.step(want_signed=False)
+    theta, m1, m2, hbox = b.theta.clone(), b.m1.clone(), b.m2.clone(), b.hbox.clone()
+    beta, it = b.beta, b.it
+    b.run(3)
+    torch.cuda.synchronize()
+    L = nat.lib()
+    st = b.st
+    sched = np.zeros(1, dtype=nat.ILT_SCHED_DTYPE)
+    sched["beta"] = sched["beta_next"] = beta
+    sched["growth"] = p.growth
+    sched["it"] = it
+    sched_dev = torch.from_numpy(sched.view(np.uint8).copy()).cuda()
+    nb = C.c_size_t(0)
+    nat.check("ws", L.litho_ilt_step_workspace(F, n, st.h, C.byref(nb)))
+    ws = torch.zeros(nb.value, dtype=torch.uint8, device="cuda")
+    mask = torch.empty_like(theta)
+    cost = torch.empty((F,), dtype=torch.float64, device="cuda")
+    perr = torch.empty((F,), dtype=torch.int64, device="cuda")
+    a = p.steepness / abs(p.level)
+    s = nat.stream_ptr(torch)
+    for _ in range(3):
+        nat.check("litho_ilt_step", L.litho_ilt_step(
+            st.tcc.data_ptr(), st.nb, st.h, F, n, b.target.data_ptr(), theta.data_ptr(), m1.data_ptr(),
+            m2.data_ptr(), sched_dev.data_ptr(), hbox.data_ptr(), mask.data_ptr(), float(p.scale), float(p.level),
+            float(p.sign), float(a), float(p.step), float(p.b1), float(p.b2), float(p.eps), cost.data_ptr(),
+            perr.data_ptr(), ws.data_ptr(), ws.numel(), s))
+    assert L.litho_ilt_step_status(F, n, st.h, ws.data_ptr(), s) == 0
+    torch.cuda.synchronize()
+    for got, ref in ((theta, b.theta), (m1, b.m1), (m2, b.m2), (mask, b.mask), (hbox, b.hbox)):
+        assert torch.equal(got, ref), float((got - ref).abs().max())
+    assert torch.equal(cost, b.cost) and torch.equal(perr, b.perr)
+    # arguments are checked before anything runs
+    assert L.litho_ilt_step(None, st.nb, st.h, F, n, b.target.data_ptr(), theta.data_ptr(), m1.data_ptr(),
+                            m2.data_ptr(), sched_dev.data_ptr(), hbox.data_ptr(), mask.data_ptr(), 1.0, 0.3, 1.0,
+                            50.0, 0.2, 0.9, 0.999, 1e-8, cost.data_ptr(), perr.data_ptr(), ws.data_ptr(),
+                            ws.numel(), s) == -1
+    assert L.litho_ilt_step(st.tcc.data_ptr(), st.nb, st.h, F, n, b.target.data_ptr(), theta.data_ptr(),
+                            m1.data_ptr(), m2.data_ptr(), sched_dev.data_ptr(), hbox.data_ptr(), mask.data_ptr(),
+                            1.0, 0.3, 1.0, 50.0, 0.2, 0.9, 0.999, 1e-8, cost.data_ptr(), perr.data_ptr(),
+                            ws.data_ptr(), 16, s) == -3
