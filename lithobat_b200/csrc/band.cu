@@ -381,7 +381,7 @@ k_band_rows_fft(const void* __restrict__ in, int n_rows, int rows_per_clip, int 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float2* tb = bf_sm + L + warp * 32 * kTbLd;
   float2* acc = bf_sm + L + kBfWarps * 32 * kTbLd + warp * 32 * 32;  // [s][lane]
-  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = tw_inv[SPLIT * i];
+  fill_lane_twiddles(tw, L, tw_inv, SPLIT);
   __syncthreads();
   const int Bm = 2 * bm + 1;
   const int lp = lane / R, rp = lane % R;

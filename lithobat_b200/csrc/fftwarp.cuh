@@ -15,7 +15,15 @@ namespace litho {
 
 constexpr int kTbLd = 33;  // row pitch of the per-warp transpose buffer (complex)
 
-// tb: this warp's 32 x kTbLd complex buffer; tw[j] = exp(+2 pi i j / L).
+// The shared twiddle table of warp_fft_lines in lane-major order:
+// t[r * 32 + p] = w^(p r), w = exp(+2 pi i / L), for lane p and register r <
+// R, so the 32 lanes of a warp read 32 consecutive entries (no bank
+// conflicts). src[stride * j] = exp(+2 pi i j / L); p r < L, so no index wraps.
+__device__ __forceinline__ void fill_lane_twiddles(float2* t, int L, const float2* __restrict__ src, int stride) {
+  for (int i = threadIdx.x; i < L; i += blockDim.x) t[i] = src[stride * ((i & 31) * (i >> 5))];
+}
+
+// tb: this warp's 32 x kTbLd complex buffer; tw: fill_lane_twiddles' table.
 template <int L, int SIGN>
 __device__ __forceinline__ void warp_fft_lines(float2 (&x)[32], float2* tb, const float2* tw) {
   constexpr int R = L / 32, LPW = 32 / R;
@@ -32,7 +40,7 @@ __device__ __forceinline__ void warp_fft_lines(float2 (&x)[32], float2* tb, cons
       if (r == 0) {
         x[l * R] = y[0];
       } else {
-        float2 w = tw[lane * r];  // lane * r < L
+        float2 w = tw[r * 32 + lane];  // w^(lane r)
         if (SIGN < 0) w.y = -w.y;
         x[l * R + r] = cmul(y[r], w);
       }

@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(kQWarps * 32, kQBlocksPerSm) k_uneven_queue(co
     if (s_ok) {
       const QGroup& G = P.g[t.group];
       if (t.group != tw_group) {
-        for (int i = threadIdx.x; i < G.L; i += blockDim.x) tw[i] = G.twL[i];
+        fill_lane_twiddles(tw, G.L, G.twL, 1);
         tw_group = t.group;
         __syncthreads();
       }

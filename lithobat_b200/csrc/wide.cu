@@ -66,7 +66,7 @@ k_wide_cols_w(const LithoJob* __restrict__ jobs, int j0, int ncomp_max, const fl
   const int tj = div_ncomp(t, ncomp_max), j = j0 + tj, c = t - tj * ncomp_max;
   const LithoJob job = jobs[j];
   if (c >= job.ncomp) return;
-  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twL[i];
+  fill_lane_twiddles(tw, L, twL, 1);
   __syncthreads();
   const int col0 = (blockIdx.y * kWfWarps + warp) * LPW;
   if (col0 >= side) return;
@@ -115,7 +115,7 @@ k_wide_rows_w(const LithoItem* __restrict__ items, const LithoJob* __restrict__ 
   const int jb = it.job_begin > j0 ? it.job_begin : j0;
   const int je = it.job_end < j0 + nj ? it.job_end : j0 + nj;
   if (jb >= je) return;
-  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twL[i];
+  fill_lane_twiddles(tw, L, twL, 1);
   __syncthreads();
   const int side = 2 * h + 1;
   const int v0 = (blockIdx.y * kWfWarps + warp) * LPW;
@@ -248,7 +248,7 @@ k_wsyn_cols(const float2* __restrict__ bbox, int o0, int n_out, int g0, const fl
   float2* tw = wsm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float2* tb = wsm + L + warp * 32 * kTbLd;
-  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twN[SPLIT * i];
+  fill_lane_twiddles(tw, L, twN, SPLIT);
   __syncthreads();
   const int pr = blockIdx.y, G = 2 * g0 + 1;
   const int c0 = (blockIdx.x * kWfWarps + warp) * LPW;
@@ -289,7 +289,7 @@ k_wsyn_rows(const float2* __restrict__ Cw, int o0, int n_out, int g0, const floa
   float2* tw = wsm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float2* tb = wsm + L + warp * 32 * kTbLd;
-  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twN[SPLIT * i];
+  fill_lane_twiddles(tw, L, twN, SPLIT);
   __syncthreads();
   const int pr = blockIdx.y, G = 2 * g0 + 1;
   const int oa = o0 + 2 * pr, ob = oa + 1;
@@ -405,7 +405,7 @@ k_wide_adj_rows_w(const LithoJob* __restrict__ jobs, int j0, int h, const float2
   float2* tw = wsm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float2* tb = wsm + L + warp * 32 * kTbLd;
-  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twL[i];
+  fill_lane_twiddles(tw, L, twL, 1);
   __syncthreads();
   const int t = blockIdx.x, side = 2 * h + 1;
   const int v0 = (blockIdx.y * kWfWarps + warp) * LPW;
@@ -458,7 +458,7 @@ k_wide_adj_cols_w(const LithoJob* __restrict__ jobs, int j0, const float2* __res
   float2* tw = wsm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float2* tb = wsm + L + warp * 32 * kTbLd;
-  for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = twL[i];
+  fill_lane_twiddles(tw, L, twL, 1);
   __syncthreads();
   const int t = blockIdx.x, side = 2 * h + 1, npts = side * side;
   const int c0 = (blockIdx.y * kWfWarps + warp) * LPW;
