@@ -519,13 +519,18 @@ static cudaError_t launch_wide_adjoint(int L, int j0, int nj, const LithoJob* jo
   }
 }
 
-// A[clip] += Yt[t] for the chunk's transforms, in job order.
+// A[clip] += Yt[t] for the chunk's transforms, in job order; each run of
+// consecutive jobs of one clip is summed in registers and stored once.
 __global__ void k_wide_adj_acc(const LithoJob* __restrict__ jobs, int j0, int nj, int npts,
                                const float2* __restrict__ Yt, float2* __restrict__ A) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += gridDim.x * blockDim.x) {
-    for (int t = 0; t < nj; ++t) {
+    int t = 0;
+    while (t < nj) {
       const int c = jobs[j0 + t].clip;
-      A[(size_t)c * npts + i] = cadd(A[(size_t)c * npts + i], Yt[(size_t)t * npts + i]);
+      float2 acc = A[(size_t)c * npts + i];
+#pragma unroll 4
+      for (; t < nj && jobs[j0 + t].clip == c; ++t) acc = cadd(acc, __ldcs(Yt + (size_t)t * npts + i));
+      A[(size_t)c * npts + i] = acc;
     }
   }
 }

@@ -434,6 +434,36 @@ class UnevenIlt:
                 cost[i] = c[j]
         return cost
 
+    def run(self, n_steps: int):
+        """``n_steps`` ILT iterations of every clip without the signed field;
+        returns the costs in batch order (device). Each group steps by
+        ``IltBatch.run`` (its fast step recorded once as a CUDA graph and
+        replayed), and the groups' replays go on parallel streams, so the
+        small groups' kernels overlap the large groups' passes. Groups are
+        independent, so the iterates are those of ``step()``."""
+        torch = self.torch
+        n_steps = int(n_steps)
+        if n_steps > 0 and any(b._graph is None for _n, _i, _k, b in self.groups):
+            for _n, _i, _k, b in self.groups:   # the first call records each group's graph (one step)
+                b.run(1)
+            n_steps -= 1
+        if n_steps > 0:
+            if getattr(self, "_streams", None) is None:
+                self._streams = [torch.cuda.Stream() for _ in self.groups]
+            main = torch.cuda.current_stream()
+            for s in self._streams:
+                s.wait_stream(main)
+            for (_n, _i, _k, b), s in zip(self.groups, self._streams):
+                with torch.cuda.stream(s):
+                    b.run(n_steps)
+            for s in self._streams:
+                main.wait_stream(s)
+        cost = [None] * len(self.sizes)
+        for _n, idx, _k, b in self.groups:
+            for j, i in enumerate(idx):
+                cost[i] = b.cost[j]
+        return cost
+
     def theta(self):
         out = [None] * len(self.sizes)
         for _n, idx, _k, b in self.groups:

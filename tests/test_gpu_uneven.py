@@ -183,3 +183,32 @@ def test_tuned_sizes_persist_as_json(lb, tmp_path):
     b = uneven.UnevenAbbe(sizes, o, 2e-9, tune=True, graph=False, tune_cache=path)
     assert b.tuned[512]["source"] == "cache" and b.tuned[256]["source"] == "cache"
     assert b.groups[1].tune == a.groups[1].tune
+
+
+def test_uneven_ilt_run_replays_groups_on_parallel_streams(lb):
+    """UnevenIlt.run: each group's step recorded as a CUDA graph and the
+    groups' replays on parallel streams give the iterates of eager steps."""
+    import torch
+    from lithobat_b200 import ilt
+    from lithobat_b200.source import Source
+    from lithobat_b200.uneven import UnevenIlt
+    o = lb.OpticsConfig(wavelength=13.5e-9, NA=0.33, source_grid=15, normalisation="clear",
+                        source_spec=Source.dipole(0.9, 0.6, opening_deg=60).to_dict())
+    sizes = [256, 128, 256, 128]
+    tg = _clips(17, sizes)
+    rng = np.random.default_rng(18)
+    th = [0.5 * rng.standard_normal((n, n)).astype(np.float32) for n in sizes]
+
+    def params(k):
+        return ilt.IltParams(scale=1.0 / k.clear, level=0.3, steepness=15.0, step=0.1, beta=4.0, growth=1.02)
+    a = UnevenIlt(tg, th, o, 2e-9, params, max_kernels=12)
+    b = UnevenIlt(tg, th, o, 2e-9, params, max_kernels=12)
+    for _ in range(4):
+        a.step()
+    cb = b.run(4)
+    torch.cuda.synchronize()
+    for ta, tb in zip(a.theta(), b.theta()):
+        assert float((ta - tb).abs().max()) < 1e-6
+    ca = [float(c) for c in a.step()]   # one more eager step of a against one more replay of b
+    cb = [float(c) for c in b.run(1)]
+    np.testing.assert_allclose(cb, ca, rtol=1e-6)
