@@ -7,10 +7,12 @@
 
 namespace litho {
 
-// sigmoid(s) with s clipped to [-60, 60] (opc/ilt.py:326, 378).
+// sigmoid(s) with s clipped to [-60, 60] (opc/ilt.py:326, 378). The
+// correctly rounded reciprocal (rcp.rn) is the IEEE quotient 1 / x itself,
+// without the general division's operand scaling and special-case path.
 __device__ __forceinline__ float sigmoid_clipped(float s) {
   s = fminf(fmaxf(s, -60.f), 60.f);
-  return 1.0f / (1.0f + expf(-s));
+  return __frcp_rn(1.0f + expf(-s));
 }
 
 // One pixel of the relaxed resist objective (opc/ilt.py:_Objective, :313-336)

@@ -142,7 +142,7 @@ __global__ void k_tcc_T2(const float2* __restrict__ T, const int32_t* __restrict
 }
 
 constexpr int kTccWarps = 8;
-constexpr int kImgClips = 8;     // clips per block of the image contraction
+constexpr int kImgClips = 4;     // clips per block of the image contraction
 constexpr int kAdjClips = 2;     // clips per block of the adjoint contraction
 
 __device__ __forceinline__ double2 warp_sum(double2 v) {
