@@ -803,6 +803,56 @@ def run_ours(args) -> None:
                        "images_per_step": E2E_IMAGES, "api": "lithobat_b200.pipeline.AbbePipeline (copies of "
                        "consecutive batches overlapped with compute)",
                        "serial_one_call_value": world * E2E_IMAGES * ser / (ser_ms / 1000.0)}
+    # ---- the same workload with the masks as level maps (1 byte per pixel) ----
+    lv_img0 = None
+    if "levels" not in args.skip:
+        absorber = torch.tensor(complex(np.sqrt(0.06) * np.exp(1j * np.pi)), dtype=torch.complex64, device=dev)
+        lv = torch.stack([torch.ones((), dtype=torch.complex64, device=dev), absorber]).repeat(B, 1)
+        imaps = [(dmasks[r] != 1).to(torch.uint8).contiguous() for r in range(ROTATE)]
+        aerial.run_abbe_levels(pd, imaps[0], lv, out, peak)
+        lv_img = out.clone()
+        aerial.run_abbe(pd, dmasks[0], out, peak)
+        lv_diff = float(((lv_img.double() - out.double()).abs().amax(dim=(1, 2))
+                         / out.double().abs().amax(dim=(1, 2))).max())
+        lv_img0 = lv_img[0].double().cpu().numpy()   # its FP64 error is taken with the CPU sample below
+        del lv_img
+        for i in range(args.warmup):
+            aerial.run_abbe_levels(pd, imaps[i % ROTATE], lv, out, peak)
+        torch.cuda.synchronize()
+        barrier()
+        e0.record()
+        for i in range(args.steps):
+            aerial.run_abbe_levels(pd, imaps[i % ROTATE], lv, out, peak)
+        e1.record()
+        torch.cuda.synchronize()
+        lms = max_over_ranks(e0.elapsed_time(e1))
+        aerial.check_status(pd, dev)
+        lvl = {"value": world * B * args.steps / (lms / 1000.0), "unit": "images/s",
+               "ms_per_step": lms / args.steps, "max_rel_diff_vs_complex_masks": lv_diff,
+               "input": "uint8 level map per clip + its two complex levels (litho_abbe_levels)",
+               "l2": f"{ROTATE} rotating input batches of {B * NN >> 20} MiB"}
+        if "e2e" not in args.skip:
+            from lithobat_b200.pipeline import AbbePipeline
+            pin_i = [imaps[r][:E2E_IMAGES].cpu().pin_memory() for r in range(ROTATE)]
+            lv_h = lv[:E2E_IMAGES].cpu()
+            res = [torch.empty((E2E_IMAGES, N, N), dtype=torch.float32).pin_memory() for _ in range(2)]
+            lpipe = AbbePipeline(o, g, E2E_IMAGES, mask_complex=True, level_masks=True)
+            lpipe.run([pin_i[i % ROTATE] for i in range(max(1, args.warmup))],
+                      [res[i % 2] for i in range(max(1, args.warmup))], levels=lv_h)
+            torch.cuda.synchronize()
+            barrier()
+            t0 = time.perf_counter()
+            lpipe.run([pin_i[i % ROTATE] for i in range(args.steps)], [res[i % 2] for i in range(args.steps)],
+                      levels=lv_h)
+            torch.cuda.synchronize()
+            le2e = max_over_ranks((time.perf_counter() - t0) * 1000.0)
+            lvl["e2e"] = {"value": world * E2E_IMAGES * args.steps / (le2e / 1000.0), "unit": "images/s",
+                          "h2d_bytes_per_step": E2E_IMAGES * NN + E2E_IMAGES * 2 * 8,
+                          "d2h_bytes_per_step": E2E_IMAGES * NN * 4, "images_per_step": E2E_IMAGES,
+                          "api": "lithobat_b200.pipeline.AbbePipeline(level_masks=True)"}
+            del lpipe, pin_i, res
+        line["level_maps"] = lvl
+        del imaps
     for key in ("c1", "c2"):
         if key not in args.skip:
             line[key] = bench_config(key, args, torch, dev, world, max_over_ranks, barrier)
@@ -823,6 +873,8 @@ def run_ours(args) -> None:
                                           f"{3 * smp.S} coherent transforms), FP64 numpy/scipy (FFT workers=-1)"}
         line["cpu"] = cpu_info()
         line["max_rel_err_vs_fp64"] = float(np.abs(gpu0 - raw[0] / rpk[0]).max())
+        if line.get("level_maps") is not None and lv_img0 is not None:
+            line["level_maps"]["max_rel_err_vs_fp64"] = float(np.abs(lv_img0 - raw[0] / rpk[0]).max())
         if line.get("ilt") and line["ilt"].get("_fp64_case"):
             case = line["ilt"].pop("_fp64_case")
             ti, e_cost, e_grad = cpu_ilt_check(case)
@@ -851,7 +903,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--images", type=int, default=IMAGES_PER_STEP,
                     help="images per step (a small value makes a profiling case)")
-    ap.add_argument("--skip", default="", help="comma list of phases to skip: plain,e2e,profile,cpu,c1,c2,ilt,iltplain,uneven,"
+    ap.add_argument("--skip", default="", help="comma list of phases to skip: plain,e2e,levels,profile,cpu,c1,c2,ilt,iltplain,uneven,"
                                         "unevenilt")
     ap.add_argument("--ilt-clips", type=int, default=ILT_CLIPS, help="clips per ILT step")
     ap.add_argument("--uneven-clips", type=int, default=256, help="clips in the uneven-size batch")

@@ -279,6 +279,20 @@ int litho_abbe_tabled(const LithoAbbePlan* plan, const void* plan_blob_dev,
                       float* peak_dev, void* workspace_dev, size_t workspace_bytes,
                       cudaStream_t stream);
 
+/* litho_abbe_tabled() for masks given as level maps: one byte per pixel,
+ * mask_idx_dev[clip][y][x] indexing that clip's complex levels
+ * levels_dev[clip][0 .. n_levels) (float2; an index >= n_levels takes the
+ * last level). Binary and attenuated phase-shift masks have two levels (the
+ * reference builds them as 0/1 arrays or as 1 and sqrt(T) e^{i phase},
+ * mask/patterns.py), so the mask crosses the host link and HBM at 1 byte per
+ * pixel instead of 8 (complex64), with the same images: the level values are
+ * exactly the complex mask's values. Coarse-grid plans (plan.L <= 64) whose
+ * band fits the register band transform; LITHO_E_UNSUPPORTED otherwise. The
+ * plan's mask_complex is ignored. */
+int litho_abbe_levels(const LithoAbbePlan* plan, const void* plan_blob_dev, const void* table_dev,
+                      const uint8_t* mask_idx_dev, const void* levels_dev, int n_levels, float* image_dev,
+                      float* peak_dev, void* workspace_dev, size_t workspace_bytes, cudaStream_t stream);
+
 /* The raw Abbe sum, normalised per output, for a batch of clips.
  * Replaces expose/aerial_image.py:_abbe_sum (:351-494) together with
  * compute_aerial_image (:502-548) and compute_aerial_planes (:551-587):

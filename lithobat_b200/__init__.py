@@ -5,7 +5,7 @@ Drop-in replacements for ``litho_sim.expose.compute_aerial_image`` and
 ``liblitho_b200.so`` (C ABI in ``include/litho_b200.h``).
 """
 
-from .aerial import (SOURCE_TILT_SIGN, compute_aerial_batch, compute_aerial_image,
+from .aerial import (SOURCE_TILT_SIGN, LevelMasks, compute_aerial_batch, compute_aerial_image,
                      compute_aerial_planes, normalisation_scale)
 from .config import GridConfig, OpticsConfig
 from .hopkins import SOCSKernels
@@ -14,7 +14,7 @@ from . import patterns
 from . import torch_ops  # registers torch.ops.litho.*
 
 __all__ = [
-    "GridConfig", "OpticsConfig", "Pole", "SOCSKernels", "Source", "SourcePoints", "SOURCE_TILT_SIGN",
+    "GridConfig", "LevelMasks", "OpticsConfig", "Pole", "SOCSKernels", "Source", "SourcePoints", "SOURCE_TILT_SIGN",
     "build_source", "compute_aerial_batch", "compute_aerial_image", "compute_aerial_planes",
     "normalisation_scale", "source_points",
 ]

@@ -133,6 +133,7 @@ def lib():
     vp, i32, f32, sz = C.c_void_p, C.c_int, C.c_float, C.c_size_t
     sigs = {
         "litho_coarse_image": [C.POINTER(AbbePlan), vp, vp, vp, vp, vp, sz, vp],
+        "litho_abbe_levels": [C.POINTER(AbbePlan), vp, vp, vp, vp, i32, vp, vp, vp, sz, vp],
         "litho_abbe_engine": [C.POINTER(AbbePlan), vp, i32],
         "litho_abbe_noalloc_status": [C.POINTER(AbbePlan), vp],
         "litho_abbe_clear": [C.POINTER(AbbePlan), vp, vp, vp],

@@ -427,6 +427,86 @@ def run_abbe(pd: AbbePlanData, masks_dev, out=None, peak=None, stream=None, engi
 SYNTHESIS = ("direct", "row_pairs", "tensor_cores", "wide")
 
 
+class LevelMasks:
+    """Masks given as level maps: ``index`` (C, N, N) uint8 (numpy or a torch
+    tensor, any device) indexing each clip's complex ``levels`` (C, n_levels),
+    n_levels <= 256. Binary masks (0/1) and attenuated phase-shift masks
+    (1 and sqrt(T) e^{i phase}, mask/patterns.py) have two levels, so a clip
+    travels to the device and through HBM at one byte per pixel instead of
+    eight; the images are those of the complex masks the levels spell out."""
+
+    def __init__(self, index, levels):
+        self.index = index
+        self.levels = np.asarray(levels, dtype=np.complex64) if not _is_torch(levels) else levels
+        shape = tuple(index.shape)
+        if len(shape) != 3 or shape[1] != shape[2]:
+            raise ValueError(f"index must be (C, N, N), got {shape}")
+        lv = tuple(self.levels.shape)
+        if len(lv) != 2 or lv[0] != shape[0] or not 1 <= lv[1] <= 256:
+            raise ValueError(f"levels must be ({shape[0]}, n_levels <= 256), got {lv}")
+
+    @staticmethod
+    def from_masks(masks, max_levels: int = 256) -> "LevelMasks":
+        """Factor (C, N, N) masks (host arrays) into a level map and each
+        clip's distinct values; raises ValueError past ``max_levels``."""
+        m = np.asarray(masks)
+        if m.ndim == 2:
+            m = m[None]
+        C = m.shape[0]
+        index = np.empty(m.shape, dtype=np.uint8)
+        uniq = []
+        for c in range(C):
+            u, inv = np.unique(m[c].astype(np.complex64).ravel(), return_inverse=True)
+            if u.size > max_levels:
+                raise ValueError(f"clip {c} has {u.size} distinct values, more than {max_levels} levels")
+            uniq.append(u)
+            index[c] = inv.reshape(m.shape[1:]).astype(np.uint8)
+        nl = max(u.size for u in uniq)
+        levels = np.zeros((C, nl), dtype=np.complex64)
+        for c, u in enumerate(uniq):
+            levels[c, :u.size] = u
+        return LevelMasks(index, levels)
+
+    def expand(self) -> np.ndarray:
+        """The complex64 masks (host) the levels spell out."""
+        idx = self.index.cpu().numpy() if _is_torch(self.index) else np.asarray(self.index)
+        lv = self.levels.cpu().numpy() if _is_torch(self.levels) else self.levels
+        return np.take_along_axis(lv[:, None, :], idx.reshape(idx.shape[0], 1, -1).astype(np.int64),
+                                  axis=2).reshape(idx.shape).astype(np.complex64)
+
+
+def run_abbe_levels(pd: AbbePlanData, index_dev, levels_dev, out=None, peak=None, stream=None):
+    """``run_abbe`` for level-map masks (``litho_abbe_levels``): index_dev
+    (C, N, N) uint8 and levels_dev (C, n_levels) complex64 on the device."""
+    torch = nat.require_cuda()
+    L = nat.lib()
+    dev = index_dev.device
+    n = pd.plan.n
+    if index_dev.dtype != torch.uint8 or tuple(index_dev.shape) != (pd.plan.n_clips, n, n):
+        raise ValueError(f"index must be uint8 {(pd.plan.n_clips, n, n)}, got {index_dev.dtype} {tuple(index_dev.shape)}")
+    if levels_dev.dtype != torch.complex64 or levels_dev.dim() != 2 or levels_dev.shape[0] != pd.plan.n_clips:
+        raise ValueError("levels must be complex64 (n_clips, n_levels)")
+    if out is None:
+        out = torch.empty((pd.n_out, n, n), dtype=torch.float32, device=dev)
+    if peak is None:
+        peak = torch.empty((pd.n_out,), dtype=torch.float32, device=dev)
+    import ctypes as C
+    ws_bytes = C.c_size_t(0)
+    nat.check("litho_abbe_workspace", L.litho_abbe_workspace(C.byref(pd.plan), C.byref(ws_bytes)))
+    ws = nat.Workspace.get(torch, dev, ws_bytes.value, tag="fused")
+    blob = getattr(pd, "_blob_dev", None)
+    if blob is None or blob.device != dev:
+        blob = torch.from_numpy(pd.blob).to(dev)
+        pd._blob_dev = blob
+    s = stream if stream is not None else nat.stream_ptr(torch, dev)
+    table = pupil_table(pd, dev, s)
+    lv = levels_dev.contiguous()
+    nat.check("litho_abbe_levels", L.litho_abbe_levels(
+        C.byref(pd.plan), blob.data_ptr(), table.data_ptr(), index_dev.data_ptr(), lv.data_ptr(), int(lv.shape[1]),
+        out.data_ptr(), peak.data_ptr(), ws.data_ptr(), ws.numel(), s))
+    return out, peak
+
+
 def engine_info(pd: AbbePlanData) -> dict:
     """Which engine and image synthesis ``run_abbe`` uses for this plan
     (``litho_abbe_engine``)."""
@@ -479,7 +559,8 @@ def compute_aerial_batch(masks, optics, grid, planes=None, dose: float = 1.0, re
                          engine: str = "fused", check: bool | None = None):
     """Abbe images of a batch of clips on the GPU.
 
-    masks: (C, N, N) numpy array or torch tensor (real or complex).
+    masks: (C, N, N) numpy array or torch tensor (real or complex), or a
+        :class:`LevelMasks` (one byte per pixel; the band-limited engines).
     optics: one optics object for all clips, or a sequence of C of them.
     planes: None (each clip's own defocus / image index), a list of
         (defocus, n_image) shared by all clips, or a list of C such lists.
@@ -492,7 +573,17 @@ def compute_aerial_batch(masks, optics, grid, planes=None, dose: float = 1.0, re
     """
     torch = nat.require_cuda()
     n, px = _grid(grid)
-    md = _as_device_masks(torch, masks, n)
+    lev = masks if isinstance(masks, LevelMasks) else None
+    if lev is not None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+        idx = lev.index if _is_torch(lev.index) else torch.from_numpy(np.ascontiguousarray(lev.index))
+        md = idx.to(dev, torch.uint8).contiguous()
+        lv = lev.levels if _is_torch(lev.levels) else torch.from_numpy(np.ascontiguousarray(lev.levels))
+        lvd = lv.to(dev, torch.complex64).contiguous()
+        if tuple(md.shape[1:]) != (n, n):
+            raise ValueError(f"masks must be (C, {n}, {n}) for this grid, got {tuple(md.shape)}")
+    else:
+        md = _as_device_masks(torch, masks, n)
     Cn = md.shape[0]
     views = [optics_view(o) for o in optics] if isinstance(optics, (list, tuple)) else \
         [optics_view(optics)] * Cn
@@ -505,9 +596,15 @@ def compute_aerial_batch(masks, optics, grid, planes=None, dose: float = 1.0, re
         pl = [list(p) for p in planes]
     else:
         pl = [list(planes)] * Cn
-    pd = plan_abbe(views, n, px, pl, dose, return_raw, md.is_complex())
-    img, pk = run_abbe(pd, md, engine=engine)
-    if check if check is not None else not _is_torch(masks):
+    pd = plan_abbe(views, n, px, pl, dose, return_raw, True if lev is not None else md.is_complex())
+    if lev is not None:
+        if engine != "fused" or not fused_supported(n, int(pd.plan.L)) or int(pd.plan.L) > 64:
+            raise ValueError("level-map masks run on the band-limited coarse-grid engine only; pass the complex "
+                             "masks (LevelMasks.expand()) for this grid and pupil")
+        img, pk = run_abbe_levels(pd, md, lvd)
+    else:
+        img, pk = run_abbe(pd, md, engine=engine)
+    if check if check is not None else (lev is not None or not _is_torch(masks)):
         check_status(pd, md.device, engine)
     P = len(pl[0])
     return img.view(Cn, P, n, n), pk.view(Cn, P), pd.clears.reshape(Cn, P)

@@ -32,6 +32,10 @@ namespace litho {
 cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_per_clip, int n,
                                 int bm, float2* out, float scale, const float2* tw_inv,
                                 int num_sms, cudaStream_t st, int* status);
+cudaError_t launch_row_band_dft_levels(const uint8_t* in, const float2* levels, int n_levels, int n_rows,
+                                       int rows_per_clip, int n, int bm, float2* out, float scale,
+                                       const float2* tw_inv, int num_sms, cudaStream_t st);
+bool row_band_levels_ok(int n, int bm);
 bool wide_plan_ok(const LithoAbbePlan& p);
 int64_t wide_workspace_bytes(const LithoAbbePlan& p);
 int abbe_wide_run(const LithoAbbePlan& p, const void* blob, const void* table_in, const void* mask, float* image,
@@ -758,17 +762,22 @@ namespace litho {
 
 // The pipeline, optionally bracketing each stage with events ev[0..7].
 // table == nullptr: the pupil table is built into the workspace first.
+// levels != nullptr: mask is a level map (uint8 per pixel indexing
+// levels[clip][0 .. n_levels)), on the coarse engines only.
 static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* table_in, const void* mask,
-                    float* image, float* peak, void* ws, size_t ws_bytes, cudaStream_t s, cudaEvent_t* ev) {
+                    float* image, float* peak, void* ws, size_t ws_bytes, cudaStream_t s, cudaEvent_t* ev,
+                    const float2* levels = nullptr, int n_levels = 0) {
   int st = check_plan(plan);
   if (st) return st;
   if (!blob || !mask || !image || !peak || !ws) return LITHO_E_NULL;
-  if (((uintptr_t)ws & 15) || ((uintptr_t)blob & 15) || ((uintptr_t)mask & 7) || ((uintptr_t)table_in & 7))
+  if (((uintptr_t)ws & 15) || ((uintptr_t)blob & 15) || (!levels && ((uintptr_t)mask & 7)) ||
+      ((uintptr_t)table_in & 7) || ((uintptr_t)levels & 7))
     return LITHO_E_ALIGN;
   const LithoAbbePlan& p = *plan;
   const AbbeLayout l = abbe_layout(p);
   if ((int64_t)ws_bytes < l.total) return LITHO_E_WORKSPACE;
   if (p.n_items == 0 || p.n_jobs == 0) return LITHO_E_SIZE;
+  if (levels && (p.L > 64 || !row_band_levels_ok(p.n, p.bm))) return LITHO_E_UNSUPPORTED;
 
   if (p.L > 64) return abbe_wide_run(p, blob, table_in, mask, image, peak, ws, s, num_sms_cached(), ev);
   const char* b = static_cast<const char*>(blob);
@@ -799,8 +808,10 @@ static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* tab
     if ((e = launch_pupil_table(p, blob, table, s)) != cudaSuccess) return (int)e;
   mark(1);
   // mask band spectrum: rows then columns, 1/N^2 folded into the second pass
-  e = launch_row_band_dft(mask, p.mask_complex != 0, p.n_clips * p.n, p.n, p.n, p.bm, u1, 1.0f, tw, sms, s,
-                          status);
+  e = levels ? launch_row_band_dft_levels(static_cast<const uint8_t*>(mask), levels, n_levels, p.n_clips * p.n, p.n,
+                                          p.n, p.bm, u1, 1.0f, tw, sms, s)
+             : launch_row_band_dft(mask, p.mask_complex != 0, p.n_clips * p.n, p.n, p.n, p.bm, u1, 1.0f, tw, sms, s,
+                                   status);
   if (e != cudaSuccess) return (int)e;
   mark(2);
   e = launch_row_band_dft(u1, true, p.n_clips * Bm, Bm, p.n, p.bm, mb, 1.0f / ((float)p.n * (float)p.n), tw,
@@ -861,6 +872,15 @@ extern "C" int litho_abbe_tabled(const LithoAbbePlan* plan, const void* blob, co
                                  float* image, float* peak, void* ws, size_t ws_bytes, cudaStream_t s) {
   if (!table) return LITHO_E_NULL;
   return abbe_run(plan, blob, table, mask, image, peak, ws, ws_bytes, s, nullptr);
+}
+
+extern "C" int litho_abbe_levels(const LithoAbbePlan* plan, const void* blob, const void* table,
+                                 const uint8_t* mask_idx, const void* levels, int n_levels, float* image, float* peak,
+                                 void* ws, size_t ws_bytes, cudaStream_t s) {
+  if (!table || !levels) return LITHO_E_NULL;
+  if (n_levels < 1 || n_levels > 256) return LITHO_E_SIZE;
+  return abbe_run(plan, blob, table, mask_idx, image, peak, ws, ws_bytes, s, nullptr,
+                  static_cast<const float2*>(levels), n_levels);
 }
 
 extern "C" int litho_coarse_image(const LithoAbbePlan* plan, const void* blob, const void* table, const void* mb,

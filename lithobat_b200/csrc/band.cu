@@ -207,10 +207,20 @@ __host__ __device__ inline BandGeo band_geo(int n, int bm, int warps) {
 // M = N / 32 is a template constant, so every shared-memory offset below is
 // an immediate; the twiddle table is laid out per (pass, register kp, residue
 // b) with zeros where band_k(kp, pass) falls outside the band.
-template <bool CPLX, int M, bool TBS>
+// LEV (with CPLX): the input is a level map, one byte per pixel indexing the
+// row's clip's levels[clip][0 .. n_levels), complex; an index past the table
+// takes the last level.
+// LEV2 (real path): a two-level map, m = L0 + (L1 - L0) b with b = [index >=
+// 1] real, so two rows of b go through one complex transform (as real rows
+// do) and each band value is (L1 - L0) B(k) + L0 N [k = 0]: half the
+// transforms of the complex level path, the same spectrum to rounding.
+template <bool CPLX, int M, bool TBS, bool LEV = false, bool LEV2 = false>
 __global__ void __launch_bounds__(256, 2)
 k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int bm, float2* __restrict__ out,
-            float scale, const float2* __restrict__ tw_inv) {
+            float scale, const float2* __restrict__ tw_inv, const float2* __restrict__ levels = nullptr,
+            int n_levels = 0) {
+  static_assert(!LEV || CPLX, "level maps are complex inputs");
+  static_assert(!LEV2 || !CPLX, "two-level maps take the real path");
   constexpr int n = 32 * M, Lp = M < 32 ? M : 32, P = 32 / Lp, Q = M / Lp, LD = M + 1;
   extern __shared__ __align__(16) float2 bsm[];
   const BandGeo g = band_geo(n, bm, blockDim.x >> 5);
@@ -241,10 +251,35 @@ k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int bm, 
         const int b = bl + qq * Lp;
         if (p == 0 || Q > 1) {
           if (live) {
-            if (CPLX) {
+            if (LEV) {
+              const uint8_t* src = static_cast<const uint8_t*>(in) + (size_t)r1 * n + b;
+              const float2* lv = levels + (size_t)(r1 / rows_per_clip) * n_levels;
+              uint32_t q[32];
+#pragma unroll
+              for (int a = 0; a < 32; ++a) q[a] = __ldcs(src + M * a);
+              if (n_levels <= 4) {   // the row's levels in registers: selects, no dependent loads
+                const float2 l0 = __ldg(lv), l1 = n_levels > 1 ? __ldg(lv + 1) : l0;
+                const float2 l2 = n_levels > 2 ? __ldg(lv + 2) : l1, l3 = n_levels > 3 ? __ldg(lv + 3) : l2;
+#pragma unroll
+                for (int a = 0; a < 32; ++a) {
+                  const uint32_t k = q[a];
+                  const float2 lo = k == 0u ? l0 : l1, hi = k == 2u ? l2 : l3;
+                  v[a] = k < 2u ? lo : hi;
+                }
+              } else {
+#pragma unroll
+                for (int a = 0; a < 32; ++a)
+                  v[a] = __ldg(lv + (q[a] < (uint32_t)n_levels ? q[a] : n_levels - 1));
+              }
+            } else if (CPLX) {
               const float2* src = static_cast<const float2*>(in) + (size_t)r1 * n + b;
 #pragma unroll
               for (int a = 0; a < 32; ++a) v[a] = __ldcs(src + M * a);
+            } else if (LEV2) {
+              const uint8_t* s1 = static_cast<const uint8_t*>(in) + (size_t)r1 * n + b;
+#pragma unroll
+              for (int a = 0; a < 32; ++a)
+                v[a] = make_float2(__ldcs(s1 + M * a) ? 1.f : 0.f, __ldcs(s1 + n + M * a) ? 1.f : 0.f);
             } else {
               const float* s1 = static_cast<const float*>(in) + (size_t)r1 * n + b;
 #pragma unroll
@@ -304,10 +339,24 @@ k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int bm, 
         if (ra < n_rows) {
           const int clip = ra / rows_per_clip, i = ra % rows_per_clip;
           const float2* zr = Z + r * npass * 32;
+          float2 dl = make_float2(0.f, 0.f), l0n = make_float2(0.f, 0.f);
+          if (LEV2) {   // this clip's L1 - L0 and L0 N scale (the DC term of the constant L0)
+            const float2 a0 = __ldg(levels + (size_t)clip * 2), a1 = __ldg(levels + (size_t)clip * 2 + 1);
+            dl = make_float2(a1.x - a0.x, a1.y - a0.y);
+            l0n = make_float2(a0.x * (float)n * scale, a0.y * (float)n * scale);
+          }
           for (int kk = lane; kk < Bm; kk += 32) {
             const float2 z = zr[kk], zm = zr[Bm - 1 - kk];       // Z(k), Z(-k)
-            const float2 o1 = make_float2((z.x + zm.x) * hs, (z.y - zm.y) * hs);
-            const float2 o2 = make_float2((z.y + zm.y) * hs, (zm.x - z.x) * hs);
+            float2 o1 = make_float2((z.x + zm.x) * hs, (z.y - zm.y) * hs);
+            float2 o2 = make_float2((z.y + zm.y) * hs, (zm.x - z.x) * hs);
+            if (LEV2) {
+              o1 = cmul(dl, o1);
+              o2 = cmul(dl, o2);
+              if (kk == bm) {
+                o1 = cadd(o1, l0n);
+                o2 = cadd(o2, l0n);
+              }
+            }
             float2* dst = out + ((size_t)clip * Bm + kk) * rows_per_clip + i;
             dst[0] = o1;
             dst[1] = o2;
@@ -319,9 +368,10 @@ k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int bm, 
   }
 }
 
-template <bool CPLX, int M>
+template <bool CPLX, int M, bool LEV = false, bool LEV2 = false>
 static cudaError_t launch_band_rows_m(const void* in, int n_rows, int rows_per_clip, int bm, float2* out,
-                                      float scale, const float2* tw_inv, int num_sms, cudaStream_t st) {
+                                      float scale, const float2* tw_inv, int num_sms, cudaStream_t st,
+                                      const float2* levels = nullptr, int n_levels = 0) {
   const int n = 32 * M;
   const int warps = n <= 1024 ? 8 : 4;
   const BandGeo g = band_geo(n, bm, warps);
@@ -331,7 +381,19 @@ static cudaError_t launch_band_rows_m(const void* in, int n_rows, int rows_per_c
   const int per_sm = (int)((227 * 1024) / g.total) >= 2 ? 2 : 1;
   long long blocks = (n_iter + warps - 1) / warps;
   if (blocks > (long long)num_sms * per_sm) blocks = (long long)num_sms * per_sm;
-  if (g.tb_smem) {
+  if (LEV2) {   // two-level maps: the real path, table in shared memory
+    if (!g.tb_smem) return cudaErrorInvalidValue;
+    cudaFuncSetAttribute(k_band_rows<false, M, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)g.total);
+    k_band_rows<false, M, true, false, true><<<(int)blocks, warps * 32, g.total, st>>>(
+        in, n_rows, rows_per_clip, bm, out, scale, tw_inv, levels, n_levels);
+  } else if (LEV) {   // level maps: the common (table in shared memory) form only
+    if (!g.tb_smem) return cudaErrorInvalidValue;
+    cudaFuncSetAttribute(k_band_rows<true, M, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)g.total);
+    k_band_rows<true, M, true, true><<<(int)blocks, warps * 32, g.total, st>>>(in, n_rows, rows_per_clip, bm, out,
+                                                                               scale, tw_inv, levels, n_levels);
+  } else if (g.tb_smem) {
     cudaFuncSetAttribute(k_band_rows<CPLX, M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.total);
     k_band_rows<CPLX, M, true><<<(int)blocks, warps * 32, g.total, st>>>(in, n_rows, rows_per_clip, bm, out, scale,
                                                                          tw_inv);
@@ -496,6 +558,56 @@ __global__ void k_twiddle_table(float2* w, int n, int sign) {
 }
 
 // Launch the row-band DFT for n_rows rows (grouped rows_per_clip per clip).
+// The first band pass of a level map (uint8 [clip][n][n] indexing levels
+// [clip][n_levels]): powers of two n in [32, 2048] whose band twiddles fit
+// shared memory; cudaErrorInvalidValue otherwise.
+cudaError_t launch_row_band_dft_levels(const uint8_t* in, const float2* levels, int n_levels, int n_rows,
+                                       int rows_per_clip, int n, int bm, float2* out, float scale,
+                                       const float2* tw_inv, int num_sms, cudaStream_t st) {
+  if (!levels || n_levels < 1) return cudaErrorInvalidValue;
+  if (n_levels == 2 && rows_per_clip % 2 == 0 && n_rows % 2 == 0) {
+    switch (n) {
+      case 32: return launch_band_rows_m<false, 1, false, true>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv,
+                                                                num_sms, st, levels, 2);
+      case 64: return launch_band_rows_m<false, 2, false, true>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv,
+                                                                num_sms, st, levels, 2);
+      case 128: return launch_band_rows_m<false, 4, false, true>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv,
+                                                                 num_sms, st, levels, 2);
+      case 256: return launch_band_rows_m<false, 8, false, true>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv,
+                                                                 num_sms, st, levels, 2);
+      case 512: return launch_band_rows_m<false, 16, false, true>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv,
+                                                                  num_sms, st, levels, 2);
+      case 1024: return launch_band_rows_m<false, 32, false, true>(in, n_rows, rows_per_clip, bm, out, scale,
+                                                                   tw_inv, num_sms, st, levels, 2);
+      case 2048: return launch_band_rows_m<false, 64, false, true>(in, n_rows, rows_per_clip, bm, out, scale,
+                                                                   tw_inv, num_sms, st, levels, 2);
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  switch (n) {
+    case 32: return launch_band_rows_m<true, 1, true>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms, st,
+                                                      levels, n_levels);
+    case 64: return launch_band_rows_m<true, 2, true>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms, st,
+                                                      levels, n_levels);
+    case 128: return launch_band_rows_m<true, 4, true>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms,
+                                                       st, levels, n_levels);
+    case 256: return launch_band_rows_m<true, 8, true>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms,
+                                                       st, levels, n_levels);
+    case 512: return launch_band_rows_m<true, 16, true>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms,
+                                                        st, levels, n_levels);
+    case 1024: return launch_band_rows_m<true, 32, true>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms,
+                                                         st, levels, n_levels);
+    case 2048: return launch_band_rows_m<true, 64, true>(in, n_rows, rows_per_clip, bm, out, scale, tw_inv, num_sms,
+                                                         st, levels, n_levels);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+bool row_band_levels_ok(int n, int bm) {
+  const bool pow2 = n >= 32 && n <= 2048 && (n & (n - 1)) == 0;
+  return pow2 && band_geo(n, bm, n <= 1024 ? 8 : 4).tb_smem && band_geo(n, bm, n <= 1024 ? 8 : 4).total <= 200 * 1024;
+}
+
 cudaError_t launch_row_band_dft(const void* in, bool cplx, int n_rows, int rows_per_clip, int n,
                                 int bm, float2* out, float scale, const float2* tw_inv,
                                 int num_sms, cudaStream_t st, int* status) {

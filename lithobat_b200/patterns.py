@@ -35,6 +35,14 @@ def to_attenuated_psm(mask, transmission=0.06, phase_shift_deg=180.0):
     return np.where(mask > 0.5, np.sqrt(transmission) * np.exp(1j * ph), 1.0 + 0.0j).astype(np.complex128)
 
 
+def attenuated_psm_levels(mask, transmission=0.06, phase_shift_deg=180.0):
+    """to_attenuated_psm as a level map: (index uint8, levels complex64 [2]),
+    index 1 where the pattern is 1 (amplitude sqrt(T) e^{i phase}), 0 clear."""
+    ph = np.deg2rad(phase_shift_deg)
+    levels = np.array([1.0 + 0.0j, np.sqrt(transmission) * np.exp(1j * ph)], dtype=np.complex128)
+    return (np.asarray(mask) > 0.5).astype(np.uint8), levels.astype(np.complex64)
+
+
 def manhattan_clip(rng, n, pixel_size, n_rect=(20, 60), width_nm=(40.0, 200.0)):
     """Union of rng-drawn axis-aligned rectangles, 0/1 float64, pixel aligned."""
     m = np.zeros((n, n), dtype=np.float64)

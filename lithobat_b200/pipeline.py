@@ -26,17 +26,23 @@ class AbbePipeline:
     pinned CPU tensors, outputs[i] (batch, N, N) float32 pinned CPU tensors
     (the same tensor may appear several times in either list; an output is
     complete once ``run`` returns). ``run`` raises ``LithoError`` if a bounded
-    wait inside any batch's kernels gave up (``LITHO_E_TIMEOUT``)."""
+    wait inside any batch's kernels gave up (``LITHO_E_TIMEOUT``).
+
+    ``level_masks=True``: inputs are level maps, (batch, N, N) uint8 indices
+    into ``run(..., levels=...)``, a (batch, n_levels) complex64 tensor shared
+    by every batch of the run (``litho_abbe_levels``): one byte per pixel over
+    the host link instead of eight for complex masks."""
 
     def __init__(self, optics, grid, batch: int, mask_complex: bool, dose: float = 1.0, return_raw: bool = False,
-                 depth: int = 2, device=None):
+                 depth: int = 2, device=None, level_masks: bool = False):
         torch = nat.require_cuda()
         self.torch, self.L = torch, nat.lib()
         self.dev = device if device is not None else torch.device("cuda", torch.cuda.current_device())
         v = optics_view(optics)
         self.n = n = int(grid.n_pixels)
         self.batch = int(batch)
-        self.complex = bool(mask_complex)
+        self.levels = bool(level_masks)
+        self.complex = bool(mask_complex) or self.levels
         self.pd = plan_abbe([v] * self.batch, n, float(grid.pixel_size), [[(v.defocus, v.image_index)]] * self.batch,
                             float(dose), bool(return_raw), self.complex)
         if not fused_supported(n, int(self.pd.plan.L)):
@@ -48,7 +54,9 @@ class AbbePipeline:
         nb = C.c_size_t(0)
         nat.check("litho_abbe_workspace", self.L.litho_abbe_workspace(C.byref(self.pd.plan), C.byref(nb)))
         self.ws = torch.empty(max(nb.value, 256), dtype=torch.uint8, device=self.dev)
-        dt = torch.complex64 if self.complex else torch.float32
+        if self.levels and int(self.pd.plan.L) > 64:
+            raise NotImplementedError("level-map masks run on the coarse-grid engines only")
+        dt = torch.uint8 if self.levels else (torch.complex64 if self.complex else torch.float32)
         self.depth = max(2, int(depth))
         self.d_in = [torch.empty((self.batch, n, n), dtype=dt, device=self.dev) for _ in range(self.depth)]
         self.d_out = [torch.empty((self.batch, n, n), dtype=torch.float32, device=self.dev) for _ in range(self.depth)]
@@ -61,10 +69,16 @@ class AbbePipeline:
         self._status = self.ws[:4].view(torch.int32)
         self._worst = torch.zeros((1,), dtype=torch.int32, device=self.dev)
 
-    def run(self, inputs, outputs) -> None:
+    def run(self, inputs, outputs, levels=None) -> None:
         torch, L = self.torch, self.L
         if len(inputs) != len(outputs):
             raise ValueError(f"{len(inputs)} input batches for {len(outputs)} outputs")
+        if self.levels:
+            if levels is None or tuple(levels.shape[:1]) != (self.batch,) or levels.dim() != 2:
+                raise ValueError(f"level-map inputs need levels of shape ({self.batch}, n_levels)")
+            with torch.cuda.stream(self.s_in):
+                d_lv = levels.to(self.dev, torch.complex64, non_blocking=True).contiguous()
+            self.s_run.wait_stream(self.s_in)
         ev = torch.cuda.Event
         read_done = [None] * self.depth    # compute finished reading d_in[slot]
         sent = [None] * self.depth         # download of d_out[slot] finished
@@ -80,10 +94,16 @@ class AbbePipeline:
                 self.s_run.wait_event(loaded)
                 if sent[k] is not None:
                     self.s_run.wait_event(sent[k])
-                nat.check("litho_abbe_tabled", L.litho_abbe_tabled(
-                    C.byref(self.pd.plan), self.pd._blob_dev.data_ptr(), self.table.data_ptr(),
-                    self.d_in[k].data_ptr(), self.d_out[k].data_ptr(), self.d_peak[k].data_ptr(),
-                    self.ws.data_ptr(), self.ws.numel(), int(self.s_run.cuda_stream)))
+                if self.levels:
+                    nat.check("litho_abbe_levels", L.litho_abbe_levels(
+                        C.byref(self.pd.plan), self.pd._blob_dev.data_ptr(), self.table.data_ptr(),
+                        self.d_in[k].data_ptr(), d_lv.data_ptr(), int(d_lv.shape[1]), self.d_out[k].data_ptr(),
+                        self.d_peak[k].data_ptr(), self.ws.data_ptr(), self.ws.numel(), int(self.s_run.cuda_stream)))
+                else:
+                    nat.check("litho_abbe_tabled", L.litho_abbe_tabled(
+                        C.byref(self.pd.plan), self.pd._blob_dev.data_ptr(), self.table.data_ptr(),
+                        self.d_in[k].data_ptr(), self.d_out[k].data_ptr(), self.d_peak[k].data_ptr(),
+                        self.ws.data_ptr(), self.ws.numel(), int(self.s_run.cuda_stream)))
                 torch.maximum(self._worst, self._status, out=self._worst)
                 done = ev()
                 done.record(self.s_run)

@@ -105,3 +105,23 @@ def test_source_presets_round_trip_through_dicts():
     d = s.to_dict()
     assert Source.from_dict(d).render(21).tolist() == s.render(21).tolist()
     assert s.n_points(21) == 34
+
+
+def test_level_masks_factor_and_expand():
+    """LevelMasks.from_masks: per-clip distinct values and a uint8 index
+    that spell out the masks exactly; too many levels or bad shapes refused."""
+    import numpy as np
+    import pytest
+    import lithobat_b200 as lb
+    rng = np.random.default_rng(3)
+    pats = (rng.random((3, 32, 32)) > 0.5).astype(np.float64)
+    m = lb.patterns.to_attenuated_psm(pats)
+    f = lb.LevelMasks.from_masks(m)
+    assert f.index.dtype == np.uint8 and f.levels.shape == (3, 2)
+    assert np.array_equal(f.expand(), m.astype(np.complex64))
+    idx, lv = lb.patterns.attenuated_psm_levels(pats)
+    assert np.array_equal(lv[idx], m.astype(np.complex64))
+    with pytest.raises(ValueError):
+        lb.LevelMasks.from_masks(rng.random((1, 32, 32)), max_levels=16)
+    with pytest.raises(ValueError):
+        lb.LevelMasks(idx[0], lv[None])
