@@ -143,26 +143,27 @@ def bench_ilt(args, torch, dev, world, max_over_ranks, barrier) -> dict:
         mk = torch.empty_like(th)
         cpart = torch.empty((nclip, 64), dtype=torch.float64, device=dev)
         ppart = torch.empty((nclip, 64), dtype=torch.int32, device=dev)
-        ev[0].record()
-        gm = st.synth(b.hbox, st.h, False)
-        ev[1].record()
-        nat_.check("update", st.L.litho_ilt_update(gm.data_ptr(), gm.numel(), b.beta, b.beta, 0.4, 0.9, 0.999, 1e-8,
-                                                   5, th.data_ptr(), m1.data_ptr(), m2.data_ptr(), mk.data_ptr(),
-                                                   st.stream()))
-        ev[2].record()
-        mbox = st.mask_box(mk)
-        ev[3].record()
-        ibox = st.image_box(mbox)
-        ev[4].record()
-        # the step's own objective call: synthesis + resist objective + the
-        # band of dJ/dI in one pass when the band form serves the grid
-        _c, gbox, _s, _p = st.objective_from_box(ibox, b.target, float(params.scale), 0.3, 1.0,
-                                                 float(params.steepness), want_signed=False)
-        ev[5].record()
-        ev[6].record()
-        st.adjoint_box(gbox, mbox)
-        ev[7].record()
-        torch.cuda.synchronize()
+        for _rep in range(2):   # the first pass sizes workspaces and loads kernels; the second is timed
+            ev[0].record()
+            gm = st.synth(b.hbox, st.h, False)
+            ev[1].record()
+            nat_.check("update", st.L.litho_ilt_update(gm.data_ptr(), gm.numel(), b.beta, b.beta, 0.4, 0.9, 0.999,
+                                                       1e-8, 5, th.data_ptr(), m1.data_ptr(), m2.data_ptr(),
+                                                       mk.data_ptr(), st.stream()))
+            ev[2].record()
+            mbox = st.mask_box(mk)
+            ev[3].record()
+            ibox = st.image_box(mbox)
+            ev[4].record()
+            # the step's own objective call: synthesis + resist objective + the
+            # band of dJ/dI in one pass when the band form serves the grid
+            _c, gbox, _s, _p = st.objective_from_box(ibox, b.target, float(params.scale), 0.3, 1.0,
+                                                     float(params.steepness), want_signed=False)
+            ev[5].record()
+            ev[6].record()
+            st.adjoint_box(gbox, mbox)
+            ev[7].record()
+            torch.cuda.synchronize()
         names = ["gradient_synthesis", "theta_grad+adam+mask", "mask_band_spectrum",
                  "image_band_box (band TCC)", "image synthesis + objective + dJ/dI band box",
                  "(in the previous stage)", "adjoint: gradient band box (band TCC)"]
