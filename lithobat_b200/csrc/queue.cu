@@ -16,7 +16,7 @@
 //       (rows of the pupil table and of the mask band are read contiguously);
 //   pass B task (group, item, row blocks): for every transform of the item
 //       and every column u of the block, the inverse FFT over ky of U[t][.][u]
-//       and J^T(u, v) += w |e|^2 on chip -> the item's partial (written once:
+//       and J^T(u, v) += w |e|^2 in registers -> the item's partial (written once:
 //       a chunk always holds whole items).
 //
 // Chunks of items own one of a few T slots; a slot holds enough transforms
@@ -73,8 +73,9 @@ struct QParams {
   int* counters;
 };
 
-// twiddles (L <= 1024), the warps' transpose buffers, the warps' J rows
-constexpr size_t kQSmem = (size_t)1024 * 8 + (size_t)kQWarps * 32 * kTbLd * 8 + (size_t)kQWarps * 32 * 32 * 4;
+// twiddles (L <= 1024) and the warps' transpose buffers (pass B keeps J in
+// registers)
+constexpr size_t kQSmem = (size_t)1024 * 8 + (size_t)kQWarps * 32 * kTbLd * 8;
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -164,13 +165,12 @@ __device__ void q_pass_a(const QGroup& G, const LithoQueueTask& t, const float2*
 // [t.count, t.count + t.rows), e(u, v) = sum_ky U[t][ky][u] e^{+2 pi i ky v / L}
 // and J^T(u, v) = sum_t w_t |e_t(u, v)|^2 -> partial[item][u][v].
 template <int L>
-__device__ void q_pass_b(const QGroup& G, const LithoQueueTask& t, const float2* tw, float2* tb, float* Jw) {
+__device__ void q_pass_b(const QGroup& G, const LithoQueueTask& t, const float2* tw, float2* tb) {
   constexpr int R = L / 32, LPW = 32 / R;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int h = G.h, side = 2 * h + 1, ncomp = G.ncomp;
   const LithoItem it = G.items[t.first];
   const float2* Ts = G.T + (size_t)t.slot * G.slot_elems;
-  float* J = Jw + lane;  // [s][lane]
   const int jb = it.job_begin, nt = (it.job_end - jb) * ncomp;
   // T rows of transform k of row block rb for this lane's registers
   auto rows_of = [&](int rb, int k) -> const float2* {
@@ -178,8 +178,9 @@ __device__ void q_pass_b(const QGroup& G, const LithoQueueTask& t, const float2*
   };
   for (int rb = t.count; rb < t.count + t.rows; ++rb) {
     const int u0 = (rb * kQWarps + warp) * LPW;
+    float Jr[32];   // this lane's J values, in registers across the item's transforms
 #pragma unroll
-    for (int s = 0; s < 32; ++s) J[s * 32] = 0.f;
+    for (int s = 0; s < 32; ++s) Jr[s] = 0.f;
     for (int k = 0; k < nt; ++k) {
       const int jl = div_ncomp(k, ncomp), c = k - jl * ncomp;
       const LithoJob job = G.jobs[jb + jl];
@@ -212,11 +213,11 @@ __device__ void q_pass_b(const QGroup& G, const LithoQueueTask& t, const float2*
       }
       warp_fft_lines<L, +1>(x, tb, tw);
 #pragma unroll
-      for (int s = 0; s < 32; ++s) J[s * 32] = fmaf(w, cabs2(x[s]), J[s * 32]);
+      for (int s = 0; s < 32; ++s) Jr[s] = fmaf(w, cabs2(x[s]), Jr[s]);
     }
     float* pj = G.partial + ((size_t)t.first * L + u0 + lane / R) * L + lane % R;
 #pragma unroll
-    for (int s = 0; s < 32; ++s) pj[R * s] = J[s * 32];
+    for (int s = 0; s < 32; ++s) pj[R * s] = Jr[s];
   }
 }
 
@@ -239,10 +240,9 @@ __device__ bool task_ok(const QParams& P, const LithoQueueTask& t) {
 }
 
 template <int L>
-__device__ __forceinline__ void q_run(const QGroup& G, const LithoQueueTask& t, const float2* tw, float2* tb,
-                                      float* Jw) {
+__device__ __forceinline__ void q_run(const QGroup& G, const LithoQueueTask& t, const float2* tw, float2* tb) {
   if (t.kind == 0) q_pass_a<L>(G, t, tw, tb);
-  else q_pass_b<L>(G, t, tw, tb, Jw);
+  else q_pass_b<L>(G, t, tw, tb);
 }
 
 __global__ void __launch_bounds__(kQWarps * 32, kQBlocksPerSm) k_uneven_queue(const __grid_constant__ QParams P) {
@@ -251,7 +251,6 @@ __global__ void __launch_bounds__(kQWarps * 32, kQBlocksPerSm) k_uneven_queue(co
   const int warp = threadIdx.x >> 5;
   float2* tw = qsm;
   float2* tb = qsm + 1024 + warp * 32 * kTbLd;
-  float* Jw = reinterpret_cast<float*>(qsm + 1024 + kQWarps * 32 * kTbLd) + warp * 32 * 32;
   int tw_group = -1;
   for (;;) {
     if (threadIdx.x == 0) s_task = atomicAdd(P.head, 1);
@@ -277,10 +276,10 @@ __global__ void __launch_bounds__(kQWarps * 32, kQBlocksPerSm) k_uneven_queue(co
         __syncthreads();
       }
       switch (G.L) {
-        case 128: q_run<128>(G, t, tw, tb, Jw); break;
-        case 256: q_run<256>(G, t, tw, tb, Jw); break;
-        case 512: q_run<512>(G, t, tw, tb, Jw); break;
-        case 1024: q_run<1024>(G, t, tw, tb, Jw); break;
+        case 128: q_run<128>(G, t, tw, tb); break;
+        case 256: q_run<256>(G, t, tw, tb); break;
+        case 512: q_run<512>(G, t, tw, tb); break;
+        case 1024: q_run<1024>(G, t, tw, tb); break;
         default: break;
       }
     }
