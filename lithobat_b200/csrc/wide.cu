@@ -46,9 +46,13 @@ constexpr int kWideSpecPairs = 4;   // output pairs per synthesis chunk
 // 32 / R lines of L = 32 R points at once; kWfWarps warps per block.
 constexpr int kWfWarps = 8;
 
-// twiddles, the warps' transpose buffers, then (pass B) the warps' J rows
-__host__ __device__ inline size_t wf_smem(int L) {
-  return (size_t)L * 8 + (size_t)kWfWarps * 32 * kTbLd * 8 + (size_t)kWfWarps * 32 * 32 * 4;
+// twiddles and the warps' transpose buffers
+__host__ __device__ inline size_t wf_smem(int L) { return (size_t)L * 8 + (size_t)kWfWarps * 32 * kTbLd * 8; }
+// pass B keeps J in registers up to L = 256; longer lines leave no registers
+// for it and keep the warps' J rows in shared memory after the buffers above
+__host__ __device__ constexpr bool wf_j_regs(int L) { return L <= 256; }
+__host__ __device__ inline size_t wf_rows_smem(int L) {
+  return wf_smem(L) + (wf_j_regs(L) ? 0 : (size_t)kWfWarps * 32 * 32 * 4);
 }
 
 // Pass A. Grid (transform t of the chunk, chunk of kWfWarps * LPW columns).
@@ -100,7 +104,8 @@ k_wide_cols_w(const LithoJob* __restrict__ jobs, int j0, int ncomp_max, const fl
 
 // Pass B. Grid (item, chunk of kWfWarps * LPW rows v). Adds the item's
 // transforms whose jobs lie in [j0, j0 + nj) to partial[item][v][u]; each
-// warp keeps its rows' J in shared memory across the transforms.
+// lane keeps its J values in registers (L <= 256) or in its warp's rows in
+// shared memory across the transforms.
 template <int L>
 __global__ void __launch_bounds__(kWfWarps * 32, 2)
 k_wide_rows_w(const LithoItem* __restrict__ items, const LithoJob* __restrict__ jobs, int j0, int nj,
@@ -120,9 +125,13 @@ k_wide_rows_w(const LithoItem* __restrict__ items, const LithoJob* __restrict__ 
   const int side = 2 * h + 1;
   const int v0 = (blockIdx.y * kWfWarps + warp) * LPW;
   float* pj = partial + ((size_t)blockIdx.x * L + v0 + lane / R) * L + lane % R;
-  float* J = reinterpret_cast<float*>(wsm + L + kWfWarps * 32 * kTbLd) + warp * 32 * 32 + lane;  // [s][lane]
+  float Jr[wf_j_regs(L) ? 32 : 1];
+  float* Js = reinterpret_cast<float*>(wsm + L + kWfWarps * 32 * kTbLd) + warp * 32 * 32 + lane;  // [s][lane]
 #pragma unroll
-  for (int s = 0; s < 32; ++s) J[s * 32] = pj[R * s];
+  for (int s = 0; s < 32; ++s) {
+    if constexpr (wf_j_regs(L)) Jr[s] = pj[R * s];
+    else Js[s * 32] = pj[R * s];
+  }
   for (int jj = jb; jj < je; ++jj) {
     const LithoJob job = jobs[jj];
     const float w = (float)job.weight;
@@ -140,11 +149,14 @@ k_wide_rows_w(const LithoItem* __restrict__ items, const LithoJob* __restrict__ 
       }
       warp_fft_lines<L, +1>(x, tb, tw);
 #pragma unroll
-      for (int s = 0; s < 32; ++s) J[s * 32] = fmaf(w, cabs2(x[s]), J[s * 32]);
+      for (int s = 0; s < 32; ++s) {
+        if constexpr (wf_j_regs(L)) Jr[s] = fmaf(w, cabs2(x[s]), Jr[s]);
+        else Js[s * 32] = fmaf(w, cabs2(x[s]), Js[s * 32]);
+      }
     }
   }
 #pragma unroll
-  for (int s = 0; s < 32; ++s) pj[R * s] = J[s * 32];
+  for (int s = 0; s < 32; ++s) pj[R * s] = wf_j_regs(L) ? Jr[s] : Js[s * 32];
 }
 
 template <int L>
@@ -153,13 +165,13 @@ static cudaError_t launch_wide_passes_l(const LithoAbbePlan& p, int j0, int nj, 
                                         const float2* twL, float2* T, float* partial, cudaStream_t s) {
   constexpr int R = L / 32, LPW = 32 / R;
   const int side = 2 * p.h + 1;
-  const size_t sm = wf_smem(L);
+  const size_t sm = wf_smem(L), smr = wf_rows_smem(L);
   cudaFuncSetAttribute(k_wide_cols_w<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  cudaFuncSetAttribute(k_wide_rows_w<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  cudaFuncSetAttribute(k_wide_rows_w<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smr);
   dim3 ga(nj * p.ncomp_max, (side + kWfWarps * LPW - 1) / (kWfWarps * LPW));
   k_wide_cols_w<L><<<ga, kWfWarps * 32, sm, s>>>(jobs, j0, p.ncomp_max, table, p.h, mb, p.bm, twL, T);
   dim3 gb(p.n_items, L / (kWfWarps * LPW));
-  k_wide_rows_w<L><<<gb, kWfWarps * 32, sm, s>>>(items, jobs, j0, nj, p.ncomp_max, p.h, twL, T, partial);
+  k_wide_rows_w<L><<<gb, kWfWarps * 32, smr, s>>>(items, jobs, j0, nj, p.ncomp_max, p.h, twL, T, partial);
   return cudaGetLastError();
 }
 
