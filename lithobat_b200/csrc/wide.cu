@@ -22,6 +22,8 @@
 // register FFTs (fftwarp.cuh); the L x L transforms of J and g_L run in shared
 // memory (fftsmem.cuh). Every reduction has a fixed order, so results are
 // deterministic.
+#include <algorithm>
+
 #include "common.cuh"
 #include "fftsmem.cuh"
 #include "fftwarp.cuh"
@@ -184,6 +186,128 @@ static cudaError_t launch_wide_passes(const LithoAbbePlan& p, int j0, int nj, co
     case 512: return launch_wide_passes_l<512>(p, j0, nj, items, jobs, table, mb, twL, T, partial, s);
     case 1024: return launch_wide_passes_l<1024>(p, j0, nj, items, jobs, table, mb, twL, T, partial, s);
     default: return cudaErrorInvalidValue;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2-D transforms of L x L planes (the coarse-grid J and g_L) with the warp
+// register FFT: rows straight from global memory (a warp takes 1024 / L rows,
+// coalesced both ways), then columns through a padded shared-memory tile of
+// 8 x 1024 / L columns (coalesced row segments in and out). Same sums as
+// plain_fft2: out = scale_cols * FFT_cols(scale_rows * FFT_rows(in)),
+// SIGN = +1 unnormalised inverse, -1 forward.
+// ---------------------------------------------------------------------------
+template <int L, int SIGN, bool REAL>
+__global__ void __launch_bounds__(kWfWarps * 32, 2)
+k_wfft_rows(const void* __restrict__ in, float2* __restrict__ out, long long n_rows, float scale,
+            const float2* __restrict__ twL) {
+  constexpr int R = L / 32, LPW = 32 / R;
+  extern __shared__ float2 wsm[];
+  float2* tw = wsm;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* tb = wsm + L + warp * 32 * kTbLd;
+  fill_lane_twiddles(tw, L, twL, 1);
+  __syncthreads();
+  const long long groups = n_rows / LPW;
+  for (long long gi = (long long)blockIdx.x * kWfWarps + warp; gi < groups; gi += (long long)gridDim.x * kWfWarps) {
+    const long long r0 = gi * LPW;
+    float2 x[32];
+#pragma unroll
+    for (int l = 0; l < LPW; ++l) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const size_t g = (size_t)(r0 + l) * L + lane + 32 * q;
+        x[l * R + q] = REAL ? make_float2(reinterpret_cast<const float*>(in)[g], 0.f)
+                            : reinterpret_cast<const float2*>(in)[g];
+      }
+    }
+    warp_fft_lines<L, SIGN>(x, tb, tw);   // lane: row r0 + lane / R, index lane % R + R s
+    float2* dst = out + (size_t)(r0 + lane / R) * L + lane % R;
+#pragma unroll
+    for (int s = 0; s < 32; ++s) dst[R * s] = cscale(x[s], scale);
+  }
+}
+
+template <int L, int SIGN>
+__global__ void __launch_bounds__(kWfWarps * 32, 1)
+k_wfft_cols(float2* __restrict__ buf, long long planes, float scale, const float2* __restrict__ twL) {
+  constexpr int R = L / 32, LPW = 32 / R, TC = kWfWarps * LPW, PT = TC + 1;
+  extern __shared__ float2 wsm[];
+  float2* tw = wsm;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* tb = wsm + L + warp * 32 * kTbLd;
+  float2* tile = wsm + L + kWfWarps * 32 * kTbLd;   // [row][TC + 1]
+  fill_lane_twiddles(tw, L, twL, 1);
+  __syncthreads();
+  const long long tiles = planes * (L / TC);
+  for (long long t = blockIdx.x; t < tiles; t += gridDim.x) {
+    float2* base = buf + (size_t)(t / (L / TC)) * L * L + (size_t)(t % (L / TC)) * TC;
+    for (int id = threadIdx.x; id < L * TC; id += blockDim.x) {
+      const int r = id / TC, c = id - r * TC;
+      tile[r * PT + c] = base[(size_t)r * L + c];
+    }
+    __syncthreads();
+    float2 x[32];
+#pragma unroll
+    for (int l = 0; l < LPW; ++l) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) x[l * R + q] = tile[(lane + 32 * q) * PT + warp * LPW + l];
+    }
+    warp_fft_lines<L, SIGN>(x, tb, tw);   // lane: column warp LPW + lane / R, row lane % R + R s
+    __syncthreads();                      // every warp has read the tile
+#pragma unroll
+    for (int s = 0; s < 32; ++s) tile[(lane % R + R * s) * PT + warp * LPW + lane / R] = cscale(x[s], scale);
+    __syncthreads();
+    for (int id = threadIdx.x; id < L * TC; id += blockDim.x) {
+      const int r = id / TC, c = id - r * TC;
+      base[(size_t)r * L + c] = tile[r * PT + c];
+    }
+    __syncthreads();
+  }
+}
+
+template <int L>
+static cudaError_t wfft2_l(const void* in, bool in_real, float2* buf, long long planes, int sign, float scale_rows,
+                           float scale_cols, const float2* twL, cudaStream_t s) {
+  constexpr int R = L / 32, LPW = 32 / R, TC = kWfWarps * LPW;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (sms <= 0) sms = 148;
+  const size_t smr = wf_smem(L), smc = wf_smem(L) + (size_t)L * (TC + 1) * 8;
+  const long long rows = planes * L, groups = rows / LPW;
+  const int gr = (int)std::min<long long>((groups + kWfWarps - 1) / kWfWarps, 2LL * sms);
+  const int gc = (int)std::min<long long>(planes * (L / TC), (long long)sms);
+  const void* src = in ? in : buf;
+  if (sign > 0) {
+    cudaFuncSetAttribute(k_wfft_rows<L, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smr);
+    k_wfft_rows<L, 1, false><<<gr, kWfWarps * 32, smr, s>>>(src, buf, rows, scale_rows, twL);
+    cudaFuncSetAttribute(k_wfft_cols<L, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smc);
+    k_wfft_cols<L, 1><<<gc, kWfWarps * 32, smc, s>>>(buf, planes, scale_cols, twL);
+  } else {
+    if (in_real) {
+      cudaFuncSetAttribute(k_wfft_rows<L, -1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smr);
+      k_wfft_rows<L, -1, true><<<gr, kWfWarps * 32, smr, s>>>(src, buf, rows, scale_rows, twL);
+    } else {
+      cudaFuncSetAttribute(k_wfft_rows<L, -1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smr);
+      k_wfft_rows<L, -1, false><<<gr, kWfWarps * 32, smr, s>>>(src, buf, rows, scale_rows, twL);
+    }
+    cudaFuncSetAttribute(k_wfft_cols<L, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smc);
+    k_wfft_cols<L, -1><<<gc, kWfWarps * 32, smc, s>>>(buf, planes, scale_cols, twL);
+  }
+  return cudaGetLastError();
+}
+
+// plain_fft2 for the wide engine's coarse grids: L in {128 .. 1024} on the
+// warp register FFT, other sizes through plain_fft2.
+static cudaError_t wide_fft2(const void* in, bool in_real, float2* buf, long long planes, int L, int sign,
+                             float scale_rows, float scale_cols, const float2* twL, cudaStream_t s) {
+  switch (L) {
+    case 128: return wfft2_l<128>(in, in_real, buf, planes, sign, scale_rows, scale_cols, twL, s);
+    case 256: return wfft2_l<256>(in, in_real, buf, planes, sign, scale_rows, scale_cols, twL, s);
+    case 512: return wfft2_l<512>(in, in_real, buf, planes, sign, scale_rows, scale_cols, twL, s);
+    case 1024: return wfft2_l<1024>(in, in_real, buf, planes, sign, scale_rows, scale_cols, twL, s);
+    default: return plain_fft2(in, in_real, buf, planes, L, sign, scale_rows, scale_cols, twL, s);
   }
 }
 
@@ -635,7 +759,7 @@ static int wide_finish_ev(const LithoAbbePlan& p, const void* blob, float* image
   const int LL = L * L;
   dim3 gr((LL + 255) / 256 < 1024 ? (LL + 255) / 256 : 1024, p.n_out);
   k_wide_reduce<<<gr, 256, 0, s>>>(out_items, partial, LL, J);
-  e = plain_fft2(J, true, F, p.n_out, L, -1, 1.0f, 1.0f / ((float)L * (float)L), twL, s);
+  e = wide_fft2(J, true, F, p.n_out, L, -1, 1.0f, 1.0f / ((float)L * (float)L), twL, s);
   if (e != cudaSuccess) return (int)e;
   dim3 gx((G * G + 255) / 256, p.n_out);
   k_wide_box<<<gx, 256, 0, s>>>(F, L, p.h, bbox, transposed ? 1 : 0);
@@ -755,7 +879,7 @@ int wide_socs_adjoint(const LithoAbbePlan& p, const void* blob, const float2* ta
   if ((e = cudaMemsetAsync(A, 0, (size_t)p.n_clips * npts * 8, s)) != cudaSuccess) return (int)e;
   const int G = 4 * h + 1;
   k_wide_scatter_box<<<dim3((G * G + 255) / 256, p.n_clips), 256, 0, s>>>(sens_box, 2 * h, L, gL);
-  e = plain_fft2(nullptr, false, gL, p.n_clips, L, +1, 1.0f, 1.0f, twL, s);
+  e = wide_fft2(nullptr, false, gL, p.n_clips, L, +1, 1.0f, 1.0f, twL, s);
   if (e != cudaSuccess) return (int)e;
   for (int j0 = 0; j0 < p.n_jobs; j0 += l.jobs_per_chunk) {
     const int nj = (p.n_jobs - j0) < l.jobs_per_chunk ? (p.n_jobs - j0) : l.jobs_per_chunk;
@@ -794,7 +918,7 @@ int wide_coarse_box(const LithoAbbePlan& p, const void* blob, const float2* tabl
   const int LL = L * L;
   k_wide_reduce<<<dim3((LL + 255) / 256 < 1024 ? (LL + 255) / 256 : 1024, p.n_out), 256, 0, s>>>(out_items, partial,
                                                                                                  LL, J);
-  e = plain_fft2(J, true, F, p.n_out, L, -1, 1.0f, 1.0f / ((float)L * (float)L), twL, s);
+  e = wide_fft2(J, true, F, p.n_out, L, -1, 1.0f, 1.0f / ((float)L * (float)L), twL, s);
   if (e != cudaSuccess) return (int)e;
   k_wide_box<<<dim3((G * G + 255) / 256, p.n_out), 256, 0, s>>>(F, L, p.h, bbox_out, 0);
   e = cudaGetLastError();
