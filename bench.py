@@ -296,6 +296,68 @@ def uneven_optics():
                            source_spec=Source.dipole(0.9, 0.6, opening_deg=60).to_dict())
 
 
+def bench_next(args, torch, dev) -> dict:
+    """Device times of the callers either side of the imaging path, each on a
+    device-resident seeded input (1 warm-up call, then the mean of 3 timed
+    calls by CUDA events): the exposure volume through a resist film, a
+    dose-focus sweep, a threshold print through SOCS kernels and EUV imaging
+    with the multilayer blank."""
+    import dataclasses
+
+    import lithobat_b200 as lb
+    from lithobat_b200 import patterns, process
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {}
+    g = lb.GridConfig(n_pixels=N, pixel_size=PX)
+    mask = masks_c3_device(torch, 77, 1, dev)[0]
+    r = lb.ResistConfig()                      # 100 nm film, n 1.70, focus at mid-film
+    nz = int(round(r.thickness / g.dz))
+    ms = timed(lambda: process.exposure_volume(mask, optics_c3(), g, r))
+    out["exposure_volume"] = {
+        "workload": f"one {N}^2 clip at 1 nm, vector TE annular 0.5-0.9 (400 source points), "
+                    f"{g.n_z_slices} optical planes through a 100 nm film -> {nz} voxel planes at 2 nm",
+        "ms": ms, "voxel_planes_per_s": nz / (ms / 1000.0),
+        "api": "lithobat_b200.process.exposure_volume"}
+    foci, doses = [float(f) for f in np.linspace(-75.0, 75.0, 11)], [0.85, 0.9, 1.0, 1.1, 1.15]
+    ms = timed(lambda: process.dose_focus_images(mask, optics_c3(), g, doses, foci))
+    out["dose_focus"] = {
+        "workload": f"one {N}^2 clip, vector TE annular (400 source points), {len(foci)} foci x {len(doses)} doses",
+        "ms": ms, "images_per_s": len(foci) * len(doses) / (ms / 1000.0),
+        "api": "lithobat_b200.process.dose_focus_images"}
+    ko = ilt_optics()
+    k = lb.SOCSKernels.build(ko, g, tol=0.0, max_kernels=24)
+    tgt = torch.from_numpy(patterns.manhattan_clip(np.random.default_rng(78), N, PX).astype(np.float32)).to(dev)
+    ms = timed(lambda: process.print_image(tgt, ko, g, r, kernels=k))
+    out["print_socs"] = {
+        "workload": f"one {N}^2 clip, ArF immersion annular 0.5-0.8, SOCS K=24 (prebuilt), PEB sigma 20 nm, threshold",
+        "ms": ms, "prints_per_s": 1000.0 / ms, "api": "lithobat_b200.process.print_image(kernels=...)"}
+    n_ml, c_ml = 512, 64
+    gm = lb.GridConfig(n_pixels=n_ml, pixel_size=2e-9)
+    om = dataclasses.replace(uneven_optics(), mask_model="multilayer", chief_ray_deg=6.0, normalisation="clear")
+    rng = np.random.default_rng(79)
+    mm = torch.from_numpy(np.stack([patterns.manhattan_clip(rng, n_ml, 2e-9, n_rect=(20, 60), width_nm=(20.0, 80.0))
+                                    for _ in range(c_ml)]).astype(np.float32)).to(dev)
+    ms = timed(lambda: lb.compute_aerial_batch(mm, om, gm))
+    out["multilayer_euv"] = {
+        "workload": f"{c_ml} clips of {n_ml}^2 at 2 nm, EUV NA 0.33 dipole (204 source points), multilayer blank, "
+                    "chief ray 6 deg",
+        "ms": ms, "images_per_s": c_ml / (ms / 1000.0), "api": "lithobat_b200.compute_aerial_batch"}
+    out["parity"] = ("reference fixtures and the FP64 oracle at 1e-5: tests/test_gpu_process.py, "
+                     "tests/test_gpu_multilayer.py")
+    return out
+
+
 def bench_uneven(args, torch, dev, world, max_over_ranks, barrier) -> dict:
     """Images/s of the uneven batch: one CUDA-graph replay per batch, work-item
     sizes tuned per grid size on first use."""
@@ -874,6 +936,8 @@ def run_ours(args) -> None:
         line["ilt"] = bench_ilt(args, torch, dev, world, max_over_ranks, barrier)
     if "uneven" not in args.skip:
         line["uneven"] = bench_uneven(args, torch, dev, world, max_over_ranks, barrier)
+    if "next" not in args.skip and rank == 0:
+        line["next_rows"] = bench_next(args, torch, dev)
     if rank == 0 and world == 1 and not args.no_cpu:
         # one whole image of the timed batch through the FP64 reference
         # algorithm: the CPU baseline, and the FP64 reference of that image
@@ -918,7 +982,7 @@ def main():
     ap.add_argument("--images", type=int, default=IMAGES_PER_STEP,
                     help="images per step (a small value makes a profiling case)")
     ap.add_argument("--skip", default="", help="comma list of phases to skip: plain,e2e,levels,profile,cpu,c1,c2,ilt,iltplain,uneven,"
-                                        "unevenilt")
+                                        "unevenilt,next")
     ap.add_argument("--ilt-clips", type=int, default=ILT_CLIPS, help="clips per ILT step")
     ap.add_argument("--uneven-clips", type=int, default=256, help="clips in the uneven-size batch")
     ap.add_argument("--no-tune", action="store_true",

@@ -674,6 +674,15 @@ int litho_dose_stack(const float* raw_dev, const float* peak_dev, const float* c
 /* x = min(max(x, lo), hi) in place: the clip after PEB diffusion
  * (bake/peb.py:65-66). */
 int litho_clamp(float* x_dev, long long count, float lo, float hi, cudaStream_t stream);
+/* Depth interpolation of an exposure volume (develop/resist3d.py:176-183,
+ * np.interp per pixel along depth): out[v][p] = a[p] + w[v] (b[p] - a[p])
+ * with a = planes[k[2v]], b = planes[k[2v + 1]] for v < n_out. planes:
+ * [n_planes][npix] optical planes; k_dev: device int32 [n_out][2] plane
+ * indices (8-byte aligned); w_dev: device float [n_out]; out: [n_out][npix].
+ * A plane index outside [0, n_planes) leaves that voxel plane unwritten and
+ * sets LITHO_E_BAND in *status_dev (zero it before the call). */
+int litho_depth_interp(const float* planes_dev, int n_planes, long long npix, const int* k_dev, const float* w_dev,
+                       int n_out, float* out_dev, int* status_dev, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

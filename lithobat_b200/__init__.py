@@ -7,7 +7,7 @@ Drop-in replacements for ``litho_sim.expose.compute_aerial_image`` and
 
 from .aerial import (SOURCE_TILT_SIGN, LevelMasks, compute_aerial_batch, compute_aerial_image,
                      compute_aerial_planes, normalisation_scale)
-from .config import GridConfig, OpticsConfig
+from .config import GridConfig, OpticsConfig, ResistConfig
 from .hopkins import SOCSKernels
 from .source import Pole, Source, SourcePoints, build_source, source_points
 from . import patterns
@@ -16,5 +16,5 @@ from . import torch_ops  # registers torch.ops.litho.*
 __all__ = [
     "GridConfig", "LevelMasks", "OpticsConfig", "Pole", "SOCSKernels", "Source", "SourcePoints", "SOURCE_TILT_SIGN",
     "build_source", "compute_aerial_batch", "compute_aerial_image", "compute_aerial_planes",
-    "normalisation_scale", "source_points",
+    "normalisation_scale", "ResistConfig", "source_points",
 ]

@@ -174,6 +174,7 @@ def lib():
         "litho_ilt_update_sched": [vp, C.c_longlong, vp, f32, f32, f32, f32, vp, vp, vp, vp, vp],
         "litho_dose_stack": [vp, vp, vp, i32, i32, C.c_longlong, vp, i32, vp, vp],
         "litho_clamp": [vp, C.c_longlong, f32, f32, vp],
+        "litho_depth_interp": [vp, i32, C.c_longlong, vp, vp, i32, vp, vp, vp],
         "litho_uneven_group_workspace": [C.POINTER(UnevenGroup), C.POINTER(sz)],
         "litho_uneven_schedule": [C.POINTER(UnevenGroup), i32, vp, i32, C.POINTER(i32), C.POINTER(i32)],
         "litho_uneven_queue_workspace": [i32, C.POINTER(sz)],

@@ -19,6 +19,7 @@ POLARISATIONS = ("unpolarised", "x", "y", "te", "tm")
 NORMALISATIONS = ("peak", "clear", "none")
 MASK_MODELS = ("thin", "multilayer", "fdtd")
 SOURCE_TYPES = ("conventional", "annular", "monopole", "dipole", "quadrupole", "quasar", "cquad")
+FOCUS_REFERENCES = ("top", "mid", "bottom")
 
 TECH_NODE_PRESETS: dict[str, dict[str, Any]] = {
     "i-line": {"wavelength": 365e-9, "NA": 0.57},
@@ -125,20 +126,53 @@ class OpticsConfig:
 
 @dataclass
 class GridConfig:
-    """Square simulation grid."""
+    """Square simulation grid (core/config.py:720-759): n_pixels x n_pixels
+    pixels of pixel_size [m]; dz [m] the voxel height and n_z_slices the
+    optical planes of a depth-resolved exposure (:func:`exposure_volume`)."""
 
     n_pixels: int = 128
     pixel_size: float = 4e-9
+    dz: float = 2e-9
+    n_z_slices: int = 21
 
     def __post_init__(self) -> None:
         if isinstance(self.n_pixels, bool) or int(self.n_pixels) != self.n_pixels:
             raise TypeError(f"GridConfig.n_pixels must be an integer, got {self.n_pixels!r}")
         _bounded("GridConfig", "n_pixels", self.n_pixels, 1)
         _bounded("GridConfig", "pixel_size", self.pixel_size, 0.0, lo_open=True)
+        # dz = 0 is accepted: two-dimensional work never reads it
+        _bounded("GridConfig", "dz", self.dz, 0.0)
+        _bounded("GridConfig", "n_z_slices", self.n_z_slices, 1)
 
     @property
     def grid_size(self) -> float:
         return self.n_pixels * self.pixel_size
+
+
+@dataclass
+class ResistConfig:
+    """The resist parameters the imaging helpers read, with the names,
+    defaults and checks of core/config.py:ResistConfig (:491-718): the
+    threshold development (threshold, diffusion_sigma [m]) and the film a
+    depth-resolved exposure images through (thickness [m], n_resist, and
+    focus_reference, the depth OpticsConfig.defocus refers to). The
+    reference's own ResistConfig is accepted wherever this one is."""
+
+    threshold: float = 0.30
+    diffusion_sigma: float = 20e-9
+    thickness: float = 100e-9
+    n_resist: float = 1.70
+    focus_reference: str = "mid"
+
+    def __post_init__(self) -> None:
+        r = "ResistConfig"
+        _finite(r, "threshold", self.threshold)
+        if not 0.0 < self.threshold < 1.0:
+            raise ValueError(f"{r}.threshold must be in (0, 1), got {self.threshold:g}")
+        _bounded(r, "diffusion_sigma", self.diffusion_sigma, 0.0)
+        _bounded(r, "thickness", self.thickness, 0.0)
+        _bounded(r, "n_resist", self.n_resist, 0.0, lo_open=True)
+        _choice(r, "focus_reference", self.focus_reference, FOCUS_REFERENCES)
 
 
 @dataclass(frozen=True)

@@ -18,9 +18,10 @@
 //       image is real): a column stage over gy, then a row stage over gx that
 //       writes both images (k_wsyn_cols, k_wsyn_rows), then the
 //       normalisation of aerial_image.py:217-241.
-// Passes A and B, the adjoint passes and the synthesis run warp-per-line
-// register FFTs (fftwarp.cuh); the L x L transforms of J and g_L run in shared
-// memory (fftsmem.cuh). Every reduction has a fixed order, so results are
+// Passes A and B, the adjoint passes, the synthesis and the L x L transforms
+// of J and g_L (rows straight from global memory, columns through a padded
+// shared tile: k_wfft_rows, k_wfft_cols) run warp-per-line register FFTs
+// (fftwarp.cuh). Every reduction has a fixed order, so results are
 // deterministic.
 #include <algorithm>
 

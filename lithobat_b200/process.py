@@ -12,6 +12,10 @@
 * :func:`print_image` — ``opc/model.py:PrintModel.print`` (:228-245) after
   rasterisation: SOCS kernels when the optics allow them (``imaging="auto"``),
   the Abbe sum otherwise, then the dose and the threshold development.
+* :func:`exposure_volume` — ``develop/resist3d.py:exposure_volume``
+  (:113-193): the aerial image through the resist film, its optical planes
+  in one batched Abbe launch and the depth interpolation onto the voxel
+  planes on the device (``litho_depth_interp``).
 
 numpy in -> numpy float64 out; torch CUDA in -> torch float32 CUDA out.
 """
@@ -148,4 +152,90 @@ def print_image(mask, optics, grid, resist, dose: float = 1.0, imaging: str = "a
     return aerial, fld, level
 
 
-__all__ = ["dose_focus_images", "apply_peb", "develop_threshold", "print_image"]
+def focus_reference_depth(resist) -> float:
+    """Depth below the resist top that the optics' defocus refers to [m]
+    (develop/resist3d.py:focus_reference_depth, :66-81)."""
+    ref = resist.focus_reference
+    if ref == "top":
+        return 0.0
+    if ref == "mid":
+        return resist.thickness / 2.0
+    if ref == "bottom":
+        return resist.thickness
+    raise ValueError(f"focus_reference must be 'top', 'mid', or 'bottom', got '{ref}'")
+
+
+def effective_defocus(depth: float, optics, resist) -> float:
+    """Defocus [m] of the plane ``depth`` metres below the resist top, in the
+    immersion medium's units (develop/resist3d.py:effective_defocus, :84-110)."""
+    d_ref = focus_reference_depth(resist)
+    return optics.defocus - (depth - d_ref) * (optics.n_immersion / resist.n_resist)
+
+
+def depth_intervals(z_query, depths):
+    """For every query depth: (lower plane, upper plane, weight) of the linear
+    interpolation np.interp(z, depths, f) takes, in FP64: the end values
+    outside [depths[0], depths[-1]], else f[j] + w (f[j+1] - f[j]) on the
+    interval with depths[j] <= z < depths[j+1]."""
+    xp = np.asarray(depths, dtype=np.float64)
+    z = np.asarray(z_query, dtype=np.float64)
+    k = np.empty((z.size, 2), dtype=np.int32)
+    w = np.zeros(z.size, dtype=np.float64)
+    last = xp.size - 1
+    for i, zi in enumerate(z):
+        if last == 0 or zi <= xp[0]:
+            k[i] = (0, 0)
+        elif zi >= xp[last]:
+            k[i] = (last, last)
+        else:
+            j = int(np.searchsorted(xp, zi, side="right")) - 1
+            k[i] = (j, j + 1)
+            w[i] = (zi - xp[j]) / (xp[j + 1] - xp[j])
+    return k, w
+
+
+def exposure_volume(mask, optics, grid, resist, dose: float = 1.0):
+    """(intensity, z): the aerial image through the resist film
+    (develop/resist3d.py:exposure_volume, :113-193).
+
+    ``grid.n_z_slices`` optical planes (at least 2, at most the voxel count)
+    span the film top to bottom; each images at its effective defocus
+    converted to resist units with the resist as the image medium
+    (sin theta = NA / n_resist), all planes in one batched Abbe launch and
+    each normalised on its own. They are interpolated linearly in depth onto
+    the ``round(thickness / dz)`` voxel planes, iz = 0 at the bottom of the
+    film. intensity: (nz, N, N), numpy float64 for a numpy mask, torch float32
+    on the device for a torch CUDA mask; z: the voxel heights above the film
+    bottom [m], numpy float64. ``resist``: the reference's ResistConfig or
+    :class:`~lithobat_b200.config.ResistConfig` (thickness, n_resist,
+    focus_reference)."""
+    torch = nat.require_cuda()
+    L = nat.lib()
+    nz = max(int(round(resist.thickness / grid.dz)), 1)
+    n_slices = int(np.clip(grid.n_z_slices, 2, nz))
+    depths = np.linspace(0.0, resist.thickness, n_slices)
+    index_ratio = resist.n_resist / optics.n_immersion
+    planes = [(effective_defocus(float(d), optics, resist) * index_ratio, resist.n_resist) for d in depths]
+    n = int(grid.n_pixels)
+    md = _as_device_masks(torch, mask, n)
+    if md.shape[0] != 1:
+        raise ValueError("exposure_volume takes one mask")
+    img, _pk, _cl = compute_aerial_batch(md, optics, grid, planes, dose, False, check=True)
+    stack = img[0].contiguous()                      # (n_slices, N, N)
+    dev = stack.device
+    z_depth = ((np.arange(nz) + 0.5) * grid.dz)[::-1]   # depth below the top, bottom voxel first
+    k, w = depth_intervals(z_depth, depths)
+    k_d = torch.from_numpy(k.reshape(-1)).to(dev)
+    w_d = torch.from_numpy(w.astype(np.float32)).to(dev)
+    status = torch.zeros((1,), dtype=torch.int32, device=dev)
+    out = torch.empty((nz, n, n), dtype=torch.float32, device=dev)
+    nat.check("litho_depth_interp", L.litho_depth_interp(
+        stack.data_ptr(), n_slices, n * n, k_d.data_ptr(), w_d.data_ptr(), nz, out.data_ptr(), status.data_ptr(),
+        nat.stream_ptr(torch, dev)))
+    nat.check("litho_depth_interp", int(status.item()))
+    z = (np.arange(nz) + 0.5) * grid.dz
+    return (out if _is_torch(mask) else out.cpu().numpy().astype(np.float64)), np.asarray(z, dtype=np.float64)
+
+
+__all__ = ["dose_focus_images", "apply_peb", "develop_threshold", "print_image", "focus_reference_depth",
+           "effective_defocus", "depth_intervals", "exposure_volume"]

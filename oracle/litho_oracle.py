@@ -718,6 +718,42 @@ def dose_focus_images(mask, optics, grid, doses, defoci_nm, normalisation="clear
     return np.array(out)
 
 
+def focus_reference_depth(resist):
+    """develop/resist3d.py:66-81 — the depth the optics' defocus refers to."""
+    ref = resist.focus_reference
+    if ref == "top":
+        return 0.0
+    if ref == "mid":
+        return resist.thickness / 2.0
+    if ref == "bottom":
+        return resist.thickness
+    raise ValueError(f"focus_reference must be 'top', 'mid', or 'bottom', got '{ref}'")
+
+
+def effective_defocus(depth, optics, resist):
+    """develop/resist3d.py:84-110."""
+    return optics.defocus - (depth - focus_reference_depth(resist)) * (optics.n_immersion / resist.n_resist)
+
+
+def exposure_volume(mask, optics, grid, resist, dose=1.0):
+    """develop/resist3d.py:113-193 — n_slices optical planes through the film
+    (resist as the image medium, defocus in resist units), then np.interp per
+    pixel onto the voxel planes, iz = 0 at the bottom. (intensity, z)."""
+    nz = max(int(round(resist.thickness / grid.dz)), 1)
+    n_slices = int(np.clip(grid.n_z_slices, 2, nz))
+    depths = np.linspace(0.0, resist.thickness, n_slices)
+    ratio = resist.n_resist / optics.n_immersion
+    planes = compute_aerial_planes(mask, optics, grid,
+                                   [(effective_defocus(float(d), optics, resist) * ratio, resist.n_resist)
+                                    for d in depths], dose=dose)
+    zq = ((np.arange(nz) + 0.5) * grid.dz)[::-1]
+    flat = planes.reshape(n_slices, -1)
+    out = np.empty((nz, flat.shape[1]), dtype=np.float64)
+    for k in range(flat.shape[1]):
+        out[:, k] = np.interp(zq, depths, flat[:, k])
+    return out.reshape(nz, grid.n_pixels, grid.n_pixels), (np.arange(nz) + 0.5) * grid.dz
+
+
 def objective(k: SOCS, target, mask, scale, level, sigma_px, sign, steepness,
               weight_tv=0.0, weight_discrete=0.0):
     """opc/ilt.py:311-360 — (cost, grad, signed, pattern_error)."""

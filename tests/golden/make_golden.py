@@ -357,6 +357,34 @@ def next_rows():
          doses=np.array(doses), stack=np.array(stack))
 
 
+def volume():
+    """The depth-resolved aerial image through a resist film
+    (develop/resist3d.py:exposure_volume): a scalar and a vector case."""
+    _import_reference()
+    from litho_sim.core.config import GridConfig, OpticsConfig, ResistConfig
+    from litho_sim.develop.resist3d import exposure_volume
+    cases = [
+        ("volume_scalar_64",
+         OpticsConfig(NA=0.93, source_type="annular", sigma_inner=0.5, sigma_outer=0.85, source_grid=11,
+                      defocus=20e-9),
+         GridConfig(n_pixels=64, pixel_size=4e-9, dz=6e-9, n_z_slices=5),
+         ResistConfig(thickness=60e-9, focus_reference="bottom"), 43, 1.0),
+        ("volume_vector_64",
+         OpticsConfig(wavelength=193e-9, NA=1.35, n_immersion=1.44, imaging_model="vector", polarisation="te",
+                      source_type="annular", sigma_inner=0.5, sigma_outer=0.9, source_grid=11,
+                      normalisation="clear", defocus=-15e-9),
+         GridConfig(n_pixels=64, pixel_size=4e-9, dz=4e-9, n_z_slices=7),
+         ResistConfig(thickness=50e-9, n_resist=1.72, focus_reference="mid"), 44, 1.3),
+    ]
+    for name, o, g, r, seed, dose in cases:
+        m = manhattan_clip(np.random.default_rng(seed), g.n_pixels, g.pixel_size, n_rect=(4, 10),
+                           width_nm=(40, 160))
+        vol, z = exposure_volume(m, o, g, r, dose=dose)
+        save(name, optics=o, grid=g, mask=m.astype(np.uint8), dz=np.array(g.dz), n_z_slices=np.array(g.n_z_slices),
+             thickness=np.array(r.thickness), n_resist=np.array(r.n_resist),
+             focus_reference=np.array(r.focus_reference), dose=np.array(dose), volume=vol, z=z)
+
+
 def multilayer():
     """The EUV blank as a Bragg mirror (mask_model="multilayer",
     expose/m3d/provider.py:190-295): images, the reflection table, the
@@ -428,5 +456,7 @@ if __name__ == "__main__":
         wide()
     elif sys.argv[1:] == ["next"]:
         next_rows()
+    elif sys.argv[1:] == ["volume"]:
+        volume()
     else:
         main()

@@ -79,3 +79,40 @@ def test_print_image_threshold_model(lb):
     assert float(np.abs(a_abbe - ref_aerial).max() / np.abs(ref_aerial).max()) <= TOL
     assert float(np.abs(a_socs - a_abbe).max() / np.abs(a_abbe).max()) <= TOL
     np.testing.assert_allclose(f_abbe, O.apply_peb(ref_aerial, 10e-9, 4e-9), rtol=0, atol=1e-5)
+
+
+def _volume_inputs(lb, name):
+    a, od, gd = load_golden(name)
+    g = lb.GridConfig(**gd, dz=float(a["dz"]), n_z_slices=int(a["n_z_slices"]))
+    r = lb.config.ResistConfig(thickness=float(a["thickness"]), n_resist=float(a["n_resist"]),
+                               focus_reference=str(a["focus_reference"]))
+    return a, _optics(lb, od), g, r
+
+
+@pytest.mark.parametrize("name", ["volume_scalar_64", "volume_vector_64"])
+def test_exposure_volume_matches_reference(lb, name):
+    from lithobat_b200.process import exposure_volume
+    a, o, g, r = _volume_inputs(lb, name)
+    vol, z = exposure_volume(a["mask"].astype(np.float64), o, g, r, dose=float(a["dose"]))
+    assert vol.shape == a["volume"].shape and vol.dtype == np.float64
+    np.testing.assert_array_equal(z, a["z"])
+    assert float(np.abs(vol - a["volume"]).max() / np.abs(a["volume"]).max()) <= TOL
+
+
+def test_exposure_volume_512_against_oracle(lb):
+    """A 512² clip through a 100 nm film at 2 nm voxels (50 voxel planes from
+    21 optical planes, the reference's defaults), on a device mask: float32
+    CUDA result against the oracle's FP64 volume."""
+    import torch
+    from lithobat_b200.process import exposure_volume
+    g = lb.GridConfig(n_pixels=512, pixel_size=2e-9)
+    o = lb.OpticsConfig(NA=1.35, n_immersion=1.44, source_type="annular", sigma_inner=0.5, sigma_outer=0.9,
+                        source_grid=9, defocus=25e-9)
+    r = lb.config.ResistConfig()
+    mask = lb.patterns.lines_and_spaces(512, 2e-9, 90e-9, 45e-9)
+    vol, z = exposure_volume(torch.from_numpy(mask).cuda(), o, g, r)
+    assert vol.is_cuda and vol.dtype == torch.float32 and tuple(vol.shape) == (50, 512, 512)
+    ref, zr = O.exposure_volume(mask, o, g, r)
+    np.testing.assert_array_equal(z, zr)
+    got = vol.cpu().numpy().astype(np.float64)
+    assert float(np.abs(got - ref).max() / np.abs(ref).max()) <= TOL

@@ -125,3 +125,39 @@ def test_level_masks_factor_and_expand():
         lb.LevelMasks.from_masks(rng.random((1, 32, 32)), max_levels=16)
     with pytest.raises(ValueError):
         lb.LevelMasks(idx[0], lv[None])
+
+
+def test_depth_intervals_follow_np_interp():
+    """The host-side interval and weight of every voxel plane reproduce
+    np.interp (develop/resist3d.py:176-183), ends and interior nodes included."""
+    from lithobat_b200.process import depth_intervals
+    rng = np.random.default_rng(3)
+    for n_slices in (1, 2, 5, 21):
+        depths = np.linspace(0.0, 80e-9, n_slices)
+        z = np.concatenate([rng.uniform(-10e-9, 90e-9, 40), depths, [0.0, 80e-9]])
+        k, w = depth_intervals(z, depths)
+        f = rng.standard_normal((n_slices, 7))
+        got = f[k[:, 0]] + w[:, None] * (f[k[:, 1]] - f[k[:, 0]])
+        want = np.stack([np.interp(z, depths, f[:, j]) for j in range(7)], axis=1)
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-12)
+        assert k.min() >= 0 and k.max() <= n_slices - 1
+
+
+def test_focus_reference_and_effective_defocus():
+    from types import SimpleNamespace
+
+    from lithobat_b200.config import ResistConfig
+    from lithobat_b200.process import effective_defocus, focus_reference_depth
+    o = SimpleNamespace(defocus=10e-9, n_immersion=1.44)
+    for ref, d_ref in (("top", 0.0), ("mid", 50e-9), ("bottom", 100e-9)):
+        r = ResistConfig(thickness=100e-9, n_resist=1.7, focus_reference=ref)
+        assert focus_reference_depth(r) == d_ref
+        assert effective_defocus(30e-9, o, r) == 10e-9 - (30e-9 - d_ref) * (1.44 / 1.7)
+    with pytest.raises(ValueError, match="focus_reference must be 'top', 'mid', or 'bottom'"):
+        focus_reference_depth(SimpleNamespace(focus_reference="centre", thickness=1e-7))
+    with pytest.raises(ValueError, match="ResistConfig.focus_reference"):
+        ResistConfig(focus_reference="centre")
+    with pytest.raises(ValueError, match="ResistConfig.threshold"):
+        ResistConfig(threshold=1.0)
+    with pytest.raises(ValueError, match="GridConfig.n_z_slices"):
+        GridConfig(n_z_slices=0)

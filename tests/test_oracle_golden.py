@@ -161,3 +161,21 @@ def test_dose_focus_images_match_reference():
     st = O.dose_focus_images(a["mask"].astype(np.float64), o, g, list(a["doses"]), list(a["defoci"]),
                              normalisation=None)
     np.testing.assert_allclose(st, a["stack"], rtol=0, atol=1e-12 * float(np.abs(a["stack"]).max()))
+
+
+def _volume_case(name):
+    from types import SimpleNamespace
+    a, od, gd = load_golden(name)
+    o = ns_optics(od)
+    g = SimpleNamespace(**gd, dz=float(a["dz"]), n_z_slices=int(a["n_z_slices"]))
+    r = SimpleNamespace(thickness=float(a["thickness"]), n_resist=float(a["n_resist"]),
+                        focus_reference=str(a["focus_reference"]))
+    return a, o, g, r
+
+
+@pytest.mark.parametrize("name", ["volume_scalar_64", "volume_vector_64"])
+def test_exposure_volume_matches_reference(name):
+    a, o, g, r = _volume_case(name)
+    vol, z = O.exposure_volume(a["mask"].astype(np.float64), o, g, r, dose=float(a["dose"]))
+    np.testing.assert_array_equal(z, a["z"])
+    np.testing.assert_allclose(vol, a["volume"], rtol=0, atol=1e-12 * float(np.abs(a["volume"]).max()))
