@@ -331,11 +331,11 @@ __global__ void k_ilt_objective(const float* __restrict__ img, const float* __re
   auto one = [&](long long i) -> void {
     const float fld = img[i] * scale;
     const float s = sign * (fld - level);
-    const float z = sigmoid_clipped(a * s);
+    const float z = objective_sigmoid(a * s);
     const float t = target[i];
     const float r = z - t;
     cost += (double)r * (double)r;
-    dfield[i] = sign * (inv_npix2 * r * (a * z * (1.0f - z)));
+    dfield[i] = (sign * inv_npix2 * a) * r * (z * (1.0f - z));
     if (signed_out) signed_out[i] = s;
     perr += ((s > 0.f) != (t > 0.5f)) ? 1u : 0u;
   };

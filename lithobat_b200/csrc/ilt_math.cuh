@@ -15,21 +15,36 @@ __device__ __forceinline__ float sigmoid_clipped(float s) {
   return __frcp_rn(1.0f + expf(-s));
 }
 
+// The resist relaxation of the objective, sigmoid(s) clipped as above, with
+// the hardware exponential and reciprocal (__expf, __fdividef). The
+// exponential's relative error grows with |s| (documented bound 2 +
+// 1.173 |s| ulps), so z is a few ulps from the correctly rounded value near
+// the threshold, where cost and dJ/dfield take their size, and up to ~70 ulps
+// at the clip, where z (1 - z) < 1e-26 and r = z - t is set by the target.
+// The mask (sigmoid_clipped), whose value feeds Adam's sign-like first
+// steps, keeps the correctly rounded form. 1 + e^60 < 2^126, the bound below
+// which __fdividef is a true quotient.
+__device__ __forceinline__ float objective_sigmoid(float s) {
+  s = fminf(fmaxf(s, -60.f), 60.f);
+  return __fdividef(1.0f, 1.0f + __expf(-s));
+}
+
 // One pixel of the relaxed resist objective (opc/ilt.py:_Objective, :313-336)
 // for image value img and target t: signed = sign (scale img - level),
 // z = sigmoid(a signed), r = z - t; accumulates r^2 into cost and the pattern
 // error into perr; returns dJ/dfield = sign (2 / npix) r a z (1 - z) (the
-// factor 2 / npix as inv_npix2); *signed_out receives signed.
+// factor 2 / npix as inv_npix2; sign (2 / npix) a is one loop-invariant
+// product); *signed_out receives signed.
 __device__ __forceinline__ float ilt_objective_pixel(float img, float t, float scale, float level, float sign,
                                                      float a, float inv_npix2, float& cost, unsigned int& perr,
                                                      float* signed_out) {
   const float s = sign * (img * scale - level);
-  const float z = sigmoid_clipped(a * s);
+  const float z = objective_sigmoid(a * s);
   const float r = z - t;
   cost = fmaf(r, r, cost);
   perr += ((s > 0.f) != (t > 0.5f)) ? 1u : 0u;
   *signed_out = s;
-  return sign * (inv_npix2 * r * (a * z * (1.0f - z)));
+  return (sign * inv_npix2 * a) * r * (z * (1.0f - z));
 }
 
 // Operands of the objective applied inside the image synthesis.
