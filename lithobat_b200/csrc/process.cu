@@ -12,6 +12,9 @@
 
 namespace litho {
 
+// One (focus, dose) plane per blockIdx.y; VEC: four pixels per thread per
+// iteration (npix % 4 == 0 and 16-byte aligned planes).
+template <bool VEC>
 __global__ void k_dose_stack(const float* __restrict__ raw, const float* __restrict__ peak,
                              const float* __restrict__ clear, int mode, long long npix,
                              const float* __restrict__ doses, int n_doses, float* __restrict__ out) {
@@ -22,9 +25,17 @@ __global__ void k_dose_stack(const float* __restrict__ raw, const float* __restr
   if (mode == 2) s = clear[f] > 0.f ? dose / clear[f] : dose;
   const float* src = raw + (size_t)f * npix;
   float* dst = out + ((size_t)f * n_doses + d) * npix;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < npix;
-       i += (long long)gridDim.x * blockDim.x)
-    dst[i] = src[i] * s;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (VEC) {
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+    float4* d4 = reinterpret_cast<float4*>(dst);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (npix >> 2); i += stride) {
+      const float4 v = s4[i];
+      __stcs(d4 + i, make_float4(v.x * s, v.y * s, v.z * s, v.w * s));
+    }
+  } else {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < npix; i += stride) dst[i] = src[i] * s;
+  }
 }
 
 __global__ void k_clamp(float* __restrict__ x, long long count, float lo, float hi) {
@@ -59,8 +70,8 @@ __global__ void k_depth_interp(const float* __restrict__ planes, int n_planes, l
     float4* d4 = reinterpret_cast<float4*>(dst);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (npix >> 2); i += stride) {
       const float4 x = a4[i], y = b4[i];
-      d4[i] = make_float4(fmaf(wv, y.x - x.x, x.x), fmaf(wv, y.y - x.y, x.y), fmaf(wv, y.z - x.z, x.z),
-                          fmaf(wv, y.w - x.w, x.w));
+      __stcs(d4 + i, make_float4(fmaf(wv, y.x - x.x, x.x), fmaf(wv, y.y - x.y, x.y), fmaf(wv, y.z - x.z, x.z),
+                                 fmaf(wv, y.w - x.w, x.w)));
     }
   } else {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < npix; i += stride)
@@ -77,10 +88,20 @@ extern "C" int litho_dose_stack(const float* raw, const float* peak, const float
   if (!raw || !doses || !out || (mode == 1 && !peak) || (mode == 2 && !clear)) return LITHO_E_NULL;
   if (n_planes < 1 || n_doses < 1 || npix < 1 || (long long)n_planes * n_doses > 65535 || mode < 0 || mode > 2)
     return LITHO_E_SIZE;
-  long long b = (npix + 255) / 256;
-  if (b > 1024) b = 1024;
-  k_dose_stack<<<dim3((unsigned)b, n_planes * n_doses), 256, 0, s>>>(raw, peak, clear, mode, npix, doses, n_doses,
-                                                                      out);
+  const bool vec = (npix & 3) == 0 && !((uintptr_t)raw & 15) && !((uintptr_t)out & 15);
+  const int planes = n_planes * n_doses;
+  long long b = ((vec ? npix >> 2 : npix) + 255) / 256;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (sms <= 0) sms = 148;
+  const long long cap = (8LL * sms + planes - 1) / planes;   // about 8 blocks per SM over all planes
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  if (vec)
+    k_dose_stack<true><<<dim3((unsigned)b, planes), 256, 0, s>>>(raw, peak, clear, mode, npix, doses, n_doses, out);
+  else
+    k_dose_stack<false><<<dim3((unsigned)b, planes), 256, 0, s>>>(raw, peak, clear, mode, npix, doses, n_doses, out);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? LITHO_OK : (int)e;
 }

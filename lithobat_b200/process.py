@@ -178,23 +178,23 @@ def depth_intervals(z_query, depths):
     outside [depths[0], depths[-1]], else f[j] + w (f[j+1] - f[j]) on the
     interval with depths[j] <= z < depths[j+1]."""
     xp = np.asarray(depths, dtype=np.float64)
-    z = np.asarray(z_query, dtype=np.float64)
-    k = np.empty((z.size, 2), dtype=np.int32)
-    w = np.zeros(z.size, dtype=np.float64)
+    z = np.asarray(z_query, dtype=np.float64).reshape(-1)
     last = xp.size - 1
-    for i, zi in enumerate(z):
-        if last == 0 or zi <= xp[0]:
-            k[i] = (0, 0)
-        elif zi >= xp[last]:
-            k[i] = (last, last)
-        else:
-            j = int(np.searchsorted(xp, zi, side="right")) - 1
-            k[i] = (j, j + 1)
-            w[i] = (zi - xp[j]) / (xp[j + 1] - xp[j])
+    k = np.zeros((z.size, 2), dtype=np.int32)
+    w = np.zeros(z.size, dtype=np.float64)
+    if last == 0:
+        return k, w
+    hi = z >= xp[last]
+    inside = (z > xp[0]) & ~hi
+    j = np.clip(np.searchsorted(xp, z, side="right") - 1, 0, last - 1)
+    k[hi] = last
+    k[inside, 0] = j[inside]
+    k[inside, 1] = j[inside] + 1
+    w[inside] = (z[inside] - xp[j[inside]]) / (xp[j[inside] + 1] - xp[j[inside]])
     return k, w
 
 
-def exposure_volume(mask, optics, grid, resist, dose: float = 1.0):
+def exposure_volume(mask, optics, grid, resist, dose: float = 1.0, check: bool | None = None):
     """(intensity, z): the aerial image through the resist film
     (develop/resist3d.py:exposure_volume, :113-193).
 
@@ -208,7 +208,10 @@ def exposure_volume(mask, optics, grid, resist, dose: float = 1.0):
     on the device for a torch CUDA mask; z: the voxel heights above the film
     bottom [m], numpy float64. ``resist``: the reference's ResistConfig or
     :class:`~lithobat_b200.config.ResistConfig` (thickness, n_resist,
-    focus_reference)."""
+    focus_reference). check: synchronise and raise ``LithoError`` if a
+    device status word reports a failure; default: for host (numpy) masks,
+    whose result is read on the host anyway (device masks keep the call
+    asynchronous, as :func:`~lithobat_b200.aerial.compute_aerial_batch`)."""
     torch = nat.require_cuda()
     L = nat.lib()
     nz = max(int(round(resist.thickness / grid.dz)), 1)
@@ -220,7 +223,9 @@ def exposure_volume(mask, optics, grid, resist, dose: float = 1.0):
     md = _as_device_masks(torch, mask, n)
     if md.shape[0] != 1:
         raise ValueError("exposure_volume takes one mask")
-    img, _pk, _cl = compute_aerial_batch(md, optics, grid, planes, dose, False, check=True)
+    if check is None:
+        check = not _is_torch(mask)
+    img, _pk, _cl = compute_aerial_batch(md, optics, grid, planes, dose, False, check=check)
     stack = img[0].contiguous()                      # (n_slices, N, N)
     dev = stack.device
     z_depth = ((np.arange(nz) + 0.5) * grid.dz)[::-1]   # depth below the top, bottom voxel first
@@ -232,7 +237,8 @@ def exposure_volume(mask, optics, grid, resist, dose: float = 1.0):
     nat.check("litho_depth_interp", L.litho_depth_interp(
         stack.data_ptr(), n_slices, n * n, k_d.data_ptr(), w_d.data_ptr(), nz, out.data_ptr(), status.data_ptr(),
         nat.stream_ptr(torch, dev)))
-    nat.check("litho_depth_interp", int(status.item()))
+    if check:
+        nat.check("litho_depth_interp", int(status.item()))
     z = (np.arange(nz) + 0.5) * grid.dz
     return (out if _is_torch(mask) else out.cpu().numpy().astype(np.float64)), np.asarray(z, dtype=np.float64)
 

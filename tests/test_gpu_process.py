@@ -110,7 +110,7 @@ def test_exposure_volume_512_against_oracle(lb):
                         source_grid=9, defocus=25e-9)
     r = lb.config.ResistConfig()
     mask = lb.patterns.lines_and_spaces(512, 2e-9, 90e-9, 45e-9)
-    vol, z = exposure_volume(torch.from_numpy(mask).cuda(), o, g, r)
+    vol, z = exposure_volume(torch.from_numpy(mask).cuda(), o, g, r, check=True)
     assert vol.is_cuda and vol.dtype == torch.float32 and tuple(vol.shape) == (50, 512, 512)
     ref, zr = O.exposure_volume(mask, o, g, r)
     np.testing.assert_array_equal(z, zr)
