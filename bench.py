@@ -226,6 +226,14 @@ def bench_ilt(args, torch, dev, world, max_over_ranks, barrier) -> dict:
     tp = torch.from_numpy(targets).pin_memory()
     hp = torch.from_numpy(theta).pin_memory()
     out = torch.empty_like(hp).pin_memory()
+    # one untimed pass of the same calls first (a batch built, stepped through
+    # its graph recording and released), so the timed pass meets a warm
+    # process as the other legs do: kernels loaded, allocator pools in place
+    wb = ilt.IltBatch(k, tp.to(dev, non_blocking=True), hp.to(dev, non_blocking=True), params)
+    for _ in range(max(args.warmup, 3)):
+        wb.run(1)
+    float(wb.cost.sum())
+    del wb
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e0.record()
