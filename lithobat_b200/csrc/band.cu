@@ -180,7 +180,7 @@ k_row_band_tma(const void* __restrict__ in, int n_rows, int rows_per_clip, int n
 // R1(k) = (Z(k) + conj Z(-k)) / 2, R2(k) = (Z(k) - conj Z(-k)) / 2i.
 // ---------------------------------------------------------------------------
 struct BandGeo {
-  int M, Lp, P, q, ld, Bm, npass, warps;
+  int M, Lp, P, q, ld, gp, Bm, npass, warps;
   bool tb_smem;                                    // per-pass twiddle table in shared memory
   size_t y_per_warp, z_per_warp, off_y, off_z, total;
 };
@@ -192,10 +192,11 @@ __host__ __device__ inline BandGeo band_geo(int n, int bm, int warps) {
   g.P = 32 / g.Lp;
   g.q = g.M / g.Lp;
   g.ld = g.M + 1;
+  g.gp = band_group_pitch(g.M);
   g.Bm = 2 * bm + 1;
   g.npass = (g.Bm + 31) >> 5;
   g.warps = warps;
-  g.y_per_warp = (size_t)g.P * 32 * g.ld;          // float2
+  g.y_per_warp = (size_t)g.P * g.gp;               // float2
   g.z_per_warp = (size_t)g.P * g.npass * 32;       // float2
   g.tb_smem = (size_t)g.npass * 32 * g.M * 8 <= 64 * 1024;
   g.off_y = g.tb_smem ? (size_t)g.npass * 32 * g.M * 8 : 0;   // after the twiddle table
@@ -227,7 +228,8 @@ k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int bm, 
   const int Bm = g.Bm, npass = g.npass;
   float2* TB = bsm;                                        // [pass][kp][b] = w^(-k b) or 0
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float2* Y = bsm + g.off_y / 8 + warp * g.y_per_warp;   // [group][kp][b]
+  constexpr int GP = band_group_pitch(M);
+  float2* Y = bsm + g.off_y / 8 + warp * g.y_per_warp;   // [group (pitch GP)][kp (pitch LD)][b]
   float2* Z = bsm + g.off_z / 8 + warp * g.z_per_warp;   // [group][k + bm] (real pairs)
   if (TBS) {
     for (int j = threadIdx.x; j < npass * 32 * M; j += blockDim.x) {
@@ -291,7 +293,7 @@ k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int bm, 
           }
           fft_reg<32, -1>(v);
         }
-        float2* yr = Y + pg * 32 * LD + b;
+        float2* yr = Y + pg * GP + b;
         if (TBS) {
           const float2* tb = TB + p * 32 * M + b;
 #pragma unroll
@@ -308,7 +310,7 @@ k_band_rows(const void* __restrict__ in, int n_rows, int rows_per_clip, int bm, 
       const int k = band_k(lane, p, bm);
 #pragma unroll
       for (int r = 0; r < P; ++r) {
-        const float2* yr = Y + (r * 32 + lane) * LD;
+        const float2* yr = Y + r * GP + lane * LD;
         float2 s0 = make_float2(0.f, 0.f), s1 = make_float2(0.f, 0.f);
 #pragma unroll
         for (int j = 0; j + 1 < M; j += 2) {

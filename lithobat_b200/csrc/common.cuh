@@ -212,6 +212,13 @@ __device__ __forceinline__ bool bin_valid(int k, int n) { return k >= -(n / 2) &
 
 __host__ __device__ __forceinline__ int64_t align16(int64_t x) { return (x + 15) & ~int64_t(15); }
 
+// Pitch (float2) of one row group's [kp][b] block (32 x (M + 1)) in the
+// transpose-sum stage of the band DFTs (band.cu, rows.cu). A half-warp's
+// 8-byte stores span 16 lanes = 16 / Lp row groups (Lp = min(M, 32) lanes
+// each); the Lp mod 16 pad starts those groups 2 Lp banks apart, so they
+// no longer land on the same banks (a whole multiple of 32 banks apart).
+__host__ __device__ constexpr int band_group_pitch(int M) { return 32 * (M + 1) + ((M < 32 ? M : 32) % 16); }
+
 // ---------------------------------------------------------------------------
 // TMA bulk copies (cp.async.bulk) completing on shared-memory mbarriers.
 // Every wait is bounded by a clock budget; a wait that gives up reports it

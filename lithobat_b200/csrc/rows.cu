@@ -58,10 +58,10 @@ __host__ __device__ inline SynthSmem synth_smem(int n, int g0, bool cols_ahead =
 // operands end with the G x G box, an odd multiple of 8 bytes for odd G).
 __host__ __device__ inline size_t obj_stage_off(const SynthSmem& s) { return (s.total + 127) & ~(size_t)127; }
 // Floats of one warp's stage in the band form: the 2 P target rows, or the
-// band DFT's transpose of P row pairs (P x 32 x (M + 1) complex), whichever
-// is larger, in 128-byte units.
+// band DFT's transpose of P row pairs (P groups of band_group_pitch(M)
+// complex), whichever is larger, in 128-byte units.
 __host__ __device__ inline int band_stage_floats(int M, int P) {
-  const int y = P * 32 * (M + 1) * 2;
+  const int y = P * band_group_pitch(M) * 2;
   const int f = y > kSyObjStage ? y : kSyObjStage;
   return (f + 31) & ~31;
 }
@@ -266,17 +266,17 @@ k_synth_pairs(const float2* __restrict__ Bbox, int g0, int n, const float2* __re
           // rows y1 + i y2 of this pair group: X_b(kp) over a, then per pass
           // the transpose-sum U(k) = sum_b w^(-k b) X_b(k mod 32)
           fft_reg<32, -1>(Q);
-          float2* Y = reinterpret_cast<float2*>(tg);     // [pair group][kp][b], pitch M + 1
-          const int LD = M + 1;
+          float2* Y = reinterpret_cast<float2*>(tg);     // [pair group (pitch GP)][kp (pitch M + 1)][b]
+          const int LD = M + 1, GP = band_group_pitch(M);
           for (int p = 0; p < npass; ++p) {
-            float2* yr = Y + pg * 32 * LD + b;
+            float2* yr = Y + pg * GP + b;
             const float2* tb = BTB + p * 32 * M + b;
 #pragma unroll
             for (int kp = 0; kp < 32; ++kp) yr[kp * LD] = cmul(Q[kp], tb[kp * M]);
             __syncwarp();
             const int k = -kb + ((lane + kb) & 31) + 32 * p;
             for (int r = 0; r < L.P; ++r) {
-              const float2* yq = Y + (r * 32 + lane) * LD;
+              const float2* yq = Y + r * GP + lane * LD;
               float2 s0 = make_float2(0.f, 0.f), s1 = make_float2(0.f, 0.f);
               for (int j = 0; j + 1 < M; j += 2) {
                 s0 = cadd(s0, yq[j]);
