@@ -753,7 +753,7 @@ def run_ours(args) -> None:
     out = torch.empty((B, N, N), dtype=torch.float32, device=dev)
     peak = torch.empty((B,), dtype=torch.float32, device=dev)
     # twiddles, band rows, band columns, coarse, reduce, then the synthesis: on the tensor cores
-    # (enough 128 x 256 output tiles for about 16 per SM) P planes, Q planes, peak pass, peak,
+    # (enough 128 x 256 output tiles for about 8 per SM) P planes, Q planes, peak pass, peak,
     # writing pass, peak; otherwise column stage, peak pass, peak, writing pass, peak
     tensor_synth = aerial.engine_info(pd)["synthesis"] == "tensor_cores"
     launches_per_step = 5 + (6 if tensor_synth else 5)

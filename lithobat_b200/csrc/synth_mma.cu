@@ -67,10 +67,11 @@ bool synth_mma_ok(int n, int g0) {
 }
 
 // Worth it when there are enough 128 x 256 output tiles to keep every SM's
-// MMA and drain pipeline busy (about 16 per SM); smaller batches use the
-// pair synthesis, whose fixed costs are lower.
+// MMA and drain pipeline busy (about 8 per SM: 1024 images of 256^2 gain
+// 9 % over the pair synthesis; 64 of 512^2, 3.5 tiles per SM, do not);
+// smaller batches use the pair synthesis, whose fixed costs are lower.
 bool synth_mma_pick(int n_out, int n, int g0) {
-  return synth_mma_ok(n, g0) && (int64_t)n_out * (n / kSmNT) * (n / kSmMT) >= 16 * 148;
+  return synth_mma_ok(n, g0) && (int64_t)n_out * (n / kSmNT) * (n / kSmMT) >= 8 * 148;
 }
 
 // P planes, then Q planes, then the per-output inverse scales.
