@@ -456,9 +456,12 @@ static size_t coarse64_smem() {
 // ---------------------------------------------------------------------------
 // 4. per output: J = sum of its items' partials (in item order), then
 //    B(gx, gy) = (1/L^2) sum_{u,v} J(v, u) exp(-2 pi i (gx u + gy v) / L).
-//    One block of 1024 threads per output; L is a power of two.
+//    Blocks of kReduceThreads per output (grid.y of them split its box rows);
+//    L is a power of two.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024)
+constexpr int kReduceThreads = 256;
+
+__global__ void __launch_bounds__(kReduceThreads)
 k_coarse_reduce(const int32_t* __restrict__ out_items, const float* __restrict__ partial, int L, int h,
                 float2* __restrict__ Bout) {
   extern __shared__ float sm_f[];
@@ -508,11 +511,12 @@ k_coarse_reduce(const int32_t* __restrict__ out_items, const float* __restrict__
   }
 }
 
-// Blocks per output of k_coarse_reduce: split the box rows when the outputs
-// alone would leave most SMs idle.
+// Blocks per output of k_coarse_reduce: split the box rows until there are
+// about 8 blocks per SM (each block of a split output sums the output's
+// partials again, in the same order, and forms its share of the box rows).
 static unsigned reduce_split(int n_out, int G) {
   int s = 1;
-  while (s < 8 && (long long)n_out * s < 2 * 148 && s * 2 <= G) s *= 2;
+  while (s < 8 && (long long)n_out * s < 8 * 148 && s * 2 <= G) s *= 2;
   return (unsigned)s;
 }
 
@@ -832,7 +836,8 @@ static int abbe_run(const LithoAbbePlan* plan, const void* blob, const void* tab
   mark(4);
   const size_t sm_red = (size_t)p.L * p.L * 4 + (size_t)p.L * G * 8 + (size_t)p.L * 8;
   cudaFuncSetAttribute(k_coarse_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_red);
-  k_coarse_reduce<<<dim3(p.n_out, reduce_split(p.n_out, G)), 1024, sm_red, s>>>(out_items, partial, p.L, p.h, bbox);
+  k_coarse_reduce<<<dim3(p.n_out, reduce_split(p.n_out, G)), kReduceThreads, sm_red, s>>>(out_items, partial, p.L,
+                                                                                          p.h, bbox);
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
   mark(5);
   if (synth_mma_pick(p.n_out, p.n, 2 * p.h)) {
@@ -917,7 +922,7 @@ extern "C" int litho_coarse_image(const LithoAbbePlan* plan, const void* blob, c
   if (e != cudaSuccess) return (int)e;
   const size_t sm_red = (size_t)p.L * p.L * 4 + (size_t)p.L * G * 8 + (size_t)p.L * 8;
   cudaFuncSetAttribute(k_coarse_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_red);
-  k_coarse_reduce<<<dim3(p.n_out, reduce_split(p.n_out, G)), 1024, sm_red, s>>>(out_items, partial, p.L, p.h,
+  k_coarse_reduce<<<dim3(p.n_out, reduce_split(p.n_out, G)), kReduceThreads, sm_red, s>>>(out_items, partial, p.L, p.h,
                                                                                  static_cast<float2*>(bbox_out));
   e = cudaGetLastError();
   return e == cudaSuccess ? LITHO_OK : (int)e;
